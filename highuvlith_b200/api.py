@@ -1,0 +1,307 @@
+"""Python face of the engine, mirroring the reference's imaging call.
+
+``SimulationEngine`` follows the reference's PyO3 class of the same name
+(crates/highuvlith-py/src/py_simulation.rs:89-566): it is built once from a
+source, optics and grid (FP64 source sampling + SOCS kernels on the host),
+then images many masks.  Images come back as FP32 on the engine grid, indexed
+``[y, x]`` with pixel centres ``x_j = -L/2 + (j + 1/2) p``.  Device memory and
+streams are torch tensors; all arithmetic runs in the library's own CUDA
+kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field, replace
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib as L
+
+ARF_WAVELENGTH_NM = 193.368
+F2_WAVELENGTH_NM = 157.63
+EUV_WAVELENGTH_NM = 13.5
+WATER_INDEX_193NM = 1.437
+
+
+@dataclass(frozen=True)
+class SourceConfig:
+    """Wavelength + pupil fill (source.rs:57-186).  ``fill`` is one of
+    conventional, annular, quadrupole, dipole, gaussian, quasar."""
+    wavelength_nm: float
+    fill: str = "conventional"
+    params: Tuple[float, ...] = (0.7,)
+
+    @staticmethod
+    def arf_laser(sigma: float = 0.7) -> "SourceConfig":
+        return SourceConfig(ARF_WAVELENGTH_NM, "conventional", (sigma,))
+
+    @staticmethod
+    def f2_laser(sigma: float = 0.7) -> "SourceConfig":
+        return SourceConfig(F2_WAVELENGTH_NM, "conventional", (sigma,))
+
+    @staticmethod
+    def euv(sigma: float = 0.5) -> "SourceConfig":
+        return SourceConfig(EUV_WAVELENGTH_NM, "conventional", (sigma,))
+
+    def with_illumination(self, fill: str, *params: float) -> "SourceConfig":
+        if fill not in L.FILL:
+            raise ValueError(f"unknown illumination {fill!r}")
+        return replace(self, fill=fill, params=tuple(float(p) for p in params))
+
+    def _c(self) -> L.Source:
+        s = L.Source()
+        s.wavelength_nm = self.wavelength_nm
+        s.fill = L.FILL[self.fill]
+        for i, p in enumerate(self.params[:4]):
+            s.p[i] = p
+        return s
+
+
+@dataclass(frozen=True)
+class OpticsConfig:
+    """ProjectionOptics (optics/mod.rs:193-357) or EuvProjectionOptics
+    (optics/euv.rs:51-160), scalar pupil, no aberrations."""
+    numerical_aperture: float
+    flare_fraction: float = 0.02
+    immersion_index: float = 1.0
+    kind: str = "projection"
+    central_obscuration: float = 0.0
+    transmission: float = 1.0
+    paraxial_defocus: bool = False
+
+    @staticmethod
+    def immersion(na: float, index: float = WATER_INDEX_193NM) -> "OpticsConfig":
+        return OpticsConfig(na, 0.02, index)
+
+    @staticmethod
+    def euv(na: float, central_obscuration: float = 0.0) -> "OpticsConfig":
+        return OpticsConfig(na, 0.0, 1.0, "euv", central_obscuration)
+
+    @staticmethod
+    def euv_nxe_033() -> "OpticsConfig":
+        return OpticsConfig.euv(0.33, 0.0)
+
+    @staticmethod
+    def euv_high_na_055() -> "OpticsConfig":
+        return OpticsConfig.euv(0.55, 0.2)
+
+    def _c(self) -> L.Optics:
+        o = L.Optics()
+        o.kind = L.OPTICS_EUV if self.kind == "euv" else L.OPTICS_PROJECTION
+        o.na = self.numerical_aperture
+        o.flare_fraction = self.flare_fraction
+        o.immersion_index = self.immersion_index
+        o.central_obscuration = self.central_obscuration
+        o.transmission = self.transmission
+        o.paraxial_defocus = int(self.paraxial_defocus)
+        return o
+
+
+@dataclass(frozen=True)
+class GridConfig:
+    size: int = 256
+    pixel_nm: float = 1.0
+
+    @property
+    def field_nm(self) -> float:
+        return self.size * self.pixel_nm
+
+    def pixel_centres(self) -> np.ndarray:
+        return -self.field_nm / 2 + (np.arange(self.size) + 0.5) * self.pixel_nm
+
+
+@dataclass
+class MaskConfig:
+    """A binary Manhattan mask: pixel-aligned rectangles (x0, y0, w, h) in
+    pixels from the field corner, clear on a dark field (``dark_field=True``)
+    or opaque on a clear field."""
+    rects: list = field(default_factory=list)
+    dark_field: bool = True
+
+    def rasterize(self, grid: GridConfig) -> np.ndarray:
+        n = grid.size
+        bg, fg = (0, 1) if self.dark_field else (1, 0)
+        out = np.full((n, n), bg, dtype=np.uint8)
+        for x0, y0, w, h in self.rects:
+            out[max(y0, 0):min(y0 + h, n), max(x0, 0):min(x0 + w, n)] = fg
+        return out
+
+
+_NORMALIZATION = {"clear_field": 0, "absolute": 1}
+
+
+class SimulationEngine:
+    """Hopkins/SOCS imaging engine on one B200 (py_simulation.rs:115-164).
+
+    Construction samples the source and builds the in-focus FP64 kernel set
+    (``max_kernels`` as in the reference's Python default, 30)."""
+
+    def __init__(self, source: SourceConfig, optics: OpticsConfig, mask: Optional[MaskConfig] = None,
+                 grid: Optional[GridConfig] = None, max_kernels: int = 30,
+                 kernel_energy_fraction: float = 1.0, source_points_per_axis: Optional[int] = None,
+                 normalization: str = "clear_field", kernel_cache_capacity: int = 32, device: int = 0):
+        if normalization not in _NORMALIZATION:
+            raise ValueError(f"normalization must be one of {sorted(_NORMALIZATION)}")
+        if source_points_per_axis is not None and source_points_per_axis < 1:
+            raise ValueError("source_points_per_axis must be >= 1 (or None for adaptive sampling)")
+        self.source, self.optics = source, optics
+        self.grid = grid or GridConfig()
+        self.mask = mask
+        self.device = device
+        st = L.Settings()
+        st.max_kernels = max_kernels
+        st.kernel_energy_fraction = kernel_energy_fraction
+        st.source_points_per_axis = source_points_per_axis or 0
+        st.normalization = _NORMALIZATION[normalization]
+        st.kernel_cache_capacity = kernel_cache_capacity
+        g = L.Grid(self.grid.size, self.grid.pixel_nm)
+        h = C.c_void_p()
+        L.check(L.lib().huv_engine_create(C.byref(source._c()), C.byref(optics._c()), C.byref(g),
+                                          C.byref(st), device, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            L.lib().huv_engine_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    # ---------------------------------------------------------- host queries
+    def source_points(self) -> np.ndarray:
+        n = C.c_int32()
+        L.check(L.lib().huv_engine_source_points(self._h, None, 0, C.byref(n)))
+        out = np.zeros((n.value, 3))
+        L.check(L.lib().huv_engine_source_points(self._h, out.ctypes.data, n.value, C.byref(n)))
+        return out
+
+    def imaging_diagnostics(self, focus_nm: float = 0.0) -> dict:
+        d = L.Diagnostics()
+        L.check(L.lib().huv_engine_diagnostics(self._h, focus_nm, C.byref(d)))
+        return {
+            "num_kernels": d.num_kernels, "captured_energy_fraction": d.captured_energy_fraction,
+            "num_frequencies": d.num_frequencies, "num_columns": d.num_columns,
+            "method": ["dense_tcc", "dense_gram"][d.method],
+            "support_exceeds_nyquist": bool(d.support_exceeds_nyquist),
+            "clear_field_intensity": d.clear_field_intensity, "normalized": bool(d.normalized),
+            "band_half_width": d.band_half_width, "num_source_points": d.num_source_points,
+            "imaging_model": "scalar", "defocus_model": "exact",
+        }
+
+    def clear_field_intensity(self, focus_nm: float = 0.0) -> float:
+        v = C.c_double()
+        L.check(L.lib().huv_engine_clear_field(self._h, focus_nm, C.byref(v)))
+        return v.value
+
+    def kernels(self, focus_nm: float = 0.0) -> Tuple[np.ndarray, np.ndarray]:
+        """(eigenvalues, kernels complex128 (k, n, n)) in FFT layout, unit norm;
+        I = sum_k lambda_k |ifft2(K_k * spectrum)|^2 before flare."""
+        k = C.c_int32()
+        L.check(L.lib().huv_engine_kernels(self._h, focus_nm, None, None, 0, C.byref(k)))
+        n = self.grid.size
+        ev = np.zeros(k.value)
+        ker = np.zeros((k.value, n, n), dtype=np.complex128)
+        L.check(L.lib().huv_engine_kernels(self._h, focus_nm, ev.ctypes.data, ker.ctypes.data, k.value,
+                                           C.byref(k)))
+        return ev, ker
+
+    # ---------------------------------------------------------- device calls
+    @staticmethod
+    def _kind(t) -> int:
+        import torch
+        if t.dtype == torch.uint8:
+            return L.INPUT_U8
+        if t.dtype == torch.float32:
+            return L.INPUT_F32
+        if t.dtype == torch.complex64:
+            return L.INPUT_C64
+        raise TypeError(f"unsupported mask dtype {t.dtype} (uint8, float32 or complex64)")
+
+    def compute_batch(self, rasters, focus_nm: float = 0.0, pixel_transfer: bool = True,
+                      form: str = "auto", eval_grid: int = 0, out=None, stream=None):
+        """Images of a batch of rasters resident on the engine's device.
+
+        ``rasters``: torch tensor (B, N, N) uint8 / float32 / complex64 on the
+        device.  ``pixel_transfer=True`` gives ``compute(mask)`` of the
+        pixel-aligned mask the raster depicts (Mask::spectrum, mask.rs:616-657);
+        ``False`` gives ``compute_from_transmittance`` (aerial.rs:1789-1798).
+        Returns a float32 (B, N, N) tensor (``out`` if given)."""
+        import torch
+        n = self.grid.size
+        if rasters.dim() == 2:
+            rasters = rasters.unsqueeze(0)
+        if rasters.shape[-2:] != (n, n):
+            raise ValueError(f"rasters must be (B, {n}, {n}), got {tuple(rasters.shape)}")
+        if not rasters.is_cuda:
+            raise ValueError("rasters must live on the CUDA device; use compute_batch_host for host arrays")
+        rasters = rasters.contiguous()
+        if out is None:
+            out = torch.empty((rasters.shape[0], n, n), dtype=torch.float32, device=rasters.device)
+        b = L.Batch(rasters.shape[0], self._kind(rasters), rasters.data_ptr(), int(pixel_transfer),
+                    float(focus_nm), L.FORM[form], int(eval_grid))
+        st = (stream or torch.cuda.current_stream(rasters.device)).cuda_stream
+        L.check(L.lib().huv_image_batch(self._h, C.byref(b), out.data_ptr(), st))
+        return out
+
+    def compute_batch_host(self, rasters: np.ndarray, focus_nm: float = 0.0, pixel_transfer: bool = True,
+                           form: str = "auto", eval_grid: int = 0, out: Optional[np.ndarray] = None,
+                           stream=None) -> np.ndarray:
+        """Same as ``compute_batch`` from host memory to host memory (copies
+        included; pinned buffers make them faster)."""
+        n = self.grid.size
+        r = np.ascontiguousarray(rasters)
+        if r.ndim == 2:
+            r = r[None]
+        kind = {np.dtype(np.uint8): L.INPUT_U8, np.dtype(np.float32): L.INPUT_F32,
+                np.dtype(np.complex64): L.INPUT_C64}.get(r.dtype)
+        if kind is None:
+            raise TypeError(f"unsupported mask dtype {r.dtype}")
+        if r.shape[-2:] != (n, n):
+            raise ValueError(f"rasters must be (B, {n}, {n})")
+        if out is None:
+            out = np.empty((r.shape[0], n, n), dtype=np.float32)
+        b = L.Batch(r.shape[0], kind, r.ctypes.data, int(pixel_transfer), float(focus_nm), L.FORM[form],
+                    int(eval_grid))
+        st = 0
+        if stream is not None:
+            st = stream.cuda_stream
+        L.check(L.lib().huv_image_batch_host(self._h, C.byref(b), out.ctypes.data, st))
+        return out
+
+    def compute_aerial_image(self, focus_nm: float = 0.0, mask: Optional[MaskConfig] = None) -> np.ndarray:
+        """Image of ``mask`` (or the engine's own mask) at ``focus_nm``
+        (py_simulation.rs:169-179)."""
+        m = mask or self.mask
+        if m is None:
+            raise ValueError("no mask given")
+        return self.compute_batch_host(m.rasterize(self.grid), focus_nm, pixel_transfer=True)[0]
+
+    def compute_from_transmittance(self, transmittance, focus_nm: float = 0.0) -> np.ndarray:
+        """Image of a complex transmittance map (n, n) [y, x]
+        (py_simulation.rs:375-393); the spectrum is the plain FFT."""
+        t = np.asarray(transmittance)
+        t = t.astype(np.complex64) if np.iscomplexobj(t) else t.astype(np.float32)
+        return self.compute_batch_host(t, focus_nm, pixel_transfer=False)[0]
+
+
+def rasterize_rects(n: int, clips: Sequence[Sequence[Tuple[int, int, int, int]]], dark_field: bool = True,
+                    device=None):
+    """Device rasters (B, n, n) uint8 of pixel-aligned rectangle clips, drawn
+    by the library's rasteriser kernel."""
+    import torch
+    device = device or torch.device("cuda")
+    flat = [r for c in clips for r in c]
+    offs = np.zeros(len(clips) + 1, dtype=np.int32)
+    offs[1:] = np.cumsum([len(c) for c in clips])
+    rects = torch.tensor(np.asarray(flat, dtype=np.int32).reshape(-1, 4) if flat else np.zeros((1, 4), np.int32),
+                         device=device)
+    offsets = torch.tensor(offs, device=device)
+    out = torch.empty((len(clips), n, n), dtype=torch.uint8, device=device)
+    st = torch.cuda.current_stream(device).cuda_stream
+    L.check(L.lib().huv_rasterize_rects(n, len(clips), rects.data_ptr(), offsets.data_ptr(),
+                                        int(dark_field), out.data_ptr(), st))
+    return out

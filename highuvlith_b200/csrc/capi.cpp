@@ -1,0 +1,154 @@
+// C ABI of the engine (include/huv_b200.h).  Every entry point catches
+// exceptions, records the message for huv_last_error() and returns a status.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+
+#include "../../include/huv_b200.h"
+#include "engine.hpp"
+
+using huv::Engine;
+using huv::Error;
+
+namespace {
+
+template <typename F>
+huv_status guarded(F&& f) {
+  try {
+    f();
+    huv::set_last_error("");
+    return HUV_OK;
+  } catch (const Error& e) {
+    huv::set_last_error(e.what());
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    huv::set_last_error("host allocation failed");
+    return HUV_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    huv::set_last_error(e.what());
+    return HUV_ERR_NUMERICAL;
+  } catch (...) {
+    huv::set_last_error("unknown failure");
+    return HUV_ERR_NUMERICAL;
+  }
+}
+
+Engine* as_engine(void* e) {
+  if (!e) throw Error(HUV_ERR_INVALID_PARAMETER, "engine: null handle");
+  return static_cast<Engine*>(e);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* huv_last_error(void) { return huv::last_error(); }
+const char* huv_version(void) { return "highuvlith_b200 0.1.0 (sm_100a)"; }
+
+huv_status huv_engine_create(const huv_source* source, const huv_optics* optics, const huv_grid* grid,
+                             const huv_settings* settings, int32_t device, void** engine_out) {
+  return guarded([&] {
+    if (!source || !optics || !grid || !settings || !engine_out)
+      throw Error(HUV_ERR_INVALID_PARAMETER, "huv_engine_create: null argument");
+    *engine_out = nullptr;
+    *engine_out = new Engine(*source, *optics, *grid, *settings, device);
+  });
+}
+
+void huv_engine_destroy(void* engine) { delete static_cast<Engine*>(engine); }
+
+huv_status huv_engine_source_points(void* engine, double* xyw, int32_t capacity, int32_t* count) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!count) throw Error(HUV_ERR_INVALID_PARAMETER, "count: null");
+    *count = static_cast<int32_t>(e->points.size());
+    if (!xyw) return;
+    if (capacity < *count) throw Error(HUV_ERR_DIMENSION_MISMATCH, "source_points: capacity too small");
+    for (size_t i = 0; i < e->points.size(); ++i) {
+      xyw[3 * i] = e->points[i].sx;
+      xyw[3 * i + 1] = e->points[i].sy;
+      xyw[3 * i + 2] = e->points[i].w;
+    }
+  });
+}
+
+huv_status huv_engine_diagnostics(void* engine, double defocus_nm, huv_diagnostics* out) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!out) throw Error(HUV_ERR_INVALID_PARAMETER, "out: null");
+    std::lock_guard<std::mutex> lock(e->mu);
+    auto ks = e->kernel_set(defocus_nm);
+    out->num_kernels = ks->num_kernels();
+    out->captured_energy_fraction = [&] {
+      double s = 0;
+      for (double v : ks->eigenvalues) s += v;
+      return s / ks->trace;
+    }();
+    out->num_frequencies = static_cast<int32_t>(ks->support.size());
+    out->num_columns = ks->num_columns;
+    out->method = ks->method;
+    out->support_exceeds_nyquist = ks->exceeds_nyquist ? 1 : 0;
+    out->clear_field_intensity = ks->clear_field;
+    out->normalized = ks->divisor(e->settings.normalization) != 0.0 ? 1 : 0;
+    out->band_half_width = ks->band_half_width();
+    out->num_source_points = static_cast<int32_t>(e->points.size());
+  });
+}
+
+huv_status huv_engine_clear_field(void* engine, double defocus_nm, double* out) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!out) throw Error(HUV_ERR_INVALID_PARAMETER, "out: null");
+    std::lock_guard<std::mutex> lock(e->mu);
+    *out = e->kernel_set(defocus_nm)->clear_field;
+  });
+}
+
+huv_status huv_engine_kernels(void* engine, double defocus_nm, double* eigenvalues, double* kernels,
+                              int32_t capacity, int32_t* count) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!count) throw Error(HUV_ERR_INVALID_PARAMETER, "count: null");
+    std::lock_guard<std::mutex> lock(e->mu);
+    auto ks = e->kernel_set(defocus_nm);
+    const int K = ks->num_kernels();
+    *count = K;
+    if (!eigenvalues && !kernels) return;
+    if (capacity < K) throw Error(HUV_ERR_DIMENSION_MISMATCH, "kernels: capacity too small");
+    double div = ks->divisor(e->settings.normalization);
+    if (div == 0.0) div = 1.0;
+    const size_t nn = static_cast<size_t>(e->n) * e->n;
+    const size_t S = ks->support.size();
+    if (eigenvalues)
+      for (int k = 0; k < K; ++k) eigenvalues[k] = ks->eigenvalues[k] / div;
+    if (kernels) {
+      std::memset(kernels, 0, sizeof(double) * 2 * nn * K);
+      for (int k = 0; k < K; ++k)
+        for (size_t t = 0; t < S; ++t) {
+          const auto v = ks->values[k * S + t];
+          const size_t o = (static_cast<size_t>(k) * nn + static_cast<size_t>(ks->support[t])) * 2;
+          kernels[o] = v.real();
+          kernels[o + 1] = v.imag();
+        }
+    }
+  });
+}
+
+huv_status huv_image_batch(void* engine, const huv_batch* batch, float* out, void* stream) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!batch) throw Error(HUV_ERR_INVALID_PARAMETER, "batch: null");
+    e->image_batch(*batch, out, static_cast<cudaStream_t>(stream));
+  });
+}
+
+huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out_host, void* stream) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!batch) throw Error(HUV_ERR_INVALID_PARAMETER, "batch: null");
+    e->image_batch_host(*batch, out_host, static_cast<cudaStream_t>(stream));
+  });
+}
+
+}  // extern "C"

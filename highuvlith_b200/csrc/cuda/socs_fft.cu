@@ -1,0 +1,289 @@
+// Plain FP32 FFT form of the SOCS aerial image, for sm_100a.
+//
+//   band_rows_fwd   : mask raster rows -> FFT along x -> keep orders [-hb, hb]
+//   band_cols_fwd   : band columns -> FFT along y -> keep [-hb, hb]^2, optional
+//                     pixel transfer, and the flare mean from the band
+//   socs_rows_inv   : per (kernel k, band row my): K_k(my, .) . M(my, .) ->
+//                     zero-padded inverse FFT along x on the evaluation grid
+//   socs_cols_inv   : per strip of columns: inverse FFT along y of every
+//                     kernel's band column, lambda-weighted |E|^2 summed over k
+//                     in shared memory, normalisation + flare epilogue
+//
+// This is the device form of socs_intensity + normalize + apply_flare
+// (crates/highuvlith-core/src/aerial.rs:1682-1748) fed by Mask::spectrum's
+// raster path (mask.rs:630-635) or compute_from_transmittance's FFT
+// (aerial.rs:1789-1798).  Kernel values arrive pre-scaled by
+// sqrt(lambda_k / divisor) / N^2, so |E|^2 sums directly to the normalised
+// image.  The flare mean is computed exactly from the band by Parseval:
+// mean(I0) = sum_f W(f) |M(f)|^2 with W = sum_k lambda_k |u_k|^2 / N^4.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_block.cuh"
+
+namespace huv_dev {
+
+// ------------------------------------------------------------ raster load
+template <int KIND>
+__device__ __forceinline__ float2 load_px(const void* base, size_t idx);
+template <>
+__device__ __forceinline__ float2 load_px<0>(const void* base, size_t idx) {
+  return make_float2(static_cast<float>(static_cast<const uint8_t*>(base)[idx]), 0.f);
+}
+template <>
+__device__ __forceinline__ float2 load_px<1>(const void* base, size_t idx) {
+  return make_float2(static_cast<const float*>(base)[idx], 0.f);
+}
+template <>
+__device__ __forceinline__ float2 load_px<2>(const void* base, size_t idx) {
+  return static_cast<const float2*>(base)[idx];
+}
+
+// Forward FFT of raster rows, band [-hb, hb] kept.  Real inputs (KIND 0, 1)
+// pack rows (2s, 2s+1) into one complex sequence and split the spectra;
+// complex input (KIND 2) transforms one row per sequence.
+// grid: (n / rows_per_block, clips); X: [clip][y][B], B = 2 hb + 1.
+template <int KIND>
+__global__ void band_rows_fwd(const void* __restrict__ in, int lg, int rows_per_block, int hb,
+                              float2* __restrict__ X, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  const int L = 1 << lg;
+  const int B = 2 * hb + 1;
+  const int clip = blockIdx.y;
+  const int row0 = blockIdx.x * rows_per_block;
+  const bool real_in = KIND != 2;
+  const int S = real_in ? rows_per_block / 2 : rows_per_block;
+  float2* a = smem;
+  float2* b = smem + (S << lg);
+  const size_t plane = static_cast<size_t>(L) * L;
+  const size_t cbase = static_cast<size_t>(clip) * plane;
+  for (int t = threadIdx.x; t < (S << lg); t += blockDim.x) {
+    const int s = t >> lg, i = t & (L - 1);
+    if (real_in) {
+      const float2 p = load_px<KIND>(in, cbase + static_cast<size_t>(row0 + 2 * s) * L + i);
+      const float2 q = load_px<KIND>(in, cbase + static_cast<size_t>(row0 + 2 * s + 1) * L + i);
+      a[t] = make_float2(p.x, q.x);
+    } else {
+      a[t] = load_px<KIND>(in, cbase + static_cast<size_t>(row0 + s) * L + i);
+    }
+  }
+  __syncthreads();
+  const float2* r = block_fft<-1>(a, b, lg, S, tw);
+  const int outs = real_in ? 2 * S : S;
+  for (int t = threadIdx.x; t < S * B; t += blockDim.x) {
+    const int s = t / B, mi = t - s * B;
+    const int m = mi - hb;
+    const int idx = m & (L - 1);
+    const float2 z = r[(s << lg) + idx];
+    if (real_in) {
+      const float2 zc = cconj(r[(s << lg) + ((L - idx) & (L - 1))]);
+      const float2 xa = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y + zc.y));
+      const float2 d = csub(z, zc);
+      const float2 xb = make_float2(0.5f * d.y, -0.5f * d.x);
+      const size_t ya = static_cast<size_t>(clip) * L + row0 + 2 * s;
+      X[ya * B + mi] = xa;
+      X[(ya + 1) * B + mi] = xb;
+    } else {
+      const size_t y = static_cast<size_t>(clip) * L + row0 + s;
+      X[y * B + mi] = z;
+    }
+  }
+  (void)outs;
+}
+
+// Forward FFT of the band columns along y; keeps [-hb, hb]^2, multiplies by
+// the separable pixel transfer ptx (B floats; NULL = none) and, when W is
+// given, writes the flare mean sum_f W(f) |M(f)|^2 per clip.
+// grid: (clips); one block walks all B columns, cols_per_pass at a time.
+__global__ void band_cols_fwd(const float2* __restrict__ X, int lg, int hb, int cols_per_pass,
+                              const float* __restrict__ ptx, const float* __restrict__ W,
+                              float2* __restrict__ Mband, float* __restrict__ mean_out,
+                              const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  __shared__ float red[32];
+  const int L = 1 << lg;
+  const int B = 2 * hb + 1;
+  const int clip = blockIdx.x;
+  float2* a = smem;
+  float2* b = smem + (cols_per_pass << lg);
+  const float2* Xc = X + static_cast<size_t>(clip) * L * B;
+  float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
+  float part = 0.f;
+  for (int c0 = 0; c0 < B; c0 += cols_per_pass) {
+    const int nc = min(cols_per_pass, B - c0);
+    for (int t = threadIdx.x; t < (cols_per_pass << lg); t += blockDim.x) {
+      const int s = t >> lg, y = t & (L - 1);
+      a[t] = s < nc ? Xc[static_cast<size_t>(y) * B + c0 + s] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2* r = block_fft<-1>(a, b, lg, cols_per_pass, tw);
+    for (int t = threadIdx.x; t < nc * B; t += blockDim.x) {
+      const int s = t / B, mi = t - s * B;
+      const int mx = c0 + s;
+      const int idx = (mi - hb) & (L - 1);
+      float2 v = r[(s << lg) + idx];
+      if (ptx) {
+        const float f = ptx[mi] * ptx[mx];
+        v.x *= f;
+        v.y *= f;
+      }
+      Mc[static_cast<size_t>(mi) * B + mx] = v;
+      if (W) part += W[mi * B + mx] * (v.x * v.x + v.y * v.y);
+    }
+    __syncthreads();
+  }
+  if (mean_out) {
+    // Deterministic block reduction (fixed order per launch configuration).
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float s = 0.f;
+      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w];
+      mean_out[clip] = s;
+    }
+  }
+}
+
+// Inverse transform along x of every (kernel, band row) product, on the
+// evaluation grid of 2^lg points.  kband: [K][B][B] (pre-scaled); Mband:
+// [clip][B][B]; T: [clip][K][B][Lg].  grid: (ceil(K*B / S), clips).
+__global__ void socs_rows_inv(const float2* __restrict__ kband, float scale,
+                              const float2* __restrict__ Mband, int K, int hb, int lg, int S,
+                              float2* __restrict__ T, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  const int L = 1 << lg;
+  const int B = 2 * hb + 1;
+  const int clip = blockIdx.y;
+  const int seq0 = blockIdx.x * S;
+  const int nseq = min(S, K * B - seq0);
+  float2* a = smem;
+  float2* b = smem + (S << lg);
+  for (int t = threadIdx.x; t < (S << lg); t += blockDim.x) a[t] = make_float2(0.f, 0.f);
+  __syncthreads();
+  const float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
+  for (int t = threadIdx.x; t < nseq * B; t += blockDim.x) {
+    const int s = t / B, mx = t - s * B;
+    const int seq = seq0 + s;
+    const int k = seq / B, my = seq - k * B;
+    const float2 m = Mc[static_cast<size_t>(my) * B + mx];
+    const float2 u = kband ? kband[(static_cast<size_t>(k) * B + my) * B + mx] : make_float2(scale, 0.f);
+    a[(s << lg) + ((mx - hb) & (L - 1))] = cmul(u, m);
+  }
+  __syncthreads();
+  const float2* r = block_fft<+1>(a, b, lg, S, tw);
+  float2* Tc = T + static_cast<size_t>(clip) * K * B * L;
+  for (int t = threadIdx.x; t < (nseq << lg); t += blockDim.x) {
+    const int s = t >> lg, x = t & (L - 1);
+    Tc[(static_cast<size_t>(seq0 + s) << lg) + x] = r[t];
+  }
+}
+
+// Column pass + accumulation.  MODE 0: out = keep * sum_k |E_k|^2 + flare * mean
+// (mean per clip from band_cols_fwd).  MODE 1 (band interpolation): one
+// "kernel" whose inverse transform is real; out = Re(E).
+// grid: (Lg / Wc, clips); T as written by socs_rows_inv; out: [clip][Lg][Lg].
+template <int MODE>
+__global__ void socs_cols_inv(const float2* __restrict__ T, int K, int hb, int lg, int Wc,
+                              float keep, float flare, const float* __restrict__ mean,
+                              float* __restrict__ out, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  const int L = 1 << lg;
+  const int B = 2 * hb + 1;
+  const int clip = blockIdx.y;
+  const int x0 = blockIdx.x * Wc;
+  float2* a = smem;
+  float2* b = smem + (Wc << lg);
+  float* acc = reinterpret_cast<float*>(smem + 2 * (Wc << lg));  // [Wc][L]
+  for (int t = threadIdx.x; t < (Wc << lg); t += blockDim.x) acc[t] = 0.f;
+  const float2* Tc = T + static_cast<size_t>(clip) * K * B * L;
+  for (int k = 0; k < K; ++k) {
+    for (int t = threadIdx.x; t < (Wc << lg); t += blockDim.x) a[t] = make_float2(0.f, 0.f);
+    __syncthreads();
+    for (int t = threadIdx.x; t < B * Wc; t += blockDim.x) {
+      const int my = t / Wc, w = t - my * Wc;
+      const float2 v = Tc[((static_cast<size_t>(k) * B + my) << lg) + x0 + w];
+      a[(w << lg) + ((my - hb) & (L - 1))] = v;
+    }
+    __syncthreads();
+    const float2* r = block_fft<+1>(a, b, lg, Wc, tw);
+    for (int t = threadIdx.x; t < (Wc << lg); t += blockDim.x) {
+      const float2 e = r[t];
+      if (MODE == 0)
+        acc[t] += e.x * e.x + e.y * e.y;
+      else
+        acc[t] += e.x;
+    }
+    __syncthreads();
+  }
+  const float add = (MODE == 0 && mean) ? flare * mean[clip] : 0.f;
+  const float mul = MODE == 0 ? keep : 1.f;
+  float* oc = out + static_cast<size_t>(clip) * L * L;
+  for (int t = threadIdx.x; t < (Wc << lg); t += blockDim.x) {
+    const int y = t / Wc, w = t - y * Wc;
+    oc[static_cast<size_t>(y) * L + x0 + w] = mul * acc[(w << lg) + y] + add;
+  }
+}
+
+}  // namespace huv_dev
+
+// ------------------------------------------------------------ launchers
+namespace huv_launch {
+
+using namespace huv_dev;
+
+static int pick_threads(int work) { return work >= 256 ? 256 : 128; }
+
+cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X,
+                         float2* Mband, const float* ptx, const float* W, float* mean,
+                         const float2* tw, cudaStream_t st) {
+  const int rows_per_block = (kind == 2) ? 2 : 4;
+  const int S = (kind == 2) ? rows_per_block : rows_per_block / 2;
+  const size_t sm1 = 2 * (static_cast<size_t>(S) << lg) * sizeof(float2);
+  dim3 g1(n / rows_per_block, clips);
+  const int th = pick_threads(S << (lg - 2));
+  switch (kind) {
+    case 0: band_rows_fwd<0><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
+    case 1: band_rows_fwd<1><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
+    default: band_rows_fwd<2><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
+  }
+  const int cpp = 4;
+  const size_t sm2 = 2 * (static_cast<size_t>(cpp) << lg) * sizeof(float2);
+  band_cols_fwd<<<clips, 256, sm2, st>>>(X, lg, hb, cpp, ptx, W, Mband, mean, tw);
+  return cudaGetLastError();
+}
+
+cudaError_t socs_inverse(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                         float2* T, float keep, float flare, const float* mean, float* out, int mode,
+                         const float2* tw, cudaStream_t st) {
+  const int B = 2 * hb + 1;
+  const int S = lgm >= 11 ? 2 : 4;
+  const size_t sm3 = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
+  dim3 g3((K * B + S - 1) / S, clips);
+  socs_rows_inv<<<g3, 256, sm3, st>>>(kband, scale, Mband, K, hb, lgm, S, T, tw);
+  const int L = 1 << lgm;
+  const int Wc = lgm >= 11 ? 4 : (L >= 8 ? 8 : L);
+  const size_t sm4 = (2 * (static_cast<size_t>(Wc) << lgm)) * sizeof(float2) +
+                     (static_cast<size_t>(Wc) << lgm) * sizeof(float);
+  dim3 g4(L / Wc, clips);
+  if (mode == 0)
+    socs_cols_inv<0><<<g4, 256, sm4, st>>>(T, K, hb, lgm, Wc, keep, flare, mean, out, tw);
+  else
+    socs_cols_inv<1><<<g4, 256, sm4, st>>>(T, K, hb, lgm, Wc, keep, flare, mean, out, tw);
+  return cudaGetLastError();
+}
+
+cudaError_t set_smem_limits() {
+  const int big = 200 * 1024;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(band_rows_fwd<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  if ((e = cudaFuncSetAttribute(band_rows_fwd<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  if ((e = cudaFuncSetAttribute(band_rows_fwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  if ((e = cudaFuncSetAttribute(band_cols_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  if ((e = cudaFuncSetAttribute(socs_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  if ((e = cudaFuncSetAttribute(socs_cols_inv<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  if ((e = cudaFuncSetAttribute(socs_cols_inv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  return cudaSuccess;
+}
+
+}  // namespace huv_launch

@@ -1,0 +1,386 @@
+// Engine: FP64 host set-up + device kernel sets + the batched image pipeline,
+// behind the C ABI of include/huv_b200.h.
+//
+// Mirrors AerialImageEngine (crates/highuvlith-core/src/aerial.rs:1472-1967):
+// construction samples the source and builds the in-focus kernel set; other
+// focus planes are built on demand and kept in a bounded LRU cache keyed by
+// the focus plane (aerial.rs:1363-1464), with a device copy of each set.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+#include "host/host.hpp"
+
+namespace huv_launch {
+cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X,
+                         float2* Mband, const float* ptx, const float* W, float* mean,
+                         const float2* tw, cudaStream_t st);
+cudaError_t socs_inverse(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm,
+                         int clips, float2* T, float keep, float flare, const float* mean, float* out,
+                         int mode, const float2* tw, cudaStream_t st);
+cudaError_t set_smem_limits();
+cudaError_t tc_prepare(huv::TcState& tc, const huv::DeviceSet& ds, int n, int lgm, cudaStream_t st);
+cudaError_t tc_socs(const huv::TcState& tc, const huv::DeviceSet& ds, const float2* Mband, int clips,
+                    int lgm, float keep, float flare, const float* mean, float* out, void* ws,
+                    cudaStream_t st);
+size_t tc_workspace_bytes(const huv::DeviceSet& ds, int lgm, int clips);
+void tc_release(huv::TcState& tc);
+}  // namespace huv_launch
+
+namespace huv {
+
+namespace {
+thread_local std::string g_last_error = "";
+
+inline int ilog2(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+}  // namespace
+
+void set_last_error(const std::string& m) { g_last_error = m; }
+const char* last_error() { return g_last_error.c_str(); }
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation)
+      throw Error(HUV_ERR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+    throw Error(HUV_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+// ------------------------------------------------------------ construction
+Engine::Engine(const huv_source& s, const huv_optics& o, const huv_grid& g, const huv_settings& st,
+               int dev)
+    : settings(st), device(dev) {
+  if (st.max_kernels < 1) throw Error(HUV_ERR_INVALID_PARAMETER, "max_kernels: must be at least 1");
+  if (!(st.kernel_energy_fraction > 0.0 && st.kernel_energy_fraction <= 1.0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "kernel_energy_fraction: must be in (0, 1]");
+  if (st.source_points_per_axis < 0)
+    throw Error(HUV_ERR_INVALID_PARAMETER, "source_points_per_axis: must be >= 0 (0 = adaptive)");
+  if (g.size < 2 || !(std::isfinite(g.pixel_nm) && g.pixel_nm > 0.0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "grid: needs size >= 2 and a positive finite pixel_nm");
+  if ((g.size & (g.size - 1)) != 0)
+    throw Error(HUV_ERR_GRID_NOT_POWER_OF_TWO, "grid size " + std::to_string(g.size) + " must be a power of 2");
+  if (g.size < 8 || g.size > 8192)
+    throw Error(HUV_ERR_UNSUPPORTED, "grid size must be in [8, 8192] for the device path");
+  if (!(std::isfinite(s.wavelength_nm) && s.wavelength_nm > 0.0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "wavelength_nm: must be positive and finite");
+  if (s.fill < HUV_FILL_CONVENTIONAL || s.fill > HUV_FILL_QUASAR)
+    throw Error(HUV_ERR_INVALID_PARAMETER, "illumination: unknown fill kind");
+  fill.kind = s.fill;
+  for (int i = 0; i < 4; ++i) fill.p[i] = s.p[i];
+  fill.prepare();
+  optics.kind = o.kind;
+  optics.na = o.na;
+  optics.flare = o.flare_fraction;
+  optics.medium = o.kind == HUV_OPTICS_EUV ? 1.0 : (o.immersion_index > 0 ? o.immersion_index : 1.0);
+  optics.obscuration = o.central_obscuration;
+  optics.transmission = o.kind == HUV_OPTICS_EUV ? o.transmission : 1.0;
+  optics.paraxial = o.paraxial_defocus != 0;
+  if (!(std::isfinite(optics.medium) && optics.medium >= 1.0 && optics.na > 0.0 && optics.na < optics.medium))
+    throw Error(HUV_ERR_INVALID_PARAMETER,
+                "numerical_aperture: must be positive and below the image-space (immersion) index");
+  if (o.kind == HUV_OPTICS_EUV && !(optics.obscuration >= 0.0 && optics.obscuration < 1.0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "central_obscuration: must be in [0, 1)");
+  if (!(optics.flare >= 0.0 && optics.flare < 1.0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "flare_fraction: must be in [0, 1)");
+  n = g.size;
+  pixel_nm = g.pixel_nm;
+  lambda = s.wavelength_nm;
+  const double cutoff = optics.cutoff(lambda);
+  const double df_sigma = (1.0 / (n * pixel_nm)) / cutoff;
+  points = sample_source(fill, st.source_points_per_axis, df_sigma);
+  focus = std::make_shared<KernelSet>(build_kernels(points, optics, n, pixel_nm, lambda, st.max_kernels,
+                                                    st.kernel_energy_fraction, 0.0));
+}
+
+Engine::~Engine() {
+  if (device_ready) {
+    cudaSetDevice(device);
+    for (auto& kv : twiddles) cudaFree(kv.second);
+    auto free_set = [](DeviceSet& d) {
+      cudaFree(d.kband);
+      cudaFree(d.W);
+      cudaFree(d.ptx);
+      huv_launch::tc_release(d.tc);
+    };
+    free_set(focus_dev);
+    for (auto& e : cache) free_set(e.dev);
+    cudaFree(ws);
+    cudaFree(io_in);
+    cudaFree(io_out);
+  }
+}
+
+std::shared_ptr<KernelSet> Engine::kernel_set(double z) {
+  if (z == 0.0) return focus;
+  for (auto& e : cache)
+    if (e.z == z) {
+      e.last_used = ++clock;
+      return e.ks;
+    }
+  auto ks = std::make_shared<KernelSet>(build_kernels(points, optics, n, pixel_nm, lambda, settings.max_kernels,
+                                                      settings.kernel_energy_fraction, z));
+  if (settings.kernel_cache_capacity <= 0) {
+    scratch_set = ks;
+    return ks;
+  }
+  if (static_cast<int>(cache.size()) >= settings.kernel_cache_capacity) {
+    auto it = std::min_element(cache.begin(), cache.end(),
+                               [](const CacheEntry& a, const CacheEntry& b) { return a.last_used < b.last_used; });
+    if (device_ready) {
+      cudaFree(it->dev.kband);
+      cudaFree(it->dev.W);
+      cudaFree(it->dev.ptx);
+      huv_launch::tc_release(it->dev.tc);
+    }
+    cache.erase(it);
+  }
+  CacheEntry e;
+  e.z = z;
+  e.ks = ks;
+  e.last_used = ++clock;
+  cache.push_back(e);
+  return ks;
+}
+
+// ------------------------------------------------------------ device side
+void Engine::ensure_device() {
+  check_cuda(cudaSetDevice(device), "cudaSetDevice");
+  if (device_ready) return;
+  check_cuda(huv_launch::set_smem_limits(), "cudaFuncSetAttribute");
+  device_ready = true;
+}
+
+const float2* Engine::twiddle(int lg) {
+  auto it = twiddles.find(lg);
+  if (it != twiddles.end()) return it->second;
+  const int L = 1 << lg;
+  std::vector<float2> h(L);
+  for (int t = 0; t < L; ++t) {
+    const double a = -2.0 * 3.14159265358979323846 * t / L;
+    h[t] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+  }
+  float2* d = nullptr;
+  check_cuda(cudaMalloc(&d, sizeof(float2) * L), "cudaMalloc(twiddle)");
+  check_cuda(cudaMemcpy(d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice), "cudaMemcpy(twiddle)");
+  twiddles[lg] = d;
+  return d;
+}
+
+DeviceSet& Engine::device_set(double z) {
+  std::shared_ptr<KernelSet> ks = kernel_set(z);
+  DeviceSet* slot = nullptr;
+  if (z == 0.0) {
+    slot = &focus_dev;
+  } else {
+    for (auto& e : cache)
+      if (e.z == z) slot = &e.dev;
+    if (!slot) slot = &scratch_dev;
+  }
+  if (slot->kband && slot->source == ks.get()) return *slot;
+  if (slot->kband) {
+    cudaFree(slot->kband);
+    cudaFree(slot->W);
+    cudaFree(slot->ptx);
+    huv_launch::tc_release(slot->tc);
+    *slot = DeviceSet();
+  }
+  const int h = ks->band_half_width();
+  const int B = 2 * h + 1;
+  const int K = ks->num_kernels();
+  const int S = static_cast<int>(ks->support.size());
+  double div = ks->divisor(settings.normalization);
+  if (div == 0.0) div = 1.0;
+  const double n2 = static_cast<double>(n) * n;
+  std::vector<float2> kb(static_cast<size_t>(K) * B * B, make_float2(0.f, 0.f));
+  std::vector<double> wd(static_cast<size_t>(B) * B, 0.0);
+  for (int k = 0; k < K; ++k) {
+    const double lam = ks->eigenvalues[k] / div;
+    const double sc = std::sqrt(lam) / n2;
+    for (int t = 0; t < S; ++t) {
+      const int64_t idx = ks->support[t];
+      const int i = static_cast<int>(idx / n), j = static_cast<int>(idx % n);
+      const int my = i < n / 2 ? i : i - n, mx = j < n / 2 ? j : j - n;
+      const cd u = ks->values[static_cast<size_t>(k) * S + t];
+      const size_t o = (static_cast<size_t>(my + h)) * B + (mx + h);
+      kb[static_cast<size_t>(k) * B * B + o] = make_float2(static_cast<float>(u.real() * sc), static_cast<float>(u.imag() * sc));
+      wd[o] += lam * std::norm(u) / (n2 * n2);
+    }
+  }
+  std::vector<float> wf(wd.begin(), wd.end());
+  std::vector<float> ptx(B);
+  for (int i = 0; i < B; ++i) {
+    const double u = 3.14159265358979323846 * (i - h) / n;
+    ptx[i] = static_cast<float>(std::fabs(u) < 1e-6 ? 1.0 - u * u / 6.0 : std::sin(u) / u);
+  }
+  DeviceSet d;
+  d.source = ks.get();
+  d.hb = h;
+  d.B = B;
+  d.K = K;
+  d.keep = optics.flare > 0.0 ? static_cast<float>(1.0 - optics.flare) : 1.f;
+  d.flare = optics.flare > 0.0 ? static_cast<float>(optics.flare) : 0.f;
+  d.eig_scaled.resize(K);
+  for (int k = 0; k < K; ++k) d.eig_scaled[k] = ks->eigenvalues[k] / div;
+  d.host_kband = kb;
+  check_cuda(cudaMalloc(&d.kband, sizeof(float2) * kb.size()), "cudaMalloc(kband)");
+  check_cuda(cudaMalloc(&d.W, sizeof(float) * wf.size()), "cudaMalloc(W)");
+  check_cuda(cudaMalloc(&d.ptx, sizeof(float) * ptx.size()), "cudaMalloc(ptx)");
+  check_cuda(cudaMemcpy(d.kband, kb.data(), sizeof(float2) * kb.size(), cudaMemcpyHostToDevice), "upload kband");
+  check_cuda(cudaMemcpy(d.W, wf.data(), sizeof(float) * wf.size(), cudaMemcpyHostToDevice), "upload W");
+  check_cuda(cudaMemcpy(d.ptx, ptx.data(), sizeof(float) * ptx.size(), cudaMemcpyHostToDevice), "upload ptx");
+  *slot = std::move(d);
+  return *slot;
+}
+
+void* Engine::workspace(size_t bytes) {
+  if (bytes > ws_bytes) {
+    if (ws) cudaFree(ws);
+    ws = nullptr;
+    ws_bytes = 0;
+    check_cuda(cudaMalloc(&ws, bytes), "cudaMalloc(workspace)");
+    ws_bytes = bytes;
+  }
+  return ws;
+}
+
+int Engine::choose_eval_grid(const DeviceSet& ds, int requested) const {
+  const int min_m = 4 * ds.hb + 1;
+  if (requested > 0) {
+    if ((requested & (requested - 1)) != 0 || requested > n || requested < min_m)
+      throw Error(HUV_ERR_INVALID_PARAMETER,
+                  "eval_grid: must be a power of two with 4h < M <= N (h = " + std::to_string(ds.hb) + ")");
+    return requested;
+  }
+  int m = 8;
+  while (m < min_m) m <<= 1;
+  return std::min(m, n);
+}
+
+static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st) {
+  const int lgn = ilog2(n), lgm = ilog2(M);
+  const int B = ds.B, K = ds.K, hb = ds.hb;
+  const bool coarse = M < n;
+  const int h2 = 2 * hb, B2 = 2 * h2 + 1;
+  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
+  // Per-clip workspace.
+  const size_t per_x = align256(sizeof(float2) * n * B);
+  const size_t per_m = align256(sizeof(float2) * B * B);
+  const size_t per_t = align256(sizeof(float2) * static_cast<size_t>(K) * B * M);
+  const size_t per_i = coarse ? align256(sizeof(float) * M * M) : 0;
+  const size_t per_x2 = coarse ? align256(sizeof(float2) * M * B2) : 0;
+  const size_t per_c = coarse ? align256(sizeof(float2) * B2 * B2) : 0;
+  const size_t per_t2 = coarse ? align256(sizeof(float2) * static_cast<size_t>(B2) * n) : 0;
+  const size_t per_clip = per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2 + 256;
+  const size_t budget = size_t(1) << 30;
+  int chunk = static_cast<int>(std::max<size_t>(1, budget / per_clip));
+  chunk = std::min(chunk, b.n_clips);
+  char* base = static_cast<char*>(workspace(per_clip * chunk + 4096));
+  float2* X = reinterpret_cast<float2*>(base);
+  float2* Mb = reinterpret_cast<float2*>(base + per_x * chunk);
+  float2* T = reinterpret_cast<float2*>(base + (per_x + per_m) * chunk);
+  float* IM = reinterpret_cast<float*>(base + (per_x + per_m + per_t) * chunk);
+  float2* X2 = reinterpret_cast<float2*>(base + (per_x + per_m + per_t + per_i) * chunk);
+  float2* C = reinterpret_cast<float2*>(base + (per_x + per_m + per_t + per_i + per_x2) * chunk);
+  float2* T2 = reinterpret_cast<float2*>(base + (per_x + per_m + per_t + per_i + per_x2 + per_c) * chunk);
+  float* mean = reinterpret_cast<float*>(base + (per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2) * chunk);
+  const float2* twn = twiddle(lgn);
+  const float2* twm = twiddle(lgm);
+  for (int c0 = 0; c0 < b.n_clips; c0 += chunk) {
+    const int nc = std::min(chunk, b.n_clips - c0);
+    const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
+    float* o = out + static_cast<size_t>(n) * n * c0;
+    check_cuda(huv_launch::band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb,
+                                        b.pixel_transfer ? ds.ptx : nullptr, ds.W, mean, twn, st),
+               "band_forward");
+    if (!coarse) {
+      check_cuda(huv_launch::socs_inverse(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, ds.keep, ds.flare, mean, o, 0,
+                                          twm, st),
+                 "socs_inverse");
+    } else {
+      check_cuda(huv_launch::socs_inverse(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, ds.keep, ds.flare, mean, IM, 0,
+                                          twm, st),
+                 "socs_inverse(coarse)");
+      check_cuda(huv_launch::band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr,
+                                          nullptr, twm, st),
+                 "band_forward(interp)");
+      const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
+      check_cuda(huv_launch::socs_inverse(nullptr, scale, C, 1, h2, lgn, nc, T2, 1.f, 0.f, nullptr, o, 1, twn,
+                                          st),
+                 "socs_inverse(interp)");
+    }
+  }
+}
+
+void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
+  std::lock_guard<std::mutex> lock(mu);
+  if (b.n_clips < 0) throw Error(HUV_ERR_INVALID_PARAMETER, "n_clips: must be >= 0");
+  if (b.n_clips == 0) return;
+  if (!b.input || !out) throw Error(HUV_ERR_INVALID_PARAMETER, "input/out: null pointer");
+  if (b.input_kind < 0 || b.input_kind > 2) throw Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
+  if (!std::isfinite(b.defocus_nm)) throw Error(HUV_ERR_INVALID_PARAMETER, "defocus_nm: must be finite");
+  ensure_device();
+  DeviceSet& ds = device_set(b.defocus_nm == 0.0 ? 0.0 : b.defocus_nm);
+  const int M = choose_eval_grid(ds, b.eval_grid);
+  int form = b.form;
+  if (form == HUV_FORM_AUTO) form = tc_supported(ds, M) ? HUV_FORM_TC : HUV_FORM_FFT;
+  if (form == HUV_FORM_TC) {
+    if (!tc_supported(ds, M)) throw Error(HUV_ERR_UNSUPPORTED, "TC form: unsupported band/grid for this build");
+    run_tc_form(b, ds, M, out, st);
+  } else if (form == HUV_FORM_FFT) {
+    run_fft_form(b, ds, M, out, st);
+  } else {
+    throw Error(HUV_ERR_INVALID_PARAMETER, "form: unknown");
+  }
+}
+
+void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t st) {
+  std::lock_guard<std::mutex> host_lock(host_mu);
+  if (b.n_clips <= 0) return;
+  if (!b.input || !out_host) throw Error(HUV_ERR_INVALID_PARAMETER, "input/out: null pointer");
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    ensure_device();
+  }
+  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
+  const size_t in_bytes = in_elem * static_cast<size_t>(n) * n * b.n_clips;
+  const size_t out_bytes = sizeof(float) * static_cast<size_t>(n) * n * b.n_clips;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (in_bytes > io_in_bytes) {
+      if (io_in) cudaFree(io_in);
+      io_in = nullptr;
+      io_in_bytes = 0;
+      check_cuda(cudaMalloc(&io_in, in_bytes), "cudaMalloc(io_in)");
+      io_in_bytes = in_bytes;
+    }
+    if (out_bytes > io_out_bytes) {
+      if (io_out) cudaFree(io_out);
+      io_out = nullptr;
+      io_out_bytes = 0;
+      check_cuda(cudaMalloc(&io_out, out_bytes), "cudaMalloc(io_out)");
+      io_out_bytes = out_bytes;
+    }
+    check_cuda(cudaMemcpyAsync(io_in, b.input, in_bytes, cudaMemcpyHostToDevice, st), "H2D input");
+  }
+  huv_batch d = b;
+  d.input = io_in;
+  image_batch(d, static_cast<float*>(io_out), st);
+  check_cuda(cudaMemcpyAsync(out_host, io_out, out_bytes, cudaMemcpyDeviceToHost, st), "D2H images");
+  check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+}
+
+}  // namespace huv

@@ -1,0 +1,93 @@
+// Engine state shared by the C ABI and the device launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "host/host.hpp"
+
+namespace huv {
+
+void set_last_error(const std::string& m);
+const char* last_error();
+void check_cuda(cudaError_t e, const char* what);
+
+// Device-side state of the tensor-core form for one kernel set.
+struct TcState {
+  int lgm = 0;          // evaluation grid the state was built for
+  int kpad = 0;         // padded contraction length of one split-BF16x3 GEMM
+  void* gy = nullptr;   // DFT operand along y (bf16, split planes)
+  void* gx = nullptr;   // DFT operand along x (bf16, split planes)
+  void* kb = nullptr;   // kernel band operand (bf16 split planes)
+  size_t bytes = 0;
+};
+
+// One kernel set on the device: band kernels K x B x B (complex FP32,
+// pre-scaled by sqrt(lambda_k / divisor) / N^2), the flare weight map W
+// (B x B) and the pixel-transfer factors (B).
+struct DeviceSet {
+  const KernelSet* source = nullptr;
+  int hb = 0, B = 0, K = 0;
+  float keep = 1.f, flare = 0.f;
+  float2* kband = nullptr;
+  float* W = nullptr;
+  float* ptx = nullptr;
+  std::vector<double> eig_scaled;
+  std::vector<float2> host_kband;
+  TcState tc;
+};
+
+struct CacheEntry {
+  double z = 0;
+  std::shared_ptr<KernelSet> ks;
+  DeviceSet dev;
+  uint64_t last_used = 0;
+};
+
+struct Engine {
+  Engine(const huv_source& s, const huv_optics& o, const huv_grid& g, const huv_settings& st, int device);
+  ~Engine();
+
+  std::shared_ptr<KernelSet> kernel_set(double z);
+  void image_batch(const huv_batch& b, float* out, cudaStream_t st);
+  void image_batch_host(const huv_batch& b, float* out_host, cudaStream_t st);
+
+  // device helpers
+  void ensure_device();
+  const float2* twiddle(int lg);
+  DeviceSet& device_set(double z);
+  void* workspace(size_t bytes);
+  int choose_eval_grid(const DeviceSet& ds, int requested) const;
+  bool tc_supported(const DeviceSet& ds, int M) const;
+  void run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st);
+  void run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st);
+
+  huv_settings settings;
+  int device;
+  Fill fill;
+  Optics optics;
+  int n = 0;
+  double pixel_nm = 0, lambda = 0;
+  std::vector<SourcePoint> points;
+  std::shared_ptr<KernelSet> focus, scratch_set;
+  std::vector<CacheEntry> cache;
+  uint64_t clock = 0;
+
+  std::mutex mu, host_mu;
+  bool device_ready = false;
+  std::map<int, float2*> twiddles;
+  DeviceSet focus_dev, scratch_dev;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  void* io_in = nullptr;
+  void* io_out = nullptr;
+  size_t io_in_bytes = 0, io_out_bytes = 0;
+};
+
+}  // namespace huv

@@ -1,0 +1,181 @@
+/*
+ * huv_b200.h - C ABI of the B200 SOCS aerial-image engine.
+ *
+ * The boundary replaces the reference's imaging call
+ *   AerialImageEngine::{with_settings, compute, compute_from_transmittance,
+ *   compute_from_spectrum, kernels, kernel_diagnostics, clear_field_intensity}
+ *   (crates/highuvlith-core/src/aerial.rs:1521-1967)
+ * and its Python face SimulationEngine (crates/highuvlith-py/src/py_simulation.rs:89-566).
+ *
+ * Rules: no exceptions cross the ABI; every call returns a huv_status and the
+ * message of the last failure on the calling thread is in huv_last_error().
+ * Output buffers are caller-owned.  Device pointers are CUDA device addresses
+ * on the engine's device; host pointers are ordinary host memory.  One engine
+ * may be used from several host threads; calls on one engine are serialised
+ * internally.  Streams are passed as `void*` (a cudaStream_t; NULL = the
+ * legacy default stream).  FP64 is used only on the host while building
+ * kernels (TCC assembly, Hermitian eigensolve, truncation); images are FP32.
+ */
+#ifndef HUV_B200_H
+#define HUV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; mirror LithographyError (crates/highuvlith-core/src/error.rs:1-72)
+ * plus device-side failures. */
+typedef enum {
+  HUV_OK = 0,
+  HUV_ERR_INVALID_PARAMETER = 1,       /* InvalidParameter */
+  HUV_ERR_GRID_NOT_POWER_OF_TWO = 2,   /* GridSizeNotPowerOfTwo */
+  HUV_ERR_NO_DIFFRACTION_ORDERS = 3,   /* NoDiffractionOrders */
+  HUV_ERR_PUPIL_SAMPLING_TOO_DENSE = 4,/* PupilSamplingTooDense */
+  HUV_ERR_TCC_DECOMPOSITION = 5,       /* TccDecomposition (eigensolver failed) */
+  HUV_ERR_DIMENSION_MISMATCH = 6,      /* DimensionMismatch */
+  HUV_ERR_NUMERICAL = 7,               /* NumericalError */
+  HUV_ERR_CUDA = 8,                    /* a CUDA runtime call failed */
+  HUV_ERR_OUT_OF_MEMORY = 9,           /* device or host allocation failed */
+  HUV_ERR_DEVICE_TIMEOUT = 10,         /* a bounded device-side wait gave up */
+  HUV_ERR_UNSUPPORTED = 11             /* valid request this build does not serve */
+} huv_status;
+
+/* Pupil fills (crates/highuvlith-core/src/source.rs:163-186, 1178-1248) plus the
+ * quasar fill (four annular sectors centred on the diagonals), which the
+ * reference expresses as a custom LithographySource::intensity_at. */
+typedef enum {
+  HUV_FILL_CONVENTIONAL = 0, /* p0 = sigma */
+  HUV_FILL_ANNULAR = 1,      /* p0 = sigma_inner, p1 = sigma_outer */
+  HUV_FILL_QUADRUPOLE = 2,   /* p0 = sigma_center, p1 = sigma_radius, p2 = opening_angle_deg */
+  HUV_FILL_DIPOLE = 3,       /* p0 = sigma_center, p1 = sigma_radius, p2 = orientation_deg */
+  HUV_FILL_GAUSSIAN = 4,     /* p0 = sigma (CoherentGaussian) */
+  HUV_FILL_QUASAR = 5        /* p0 = sigma_inner, p1 = sigma_outer, p2 = opening_angle_deg */
+} huv_fill_kind;
+
+typedef struct {
+  double wavelength_nm; /* LithographySource::wavelength_nm (source.rs:59) */
+  int32_t fill;         /* huv_fill_kind */
+  double p[4];
+} huv_source;
+
+/* Optics (optics/mod.rs:193-357, optics/euv.rs:51-160): scalar pupils. */
+typedef enum { HUV_OPTICS_PROJECTION = 0, HUV_OPTICS_EUV = 1 } huv_optics_kind;
+
+typedef struct {
+  int32_t kind;               /* huv_optics_kind */
+  double na;
+  double flare_fraction;      /* ProjectionOptics::flare_fraction / EuvProjectionOptics::flare */
+  double immersion_index;     /* ProjectionOptics only (1 = dry) */
+  double central_obscuration; /* EUV only, fraction of NA */
+  double transmission;        /* EUV only (1 in the presets) */
+  int32_t paraxial_defocus;   /* 0 = exact defocus phase */
+} huv_optics;
+
+typedef struct {
+  int32_t size;    /* GridConfig::size, power of two */
+  double pixel_nm; /* GridConfig::pixel_nm */
+} huv_grid;
+
+/* ImagingSettings (aerial.rs:166-206), scalar imaging, exact defocus. */
+typedef struct {
+  int32_t max_kernels;            /* >= 1 */
+  double kernel_energy_fraction;  /* (0, 1] */
+  int32_t source_points_per_axis; /* 0 = adaptive sampling, n >= 1 = n x n grid */
+  int32_t normalization;          /* 0 = clear field (relative), 1 = absolute */
+  int32_t kernel_cache_capacity;  /* kernel sets kept per engine (focus planes) */
+} huv_settings;
+
+/* KernelDiagnostics (aerial.rs:254-276). method: 0 dense_tcc, 1 dense_gram. */
+typedef struct {
+  int32_t num_kernels;
+  double captured_energy_fraction;
+  int32_t num_frequencies;
+  int32_t num_columns;
+  int32_t method;
+  int32_t support_exceeds_nyquist;
+  double clear_field_intensity;
+  int32_t normalized;
+  int32_t band_half_width; /* h: the support lies in orders [-h, h]^2 */
+  int32_t num_source_points;
+} huv_diagnostics;
+
+/* Mask input kinds for the batched image call. */
+typedef enum {
+  HUV_INPUT_RASTER_U8 = 0,       /* N*N uint8 transmittance 0/1 (binary mask raster) */
+  HUV_INPUT_RASTER_F32 = 1,      /* N*N float real transmittance */
+  HUV_INPUT_TRANSMITTANCE_C64 = 2/* N*N interleaved (re, im) float complex transmittance */
+} huv_input_kind;
+
+/* Which device form evaluates the SOCS sum. */
+typedef enum {
+  HUV_FORM_AUTO = 0, /* autotuned choice */
+  HUV_FORM_FFT = 1,  /* plain FP32 FFT form */
+  HUV_FORM_TC = 2    /* split-BF16x3 tcgen05 DFT-GEMM form */
+} huv_form;
+
+typedef struct {
+  int32_t n_clips;
+  int32_t input_kind;     /* huv_input_kind */
+  const void* input;      /* device pointer: n_clips rasters of N*N, [y, x] row-major */
+  int32_t pixel_transfer; /* 1: spectrum of a pixel-aligned raster (Mask::spectrum, mask.rs:630-635);
+                             0: plain FFT of the samples (compute_from_transmittance, aerial.rs:1789) */
+  double defocus_nm;      /* focus plane; kernel sets are built and cached per plane */
+  int32_t form;           /* huv_form */
+  int32_t eval_grid;      /* 0 = autotuned; N = evaluate on the full grid; M < N (power of two,
+                             M > 4h) = exact evaluation on an M grid + exact band interpolation */
+} huv_batch;
+
+/* Last error message on this thread (never NULL). */
+const char* huv_last_error(void);
+/* Library version string. */
+const char* huv_version(void);
+
+/* Engine construction: source sampling + in-focus FP64 kernel build
+ * (AerialImageEngine::with_settings, aerial.rs:1521-1637).  `device` is the
+ * CUDA ordinal used for device kernel sets and images; the host build needs
+ * no device. */
+huv_status huv_engine_create(const huv_source* source, const huv_optics* optics,
+                             const huv_grid* grid, const huv_settings* settings,
+                             int32_t device, void** engine_out);
+void huv_engine_destroy(void* engine);
+
+/* Source points (AerialImageEngine::source_points): xyw is count*3 doubles. */
+huv_status huv_engine_source_points(void* engine, double* xyw, int32_t capacity, int32_t* count);
+
+/* kernel_diagnostics (aerial.rs:1946-1958) at the centre wavelength. */
+huv_status huv_engine_diagnostics(void* engine, double defocus_nm, huv_diagnostics* out);
+
+/* clear_field_intensity (aerial.rs:1965-1967). */
+huv_status huv_engine_clear_field(void* engine, double defocus_nm, double* out);
+
+/* kernels(z) (aerial.rs:1912-1942): eigenvalues (already divided by the
+ * normalisation) and dense N*N kernels in FFT layout, interleaved (re, im)
+ * doubles, k-major.  Pass kernels = NULL to query the count only. */
+huv_status huv_engine_kernels(void* engine, double defocus_nm, double* eigenvalues,
+                              double* kernels, int32_t capacity, int32_t* count);
+
+/* Batched aerial images on the device: out is n_clips*N*N floats (device),
+ * [clip][y][x], pixel centres x_j = -L/2 + (j + 1/2) p.  Equivalent per clip to
+ * compute(mask, z) (pixel_transfer = 1) or compute_from_transmittance(t, z)
+ * (pixel_transfer = 0), normalisation and flare included (aerial.rs:1775-1816). */
+huv_status huv_image_batch(void* engine, const huv_batch* batch, float* out, void* stream);
+
+/* Same call with HOST input and output buffers: copies in, images, copies out
+ * on `stream` and synchronises it (the reference-facing end-to-end call). */
+huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out_host, void* stream);
+
+/* Axis-aligned rectangles -> pixel-aligned binary rasters on the device
+ * (mask.rs:1717-1741 for pixel-aligned Rect features on a dark- or bright-field
+ * binary mask).  rects: n_rects*4 int32 (x0, y0, w, h) in pixels, row-major from
+ * the field corner; clip_offsets: n_clips+1 prefix offsets into rects. */
+huv_status huv_rasterize_rects(int32_t n, int32_t n_clips, const int32_t* rects_dev,
+                               const int32_t* clip_offsets_dev, int32_t dark_field,
+                               uint8_t* raster_out_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HUV_B200_H */
