@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark of the batched SOCS aerial-image path on B200.
+
+Workload (one step = one pass of the imaging path over one batch):
+256 seeded Manhattan clips, 1024 x 1024 at 1 nm, EUV 13.5 nm, NA 0.33,
+conventional sigma 0.5, max_kernels 32 (the truncation rule keeps 31 because
+32 would split a degenerate pair), FP32 images out.  Clips are drawn with
+numpy PCG64 seeds 2026 + id (rectangles 10-80 nm, 30-50 % density, binary
+0/1) and are resident in HBM when the timed region starts; the host-buffer
+end-to-end number copies rasters in and images out inside the timed region.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun every rank images its own 256 clips (replicas, weak scaling,
+no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 1024
+N_CLIPS = 256
+MAX_KERNELS = 32
+METRIC = "aerial images/s (1024^2, K=32 requested) at <=1e-3 rel err vs FP64"
+WORKLOAD = "EUV 13.5 nm NA 0.33 conventional sigma 0.5, 256 Manhattan clips 1024x1024 @ 1 nm"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return p["hbm_gbs"], p["bf16_tflops"], p.get("bf16_tflops_sustained", p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(n_gpus: int):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def c2_engine(device: int):
+    import highuvlith_b200 as HB
+    return HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(),
+                               grid=HB.GridConfig(N_GRID, 1.0), max_kernels=MAX_KERNELS, device=device)
+
+
+def oracle_kernel_set():
+    from oracle import hopkins as H
+    eng = H.Engine(H.fill_conventional(0.5), H.euv_nxe_033(), H.Grid(N_GRID, 1.0), 13.5, max_kernels=MAX_KERNELS)
+    return eng, eng.kernel_set(0.0)
+
+
+def cpu_sample(ks, rasters, threads):
+    """Time the oracle's C port (FP64, all threads) on a bounded sample."""
+    from oracle import cpu
+    t0 = time.perf_counter()
+    cpu.images(ks, rasters, 0.0, pixel_transfer=True, threads=threads, want_output=False)
+    return time.perf_counter() - t0
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU algorithm (C restatement of the
+    Rust path; the Rust crate cannot be built here) on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from highuvlith_b200.clips import gen_batch
+    threads = os.cpu_count() or 1
+    _, ks = oracle_kernel_set()
+    per_step = max(4, min(threads, 64))
+    _, rasters = gen_batch(per_step, N_GRID, base_seed=2026)
+    for _ in range(args.warmup):
+        cpu_sample(ks, rasters, threads)
+    t = 0.0
+    for _ in range(args.steps):
+        t += cpu_sample(ks, rasters, threads)
+    v = per_step * args.steps / t
+    sample = f"{per_step} clips of the workload per step ({cpu_model()})"
+    line = {
+        "metric": METRIC, "value": v, "unit": "images/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "clips_per_step": per_step},
+        "cpu_baseline": {"value": v, "unit": "images/s", "cores": threads, "kind": "port", "sample": sample,
+                         "note": "C restatement of the reference's Rust CPU path (reference binary unavailable)"},
+        "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def accuracy(img: np.ndarray, raster: np.ndarray):
+    """Max relative intensity error and max edge (CD) error vs the FP64 oracle."""
+    from oracle import hopkins as H
+    oeng, _ = oracle_kernel_set()
+    ref = oeng.compute_from_spectrum(H.spectrum_from_raster(raster))
+    rel = float(np.max(np.abs(img - ref)) / np.max(ref))
+    x = -N_GRID / 2 + (np.arange(N_GRID) + 0.5)
+    worst_r, un_r = _edges(img, ref, x, 0.3, 8)  # every 8th row and column cutline
+    return {"max_rel_err": rel, "cd_err_nm": worst_r, "unmatched_edges": un_r, "threshold": 0.3,
+            "cutlines": "every 8th row and column"}
+
+
+def _edges(img, ref, x, t, step):
+    from oracle import metrics as M
+    period = float(len(x))
+    worst, unmatched = 0.0, 0
+    for axis in (0, 1):
+        a = img if axis == 0 else img.T
+        b = ref if axis == 0 else ref.T
+        for r in range(0, a.shape[0], step):
+            ca = M.find_crossings(list(a[r]), list(x), t, period)
+            cb = M.find_crossings(list(b[r]), list(x), t, period)
+            if len(ca) != len(cb):
+                unmatched += abs(len(ca) - len(cb))
+                continue
+            for p, q in zip(ca, cb):
+                worst = max(worst, abs(p[0] - q[0]))
+    return worst, unmatched
+
+
+def run_ours(args):
+    import torch
+    from highuvlith_b200.clips import gen_batch
+    rank, world, local = dist_setup(args.gpus)
+    eng = c2_engine(local)
+    diag = eng.imaging_diagnostics()
+    _, rasters = gen_batch(N_CLIPS, N_GRID, base_seed=2026 + rank * N_CLIPS)
+    d_in = torch.from_numpy(rasters).cuda()
+    d_out = torch.empty((N_CLIPS, N_GRID, N_GRID), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(form, eval_grid):
+        eng.compute_batch(d_in, form=form, eval_grid=eval_grid, out=d_out, stream=stream)
+
+    for _ in range(args.warmup):
+        step(args.form, args.eval_grid)
+    torch.cuda.synchronize()
+    barrier(world)
+    eng.profile(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step(args.form, args.eval_grid)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    prof = eng.profile_read()
+    eng.profile(False)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms, world)
+    value = world * N_CLIPS / (ms / 1e3)
+
+    # roofline of the dominant kernel
+    hbm, tc_burst, tc_sus, peak_kind = peaks()
+    K, S = diag["num_kernels"], diag["num_frequencies"]
+    bytes_per_image = 4 * N_GRID ** 2 + 4 * N_GRID ** 2 + 8 * K * S
+    launches = max(prof["launches"], 1)
+    per_launch_s = prof["ms"] / launches / 1e3
+    images_per_launch = N_CLIPS * args.steps / launches
+    achieved = bytes_per_image * images_per_launch / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": None, "kernel": prof["kernel"], "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                "algorithmic_bytes_per_image": bytes_per_image,
+                "kernel_share_of_step": prof["ms"] / (ms * args.steps) if ms > 0 else None}
+
+    # end to end through the host-buffer C ABI call (pinned buffers)
+    h_in = torch.from_numpy(rasters).pin_memory()
+    h_out = torch.empty((N_CLIPS, N_GRID, N_GRID), dtype=torch.float32).pin_memory()
+    hin_np, hout_np = h_in.numpy(), h_out.numpy()
+    for _ in range(max(1, args.warmup // 2)):
+        eng.compute_batch_host(hin_np, form=args.form, eval_grid=args.eval_grid, out=hout_np, stream=stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.compute_batch_host(hin_np, form=args.form, eval_grid=args.eval_grid, out=hout_np, stream=stream)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    e2e = {"value": world * N_CLIPS / (e2e_ms / 1e3), "unit": "images/s", "h2d_bytes_per_step": int(rasters.nbytes),
+           "d2h_bytes_per_step": int(h_out.numel() * 4), "call": "huv_image_batch_host (pinned host buffers)"}
+
+    extra = {}
+    if rank == 0 and world == 1 and not args.quick:
+        # other device forms on the same batch (fewer steps), for the TC-vs-plain factor
+        forms = {}
+        for name, form, eg in (("fft_full_grid", "fft", N_GRID), ("fft_coarse_grid", "fft", 0), ("tc", "tc", 0)):
+            try:
+                step(form, eg)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(2):
+                    step(form, eg)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                fms = e0.elapsed_time(e1) / 2
+                forms[name] = {"ms_per_step": fms, "images_per_s": N_CLIPS / (fms / 1e3)}
+            except Exception as exc:  # report, do not hide
+                forms[name] = {"unavailable": str(exc)[:200]}
+        extra["forms"] = forms
+        step(args.form, args.eval_grid)
+        torch.cuda.synchronize()
+        extra["accuracy"] = accuracy(d_out[0].cpu().numpy(), rasters[0])
+        # CPU baseline: the oracle's C port on host cores, bounded sample
+        threads = os.cpu_count() or 1
+        _, ks = oracle_kernel_set()
+        sample_n = max(4, min(threads, 32))
+        _, srast = gen_batch(sample_n, N_GRID, base_seed=2026)
+        t = cpu_sample(ks, srast, threads)
+        while t < 8.0 and sample_n < 512:
+            sample_n *= 2
+            _, srast = gen_batch(sample_n, N_GRID, base_seed=2026)
+            t = cpu_sample(ks, srast, threads)
+        extra["cpu_baseline"] = {"value": sample_n / t, "unit": "images/s", "cores": threads, "kind": "port",
+                                 "sample": f"{sample_n} clips of the workload, FP64, {cpu_model()}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "clips_per_gpu": N_CLIPS, "grid": N_GRID, "kernels": K,
+                       "support": S, "band_half_width": diag["band_half_width"], "form": args.form,
+                       "eval_grid": args.eval_grid or "auto",
+                       "l2": "inputs 256 MB + outputs 1 GB per step exceed the 126 MB L2"},
+            "roofline": roofline, "e2e": e2e, "clocks": clocks.summary(),
+            "gpu_launches": prof["total_launches"],
+        }
+        line.update(extra)
+        if "cpu_baseline" not in line:
+            line["cpu_baseline"] = None
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="auto", choices=["auto", "fft", "tc"])
+    ap.add_argument("--eval-grid", dest="eval_grid", type=int, default=0)
+    ap.add_argument("--quick", action="store_true", help="skip the extra forms, accuracy and CPU baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

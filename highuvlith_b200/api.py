@@ -209,6 +209,19 @@ class SimulationEngine:
                                            C.byref(k)))
         return ev, ker
 
+    # ---------------------------------------------------------- measurement
+    def profile(self, on: bool = True) -> None:
+        """Turn live timing of the dominant kernel on or off (resets counters)."""
+        L.check(L.lib().huv_profile_enable(self._h, int(on)))
+
+    def profile_read(self) -> dict:
+        """{'kernel', 'ms', 'launches', 'total_launches'} since the last read."""
+        ms, nl, tot = C.c_double(), C.c_int32(), C.c_int64()
+        name = C.create_string_buffer(64)
+        L.check(L.lib().huv_profile_read(self._h, C.byref(ms), C.byref(nl), C.byref(tot), name, 64))
+        return {"kernel": name.value.decode(), "ms": ms.value, "launches": nl.value,
+                "total_launches": tot.value}
+
     # ---------------------------------------------------------- device calls
     @staticmethod
     def _kind(t) -> int:

@@ -151,4 +151,29 @@ huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out
   });
 }
 
+huv_status huv_profile_enable(void* engine, int32_t on) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    std::lock_guard<std::mutex> lock(e->mu);
+    e->prof.on = on != 0;
+    e->prof.reset();
+  });
+}
+
+huv_status huv_profile_read(void* engine, double* dominant_ms, int32_t* dominant_launches, int64_t* total_launches,
+                            char* dominant_name, int32_t name_capacity) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    std::lock_guard<std::mutex> lock(e->mu);
+    if (dominant_ms) *dominant_ms = e->prof.total_ms();
+    if (dominant_launches) *dominant_launches = static_cast<int32_t>(e->prof.used);
+    if (total_launches) *total_launches = e->prof.launches;
+    if (dominant_name && name_capacity > 0) {
+      std::strncpy(dominant_name, e->prof.name.c_str(), static_cast<size_t>(name_capacity) - 1);
+      dominant_name[name_capacity - 1] = 0;
+    }
+    e->prof.reset();
+  });
+}
+
 }  // extern "C"

@@ -253,14 +253,18 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   return cudaGetLastError();
 }
 
-cudaError_t socs_inverse(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
-                         float2* T, float keep, float flare, const float* mean, float* out, int mode,
-                         const float2* tw, cudaStream_t st) {
+cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                      float2* T, const float2* tw, cudaStream_t st) {
   const int B = 2 * hb + 1;
   const int S = lgm >= 11 ? 2 : 4;
   const size_t sm3 = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
   dim3 g3((K * B + S - 1) / S, clips);
   socs_rows_inv<<<g3, 256, sm3, st>>>(kband, scale, Mband, K, hb, lgm, S, T, tw);
+  return cudaGetLastError();
+}
+
+cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+                      const float* mean, float* out, int mode, const float2* tw, cudaStream_t st) {
   const int L = 1 << lgm;
   const int Wc = lgm >= 11 ? 4 : (L >= 8 ? 8 : L);
   const size_t sm4 = (2 * (static_cast<size_t>(Wc) << lgm)) * sizeof(float2) +

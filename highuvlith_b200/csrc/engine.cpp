@@ -23,9 +23,10 @@ namespace huv_launch {
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X,
                          float2* Mband, const float* ptx, const float* W, float* mean,
                          const float2* tw, cudaStream_t st);
-cudaError_t socs_inverse(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm,
-                         int clips, float2* T, float keep, float flare, const float* mean, float* out,
-                         int mode, const float2* tw, cudaStream_t st);
+cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                      float2* T, const float2* tw, cudaStream_t st);
+cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+                      const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 cudaError_t set_smem_limits();
 cudaError_t tc_prepare(huv::TcState& tc, const huv::DeviceSet& ds, int n, int lgm, cudaStream_t st);
 cudaError_t tc_socs(const huv::TcState& tc, const huv::DeviceSet& ds, const float2* Mband, int clips,
@@ -116,6 +117,7 @@ Engine::~Engine() {
     };
     free_set(focus_dev);
     for (auto& e : cache) free_set(e.dev);
+    prof.release();
     cudaFree(ws);
     cudaFree(io_in);
     cudaFree(io_out);
@@ -306,21 +308,21 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
     check_cuda(huv_launch::band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb,
                                         b.pixel_transfer ? ds.ptx : nullptr, ds.W, mean, twn, st),
                "band_forward");
-    if (!coarse) {
-      check_cuda(huv_launch::socs_inverse(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, ds.keep, ds.flare, mean, o, 0,
-                                          twm, st),
-                 "socs_inverse");
-    } else {
-      check_cuda(huv_launch::socs_inverse(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, ds.keep, ds.flare, mean, IM, 0,
-                                          twm, st),
-                 "socs_inverse(coarse)");
+    prof.launches += 2;
+    check_cuda(huv_launch::socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");
+    prof.begin("socs_cols_inv", st);
+    check_cuda(huv_launch::socs_cols(T, K, hb, lgm, nc, ds.keep, ds.flare, mean, coarse ? IM : o, 0, twm, st),
+               "socs_cols");
+    prof.end(st);
+    prof.launches += 2;
+    if (coarse) {
       check_cuda(huv_launch::band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr,
                                           nullptr, twm, st),
                  "band_forward(interp)");
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
-      check_cuda(huv_launch::socs_inverse(nullptr, scale, C, 1, h2, lgn, nc, T2, 1.f, 0.f, nullptr, o, 1, twn,
-                                          st),
-                 "socs_inverse(interp)");
+      check_cuda(huv_launch::socs_rows(nullptr, scale, C, 1, h2, lgn, nc, T2, twn, st), "socs_rows(interp)");
+      check_cuda(huv_launch::socs_cols(T2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, o, 1, twn, st), "socs_cols(interp)");
+      prof.launches += 4;
     }
   }
 }

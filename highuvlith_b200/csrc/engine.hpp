@@ -43,6 +43,56 @@ struct DeviceSet {
   TcState tc;
 };
 
+// Launch accounting and live timing of the dominant kernel.  When `on`,
+// each launch of the dominant kernel is bracketed by a pair of CUDA events
+// recorded on the launching stream; `launches` counts every launch of this
+// library's kernels.
+struct Prof {
+  bool on = false;
+  std::string name;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+  size_t used = 0;
+  int64_t launches = 0;
+  void begin(const char* nm, cudaStream_t st) {
+    if (!on) return;
+    name = nm;
+    if (used == pool.size()) {
+      cudaEvent_t a, b;
+      check_cuda(cudaEventCreate(&a), "cudaEventCreate");
+      check_cuda(cudaEventCreate(&b), "cudaEventCreate");
+      pool.emplace_back(a, b);
+    }
+    check_cuda(cudaEventRecord(pool[used].first, st), "cudaEventRecord");
+  }
+  void end(cudaStream_t st) {
+    if (!on) return;
+    check_cuda(cudaEventRecord(pool[used].second, st), "cudaEventRecord");
+    ++used;
+  }
+  double total_ms() {
+    double t = 0;
+    for (size_t i = 0; i < used; ++i) {
+      check_cuda(cudaEventSynchronize(pool[i].second), "cudaEventSynchronize");
+      float ms = 0;
+      check_cuda(cudaEventElapsedTime(&ms, pool[i].first, pool[i].second), "cudaEventElapsedTime");
+      t += ms;
+    }
+    return t;
+  }
+  void reset() {
+    used = 0;
+    launches = 0;
+  }
+  void release() {
+    for (auto& pr : pool) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+    pool.clear();
+    used = 0;
+  }
+};
+
 struct CacheEntry {
   double z = 0;
   std::shared_ptr<KernelSet> ks;
@@ -79,6 +129,7 @@ struct Engine {
   std::vector<CacheEntry> cache;
   uint64_t clock = 0;
 
+  Prof prof;
   std::mutex mu, host_mu;
   bool device_ready = false;
   std::map<int, float2*> twiddles;

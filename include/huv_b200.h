@@ -175,6 +175,16 @@ huv_status huv_rasterize_rects(int32_t n, int32_t n_clips, const int32_t* rects_
                                const int32_t* clip_offsets_dev, int32_t dark_field,
                                uint8_t* raster_out_dev, void* stream);
 
+/* Measurement hooks (no counterpart in the reference, which has no device
+ * path).  While profiling is on, each launch of the dominant SOCS kernel is
+ * bracketed by CUDA events recorded on its own stream.  huv_profile_read
+ * synchronises those events, returns the summed kernel time, the number of
+ * bracketed launches, the number of all kernel launches made by this engine
+ * since the last read, and the dominant kernel's name, then resets. */
+huv_status huv_profile_enable(void* engine, int32_t on);
+huv_status huv_profile_read(void* engine, double* dominant_ms, int32_t* dominant_launches,
+                            int64_t* total_launches, char* dominant_name, int32_t name_capacity);
+
 #ifdef __cplusplus
 }
 #endif
