@@ -209,6 +209,12 @@ class SimulationEngine:
                                            C.byref(k)))
         return ev, ker
 
+    def device_status(self, stream=None) -> None:
+        """Synchronise and raise HuvError(DEVICE_TIMEOUT) if a bounded device
+        wait of an earlier call gave up."""
+        st = stream.cuda_stream if stream is not None else None
+        L.check(L.lib().huv_device_status(self._h, st))
+
     # ---------------------------------------------------------- measurement
     def profile(self, on: bool = True) -> None:
         """Turn live timing of the dominant kernel on or off (resets counters)."""

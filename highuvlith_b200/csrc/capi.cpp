@@ -34,6 +34,15 @@ huv_status guarded(F&& f) {
   }
 }
 
+void check_cuda_sync(Engine* e, cudaStream_t st) {
+  std::lock_guard<std::mutex> lock(e->mu);
+  if (!e->device_ready) return;
+  huv::check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+  huv::check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  if (e->read_device_error() != 0)
+    throw Error(HUV_ERR_DEVICE_TIMEOUT, "a bounded device-side wait gave up; results of the last calls are not valid");
+}
+
 Engine* as_engine(void* e) {
   if (!e) throw Error(HUV_ERR_INVALID_PARAMETER, "engine: null handle");
   return static_cast<Engine*>(e);
@@ -148,6 +157,13 @@ huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out
     Engine* e = as_engine(engine);
     if (!batch) throw Error(HUV_ERR_INVALID_PARAMETER, "batch: null");
     e->image_batch_host(*batch, out_host, static_cast<cudaStream_t>(stream));
+  });
+}
+
+huv_status huv_device_status(void* engine, void* stream) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    check_cuda_sync(e, static_cast<cudaStream_t>(stream));
   });
 }
 

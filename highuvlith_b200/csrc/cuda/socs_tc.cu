@@ -1,22 +1,562 @@
-// Tensor-core (split-BF16x3 tcgen05) form of the SOCS sum.  Placeholder
-// until the tcgen05 kernels land: reports the form as unsupported.
+// Tensor-core (split-BF16x3, tcgen05) form of the SOCS aerial image, sm_100a.
+//
+// The cropped-band inverse transform along y is a dense DFT-matrix
+// contraction.  For every kernel k the per-kernel field on the evaluation
+// grid is E_k(y, x) = sum_my G(y, my) T_k(my, x), with T_k the row transform
+// (FFT along x, FP32) of the band product K_k . M.  Complex arithmetic is laid
+// out as a real GEMM whose rows are (y, re/im) pairs:
+//     row (y, re) = [ cos t, -sin t ] , row (y, im) = [ sin t, cos t ]
+// against B rows x = [ Tr(my), Ti(my) ] (K index 2 my + re/im).  Each FP32
+// value v is split v = hi + lo (two BF16 planes) and the product is taken as
+// hi.hi + hi.lo + lo.hi with FP32 accumulation in tensor memory; B's hi plane
+// is read twice from the same shared-memory tile.  The epilogue squares the
+// accumulator, combines the (re, im) lanes with one shuffle and sums
+// lambda_k |E_k|^2 over k in registers (lambda folded into the kernels), then
+// applies normalisation and flare.  The same kernel, in store mode, performs
+// the exact band interpolation from the evaluation grid to the N x N output
+// (Hermitian half band, real part only).
+//
+// Roles per CTA (6 warps): warp 0 issues TMA loads (no multicast), warp 1
+// issues tcgen05.mma from one thread, warps 2-5 drain tensor memory.  All
+// mbarrier waits are bounded in time; a timeout sets an error flag, drains
+// in-flight work with bounded waits, frees tensor memory and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
 
 #include "../engine.hpp"
+#include "fft_block.cuh"
+#include "tc_ptx.cuh"
 
-namespace huv_launch {
-cudaError_t tc_prepare(huv::TcState&, const huv::DeviceSet&, int, int, cudaStream_t) { return cudaErrorNotSupported; }
-cudaError_t tc_socs(const huv::TcState&, const huv::DeviceSet&, const float2*, int, int, float, float,
-                    const float*, float*, void*, cudaStream_t) {
-  return cudaErrorNotSupported;
+namespace huv_dev {
+
+constexpr int kTcStages = 3;
+constexpr int kTcBN = 128;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s per wait
+constexpr uint32_t kABox = 128 * 128;             // 128 rows x 64 bf16
+constexpr uint32_t kBBox = kTcBN * 128;           // BN rows x 64 bf16
+
+struct TcGemmParams {
+  int kboxes;       // 64-wide K boxes loaded
+  int ksteps;       // 16-wide MMA K steps issued
+  int G;            // accumulation steps per output tile (kernels)
+  int a_rows;       // rows of A per split plane
+  int b_rows;       // rows of B per (problem, step, plane)
+  int out_ld;       // output row stride (floats)
+  long long out_plane;
+  float keep, flare;
+  const float* mean;
+  float* out;
+  int* err;
+};
+
+__host__ __device__ constexpr size_t tc_smem_bytes(int kboxes) {
+  return 1024 + 2 * static_cast<size_t>(kboxes) * kABox + kTcStages * 2 * static_cast<size_t>(kBBox) + 256;
 }
-size_t tc_workspace_bytes(const huv::DeviceSet&, int, int) { return 0; }
-void tc_release(huv::TcState& tc) { tc = huv::TcState(); }
+
+// MODE 0: sum over G steps of |E|^2 with (re, im) in adjacent accumulator
+// rows; out(y, x) = keep * sum + flare * mean[problem].  MODE 1: G = 1, out
+// = accumulator.  grid: (b_rows / BN, a_rows / 128, problems).
+template <int MODE>
+__global__ void __launch_bounds__(192, 1)
+    tc_dft_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcGemmParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  uint8_t* sA = base;
+  uint8_t* sB = base + 2 * p.kboxes * kABox;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + kTcStages * 2 * kBBox);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + kTcStages;
+  uint64_t* a_full = bars + 2 * kTcStages;
+  uint64_t* tfull = bars + 2 * kTcStages + 1;
+  uint64_t* tempty = bars + 2 * kTcStages + 3;
+  uint64_t* done = bars + 2 * kTcStages + 5;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kTcStages + 6);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_tile = blockIdx.x, m_tile = blockIdx.y, prob = blockIdx.z;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kTcStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(a_full, 1);
+    mbar_init(&tfull[0], 1);
+    mbar_init(&tfull[1], 1);
+    mbar_init(&tempty[0], 4);
+    mbar_init(&tempty[1], 4);
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, 2 * kTcBN);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  auto fail = [&](int code) {
+    *abort_flag = 1;
+    if (p.err) atomicExch(p.err, code);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      prefetch_tmap(&tmA);
+      prefetch_tmap(&tmB);
+      mbar_arrive_expect_tx(a_full, 2u * p.kboxes * kABox);
+      for (int part = 0; part < 2; ++part)
+        for (int kb = 0; kb < p.kboxes; ++kb)
+          tma_load_2d(sA + (part * p.kboxes + kb) * kABox, &tmA, kb * 64, part * p.a_rows + m_tile * 128, a_full);
+      int it = 0;
+      for (int g = 0; g < p.G && !*abort_flag; ++g) {
+        for (int kb = 0; kb < p.kboxes; ++kb, ++it) {
+          const int s = it % kTcStages;
+          const uint32_t ph = (it / kTcStages) & 1;
+          if (!mbar_wait(&empty[s], ph ^ 1, kWaitLimitNs)) {
+            fail(1);
+            break;
+          }
+          mbar_arrive_expect_tx(&full[s], 2u * kBBox);
+          const int row = ((prob * p.G + g) * 2) * p.b_rows + n_tile * kTcBN;
+          tma_load_2d(sB + (s * 2 + 0) * kBBox, &tmB, kb * 64, row, &full[s]);
+          tma_load_2d(sB + (s * 2 + 1) * kBBox, &tmB, kb * 64, row + p.b_rows, &full[s]);
+        }
+      }
+      // Drain: every load issued must have landed before the CTA may exit.
+      mbar_wait(a_full, 0, kWaitLimitNs);
+      for (int q = (it > kTcStages ? it - kTcStages : 0); q < it; ++q)
+        mbar_wait(&full[q % kTcStages], (q / kTcStages) & 1, kWaitLimitNs);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16(128, kTcBN);
+      bool ok = mbar_wait(a_full, 0, kWaitLimitNs);
+      if (!ok) fail(2);
+      tc_fence_after();
+      int it = 0;
+      for (int g = 0; g < p.G && ok && !*abort_flag; ++g) {
+        const int buf = g & 1;
+        if (!mbar_wait(&tempty[buf], ((g >> 1) & 1) ^ 1, kWaitLimitNs)) {
+          fail(3);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + buf * kTcBN;
+        for (int kb = 0; kb < p.kboxes; ++kb, ++it) {
+          const int s = it % kTcStages;
+          if (!mbar_wait(&full[s], (it / kTcStages) & 1, kWaitLimitNs)) {
+            fail(4);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t a_hi = smem_desc_sw128(smem_u32(sA + (0 * p.kboxes + kb) * kABox));
+          const uint64_t a_lo = smem_desc_sw128(smem_u32(sA + (1 * p.kboxes + kb) * kABox));
+          const uint64_t b_hi = smem_desc_sw128(smem_u32(sB + (s * 2 + 0) * kBBox));
+          const uint64_t b_lo = smem_desc_sw128(smem_u32(sB + (s * 2 + 1) * kBBox));
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            const int kstep = kb * 4 + ks;
+            if (kstep < p.ksteps) {
+              const uint64_t adv = static_cast<uint64_t>(2 * ks);  // 32 bytes per 16-wide K step
+              tc_mma_bf16(d, a_hi + adv, b_hi + adv, idesc, kstep > 0 ? 1u : 0u);
+              tc_mma_bf16(d, a_hi + adv, b_lo + adv, idesc, 1u);
+              tc_mma_bf16(d, a_lo + adv, b_hi + adv, idesc, 1u);
+            }
+          }
+          tc_commit(&empty[s]);
+        }
+        if (!ok) break;
+        tc_commit(&tfull[buf]);
+      }
+      // All MMAs issued by this thread have completed once `done` flips.
+      tc_commit(done);
+      mbar_wait(done, 0, kWaitLimitNs);
+    }
+  } else {
+    // Epilogue warps 2..5: TMEM lane quadrant = warp % 4.
+    const int quad = warp & 3;
+    const int row = quad * 32 + lane;  // accumulator row within the tile
+    constexpr int HALF = kTcBN / 2;
+    float acc[MODE == 0 ? HALF : 1];
+#pragma unroll
+    for (int i = 0; i < (MODE == 0 ? HALF : 1); ++i) acc[i] = 0.f;
+    const int odd = lane & 1;
+    bool ok = true;
+    for (int g = 0; g < p.G; ++g) {
+      const int buf = g & 1;
+      // Warp-uniform outcome: tcgen05.ld below is .sync.aligned.
+      const bool got = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (g >> 1) & 1, kWaitLimitNs));
+      if (!got) {
+        if (lane == 0) fail(5);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + buf * kTcBN;
+#pragma unroll
+      for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+        float v[32];
+        tmem_ld32(taddr + c0, v);
+        if (MODE == 0) {
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            float e = v[i] * v[i];
+            e += __shfl_xor_sync(0xffffffffu, e, 1);
+            const int j = c0 + i;
+            if ((j / HALF) == odd) acc[j % HALF] += e;
+          }
+        } else {
+          const int y = m_tile * 128 + row;
+          float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + n_tile * kTcBN + c0;
+#pragma unroll
+          for (int i = 0; i < 32; i += 4)
+            *reinterpret_cast<float4*>(o + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[buf]);
+    }
+    if (MODE == 0 && ok) {
+      const int y = (m_tile * 128 + row) >> 1;
+      const float add = p.mean ? p.flare * p.mean[prob] : 0.f;
+      float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + n_tile * kTcBN + odd * HALF;
+#pragma unroll
+      for (int i = 0; i < HALF; i += 4)
+        *reinterpret_cast<float4*>(o + i) = make_float4(p.keep * acc[i] + add, p.keep * acc[i + 1] + add,
+                                                        p.keep * acc[i + 2] + add, p.keep * acc[i + 3] + add);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem_base, 2 * kTcBN);
+}
+
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(v);
+  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+// Row transform along x of the band products, written as the tensor-core
+// B operand: Bop[problem][k][plane][x][kk], kk = 2 * (row - row_off) + re/im,
+// planes hi / lo, K-major with row stride kp.  Rows [row_off, row_off + nrows)
+// of the band are used.  Columns [2 * nrows, zero_to) are written as zeros.
+// grid: (ceil(K * nrows / S), problems).
+__global__ void socs_rows_tc(const float2* __restrict__ kband, float scale, const float2* __restrict__ Mband,
+                             int K, int hb, int row_off, int nrows, int lg, int S, int kp, int zero_to,
+                             __nv_bfloat16* __restrict__ Bop, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  const int L = 1 << lg;
+  const int B = 2 * hb + 1;
+  const int prob = blockIdx.y;
+  const int seq0 = blockIdx.x * S;
+  const int nseq = min(S, K * nrows - seq0);
+  float2* a = smem;
+  float2* b = smem + (S << lg);
+  for (int t = threadIdx.x; t < (S << lg); t += blockDim.x) a[t] = make_float2(0.f, 0.f);
+  __syncthreads();
+  const float2* Mc = Mband + static_cast<size_t>(prob) * B * B;
+  for (int t = threadIdx.x; t < nseq * B; t += blockDim.x) {
+    const int s = t / B, mx = t - s * B;
+    const int seq = seq0 + s;
+    const int k = seq / nrows, my = row_off + (seq - k * nrows);
+    const float2 m = Mc[static_cast<size_t>(my) * B + mx];
+    const float2 u = kband ? kband[(static_cast<size_t>(k) * B + my) * B + mx] : make_float2(scale, 0.f);
+    a[(s << lg) + ((mx - hb) & (L - 1))] = cmul(u, m);
+  }
+  __syncthreads();
+  const float2* r = block_fft<+1>(a, b, lg, S, tw);
+  const size_t plane = static_cast<size_t>(L) * kp;
+  for (int t = threadIdx.x; t < (nseq << lg); t += blockDim.x) {
+    const int s = t % nseq, x = t / nseq;
+    const int seq = seq0 + s;
+    const int k = seq / nrows, myr = seq - k * nrows;
+    const float2 v = r[(s << lg) + x];
+    __nv_bfloat16 rh, rl, ih, il;
+    split_bf16(v.x, rh, rl);
+    split_bf16(v.y, ih, il);
+    __nv_bfloat16* hi = Bop + (static_cast<size_t>(prob) * K + k) * 2 * plane + static_cast<size_t>(x) * kp;
+    __nv_bfloat16* lo = hi + plane;
+    __nv_bfloat162 hv, lv;
+    hv.x = rh;
+    hv.y = ih;
+    lv.x = rl;
+    lv.y = il;
+    *reinterpret_cast<__nv_bfloat162*>(hi + 2 * myr) = hv;
+    *reinterpret_cast<__nv_bfloat162*>(lo + 2 * myr) = lv;
+    if (myr == nrows - 1) {
+      const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
+      for (int kk = 2 * nrows; kk < zero_to; ++kk) {
+        hi[kk] = z;
+        lo[kk] = z;
+      }
+    }
+  }
+}
+
+}  // namespace huv_dev
+
+// ------------------------------------------------------------------ host
+namespace huv_launch {
+
+using namespace huv_dev;
+cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
+                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st);
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }
+  return fn;
+}
+
+// 2-D bf16 tensor map over a K-major [rows][kp] array, box 64 x box_rows, 128B swizzle.
+bool make_map(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(kp), rows};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(kp) * 2};
+  cuuint32_t box[2] = {64, static_cast<cuuint32_t>(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+uint16_t host_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  const uint32_t rounding = 0x7FFFu + ((u >> 16) & 1u);
+  return static_cast<uint16_t>((u + rounding) >> 16);
+}
+float host_bf16_to_f(uint16_t h) {
+  const uint32_t u = static_cast<uint32_t>(h) << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// Split planes [2][rows][kp] of a real matrix given row-major values [rows][kc].
+std::vector<uint16_t> split_planes(const std::vector<double>& v, int rows, int kc, int kp) {
+  std::vector<uint16_t> out(2 * static_cast<size_t>(rows) * kp, 0);
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < kc; ++c) {
+      const float f = static_cast<float>(v[static_cast<size_t>(r) * kc + c]);
+      const uint16_t hi = host_bf16(f);
+      const uint16_t lo = host_bf16(f - host_bf16_to_f(hi));
+      out[static_cast<size_t>(r) * kp + c] = hi;
+      out[(static_cast<size_t>(rows) + r) * kp + c] = lo;
+    }
+  return out;
+}
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+}  // namespace
+
+cudaError_t tc_set_smem() {
+  const int bytes = static_cast<int>(tc_smem_bytes(3));
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+  if ((e = cudaFuncSetAttribute(socs_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+  return cudaSuccess;
+}
+
+void tc_release(huv::TcState& tc) {
+  cudaFree(tc.gy);
+  cudaFree(tc.gx);
+  tc = huv::TcState();
+}
+
 }  // namespace huv_launch
 
 namespace huv {
-bool Engine::tc_supported(const DeviceSet&, int) const { return false; }
-void Engine::run_tc_form(const huv_batch&, DeviceSet&, int, float*, cudaStream_t) {
-  throw Error(HUV_ERR_UNSUPPORTED, "TC form not available in this build");
+
+namespace {
+constexpr double kPi = 3.14159265358979323846;
+inline int ilog2i(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
 }
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+}  // namespace
+
+bool Engine::tc_supported(const DeviceSet& ds, int M) const {
+  const int kpE = ((2 * ds.B) + 63) / 64 * 64;
+  const int kpI = ((2 * (2 * ds.hb + 1)) + 63) / 64 * 64;
+  return M >= 128 && n >= 128 && M % huv_dev::kTcBN == 0 && kpE <= 192 && kpI <= 192 &&
+         huv_launch::encode_fn() != nullptr;
+}
+
+void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st) {
+  using namespace huv_launch;
+  static bool smem_set = false;
+  if (!smem_set) {
+    check_cuda(tc_set_smem(), "cudaFuncSetAttribute(tc)");
+    smem_set = true;
+  }
+  const int lgn = ilog2i(n), lgm = ilog2i(M);
+  const int B = ds.B, K = ds.K, hb = ds.hb;
+  const int h2 = 2 * hb, B2 = 2 * h2 + 1;
+  const int kcE = 2 * B, kpE = round_up(kcE, 64), kstE = (kcE + 15) / 16;
+  const int nrI = h2 + 1, kcI = 2 * nrI, kpI = round_up(kcI, 64), kstI = (kcI + 15) / 16;
+  TcState& tc = ds.tc;
+  if (tc.lgm != lgm || !tc.gy) {
+    tc_release(tc);
+    // A_E: rows (y, re/im) over the M grid, K = (my, re/im).
+    std::vector<double> ae(static_cast<size_t>(2 * M) * kcE);
+    for (int y = 0; y < M; ++y)
+      for (int mi = 0; mi < B; ++mi) {
+        const double th = 2.0 * kPi * (mi - hb) * static_cast<double>(y) / M;
+        const double c = std::cos(th), s = std::sin(th);
+        double* re = &ae[static_cast<size_t>(2 * y) * kcE];
+        double* im = &ae[static_cast<size_t>(2 * y + 1) * kcE];
+        re[2 * mi] = c;
+        re[2 * mi + 1] = -s;
+        im[2 * mi] = s;
+        im[2 * mi + 1] = c;
+      }
+    // A_I: rows y over the N grid, K = (qy >= 0, re/im), Hermitian weights.
+    std::vector<double> ai(static_cast<size_t>(n) * kcI);
+    for (int y = 0; y < n; ++y)
+      for (int q = 0; q <= h2; ++q) {
+        const double th = 2.0 * kPi * q * static_cast<double>(y) / n;
+        const double w = q == 0 ? 1.0 : 2.0;
+        ai[static_cast<size_t>(y) * kcI + 2 * q] = w * std::cos(th);
+        ai[static_cast<size_t>(y) * kcI + 2 * q + 1] = -w * std::sin(th);
+      }
+    const auto pe = split_planes(ae, 2 * M, kcE, kpE);
+    const auto pi = split_planes(ai, n, kcI, kpI);
+    check_cuda(cudaMalloc(&tc.gy, pe.size() * 2), "cudaMalloc(A_E)");
+    check_cuda(cudaMalloc(&tc.gx, pi.size() * 2), "cudaMalloc(A_I)");
+    check_cuda(cudaMemcpy(tc.gy, pe.data(), pe.size() * 2, cudaMemcpyHostToDevice), "upload A_E");
+    check_cuda(cudaMemcpy(tc.gx, pi.data(), pi.size() * 2, cudaMemcpyHostToDevice), "upload A_I");
+    if (!make_map(&tc.map_ae, tc.gy, 2ull * 2 * M, kpE, 128) || !make_map(&tc.map_ai, tc.gx, 2ull * n, kpI, 128))
+      throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the DFT operands");
+    tc.lgm = lgm;
+  }
+  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
+  const size_t per_x = align256(sizeof(float2) * n * B);
+  const size_t per_m = align256(sizeof(float2) * B * B);
+  const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kpE * 2);
+  const size_t per_i = align256(sizeof(float) * M * M);
+  const size_t per_x2 = align256(sizeof(float2) * M * B2);
+  const size_t per_c = align256(sizeof(float2) * B2 * B2);
+  const size_t per_bi = align256(static_cast<size_t>(2) * n * kpI * 2);
+  const size_t per_clip = per_x + per_m + per_be + per_i + per_x2 + per_c + per_bi + 256;
+  const size_t budget = size_t(1) << 30;
+  int chunk = static_cast<int>(std::max<size_t>(1, budget / per_clip));
+  chunk = std::min(chunk, b.n_clips);
+  char* base = static_cast<char*>(workspace(per_clip * chunk + 4096));
+  size_t off = 0;
+  auto take = [&](size_t per) {
+    char* p = base + off;
+    off += per * chunk;
+    return p;
+  };
+  float2* X = reinterpret_cast<float2*>(take(per_x));
+  float2* Mb = reinterpret_cast<float2*>(take(per_m));
+  __nv_bfloat16* BE = reinterpret_cast<__nv_bfloat16*>(take(per_be));
+  float* IM = reinterpret_cast<float*>(take(per_i));
+  float2* X2 = reinterpret_cast<float2*>(take(per_x2));
+  float2* C = reinterpret_cast<float2*>(take(per_c));
+  __nv_bfloat16* BI = reinterpret_cast<__nv_bfloat16*>(take(per_bi));
+  float* mean = reinterpret_cast<float*>(take(256));
+  const float2* twn = twiddle(lgn);
+  const float2* twm = twiddle(lgm);
+  const size_t smem_tc = tc_smem_bytes(3);
+  for (int c0 = 0; c0 < b.n_clips; c0 += chunk) {
+    const int nc = std::min(chunk, b.n_clips - c0);
+    const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
+    float* o = out + static_cast<size_t>(n) * n * c0;
+    check_cuda(band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb, b.pixel_transfer ? ds.ptx : nullptr, ds.W,
+                            mean, twn, st),
+               "band_forward");
+    {
+      const int S = 8;
+      dim3 g((K * B + S - 1) / S, nc);
+      const size_t sm = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
+      socs_rows_tc<<<g, 256, sm, st>>>(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, S, kpE, kstE * 16, BE, twm);
+      check_cuda(cudaGetLastError(), "socs_rows_tc");
+    }
+    CUtensorMap mbE, mbI;
+    if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kpE, kTcBN) ||
+        !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kpI, kTcBN))
+      throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
+    {
+      TcGemmParams p{};
+      p.kboxes = kpE / 64;
+      p.ksteps = kstE;
+      p.G = K;
+      p.a_rows = 2 * M;
+      p.b_rows = M;
+      p.out_ld = M;
+      p.out_plane = static_cast<long long>(M) * M;
+      p.keep = ds.keep;
+      p.flare = ds.flare;
+      p.mean = mean;
+      p.out = IM;
+      p.err = dev_err;
+      dim3 g(M / kTcBN, 2 * M / 128, nc);
+      prof.begin("tc_dft_gemm<sumsq>", st);
+      tc_dft_gemm<0><<<g, 192, smem_tc, st>>>(tc.map_ae, mbE, p);
+      prof.end(st);
+      check_cuda(cudaGetLastError(), "tc_dft_gemm<0>");
+    }
+    check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st),
+               "band_forward(interp)");
+    {
+      const int S = 8;
+      dim3 g((nrI + S - 1) / S, nc);
+      const size_t sm = 2 * (static_cast<size_t>(S) << lgn) * sizeof(float2);
+      const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
+      socs_rows_tc<<<g, 256, sm, st>>>(nullptr, scale, C, 1, h2, h2, nrI, lgn, S, kpI, kstI * 16, BI, twn);
+      check_cuda(cudaGetLastError(), "socs_rows_tc(interp)");
+    }
+    {
+      TcGemmParams p{};
+      p.kboxes = kpI / 64;
+      p.ksteps = kstI;
+      p.G = 1;
+      p.a_rows = n;
+      p.b_rows = n;
+      p.out_ld = n;
+      p.out_plane = static_cast<long long>(n) * n;
+      p.keep = 1.f;
+      p.flare = 0.f;
+      p.mean = nullptr;
+      p.out = o;
+      p.err = dev_err;
+      dim3 g(n / kTcBN, n / 128, nc);
+      tc_dft_gemm<1><<<g, 192, smem_tc, st>>>(tc.map_ai, mbI, p);
+      check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
+    }
+    prof.launches += 7;
+  }
+}
+
 }  // namespace huv

@@ -28,11 +28,6 @@ cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
                       const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 cudaError_t set_smem_limits();
-cudaError_t tc_prepare(huv::TcState& tc, const huv::DeviceSet& ds, int n, int lgm, cudaStream_t st);
-cudaError_t tc_socs(const huv::TcState& tc, const huv::DeviceSet& ds, const float2* Mband, int clips,
-                    int lgm, float keep, float flare, const float* mean, float* out, void* ws,
-                    cudaStream_t st);
-size_t tc_workspace_bytes(const huv::DeviceSet& ds, int lgm, int clips);
 void tc_release(huv::TcState& tc);
 }  // namespace huv_launch
 
@@ -118,6 +113,7 @@ Engine::~Engine() {
     free_set(focus_dev);
     for (auto& e : cache) free_set(e.dev);
     prof.release();
+    cudaFree(dev_err);
     cudaFree(ws);
     cudaFree(io_in);
     cudaFree(io_out);
@@ -161,6 +157,8 @@ void Engine::ensure_device() {
   check_cuda(cudaSetDevice(device), "cudaSetDevice");
   if (device_ready) return;
   check_cuda(huv_launch::set_smem_limits(), "cudaFuncSetAttribute");
+  check_cuda(cudaMalloc(&dev_err, sizeof(int)), "cudaMalloc(error flag)");
+  check_cuda(cudaMemset(dev_err, 0, sizeof(int)), "cudaMemset(error flag)");
   device_ready = true;
 }
 
@@ -337,11 +335,14 @@ void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
   ensure_device();
   DeviceSet& ds = device_set(b.defocus_nm == 0.0 ? 0.0 : b.defocus_nm);
   const int M = choose_eval_grid(ds, b.eval_grid);
+  // The tensor-core form tiles the evaluation grid by 128; an automatically
+  // chosen grid below that is raised to 128 (still exact: any M > 4h is).
+  const int Mtc = (b.eval_grid == 0 && M < 128 && n >= 128) ? 128 : M;
   int form = b.form;
-  if (form == HUV_FORM_AUTO) form = tc_supported(ds, M) ? HUV_FORM_TC : HUV_FORM_FFT;
+  if (form == HUV_FORM_AUTO) form = tc_supported(ds, Mtc) ? HUV_FORM_TC : HUV_FORM_FFT;
   if (form == HUV_FORM_TC) {
-    if (!tc_supported(ds, M)) throw Error(HUV_ERR_UNSUPPORTED, "TC form: unsupported band/grid for this build");
-    run_tc_form(b, ds, M, out, st);
+    if (!tc_supported(ds, Mtc)) throw Error(HUV_ERR_UNSUPPORTED, "TC form: unsupported band/grid for this build");
+    run_tc_form(b, ds, Mtc, out, st);
   } else if (form == HUV_FORM_FFT) {
     run_fft_form(b, ds, M, out, st);
   } else {
@@ -383,6 +384,17 @@ void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t 
   image_batch(d, static_cast<float*>(io_out), st);
   check_cuda(cudaMemcpyAsync(out_host, io_out, out_bytes, cudaMemcpyDeviceToHost, st), "D2H images");
   check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  std::lock_guard<std::mutex> lock(mu);
+  if (read_device_error() != 0)
+    throw Error(HUV_ERR_DEVICE_TIMEOUT, "a bounded device-side wait gave up; the images are not valid");
+}
+
+int Engine::read_device_error() {
+  if (!dev_err) return 0;
+  int v = 0;
+  check_cuda(cudaMemcpy(&v, dev_err, sizeof(int), cudaMemcpyDeviceToHost), "read device error flag");
+  if (v) check_cuda(cudaMemset(dev_err, 0, sizeof(int)), "reset device error flag");
+  return v;
 }
 
 }  // namespace huv

@@ -1,6 +1,7 @@
 // Engine state shared by the C ABI and the device launchers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -18,14 +19,14 @@ void set_last_error(const std::string& m);
 const char* last_error();
 void check_cuda(cudaError_t e, const char* what);
 
-// Device-side state of the tensor-core form for one kernel set.
+// Device-side state of the tensor-core form for one kernel set: the split
+// BF16 DFT operands (A_E over the evaluation grid, A_I for the interpolation
+// to the output grid) and their TMA descriptors.
 struct TcState {
-  int lgm = 0;          // evaluation grid the state was built for
-  int kpad = 0;         // padded contraction length of one split-BF16x3 GEMM
-  void* gy = nullptr;   // DFT operand along y (bf16, split planes)
-  void* gx = nullptr;   // DFT operand along x (bf16, split planes)
-  void* kb = nullptr;   // kernel band operand (bf16 split planes)
-  size_t bytes = 0;
+  int lgm = 0;          // evaluation grid the state was built for (log2)
+  void* gy = nullptr;   // A_E planes [2][2M][kpE] bf16
+  void* gx = nullptr;   // A_I planes [2][N][kpI] bf16
+  CUtensorMap map_ae, map_ai;
 };
 
 // One kernel set on the device: band kernels K x B x B (complex FP32,
@@ -117,6 +118,8 @@ struct Engine {
   bool tc_supported(const DeviceSet& ds, int M) const;
   void run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st);
   void run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st);
+  // Device error flag written by bounded waits that gave up (0 = none).
+  int read_device_error();
 
   huv_settings settings;
   int device;
@@ -136,6 +139,7 @@ struct Engine {
   DeviceSet focus_dev, scratch_dev;
   void* ws = nullptr;
   size_t ws_bytes = 0;
+  int* dev_err = nullptr;
   void* io_in = nullptr;
   void* io_out = nullptr;
   size_t io_in_bytes = 0, io_out_bytes = 0;

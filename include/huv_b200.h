@@ -167,6 +167,12 @@ huv_status huv_image_batch(void* engine, const huv_batch* batch, float* out, voi
  * on `stream` and synchronises it (the reference-facing end-to-end call). */
 huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out_host, void* stream);
 
+/* Synchronise `stream` and report device-side failures of earlier calls on
+ * this engine: HUV_ERR_DEVICE_TIMEOUT when a bounded device wait gave up
+ * (the flag is cleared by the report).  The device calls above are
+ * asynchronous and cannot report such failures themselves. */
+huv_status huv_device_status(void* engine, void* stream);
+
 /* Axis-aligned rectangles -> pixel-aligned binary rasters on the device
  * (mask.rs:1717-1741 for pixel-aligned Rect features on a dark- or bright-field
  * binary mask).  rects: n_rects*4 int32 (x0, y0, w, h) in pixels, row-major from

@@ -143,3 +143,44 @@ def test_c2_clips_full_size_parity_and_cd():
                 sub = slice(0, 1024, 16)
                 worst, unmatched = M.max_edge_error(out[c][sub], ref[sub], x, 0.3)
                 assert unmatched == 0 and worst < CD_TOL_NM, (worst, unmatched)
+
+
+TC_CASES = [c for c in SMALL if c[3].size >= 128]
+
+
+@pytest.mark.parametrize("case", TC_CASES, ids=[c[0] for c in TC_CASES])
+def test_tc_form_matches_oracle(case):
+    """Split-BF16x3 tcgen05 form vs the FP64 oracle (tolerance 1e-3; the
+    split products carry ~2^-16 relative precision)."""
+    torch = _torch()
+    _, src, opt, grid, kmax, fill, oopt = case
+    eng = HB.SimulationEngine(src, opt, grid=grid, max_kernels=kmax)
+    oeng = _oracle_engine(fill, oopt, grid, src.wavelength_nm, kmax)
+    n = grid.size
+    _, rasters = gen_batch(3, n, base_seed=13, wmin=max(2, n // 40), wmax=max(4, n // 8), dmin=0.2, dmax=0.6)
+    d = torch.from_numpy(rasters).cuda()
+    out = eng.compute_batch(d, form="tc").cpu().numpy()
+    eng.device_status()
+    for c in range(3):
+        ref = oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[c]))
+        assert rel_err(out[c], ref) < 1e-4, (c, rel_err(out[c], ref))
+
+
+def test_tc_form_c2_full_size():
+    """C2 at full size through the tensor-core form: parity and CD error."""
+    torch = _torch()
+    grid = HB.GridConfig(1024, 1.0)
+    eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(), grid=grid, max_kernels=32)
+    oeng = _oracle_engine(H.fill_conventional(0.5), H.euv_nxe_033(), grid, 13.5, 32)
+    _, rasters = gen_batch(3, 1024, base_seed=2026)
+    d = torch.from_numpy(rasters).cuda()
+    out = eng.compute_batch(d, form="tc").cpu().numpy()
+    eng.device_status()
+    fft = eng.compute_batch(d, form="fft").cpu().numpy()
+    x = grid.pixel_centres()
+    for c in range(3):
+        ref = oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[c]))
+        assert rel_err(out[c], ref) < REL_TOL
+        assert rel_err(out[c], fft[c]) < REL_TOL
+    worst, unmatched = M.max_edge_error(out[0], oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[0])), x, 0.3)
+    assert unmatched == 0 and worst < CD_TOL_NM, (worst, unmatched)
