@@ -345,7 +345,11 @@ def main():
     ap.add_argument("--form", default="auto", choices=["auto", "fft", "tc"])
     ap.add_argument("--eval-grid", dest="eval_grid", type=int, default=0)
     ap.add_argument("--quick", action="store_true", help="skip the extra forms, accuracy and CPU baseline")
+    ap.add_argument("--clips", type=int, default=N_CLIPS,
+                    help="clips per GPU (default 256, the workload; smaller only for profiler captures)")
     args = ap.parse_args()
+    global N_CLIPS
+    N_CLIPS = args.clips
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
