@@ -337,6 +337,7 @@ def run_ours(args):
 
 
 def main():
+    global N_CLIPS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -348,7 +349,6 @@ def main():
     ap.add_argument("--clips", type=int, default=N_CLIPS,
                     help="clips per GPU (default 256, the workload; smaller only for profiler captures)")
     args = ap.parse_args()
-    global N_CLIPS
     N_CLIPS = args.clips
     if args.impl == "reference":
         return run_reference(args)
