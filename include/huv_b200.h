@@ -167,6 +167,20 @@ huv_status huv_image_batch(void* engine, const huv_batch* batch, float* out, voi
  * on `stream` and synchronises it (the reference-facing end-to-end call). */
 huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out_host, void* stream);
 
+/* Allocation-free variant of huv_image_batch (no counterpart in the
+ * reference, which has no device path).  For callers that cannot call
+ * cudaMalloc: applications whose memory pool already owns the device, and
+ * latency-critical loops that cannot take cudaMalloc's device-wide
+ * synchronisation.  Runs the plain FP32 FFT form with all intermediates in
+ * one fixed 32 MiB device array compiled into the library (every GPU that
+ * loads the library holds it until exit); batches are processed in chunks
+ * that fit it, and a grid whose single clip does not fit is rejected with
+ * HUV_ERR_INVALID_PARAMETER.  The first call on a device performs the
+ * set-up (takes the array's device address); make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * form must be HUV_FORM_AUTO or HUV_FORM_FFT. */
+huv_status huv_image_batch_noalloc(void* engine, const huv_batch* batch, float* out, void* stream);
+
 /* Synchronise `stream` and report device-side failures of earlier calls on
  * this engine: HUV_ERR_DEVICE_TIMEOUT when a bounded device wait gave up
  * (the flag is cleared by the report).  The device calls above are
