@@ -163,7 +163,8 @@ extern "C" huv_status huv_image_batch_noalloc(void* engine, const huv_batch* bat
     const size_t per_x2 = coarse ? align256(sizeof(float2) * M * B2) : 0;
     const size_t per_c = coarse ? align256(sizeof(float2) * B2 * B2) : 0;
     const size_t per_t2 = coarse ? align256(sizeof(float2) * static_cast<size_t>(B2) * n) : 0;
-    const size_t per_clip = per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2 + 256;
+    const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
+    const size_t per_clip = per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2 + per_mean;
     if (off + per_clip > kNoAllocScratchBytes)
       throw huv::Error(HUV_ERR_INVALID_PARAMETER,
                        "allocation-free path: one clip needs " + std::to_string((off + per_clip) >> 20) +

@@ -93,56 +93,63 @@ __global__ void band_rows_fwd(const void* __restrict__ in, int lg, int rows_per_
 
 // Forward FFT of the band columns along y; keeps [-hb, hb]^2, multiplies by
 // the separable pixel transfer ptx (B floats; NULL = none) and, when W is
-// given, writes the flare mean sum_f W(f) |M(f)|^2 per clip.
-// grid: (clips); one block walks all B columns, cols_per_pass at a time.
-__global__ void band_cols_fwd(const float2* __restrict__ X, int lg, int hb, int cols_per_pass,
+// given, writes this block's part of the flare mean sum_f W(f) |M(f)|^2 to
+// parts[clip * gridDim.x + blockIdx.x] (summed in order by mean_reduce).
+// grid: (ceil(B / cols_per_block), clips).
+__global__ void band_cols_fwd(const float2* __restrict__ X, int lg, int hb, int cols_per_block,
                               const float* __restrict__ ptx, const float* __restrict__ W,
-                              float2* __restrict__ Mband, float* __restrict__ mean_out,
+                              float2* __restrict__ Mband, float* __restrict__ parts,
                               const float2* __restrict__ tw) {
   extern __shared__ float2 smem[];
   __shared__ float red[32];
   const int L = 1 << lg;
   const int B = 2 * hb + 1;
-  const int clip = blockIdx.x;
+  const int clip = blockIdx.y;
+  const int c0 = blockIdx.x * cols_per_block;
+  const int nc = min(cols_per_block, B - c0);
   float2* a = smem;
-  float2* b = smem + (cols_per_pass << lg);
+  float2* b = smem + (cols_per_block << lg);
   const float2* Xc = X + static_cast<size_t>(clip) * L * B;
   float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
-  float part = 0.f;
-  for (int c0 = 0; c0 < B; c0 += cols_per_pass) {
-    const int nc = min(cols_per_pass, B - c0);
-    for (int t = threadIdx.x; t < (cols_per_pass << lg); t += blockDim.x) {
-      const int s = t >> lg, y = t & (L - 1);
-      a[t] = s < nc ? Xc[static_cast<size_t>(y) * B + c0 + s] : make_float2(0.f, 0.f);
-    }
-    __syncthreads();
-    const float2* r = block_fft<-1>(a, b, lg, cols_per_pass, tw);
-    for (int t = threadIdx.x; t < nc * B; t += blockDim.x) {
-      const int s = t / B, mi = t - s * B;
-      const int mx = c0 + s;
-      const int idx = (mi - hb) & (L - 1);
-      float2 v = r[(s << lg) + idx];
-      if (ptx) {
-        const float f = ptx[mi] * ptx[mx];
-        v.x *= f;
-        v.y *= f;
-      }
-      Mc[static_cast<size_t>(mi) * B + mx] = v;
-      if (W) part += W[mi * B + mx] * (v.x * v.x + v.y * v.y);
-    }
-    __syncthreads();
+  for (int t = threadIdx.x; t < (cols_per_block << lg); t += blockDim.x) {
+    const int s = t & (cols_per_block - 1), y = t / cols_per_block;
+    a[(s << lg) + y] = s < nc ? Xc[static_cast<size_t>(y) * B + c0 + s] : make_float2(0.f, 0.f);
   }
-  if (mean_out) {
-    // Deterministic block reduction (fixed order per launch configuration).
+  __syncthreads();
+  const float2* r = block_fft<-1>(a, b, lg, cols_per_block, tw);
+  float part = 0.f;
+  for (int t = threadIdx.x; t < nc * B; t += blockDim.x) {
+    const int s = t / B, mi = t - s * B;
+    const int mx = c0 + s;
+    const int idx = (mi - hb) & (L - 1);
+    float2 v = r[(s << lg) + idx];
+    if (ptx) {
+      const float f = ptx[mi] * ptx[mx];
+      v.x *= f;
+      v.y *= f;
+    }
+    Mc[static_cast<size_t>(mi) * B + mx] = v;
+    if (W) part += W[mi * B + mx] * (v.x * v.x + v.y * v.y);
+  }
+  if (parts) {
     for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
     __syncthreads();
     if (threadIdx.x == 0) {
-      float s = 0.f;
-      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w];
-      mean_out[clip] = s;
+      float sum = 0.f;
+      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) sum += red[w];
+      parts[static_cast<size_t>(clip) * gridDim.x + blockIdx.x] = sum;
     }
   }
+}
+
+// mean[clip] = sum of the clip's parts in index order (deterministic).
+__global__ void mean_reduce(const float* __restrict__ parts, int nparts, int clips, float* __restrict__ mean) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= clips) return;
+  float s = 0.f;
+  for (int i = 0; i < nparts; ++i) s += parts[static_cast<size_t>(c) * nparts + i];
+  mean[c] = s;
 }
 
 // Inverse transform along x of every (kernel, band row) product, on the
@@ -234,6 +241,9 @@ using namespace huv_dev;
 
 static int pick_threads(int work) { return work >= 256 ? 256 : 128; }
 
+// Mask (or image) band: rows then columns.  When W is given, `mean` must hold
+// clips + clips * ceil(B / 4) floats: the first `clips` receive the flare
+// means, the rest holds the per-block parts.
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X,
                          float2* Mband, const float* ptx, const float* W, float* mean,
                          const float2* tw, cudaStream_t st) {
@@ -247,9 +257,13 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     case 1: band_rows_fwd<1><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
     default: band_rows_fwd<2><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
   }
-  const int cpp = 4;
-  const size_t sm2 = 2 * (static_cast<size_t>(cpp) << lg) * sizeof(float2);
-  band_cols_fwd<<<clips, 256, sm2, st>>>(X, lg, hb, cpp, ptx, W, Mband, mean, tw);
+  const int B = 2 * hb + 1;
+  const int cpb = 4;
+  const int nblk = (B + cpb - 1) / cpb;
+  const size_t sm2 = 2 * (static_cast<size_t>(cpb) << lg) * sizeof(float2);
+  float* parts = (W && mean) ? mean + clips : nullptr;
+  band_cols_fwd<<<dim3(nblk, clips), 256, sm2, st>>>(X, lg, hb, cpb, ptx, W, Mband, parts, tw);
+  if (parts) mean_reduce<<<(clips + 127) / 128, 128, 0, st>>>(parts, nblk, clips, mean);
   return cudaGetLastError();
 }
 

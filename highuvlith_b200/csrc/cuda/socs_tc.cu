@@ -45,9 +45,11 @@ constexpr uint32_t kBBox = kTcBN * 128;           // BN rows x 64 bf16
 struct TcGemmParams {
   int kboxes;       // 64-wide K boxes loaded
   int ksteps;       // 16-wide MMA K steps issued
-  int G;            // accumulation steps per output tile (kernels)
+  int G;            // steps per CTA: kernels (MODE 0) or x tiles (MODE 1)
   int a_rows;       // rows of A per split plane
-  int b_rows;       // rows of B per (problem, step, plane)
+  int b_prob;       // B rows between problems
+  int b_step;       // B rows between steps
+  int b_plane;      // B rows between the hi and lo planes
   int out_ld;       // output row stride (floats)
   long long out_plane;
   float keep, flare;
@@ -60,9 +62,11 @@ __host__ __device__ constexpr size_t tc_smem_bytes(int kboxes) {
   return 1024 + 2 * static_cast<size_t>(kboxes) * kABox + kTcStages * 2 * static_cast<size_t>(kBBox) + 256;
 }
 
-// MODE 0: sum over G steps of |E|^2 with (re, im) in adjacent accumulator
-// rows; out(y, x) = keep * sum + flare * mean[problem].  MODE 1: G = 1, out
-// = accumulator.  grid: (b_rows / BN, a_rows / 128, problems).
+// MODE 0: sum over G steps (kernels) of |E|^2 with (re, im) in adjacent
+// accumulator rows; out(y, x) = keep * sum + flare * mean[problem];
+// grid: (x tiles, a_rows / 128, problems).  MODE 1: step g is x tile g of the
+// same rows (the A tile stays resident), out(y, g * BN + j) = accumulator;
+// grid: (1, a_rows / 128, problems).
 template <int MODE>
 __global__ void __launch_bounds__(192, 1)
     tc_dft_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcGemmParams p) {
@@ -130,9 +134,9 @@ __global__ void __launch_bounds__(192, 1)
             break;
           }
           mbar_arrive_expect_tx(&full[s], 2u * kBBox);
-          const int row = ((prob * p.G + g) * 2) * p.b_rows + n_tile * kTcBN;
+          const int row = prob * p.b_prob + g * p.b_step + n_tile * kTcBN;
           tma_load_2d(sB + (s * 2 + 0) * kBBox, &tmB, kb * 64, row, &full[s]);
-          tma_load_2d(sB + (s * 2 + 1) * kBBox, &tmB, kb * 64, row + p.b_rows, &full[s]);
+          tma_load_2d(sB + (s * 2 + 1) * kBBox, &tmB, kb * 64, row + p.b_plane, &full[s]);
         }
       }
       // Drain: every load issued must have landed before the CTA may exit.
@@ -221,7 +225,7 @@ __global__ void __launch_bounds__(192, 1)
           }
         } else {
           const int y = m_tile * 128 + row;
-          float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + n_tile * kTcBN + c0;
+          float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + g * kTcBN + c0;
 #pragma unroll
           for (int i = 0; i < 32; i += 4)
             *reinterpret_cast<float4*>(o + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
@@ -467,7 +471,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const size_t per_x2 = align256(sizeof(float2) * M * B2);
   const size_t per_c = align256(sizeof(float2) * B2 * B2);
   const size_t per_bi = align256(static_cast<size_t>(2) * n * kpI * 2);
-  const size_t per_clip = per_x + per_m + per_be + per_i + per_x2 + per_c + per_bi + 256;
+  const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
+  const size_t per_clip = per_x + per_m + per_be + per_i + per_x2 + per_c + per_bi + per_mean;
   const size_t budget = size_t(1) << 30;
   int chunk = static_cast<int>(std::max<size_t>(1, budget / per_clip));
   chunk = std::min(chunk, b.n_clips);
@@ -485,7 +490,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   float2* X2 = reinterpret_cast<float2*>(take(per_x2));
   float2* C = reinterpret_cast<float2*>(take(per_c));
   __nv_bfloat16* BI = reinterpret_cast<__nv_bfloat16*>(take(per_bi));
-  float* mean = reinterpret_cast<float*>(take(256));
+  float* mean = reinterpret_cast<float*>(take(per_mean));
   const float2* twn = twiddle(lgn);
   const float2* twm = twiddle(lgm);
   const size_t smem_tc = tc_smem_bytes(3);
@@ -513,7 +518,9 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.ksteps = kstE;
       p.G = K;
       p.a_rows = 2 * M;
-      p.b_rows = M;
+      p.b_prob = K * 2 * M;
+      p.b_step = 2 * M;
+      p.b_plane = M;
       p.out_ld = M;
       p.out_plane = static_cast<long long>(M) * M;
       p.keep = ds.keep;
@@ -541,9 +548,11 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       TcGemmParams p{};
       p.kboxes = kpI / 64;
       p.ksteps = kstI;
-      p.G = 1;
+      p.G = n / kTcBN;
       p.a_rows = n;
-      p.b_rows = n;
+      p.b_prob = 2 * n;
+      p.b_step = kTcBN;
+      p.b_plane = n;
       p.out_ld = n;
       p.out_plane = static_cast<long long>(n) * n;
       p.keep = 1.f;
@@ -551,7 +560,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.mean = nullptr;
       p.out = o;
       p.err = dev_err;
-      dim3 g(n / kTcBN, n / 128, nc);
+      dim3 g(1, n / 128, nc);
       tc_dft_gemm<1><<<g, 192, smem_tc, st>>>(tc.map_ai, mbI, p);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
     }

@@ -284,7 +284,8 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
   const size_t per_x2 = coarse ? align256(sizeof(float2) * M * B2) : 0;
   const size_t per_c = coarse ? align256(sizeof(float2) * B2 * B2) : 0;
   const size_t per_t2 = coarse ? align256(sizeof(float2) * static_cast<size_t>(B2) * n) : 0;
-  const size_t per_clip = per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2 + 256;
+  const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
+  const size_t per_clip = per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2 + per_mean;
   const size_t budget = size_t(1) << 30;
   int chunk = static_cast<int>(std::max<size_t>(1, budget / per_clip));
   chunk = std::min(chunk, b.n_clips);
