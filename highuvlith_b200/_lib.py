@@ -60,6 +60,17 @@ class Diagnostics(C.Structure):
                 ("num_source_points", C.c_int32)]
 
 
+class IltParams(C.Structure):
+    _fields_ = [("cost_kind", C.c_int32), ("threshold", C.c_double), ("steepness", C.c_double),
+                ("beta", C.c_double), ("tv_weight", C.c_double), ("tv_epsilon", C.c_double),
+                ("binarization_weight", C.c_double), ("dose", C.c_double), ("weight", C.c_double),
+                ("absorber", C.c_double), ("defocus_nm", C.c_double)]
+
+
+class IltOpt(C.Structure):
+    _fields_ = [("max_iterations", C.c_int32), ("learning_rate", C.c_double), ("convergence_tol", C.c_double)]
+
+
 class Batch(C.Structure):
     _fields_ = [("n_clips", C.c_int32), ("input_kind", C.c_int32), ("input", C.c_void_p),
                 ("pixel_transfer", C.c_int32), ("defocus_nm", C.c_double), ("form", C.c_int32),
@@ -85,6 +96,10 @@ SIGNATURES = {
     "huv_rasterize_rects": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                       C.c_void_p, C.c_void_p]),
     "huv_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "huv_ilt_cost_grad": (C.c_int, [C.c_void_p, C.POINTER(IltParams), C.c_int32, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]),
+    "huv_ilt_optimize": (C.c_int, [C.c_void_p, C.POINTER(IltParams), C.POINTER(IltOpt), C.c_int32, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "huv_image_batch_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),
     "huv_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
     "huv_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32),

@@ -2,6 +2,7 @@
 // exceptions, records the message for huv_last_error() and returns a status.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -41,6 +42,20 @@ void check_cuda_sync(Engine* e, cudaStream_t st) {
   huv::check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   if (e->read_device_error() != 0)
     throw Error(HUV_ERR_DEVICE_TIMEOUT, "a bounded device-side wait gave up; results of the last calls are not valid");
+}
+
+void check_ilt_params(const huv_ilt_params& p) {
+  auto pos = [](double v) { return std::isfinite(v) && v > 0; };
+  if (p.cost_kind != 0 && p.cost_kind != 1) throw Error(HUV_ERR_INVALID_PARAMETER, "cost_kind: 0 or 1");
+  if (!pos(p.beta)) throw Error(HUV_ERR_INVALID_PARAMETER, "sigmoid_steepness: must be positive and finite");
+  if (!pos(p.tv_epsilon)) throw Error(HUV_ERR_INVALID_PARAMETER, "tv_epsilon: must be positive and finite");
+  if (!(p.tv_weight >= 0) || !(p.binarization_weight >= 0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "regularization weights: must be non-negative");
+  if (p.cost_kind == 1 && (!pos(p.threshold) || !pos(p.steepness)))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "threshold/steepness: must be positive and finite");
+  if (!pos(p.dose) || !(p.weight >= 0) || !std::isfinite(p.defocus_nm))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "condition: dose > 0, weight >= 0, finite defocus");
+  if (!(p.absorber >= 0 && p.absorber < 1)) throw Error(HUV_ERR_INVALID_PARAMETER, "absorber: real, in [0, 1)");
 }
 
 Engine* as_engine(void* e) {
@@ -157,6 +172,42 @@ huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out
     Engine* e = as_engine(engine);
     if (!batch) throw Error(HUV_ERR_INVALID_PARAMETER, "batch: null");
     e->image_batch_host(*batch, out_host, static_cast<cudaStream_t>(stream));
+  });
+}
+
+huv_status huv_ilt_cost_grad(void* engine, const huv_ilt_params* params, int32_t n_masks, const float* theta,
+                             const float* target, double* cost_host, float* grad, void* stream) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!params || !theta || !target || !cost_host) throw Error(HUV_ERR_INVALID_PARAMETER, "ilt: null argument");
+    check_ilt_params(*params);
+    if (n_masks <= 0) return;
+    std::lock_guard<std::mutex> lock(e->mu);
+    e->ensure_device();
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* d = nullptr;
+    huv::check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(double) * n_masks, st), "cudaMallocAsync");
+    e->ilt_eval(*params, n_masks, theta, target, grad, d, st);
+    huv::check_cuda(cudaMemcpyAsync(cost_host, d, sizeof(double) * n_masks, cudaMemcpyDeviceToHost, st), "D2H cost");
+    huv::check_cuda(cudaFreeAsync(d, st), "cudaFreeAsync");
+    huv::check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  });
+}
+
+huv_status huv_ilt_optimize(void* engine, const huv_ilt_params* params, const huv_ilt_opt* opt, int32_t n_masks,
+                            float* theta, const float* target, double* final_cost, int32_t* iterations,
+                            double* history, void* stream) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!params || !opt || !theta || !target) throw Error(HUV_ERR_INVALID_PARAMETER, "ilt: null argument");
+    check_ilt_params(*params);
+    if (opt->max_iterations < 0 || !(opt->learning_rate > 0) || !(opt->convergence_tol >= 0))
+      throw Error(HUV_ERR_INVALID_PARAMETER, "ilt optimizer: max_iterations >= 0, learning_rate > 0, tol >= 0");
+    if (n_masks <= 0) return;
+    std::lock_guard<std::mutex> lock(e->mu);
+    e->ensure_device();
+    e->ilt_optimize(*params, *opt, n_masks, theta, target, final_cost, iterations, history,
+                    static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -1,0 +1,662 @@
+// Pixel ILT on the device: batched cost, exact SOCS adjoint gradient and the
+// CG (Polak-Ribiere+) / Armijo optimizer, for many masks at once.
+//
+// Follows crates/highuvlith-core/src/ilt.rs: m = sigmoid(beta theta)
+// (538-542), t = a + (1 - a) m and M = FFT(t) (544-550), the resist-contour or
+// image-fidelity data term (564-603), TV + binarisation regularisers
+// (606-645), the adjoint of cost_and_gradient_with (667-738) and run_stage
+// (755-866).  The forward fields are band-limited (kernels live on |m| <= h),
+// so the adjoint needs only the band of FFT(G0 . E_k):
+//     Q = sum_k conj(kappa_k) . band(FFT(G0 . E_k)),   dC/dm = 2 (1 - a) Re IFFT(Q)
+// with E_k = IFFT(kappa_k . M) on the full grid and kappa_k the pre-scaled band
+// kernels (sqrt(lambda_k) / N^2 folded in), G0 = (1 - phi) dC/dI + phi mean(dC/dI).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "../engine.hpp"
+#include "fft_block.cuh"
+
+namespace huv_dev {
+
+// ------------------------------------------------------------ elementwise
+// t = a + (1 - a) sigmoid(beta theta) (the transmittance fed to the band FFT).
+__global__ void ilt_transmittance(const float* __restrict__ theta, size_t n, float beta, float absorber,
+                                  float* __restrict__ t) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float m = 1.f / (1.f + __expf(-beta * theta[i]));
+    t[i] = absorber + (1.f - absorber) * m;
+  }
+}
+
+__device__ __forceinline__ double block_sum_double(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+// Data term on the image: cost parts sum r^2 and the image adjoint G = dC/dI.
+// grid: (blocks_per_mask, masks); parts: [mask][block][2] = (sum r^2, sum G).
+__global__ void ilt_data(const float* __restrict__ img, const float* __restrict__ target, size_t npix,
+                         int kind, float thr, float steep, float dose, float* __restrict__ G,
+                         double* __restrict__ parts) {
+  __shared__ double red[32];
+  const int mask = blockIdx.y;
+  const float* im = img + mask * npix;
+  const float* tg = target + mask * npix;
+  float* g = G + mask * npix;
+  const float inv_n = 1.f / static_cast<float>(npix);
+  double sr = 0.0, sg = 0.0;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < npix;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float I = im[i];
+    float r, gv;
+    if (kind == 0) {
+      r = dose * I - tg[i];
+      gv = 2.f * r * dose * inv_n;
+    } else {
+      const float R = 1.f / (1.f + __expf(-steep * (dose * I - thr)));
+      r = R - tg[i];
+      gv = 2.f * r * steep * R * (1.f - R) * dose * inv_n;
+    }
+    g[i] = gv;
+    sr += static_cast<double>(r) * r;
+    sg += gv;
+  }
+  const double a = block_sum_double(sr, red);
+  const double b = block_sum_double(sg, red);
+  if (threadIdx.x == 0) {
+    double* p = parts + (static_cast<size_t>(mask) * gridDim.x + blockIdx.x) * 2;
+    p[0] = a;
+    p[1] = b;
+  }
+}
+
+// Sum parts[mask][i][c] over i in order (deterministic). out[mask * ncomp + c].
+__global__ void sum_parts(const double* __restrict__ parts, int nparts, int ncomp, int masks,
+                          double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= masks * ncomp) return;
+  const int mask = t / ncomp, c = t % ncomp;
+  double s = 0.0;
+  for (int i = 0; i < nparts; ++i) s += parts[(static_cast<size_t>(mask) * nparts + i) * ncomp + c];
+  out[t] = s;
+}
+
+// Adjoint column pass.  CTA per (mask, strip of Wc columns): for every kernel
+// k the column field E_k(., x) = IFFT_y of the band rows T_k(my, x), times
+// G0(., x) = keep * G + add[mask], forward FFT_y, band rows [-hb, hb] kept:
+// V[mask][k][my'][x].  grid: (L / Wc, masks).
+__global__ void ilt_cols_adj(const float2* __restrict__ T, const float* __restrict__ G, int K, int hb, int lg,
+                             int Wc, float keep, const double* __restrict__ sums, float flare_over_n,
+                             float2* __restrict__ V, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  const int L = 1 << lg;
+  const int B = 2 * hb + 1;
+  const int mask = blockIdx.y;
+  const int x0 = blockIdx.x * Wc;
+  float2* a = smem;
+  float2* b = smem + (Wc << lg);
+  float* g0 = reinterpret_cast<float*>(smem + 2 * (Wc << lg));  // [Wc][L]
+  const float add = sums ? flare_over_n * static_cast<float>(sums[mask * 2 + 1]) : 0.f;
+  const float* Gm = G + static_cast<size_t>(mask) * L * L;
+  for (int t = threadIdx.x; t < (Wc << lg); t += blockDim.x) {
+    const int y = t / Wc, w = t - y * Wc;
+    g0[(w << lg) + y] = keep * Gm[static_cast<size_t>(y) * L + x0 + w] + add;
+  }
+  const float2* Tm = T + static_cast<size_t>(mask) * K * B * L;
+  float2* Vm = V + static_cast<size_t>(mask) * K * B * L;
+  for (int k = 0; k < K; ++k) {
+    for (int t = threadIdx.x; t < (Wc << lg); t += blockDim.x) a[t] = make_float2(0.f, 0.f);
+    __syncthreads();
+    for (int t = threadIdx.x; t < B * Wc; t += blockDim.x) {
+      const int my = t / Wc, w = t - my * Wc;
+      a[(w << lg) + ((my - hb) & (L - 1))] = Tm[((static_cast<size_t>(k) * B + my) << lg) + x0 + w];
+    }
+    __syncthreads();
+    float2* r = block_fft<+1>(a, b, lg, Wc, tw);
+    float2* o = (r == a) ? b : a;
+    for (int t = threadIdx.x; t < (Wc << lg); t += blockDim.x) {
+      const float s = g0[t];
+      r[t] = make_float2(r[t].x * s, r[t].y * s);
+    }
+    __syncthreads();
+    const float2* f = block_fft<-1>(r, o, lg, Wc, tw);
+    for (int t = threadIdx.x; t < B * Wc; t += blockDim.x) {
+      const int my = t / Wc, w = t - my * Wc;
+      Vm[((static_cast<size_t>(k) * B + my) << lg) + x0 + w] = f[(w << lg) + ((my - hb) & (L - 1))];
+    }
+    __syncthreads();
+  }
+}
+
+// Adjoint row pass.  CTA per (mask, band row my'): forward FFT_x of every
+// kernel's V row, band columns kept, Q(my', mx') = sum_k conj(kappa_k) . value.
+// grid: (B, masks).
+__global__ void ilt_rows_adj(const float2* __restrict__ V, const float2* __restrict__ kband, int K, int hb, int lg,
+                             int S, float2* __restrict__ Q, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  const int L = 1 << lg;
+  const int B = 2 * hb + 1;
+  const int mask = blockIdx.y, my = blockIdx.x;
+  float2* a = smem;
+  float2* b = smem + (S << lg);
+  float2 acc = make_float2(0.f, 0.f);
+  const float2* Vm = V + static_cast<size_t>(mask) * K * B * L;
+  for (int k0 = 0; k0 < K; k0 += S) {
+    const int ns = min(S, K - k0);
+    for (int t = threadIdx.x; t < (S << lg); t += blockDim.x) {
+      const int s = t >> lg, x = t & (L - 1);
+      a[t] = s < ns ? Vm[((static_cast<size_t>(k0 + s) * B + my) << lg) + x] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2* r = block_fft<-1>(a, b, lg, S, tw);
+    if (threadIdx.x < B) {
+      const int mx = threadIdx.x;
+      for (int s = 0; s < ns; ++s) {
+        const float2 v = r[(s << lg) + ((mx - hb) & (L - 1))];
+        const float2 u = kband[(static_cast<size_t>(k0 + s) * B + my) * B + mx];
+        // conj(u) * v
+        acc.x += u.x * v.x + u.y * v.y;
+        acc.y += u.x * v.y - u.y * v.x;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < B) Q[(static_cast<size_t>(mask) * B + my) * B + threadIdx.x] = acc;
+}
+
+// Regularisers and the chain rule: grad = (dC/dm + reg) * beta m (1 - m), with
+// m = sigmoid(beta theta) recomputed; TV on forward differences (periodic).
+// parts: [mask][block] reg cost.  dcdm may be NULL (cost only).
+__global__ void ilt_finish(const float* __restrict__ theta, const float* __restrict__ dcdm, int n, float beta,
+                           float tv_w, float tv_eps, float bin_w, float* __restrict__ grad,
+                           double* __restrict__ parts) {
+  __shared__ double red[32];
+  const int mask = blockIdx.y;
+  const size_t npix = static_cast<size_t>(n) * n;
+  const float* th = theta + mask * npix;
+  const float inv_n = 1.f / static_cast<float>(npix);
+  auto M = [&](int i, int j) {
+    i = (i + n) % n;
+    j = (j + n) % n;
+    return 1.f / (1.f + __expf(-beta * th[static_cast<size_t>(i) * n + j]));
+  };
+  double cost = 0.0;
+  for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < npix;
+       p += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(p / n), j = static_cast<int>(p % n);
+    const float m = M(i, j);
+    float g = 0.f;
+    if (tv_w > 0.f) {
+      const float gx = M(i, j + 1) - m, gy = M(i + 1, j) - m;
+      const float s = sqrtf(gx * gx + gy * gy + tv_eps * tv_eps);
+      cost += static_cast<double>(tv_w) * (s - tv_eps) * inv_n;
+      if (grad) {
+        const float ml = M(i, j - 1), mu = M(i - 1, j);
+        const float gxl = m - ml, gyl = M(i + 1, j - 1) - ml;
+        const float sl = sqrtf(gxl * gxl + gyl * gyl + tv_eps * tv_eps);
+        const float gxu = M(i - 1, j + 1) - mu, gyu = m - mu;
+        const float su = sqrtf(gxu * gxu + gyu * gyu + tv_eps * tv_eps);
+        g += tv_w * inv_n * (-(gx + gy) / s + gxl / sl + gyu / su);
+      }
+    }
+    if (bin_w > 0.f) {
+      cost += static_cast<double>(bin_w) * 4.0 * m * (1.0 - m) * inv_n;
+      g += bin_w * 4.f * (1.f - 2.f * m) * inv_n;
+    }
+    if (grad) grad[mask * npix + p] = ((dcdm ? dcdm[mask * npix + p] : 0.f) + g) * beta * m * (1.f - m);
+  }
+  const double c = block_sum_double(cost, red);
+  if (threadIdx.x == 0) parts[static_cast<size_t>(mask) * gridDim.x + blockIdx.x] = c;
+}
+
+// ------------------------------------------------------------ optimizer algebra
+// Per-mask reductions over n elements: out[mask] = sum a*b (dot) or max |a|.
+__global__ void batched_dot(const float* __restrict__ a, const float* __restrict__ b, size_t n,
+                            double* __restrict__ parts) {
+  __shared__ double red[32];
+  const int mask = blockIdx.y;
+  double s = 0.0;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    s += static_cast<double>(a[mask * n + i]) * b[mask * n + i];
+  const double t = block_sum_double(s, red);
+  if (threadIdx.x == 0) parts[static_cast<size_t>(mask) * gridDim.x + blockIdx.x] = t;
+}
+
+__global__ void batched_maxabs(const float* __restrict__ a, size_t n, double* __restrict__ parts) {
+  __shared__ double red[32];
+  const int mask = blockIdx.y;
+  float m = 0.f;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    m = fmaxf(m, fabsf(a[mask * n + i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) r = fmax(r, red[w]);
+    parts[static_cast<size_t>(mask) * gridDim.x + blockIdx.x] = r;
+  }
+}
+
+__global__ void max_parts(const double* __restrict__ parts, int nparts, int masks, double* __restrict__ out) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= masks) return;
+  double r = 0.0;
+  for (int i = 0; i < nparts; ++i) r = fmax(r, parts[static_cast<size_t>(m) * nparts + i]);
+  out[m] = r;
+}
+
+// y[mask] = alpha[mask] * x[mask] + gamma[mask] * y[mask]   (per-mask scalars)
+__global__ void batched_axpby(const float* __restrict__ x, float* __restrict__ y, size_t n,
+                              const float* __restrict__ alpha, const float* __restrict__ gamma,
+                              float* __restrict__ out) {
+  const int mask = blockIdx.y;
+  const float al = alpha[mask], ga = gamma[mask];
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    out[mask * n + i] = al * x[mask * n + i] + ga * y[mask * n + i];
+}
+
+// cost[c] = weight * data[2c] + reg[c]
+__global__ void ilt_combine(const double* __restrict__ data, const double* __restrict__ reg, int masks, double w,
+                            double* __restrict__ cost) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < masks) cost[c] = w * data[2 * c] + reg[c];
+}
+
+// out[j] = alpha[j] * x[idx[j]] + gamma[j] * y[idx[j]]   (blocks of n floats)
+__global__ void gather_axpby(const int* __restrict__ idx, const float* __restrict__ alpha,
+                             const float* __restrict__ gamma, const float* __restrict__ x,
+                             const float* __restrict__ y, size_t n, float* __restrict__ out) {
+  const int j = blockIdx.y;
+  const size_t m = static_cast<size_t>(idx[j]);
+  const float al = alpha[j], ga = gamma[j];
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float xv = x ? x[m * n + i] : 0.f;
+    const float yv = y ? y[m * n + i] : 0.f;
+    out[j * n + i] = al * xv + ga * yv;
+  }
+}
+
+// dst[idx[j]] = src[j]   (blocks of n floats)
+__global__ void scatter_blocks(const int* __restrict__ idx, const float* __restrict__ src, size_t n,
+                               float* __restrict__ dst) {
+  const int j = blockIdx.y;
+  const size_t m = static_cast<size_t>(idx[j]);
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    dst[m * n + i] = src[j * n + i];
+}
+
+}  // namespace huv_dev
+
+// ================================================================== host
+namespace huv_launch {
+cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
+                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st);
+cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                      float2* T, const float2* tw, cudaStream_t st);
+cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+                      const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
+
+cudaError_t ilt_set_smem() {
+  const int big = 200 * 1024;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_rows_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  return cudaSuccess;
+}
+}  // namespace huv_launch
+
+namespace huv {
+
+namespace {
+size_t a256(size_t v) { return (v + 255) & ~size_t(255); }
+int ilog2i(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+constexpr int kRedBlocks = 64;  // blocks per mask for reductions
+}  // namespace
+
+// Cost (and gradient when grad != nullptr) for `masks` masks on the device.
+// cost_dev: masks doubles on the device.
+void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, const float* target, float* grad,
+                      double* cost_dev, cudaStream_t st) {
+  using namespace huv_dev;
+  using namespace huv_launch;
+  static bool smem_set = false;
+  if (!smem_set) {
+    check_cuda(ilt_set_smem(), "cudaFuncSetAttribute(ilt)");
+    smem_set = true;
+  }
+  DeviceSet& ds = device_set(p.defocus_nm == 0.0 ? 0.0 : p.defocus_nm);
+  const int K = ds.K, hb = ds.hb, B = ds.B;
+  const int lg = ilog2i(n);
+  const size_t npix = static_cast<size_t>(n) * n;
+  const float2* tw = twiddle(lg);
+  const float flare = ds.flare, keep = ds.keep;
+  // Per-mask workspace.
+  const size_t s_t = a256(sizeof(float) * npix);           // transmittance, then dC/dm
+  const size_t s_x = a256(sizeof(float2) * n * B);
+  const size_t s_m = a256(sizeof(float2) * B * B);
+  const size_t s_mean = a256(sizeof(float) * (1 + (B + 3) / 4));
+  const size_t s_T = a256(sizeof(float2) * static_cast<size_t>(K) * B * n);
+  const size_t s_img = a256(sizeof(float) * npix);         // image, then G
+  const size_t s_V = grad ? a256(sizeof(float2) * static_cast<size_t>(K) * B * n) : 0;
+  const size_t s_q = grad ? a256(sizeof(float2) * B * B) : 0;
+  const size_t s_t2 = grad ? a256(sizeof(float2) * static_cast<size_t>(B) * n) : 0;
+  const size_t s_parts = a256(sizeof(double) * kRedBlocks * 2);
+  const size_t per = s_t + s_x + s_m + s_mean + s_T + s_img + s_V + s_q + s_t2 + 3 * s_parts + a256(sizeof(double) * 4);
+  const size_t budget = size_t(2) << 30;
+  int chunk = static_cast<int>(std::max<size_t>(1, budget / per));
+  chunk = std::min(chunk, masks);
+  char* base = static_cast<char*>(workspace(per * chunk + 4096));
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* q = base + off;
+    off += bytes * chunk;
+    return q;
+  };
+  float* tbuf = reinterpret_cast<float*>(take(s_t));
+  float2* X = reinterpret_cast<float2*>(take(s_x));
+  float2* Mb = reinterpret_cast<float2*>(take(s_m));
+  float* mean = reinterpret_cast<float*>(take(s_mean));
+  float2* T = reinterpret_cast<float2*>(take(s_T));
+  float* img = reinterpret_cast<float*>(take(s_img));
+  float2* V = reinterpret_cast<float2*>(take(s_V));
+  float2* Q = reinterpret_cast<float2*>(take(s_q));
+  float2* T2 = reinterpret_cast<float2*>(take(s_t2));
+  double* pdata = reinterpret_cast<double*>(take(s_parts));
+  double* preg = reinterpret_cast<double*>(take(s_parts));
+  double* sums = reinterpret_cast<double*>(take(s_parts));
+  double* regsum = reinterpret_cast<double*>(take(a256(sizeof(double) * 4)));
+  const int lgn = lg;
+  const dim3 red_grid(kRedBlocks, 1);
+  for (int c0 = 0; c0 < masks; c0 += chunk) {
+    const int nc = std::min(chunk, masks - c0);
+    const float* th = theta + npix * c0;
+    const float* tg = target + npix * c0;
+    ilt_transmittance<<<1184, 256, 0, st>>>(th, npix * nc, static_cast<float>(p.beta),
+                                            static_cast<float>(p.absorber), tbuf);
+    check_cuda(band_forward(tbuf, HUV_INPUT_RASTER_F32, n, lgn, hb, nc, X, Mb, nullptr, ds.W, mean, tw, st),
+               "ilt band_forward");
+    check_cuda(socs_rows(ds.kband, 0.f, Mb, K, hb, lgn, nc, T, tw, st), "ilt socs_rows");
+    check_cuda(socs_cols(T, K, hb, lgn, nc, keep, flare, mean, img, 0, tw, st), "ilt socs_cols");
+    ilt_data<<<dim3(kRedBlocks, nc), 256, 0, st>>>(img, tg, npix, p.cost_kind, static_cast<float>(p.threshold),
+                                                   static_cast<float>(p.steepness), static_cast<float>(p.dose),
+                                                   img, pdata);
+    sum_parts<<<(nc * 2 + 127) / 128, 128, 0, st>>>(pdata, kRedBlocks, 2, nc, sums);
+    float* dcdm = nullptr;
+    if (grad) {
+      const int Wc = lgn >= 11 ? 4 : 8;
+      const size_t sm = 2 * (static_cast<size_t>(Wc) << lgn) * sizeof(float2) + (static_cast<size_t>(Wc) << lgn) * sizeof(float);
+      ilt_cols_adj<<<dim3(n / Wc, nc), 256, sm, st>>>(T, img, K, hb, lgn, Wc, keep, sums,
+                                                      flare / static_cast<float>(npix), V, tw);
+      const int S = lgn >= 11 ? 2 : 4;
+      const size_t sm2 = 2 * (static_cast<size_t>(S) << lgn) * sizeof(float2);
+      ilt_rows_adj<<<dim3(B, nc), 256, sm2, st>>>(V, ds.kband, K, hb, lgn, S, Q, tw);
+      const float scale = static_cast<float>(2.0 * (1.0 - p.absorber) * p.weight);
+      check_cuda(socs_rows(nullptr, scale, Q, 1, hb, lgn, nc, T2, tw, st), "ilt grad rows");
+      dcdm = tbuf;  // the transmittance is no longer needed
+      check_cuda(socs_cols(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, tw, st), "ilt grad cols");
+    }
+    ilt_finish<<<dim3(kRedBlocks, nc), 256, 0, st>>>(th, dcdm, n, static_cast<float>(p.beta),
+                                                     static_cast<float>(p.tv_weight), static_cast<float>(p.tv_epsilon),
+                                                     static_cast<float>(p.binarization_weight),
+                                                     grad ? grad + npix * c0 : nullptr, preg);
+    sum_parts<<<(nc + 127) / 128, 128, 0, st>>>(preg, kRedBlocks, 1, nc, regsum);
+    ilt_combine<<<(nc + 127) / 128, 128, 0, st>>>(sums, regsum, nc, p.weight, cost_dev + c0);
+    check_cuda(cudaGetLastError(), "ilt kernels");
+    prof.launches += grad ? 16 : 10;
+  }
+}
+
+}  // namespace huv
+
+// ------------------------------------------------------------ optimizer
+namespace huv {
+
+namespace {
+
+struct DevVec {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t b) {
+    if (b <= bytes) return;
+    cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    check_cuda(cudaMalloc(&p, b), "cudaMalloc(ilt state)");
+    bytes = b;
+  }
+  ~DevVec() { cudaFree(p); }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+}  // namespace
+
+void Engine::ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int masks, float* theta, const float* target,
+                          double* final_cost, int* iterations, double* history, cudaStream_t st) {
+  using namespace huv_dev;
+  const size_t npix = static_cast<size_t>(n) * n;
+  const size_t blk = sizeof(float) * npix;
+  DevVec grad, dir, gnew, trial, tgt, gold, cost_d, parts, dots, alpha, gamma, idx;
+  grad.ensure(blk * masks);
+  dir.ensure(blk * masks);
+  gnew.ensure(blk * masks);
+  trial.ensure(blk * masks);
+  tgt.ensure(blk * masks);
+  gold.ensure(blk * masks);
+  cost_d.ensure(sizeof(double) * masks);
+  parts.ensure(sizeof(double) * masks * kRedBlocks);
+  dots.ensure(sizeof(double) * masks);
+  alpha.ensure(sizeof(float) * masks);
+  gamma.ensure(sizeof(float) * masks);
+  idx.ensure(sizeof(int) * masks);
+  const int max_it = o.max_iterations;
+  const double lr = o.learning_rate, tol = o.convergence_tol;
+  const int threads = 256;
+
+  auto upload = [&](DevVec& v, const void* h, size_t b) {
+    check_cuda(cudaMemcpyAsync(v.p, h, b, cudaMemcpyHostToDevice, st), "upload ilt scalars");
+  };
+  auto fetch = [&](const DevVec& v, void* h, size_t b) {
+    check_cuda(cudaMemcpyAsync(h, v.p, b, cudaMemcpyDeviceToHost, st), "fetch ilt scalars");
+    check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize(ilt)");
+  };
+  // per-mask dot products of compact blocks a[j], b[j], j < count
+  auto dot = [&](const float* a, const float* b, int count) {
+    batched_dot<<<dim3(kRedBlocks, count), threads, 0, st>>>(a, b, npix, parts.as<double>());
+    sum_parts<<<(count + 127) / 128, 128, 0, st>>>(parts.as<double>(), kRedBlocks, 1, count, dots.as<double>());
+    std::vector<double> h(count);
+    fetch(dots, h.data(), sizeof(double) * count);
+    prof.launches += 2;
+    return h;
+  };
+  auto maxabs = [&](const float* a, int count) {
+    batched_maxabs<<<dim3(kRedBlocks, count), threads, 0, st>>>(a, npix, parts.as<double>());
+    max_parts<<<(count + 127) / 128, 128, 0, st>>>(parts.as<double>(), kRedBlocks, count, dots.as<double>());
+    std::vector<double> h(count);
+    fetch(dots, h.data(), sizeof(double) * count);
+    prof.launches += 2;
+    return h;
+  };
+  // out[j] = al[j] x[ix[j]] + ga[j] y[ix[j]]
+  auto gaxpby = [&](const std::vector<int>& ix, const std::vector<float>& al, const std::vector<float>& ga,
+                    const float* x, const float* y, float* out) {
+    const int c = static_cast<int>(ix.size());
+    if (!c) return;
+    upload(idx, ix.data(), sizeof(int) * c);
+    upload(alpha, al.data(), sizeof(float) * c);
+    upload(gamma, ga.data(), sizeof(float) * c);
+    gather_axpby<<<dim3(256, c), threads, 0, st>>>(idx.as<int>(), alpha.as<float>(), gamma.as<float>(), x, y, npix,
+                                                   out);
+    prof.launches += 1;
+  };
+  auto scatter = [&](const std::vector<int>& ix, const float* src, float* dst) {
+    const int c = static_cast<int>(ix.size());
+    if (!c) return;
+    upload(idx, ix.data(), sizeof(int) * c);
+    scatter_blocks<<<dim3(256, c), threads, 0, st>>>(idx.as<int>(), src, npix, dst);
+    prof.launches += 1;
+  };
+  auto eval = [&](const float* th, const float* tg, int count, float* g) {
+    ilt_eval(p, count, th, tg, g, cost_d.as<double>(), st);
+    std::vector<double> h(count);
+    fetch(cost_d, h.data(), sizeof(double) * count);
+    return h;
+  };
+  auto ones = [](size_t c, float v) { return std::vector<float>(c, v); };
+
+  std::vector<int> all(masks);
+  for (int m = 0; m < masks; ++m) all[m] = m;
+  std::vector<double> cost = eval(theta, target, masks, grad.as<float>());
+  std::vector<std::vector<double>> hist(masks);
+  for (int m = 0; m < masks; ++m) hist[m].push_back(cost[m]);
+  gaxpby(all, ones(masks, -1.f), ones(masks, 0.f), grad.as<float>(), nullptr, dir.as<float>());
+  std::vector<double> step(masks, lr);
+  std::vector<int> small(masks, 0), its(masks, 0);
+  std::vector<char> done(masks, 0);
+  for (int it = 0; it < max_it; ++it) {
+    std::vector<int> act;
+    for (int m = 0; m < masks; ++m)
+      if (!done[m]) act.push_back(m);
+    if (act.empty()) break;
+    std::vector<double> acc_cost(masks, 0.0), acc_s(masks, 0.0);
+    std::vector<char> accepted(masks, 0);
+    std::vector<int> attempt_set = act;
+    for (int attempt = 0; attempt < 2 && !attempt_set.empty(); ++attempt) {
+      // direction data for the attempt set (gathered into `trial` compactly)
+      const int c = static_cast<int>(attempt_set.size());
+      gaxpby(attempt_set, ones(c, 1.f), ones(c, 0.f), dir.as<float>(), nullptr, trial.as<float>());
+      gaxpby(attempt_set, ones(c, 1.f), ones(c, 0.f), grad.as<float>(), nullptr, gold.as<float>());
+      const std::vector<double> dmax = maxabs(trial.as<float>(), c);
+      const std::vector<double> gd = dot(gold.as<float>(), trial.as<float>(), c);
+      std::vector<int> search, restart;
+      std::vector<double> slope(masks, 0.0), dm(masks, 0.0);
+      for (int j = 0; j < c; ++j) {
+        const int m = attempt_set[j];
+        if (dmax[j] == 0.0) continue;  // no direction: the mask stops
+        dm[m] = dmax[j];
+        slope[m] = gd[j] / dmax[j];
+        if (slope[m] >= 0.0)
+          restart.push_back(m);
+        else
+          search.push_back(m);
+      }
+      // Armijo backtracking for `search`.
+      std::vector<double> s(masks);
+      for (int m : search) s[m] = step[m];
+      std::vector<int> pending = search;
+      for (int bt = 0; bt < 25 && !pending.empty(); ++bt) {
+        const int pc = static_cast<int>(pending.size());
+        std::vector<float> al(pc), ga(pc, 1.f);
+        for (int j = 0; j < pc; ++j) al[j] = static_cast<float>(s[pending[j]] / dm[pending[j]]);
+        gaxpby(pending, al, ga, dir.as<float>(), theta, trial.as<float>());
+        gaxpby(pending, ones(pc, 1.f), ones(pc, 0.f), target, nullptr, tgt.as<float>());
+        const std::vector<double> ct = eval(trial.as<float>(), tgt.as<float>(), pc, nullptr);
+        std::vector<int> ok_j, ok_m, next;
+        for (int j = 0; j < pc; ++j) {
+          const int m = pending[j];
+          if (std::isfinite(ct[j]) && ct[j] <= cost[m] + 1e-4 * s[m] * slope[m]) {
+            accepted[m] = 1;
+            acc_cost[m] = ct[j];
+            acc_s[m] = s[m];
+            ok_j.push_back(j);
+            ok_m.push_back(m);
+          } else {
+            s[m] *= 0.5;
+            next.push_back(m);
+          }
+        }
+        // accepted trials become the new theta
+        if (!ok_j.empty()) {
+          std::vector<float> one(ok_j.size(), 1.f), zero(ok_j.size(), 0.f);
+          gaxpby(ok_j, one, zero, trial.as<float>(), nullptr, gnew.as<float>());
+          scatter(ok_m, gnew.as<float>(), theta);
+        }
+        pending = next;
+      }
+      // next attempt: restarts, and (first attempt only) failed searches, along -grad
+      std::vector<int> nxt = restart;
+      if (attempt == 0)
+        for (int m : search)
+          if (!accepted[m]) nxt.push_back(m);
+      if (!nxt.empty()) {
+        const int nc = static_cast<int>(nxt.size());
+        gaxpby(nxt, ones(nc, -1.f), ones(nc, 0.f), grad.as<float>(), nullptr, gnew.as<float>());
+        scatter(nxt, gnew.as<float>(), dir.as<float>());
+      }
+      attempt_set = attempt == 0 ? nxt : std::vector<int>();
+    }
+    std::vector<int> acc;
+    for (int m : act) {
+      if (accepted[m])
+        acc.push_back(m);
+      else
+        done[m] = 1;  // line search failed (or no direction)
+    }
+    if (acc.empty()) break;
+    // gradient at the accepted points (compact), then the CG direction
+    const int ac = static_cast<int>(acc.size());
+    gaxpby(acc, ones(ac, 1.f), ones(ac, 0.f), theta, nullptr, trial.as<float>());
+    gaxpby(acc, ones(ac, 1.f), ones(ac, 0.f), target, nullptr, tgt.as<float>());
+    const std::vector<double> cn = eval(trial.as<float>(), tgt.as<float>(), ac, gnew.as<float>());
+    gaxpby(acc, ones(ac, 1.f), ones(ac, 0.f), grad.as<float>(), nullptr, gold.as<float>());
+    const std::vector<double> gg = dot(gold.as<float>(), gold.as<float>(), ac);
+    const std::vector<double> nn = dot(gnew.as<float>(), gnew.as<float>(), ac);
+    const std::vector<double> ng = dot(gnew.as<float>(), gold.as<float>(), ac);
+    std::vector<float> al(ac, -1.f), be(ac);
+    for (int j = 0; j < ac; ++j) be[j] = static_cast<float>(gg[j] > 0 ? std::max((nn[j] - ng[j]) / gg[j], 0.0) : 0.0);
+    // dir = -gnew + beta * dir  (compact gnew with index j; dir with index m): do it in two steps
+    gaxpby(acc, ones(ac, 0.f), be, dir.as<float>(), dir.as<float>(), gold.as<float>());  // gold[j] = beta dir[m]
+    {
+      // gold[j] -= gnew[j]; with identity indices
+      std::vector<int> id(ac);
+      for (int j = 0; j < ac; ++j) id[j] = j;
+      gaxpby(id, ones(ac, -1.f), ones(ac, 1.f), gnew.as<float>(), gold.as<float>(), trial.as<float>());
+      scatter(acc, trial.as<float>(), dir.as<float>());
+      scatter(acc, gnew.as<float>(), grad.as<float>());
+    }
+    for (int j = 0; j < ac; ++j) {
+      const int m = acc[j];
+      const double prev = cost[m];
+      cost[m] = cn[j];
+      hist[m].push_back(cost[m]);
+      ++its[m];
+      step[m] = std::min(acc_s[m] * 1.5, 10.0 * lr);
+      const double rel = prev > 0 ? (prev - cost[m]) / prev : 0.0;
+      small[m] = rel < tol ? small[m] + 1 : 0;
+      if (small[m] >= 3 || cost[m] == 0.0) done[m] = 1;
+    }
+  }
+  for (int m = 0; m < masks; ++m) {
+    if (final_cost) final_cost[m] = cost[m];
+    if (iterations) iterations[m] = its[m];
+    if (history)
+      for (int i = 0; i <= max_it; ++i)
+        history[static_cast<size_t>(m) * (max_it + 1) + i] =
+            i < static_cast<int>(hist[m].size()) ? hist[m][i] : std::nan("");
+  }
+}
+
+}  // namespace huv

@@ -118,6 +118,11 @@ struct Engine {
   bool tc_supported(const DeviceSet& ds, int M) const;
   void run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st);
   void run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st);
+  // ILT (batched): cost and optional gradient; the optimizer.
+  void ilt_eval(const huv_ilt_params& p, int masks, const float* theta, const float* target, float* grad,
+                double* cost_dev, cudaStream_t st);
+  void ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int masks, float* theta, const float* target,
+                    double* final_cost, int* iterations, double* history, cudaStream_t st);
   // Device error flag written by bounded waits that gave up (0 = none).
   int read_device_error();
 

@@ -167,6 +167,46 @@ huv_status huv_image_batch(void* engine, const huv_batch* batch, float* out, voi
  * on `stream` and synchronises it (the reference-facing end-to-end call). */
 huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out_host, void* stream);
 
+/* Pixel ILT (crates/highuvlith-core/src/ilt.rs).  One process condition
+ * (focus, dose, weight); m = sigmoid(beta theta), t = a + (1 - a) m with a
+ * real absorber amplitude a (0 = binary). */
+typedef struct {
+  int32_t cost_kind;          /* 0 ImageFidelity, 1 ResistContour (ilt.rs:126-144) */
+  double threshold;           /* ResistContour print threshold */
+  double steepness;           /* ResistContour sigmoid steepness alpha */
+  double beta;                /* mask sigmoid steepness (ILTConfig::sigmoid_steepness, default 4) */
+  double tv_weight;           /* total-variation weight mu_TV (default 0.01) */
+  double tv_epsilon;          /* TV smoothing (default 0.01) */
+  double binarization_weight; /* mu_B (default 0) */
+  double dose;                /* ProcessCondition::dose */
+  double weight;              /* ProcessCondition::weight */
+  double absorber;            /* real absorber amplitude a in [0, 1) */
+  double defocus_nm;          /* ProcessCondition::defocus_nm */
+} huv_ilt_params;
+
+typedef struct {
+  int32_t max_iterations;  /* ILTConfig::max_iterations */
+  double learning_rate;    /* initial max |d theta| of a step (default 0.5) */
+  double convergence_tol;  /* relative decrease tolerance (default 1e-4) */
+} huv_ilt_opt;
+
+/* Cost and exact adjoint gradient dC/dtheta for n_masks masks at once
+ * (IltProblem::cost_and_gradient_with, ilt.rs:667-738).  theta, target, grad:
+ * device arrays of n_masks*N*N floats; cost_host: n_masks doubles (the call
+ * synchronises `stream`).  grad = NULL computes the cost only (IltProblem::cost,
+ * ilt.rs:648-659). */
+huv_status huv_ilt_cost_grad(void* engine, const huv_ilt_params* params, int32_t n_masks, const float* theta,
+                             const float* target, double* cost_host, float* grad, void* stream);
+
+/* optimize_ilt's stage loop (run_stage, ilt.rs:755-866) for n_masks masks
+ * concurrently: CG Polak-Ribiere+ with Armijo backtracking, per mask.  theta
+ * (device) is updated in place.  final_cost, iterations: n_masks each (host);
+ * history: n_masks*(max_iterations+1) doubles (host, NaN after termination)
+ * or NULL. */
+huv_status huv_ilt_optimize(void* engine, const huv_ilt_params* params, const huv_ilt_opt* opt, int32_t n_masks,
+                            float* theta, const float* target, double* final_cost, int32_t* iterations,
+                            double* history, void* stream);
+
 /* Allocation-free variant of huv_image_batch (no counterpart in the
  * reference, which has no device path).  For callers that cannot call
  * cudaMalloc: applications whose memory pool already owns the device, and

@@ -1,0 +1,92 @@
+"""ILT: oracle pinned to the reference's adjoint-vs-finite-difference KAT
+(CPU), then the device cost/gradient/optimizer against the FP64 oracle."""
+import numpy as np
+import pytest
+
+import highuvlith_b200 as HB
+from oracle import hopkins as H
+from oracle import ilt as OI
+
+
+def _problem(n=64, pixel=8.0, kmax=8, cost="resist", flare=0.02):
+    eng = H.Engine(H.fill_conventional(0.6), H.ProjectionOptics(0.75, flare_fraction=flare), H.Grid(n, pixel),
+                   157.63, max_kernels=kmax)
+    ks = eng.kernel_set()
+    d = ks.divisor()
+    target = OI.contact_array_target(n, pixel, 60.0, 128.0, 128.0, 2, 2)
+    cfg = OI.IltConfig(cost=cost, threshold=0.25, steepness=50.0, flare=flare, tv_weight=0.01, bin_weight=0.05)
+    return OI.IltProblem(ks.eigenvalues / d, ks.dense(), target, cfg), target
+
+
+@pytest.mark.parametrize("cost", ["resist", "image"])
+def test_oracle_adjoint_matches_finite_differences(cost):
+    """ilt.rs:1084-1148: exact adjoint vs central finite differences
+    (directional, relative error <= 1e-6)."""
+    prob, target = _problem(cost=cost)
+    rng = np.random.default_rng(3)
+    theta = target - 0.5 + 0.1 * rng.standard_normal(target.shape)
+    _, g = prob.cost_and_gradient(theta)
+    d = rng.standard_normal(theta.shape)
+    h = 1e-5
+    fd = (prob.cost(theta + h * d) - prob.cost(theta - h * d)) / (2 * h)
+    an = float(np.sum(g * d))
+    assert abs(fd - an) <= 1e-6 * max(abs(fd), abs(an)) + 1e-14
+
+
+def test_contact_target_area():
+    t = OI.contact_array_target(256, 1.0, 20.0, 40.0, 40.0, 3, 2)
+    assert abs(t.sum() - 6 * 20 * 20) < 1e-9
+
+
+# ----------------------------------------------------------------- device
+def _device_case(n=128, kmax=16):
+    grid = HB.GridConfig(n, 1.0)
+    eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(), grid=grid, max_kernels=kmax)
+    ev, ker = eng.kernels(0.0)
+    return eng, ev, ker
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cost", ["resist", "image"])
+def test_device_cost_and_gradient_match_oracle(cost):
+    import torch
+    from highuvlith_b200 import ilt
+    n = 128
+    eng, ev, ker = _device_case(n)
+    rng = np.random.default_rng(7)
+    targets = np.stack([OI.contact_array_target(n, 1.0, s, p, p, c, c)
+                        for s, p, c in ((18.0, 36.0, 2), (22.0, 44.0, 3))])
+    theta = (targets - 0.5 + 0.2 * rng.standard_normal(targets.shape)).astype(np.float32)
+    st = ilt.IltSettings(cost=cost, binarization_weight=0.02)
+    c_dev, g_dev = ilt.cost_and_gradient(eng, torch.from_numpy(theta).cuda(),
+                                         torch.from_numpy(targets.astype(np.float32)).cuda(), st)
+    g_dev = g_dev.cpu().numpy()
+    for i in range(2):
+        cfg = OI.IltConfig(cost=cost, threshold=0.25, steepness=50.0, flare=0.0, tv_weight=0.01,
+                           bin_weight=0.02)
+        prob = OI.IltProblem(ev, ker, targets[i], cfg)
+        c_ref, g_ref = prob.cost_and_gradient(theta[i].astype(np.float64))
+        assert abs(c_dev[i] - c_ref) <= 1e-4 * abs(c_ref), (c_dev[i], c_ref)
+        assert np.max(np.abs(g_dev[i] - g_ref)) <= 2e-3 * np.max(np.abs(g_ref)), \
+            np.max(np.abs(g_dev[i] - g_ref)) / np.max(np.abs(g_ref))
+
+
+@pytest.mark.gpu
+def test_device_optimizer_decreases_cost_monotonically():
+    import torch
+    from highuvlith_b200 import ilt
+    n = 128
+    eng, _, _ = _device_case(n)
+    targets = np.stack([OI.contact_array_target(n, 1.0, s, p, p, c, c)
+                        for s, p, c in ((18.0, 36.0, 2), (20.0, 40.0, 2), (24.0, 48.0, 2))]).astype(np.float32)
+    theta = torch.from_numpy(targets - 0.5).cuda()
+    st = ilt.IltSettings(max_iterations=8)
+    res = ilt.optimize(eng, theta, torch.from_numpy(targets).cuda(), st)
+    for m in range(3):
+        h = res["cost_history"][m]
+        h = h[~np.isnan(h)]
+        assert len(h) >= 2 and np.all(np.diff(h) <= 1e-12), h
+        assert res["final_cost"][m] < h[0]
+    # the returned theta images to the recorded final cost
+    c, _ = ilt.cost_and_gradient(eng, theta, torch.from_numpy(targets).cuda(), st, want_gradient=False)
+    np.testing.assert_allclose(c, res["final_cost"], rtol=1e-6)
