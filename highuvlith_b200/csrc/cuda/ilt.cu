@@ -270,11 +270,11 @@ __global__ void batched_axpby(const float* __restrict__ x, float* __restrict__ y
     out[mask * n + i] = al * x[mask * n + i] + ga * y[mask * n + i];
 }
 
-// cost[c] = weight * data[2c] + reg[c]
+// cost[c] = weight * (sum r^2) / npix + reg[c]
 __global__ void ilt_combine(const double* __restrict__ data, const double* __restrict__ reg, int masks, double w,
-                            double* __restrict__ cost) {
+                            double inv_npix, double* __restrict__ cost) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < masks) cost[c] = w * data[2 * c] + reg[c];
+  if (c < masks) cost[c] = w * data[2 * c] * inv_npix + reg[c];
 }
 
 // out[j] = alpha[j] * x[idx[j]] + gamma[j] * y[idx[j]]   (blocks of n floats)
@@ -421,7 +421,8 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
                                                      static_cast<float>(p.binarization_weight),
                                                      grad ? grad + npix * c0 : nullptr, preg);
     sum_parts<<<(nc + 127) / 128, 128, 0, st>>>(preg, kRedBlocks, 1, nc, regsum);
-    ilt_combine<<<(nc + 127) / 128, 128, 0, st>>>(sums, regsum, nc, p.weight, cost_dev + c0);
+    ilt_combine<<<(nc + 127) / 128, 128, 0, st>>>(sums, regsum, nc, p.weight, 1.0 / static_cast<double>(npix),
+                                                  cost_dev + c0);
     check_cuda(cudaGetLastError(), "ilt kernels");
     prof.launches += grad ? 16 : 10;
   }
