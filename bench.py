@@ -241,6 +241,68 @@ def ilt_leg(eng, stream, masks=64, iterations=3):
             "mean_cost_start": float(np.mean(costs)), "mean_cost_end": float(np.mean(res["final_cost"]))}
 
 
+def uneven_leg(stream, n_clips=2048, steps=3):
+    """C3: an uneven batch in one graph launch: sides from {256, 512, 1024,
+    2048} at 1 nm, kernel budgets from {16, 32, 48, 64}, sources alternating
+    ArF immersion NA 1.35 dipole (sigma 0.8 +- 0.1) and EUV NA 0.33 quasar
+    (0.7-0.9, 45 deg poles), Manhattan clips at 20-60 % density; autotuned."""
+    import torch
+    import highuvlith_b200 as HB
+    from highuvlith_b200.clips import gen_clip
+    t0 = time.perf_counter()
+    sizes = (256, 512, 1024, 2048)
+    engines = {}
+    for n in sizes:
+        engines[("arfi", n)] = HB.SimulationEngine(HB.SourceConfig(193.368, "dipole", (0.8, 0.1, 0.0)),
+                                                   HB.OpticsConfig.immersion(1.35), grid=HB.GridConfig(n, 1.0),
+                                                   max_kernels=64)
+        engines[("euv", n)] = HB.SimulationEngine(HB.SourceConfig(13.5, "quasar", (0.7, 0.9, 45.0)),
+                                                  HB.OpticsConfig.euv_nxe_033(), grid=HB.GridConfig(n, 1.0),
+                                                  max_kernels=64)
+    t_engines = time.perf_counter() - t0
+    rng = np.random.Generator(np.random.PCG64(2048))
+    spec = [(("arfi", "euv")[i % 2], int(rng.choice(sizes)), int(rng.choice((16, 32, 48, 64))))
+            for i in range(n_clips)]
+    # group-contiguous device storage: one tensor per (source, size, budget)
+    keys = sorted(set(spec))
+    counts = {k: sum(1 for s in spec if s == k) for k in keys}
+    store = {k: (torch.empty((counts[k], k[1], k[1]), dtype=torch.uint8, device="cuda"),
+                 torch.empty((counts[k], k[1], k[1]), dtype=torch.float32, device="cuda")) for k in keys}
+    fill = {k: 0 for k in keys}
+    clips = []
+    t1 = time.perf_counter()
+    for i, k in enumerate(spec):
+        _, raster = gen_clip(4096 + i, k[1], 10, 80, 0.20, 0.60)
+        j = fill[k]
+        fill[k] += 1
+        store[k][0][j].copy_(torch.from_numpy(raster))
+    t_gen = time.perf_counter() - t1
+    for k in keys:
+        for j in range(counts[k]):
+            clips.append((engines[(k[0], k[1])], k[2], store[k][0][j], store[k][1][j]))
+    t2 = time.perf_counter()
+    plan = HB.UnevenPlan(clips, autotune=True)
+    t_plan = time.perf_counter() - t2
+    plan.launch(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        plan.launch(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    groups = plan.describe()
+    forms = {}
+    for g in groups:
+        forms[g["form"]] = forms.get(g["form"], 0) + g["clips"]
+    out_px = sum(k[1] * k[1] * counts[k] for k in keys)
+    return {"workload": f"{n_clips} uneven clips (N in 256..2048, K in 16..64, ArFi dipole + EUV quasar)",
+            "clips_per_s": n_clips / (ms / 1e3), "ms_per_launch": ms, "graph_launches_per_step": 1,
+            "groups": len(groups), "clips_by_form": forms, "output_gpix_per_s": out_px / (ms / 1e3) / 1e9,
+            "setup_s": {"engines": t_engines, "clip_generation": t_gen, "plan_autotune_capture": t_plan}}
+
+
 def run_ours(args):
     import torch
     from highuvlith_b200.clips import gen_batch
@@ -326,6 +388,7 @@ def run_ours(args):
                 forms[name] = {"unavailable": str(exc)[:200]}
         extra["forms"] = forms
         extra["ilt"] = ilt_leg(eng, stream)
+        extra["uneven_batch"] = uneven_leg(stream, n_clips=args.uneven_clips)
         step(args.form, args.eval_grid)
         torch.cuda.synchronize()
         extra["accuracy"] = accuracy(d_out[0].cpu().numpy(), rasters[0])
@@ -374,6 +437,7 @@ def main():
     ap.add_argument("--form", default="auto", choices=["auto", "fft", "tc"])
     ap.add_argument("--eval-grid", dest="eval_grid", type=int, default=0)
     ap.add_argument("--quick", action="store_true", help="skip the extra forms, accuracy and CPU baseline")
+    ap.add_argument("--uneven-clips", dest="uneven_clips", type=int, default=2048)
     ap.add_argument("--clips", type=int, default=N_CLIPS,
                     help="clips per GPU (default 256, the workload; smaller only for profiler captures)")
     args = ap.parse_args()

@@ -60,6 +60,11 @@ class Diagnostics(C.Structure):
                 ("num_source_points", C.c_int32)]
 
 
+class Clip(C.Structure):
+    _fields_ = [("engine", C.c_void_p), ("max_kernels", C.c_int32), ("input_kind", C.c_int32),
+                ("input", C.c_void_p), ("out", C.c_void_p)]
+
+
 class IltParams(C.Structure):
     _fields_ = [("cost_kind", C.c_int32), ("threshold", C.c_double), ("steepness", C.c_double),
                 ("beta", C.c_double), ("tv_weight", C.c_double), ("tv_epsilon", C.c_double),
@@ -96,6 +101,10 @@ SIGNATURES = {
     "huv_rasterize_rects": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                       C.c_void_p, C.c_void_p]),
     "huv_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "huv_plan_create": (C.c_int, [C.POINTER(Clip), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "huv_plan_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "huv_plan_describe": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
+    "huv_plan_destroy": (None, [C.c_void_p]),
     "huv_ilt_cost_grad": (C.c_int, [C.c_void_p, C.POINTER(IltParams), C.c_int32, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p]),
     "huv_ilt_optimize": (C.c_int, [C.c_void_p, C.POINTER(IltParams), C.POINTER(IltOpt), C.c_int32, C.c_void_p,

@@ -324,3 +324,38 @@ def rasterize_rects(n: int, clips: Sequence[Sequence[Tuple[int, int, int, int]]]
     L.check(L.lib().huv_rasterize_rects(n, len(clips), rects.data_ptr(), offsets.data_ptr(),
                                         int(dark_field), out.data_ptr(), st))
     return out
+
+
+class UnevenPlan:
+    """Many clips of different grids, sources and kernel budgets imaged by one
+    CUDA-graph launch (huv_plan_*).  ``clips``: sequence of
+    (engine, max_kernels, input_tensor (N, N) on the device, output_tensor
+    (N, N) float32 on the device).  Group-contiguous storage (clips of the
+    same engine and budget adjacent in one tensor) avoids staging copies."""
+
+    def __init__(self, clips, pixel_transfer: bool = True, autotune: bool = True):
+        arr = (L.Clip * len(clips))()
+        self._keep = []
+        for i, (eng, kmax, inp, out) in enumerate(clips):
+            arr[i] = L.Clip(eng.handle, int(kmax), SimulationEngine._kind(inp), inp.data_ptr(), out.data_ptr())
+            self._keep.append((eng, inp, out))
+        h = C.c_void_p()
+        L.check(L.lib().huv_plan_create(arr, len(clips), int(pixel_transfer), int(autotune), C.byref(h)))
+        self._h = h
+
+    def launch(self, stream=None):
+        import torch
+        st = (stream or torch.cuda.current_stream()).cuda_stream
+        L.check(L.lib().huv_plan_launch(self._h, st))
+
+    def describe(self):
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        L.check(L.lib().huv_plan_describe(self._h, buf, 1 << 16))
+        return json.loads(buf.value.decode())
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            L.lib().huv_plan_destroy(h)
+            self._h = None

@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "../engine.hpp"
@@ -395,6 +396,11 @@ void tc_release(huv::TcState& tc) {
   tc = huv::TcState();
 }
 
+void tc_release_all(std::map<int, huv::TcState>& m) {
+  for (auto& kv : m) tc_release(kv.second);
+  m.clear();
+}
+
 }  // namespace huv_launch
 
 namespace huv {
@@ -416,7 +422,8 @@ bool Engine::tc_supported(const DeviceSet& ds, int M) const {
          huv_launch::encode_fn() != nullptr;
 }
 
-void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st) {
+void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use,
+                         const float* W_use) {
   using namespace huv_launch;
   static bool smem_set = false;
   if (!smem_set) {
@@ -424,13 +431,13 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     smem_set = true;
   }
   const int lgn = ilog2i(n), lgm = ilog2i(M);
-  const int B = ds.B, K = ds.K, hb = ds.hb;
+  const int B = ds.B, K = K_use > 0 ? K_use : ds.K, hb = ds.hb;
+  const float* Wf = W_use ? W_use : ds.W;
   const int h2 = 2 * hb, B2 = 2 * h2 + 1;
   const int kcE = 2 * B, kpE = round_up(kcE, 64), kstE = (kcE + 15) / 16;
   const int nrI = h2 + 1, kcI = 2 * nrI, kpI = round_up(kcI, 64), kstI = (kcI + 15) / 16;
-  TcState& tc = ds.tc;
-  if (tc.lgm != lgm || !tc.gy) {
-    tc_release(tc);
+  TcState& tc = ds.tc[lgm];
+  if (!tc.gy) {
     // A_E: rows (y, re/im) over the M grid, K = (my, re/im).
     std::vector<double> ae(static_cast<size_t>(2 * M) * kcE);
     for (int y = 0; y < M; ++y)
@@ -498,7 +505,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     const int nc = std::min(chunk, b.n_clips - c0);
     const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
     float* o = out + static_cast<size_t>(n) * n * c0;
-    check_cuda(band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb, b.pixel_transfer ? ds.ptx : nullptr, ds.W,
+    check_cuda(band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb, b.pixel_transfer ? ds.ptx : nullptr, Wf,
                             mean, twn, st),
                "band_forward");
     {

@@ -29,6 +29,7 @@ cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float 
                       const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 cudaError_t set_smem_limits();
 void tc_release(huv::TcState& tc);
+void tc_release_all(std::map<int, huv::TcState>& m);
 }  // namespace huv_launch
 
 namespace huv {
@@ -105,10 +106,11 @@ Engine::~Engine() {
     cudaSetDevice(device);
     for (auto& kv : twiddles) cudaFree(kv.second);
     auto free_set = [](DeviceSet& d) {
+      for (auto& kv : d.W_by_k) cudaFree(kv.second);
       cudaFree(d.kband);
       cudaFree(d.W);
       cudaFree(d.ptx);
-      huv_launch::tc_release(d.tc);
+      huv_launch::tc_release_all(d.tc);
     };
     free_set(focus_dev);
     for (auto& e : cache) free_set(e.dev);
@@ -137,10 +139,11 @@ std::shared_ptr<KernelSet> Engine::kernel_set(double z) {
     auto it = std::min_element(cache.begin(), cache.end(),
                                [](const CacheEntry& a, const CacheEntry& b) { return a.last_used < b.last_used; });
     if (device_ready) {
+      for (auto& kv : it->dev.W_by_k) cudaFree(kv.second);
       cudaFree(it->dev.kband);
       cudaFree(it->dev.W);
       cudaFree(it->dev.ptx);
-      huv_launch::tc_release(it->dev.tc);
+      huv_launch::tc_release_all(it->dev.tc);
     }
     cache.erase(it);
   }
@@ -190,10 +193,11 @@ DeviceSet& Engine::device_set(double z) {
   }
   if (slot->kband && slot->source == ks.get()) return *slot;
   if (slot->kband) {
+    for (auto& kv : slot->W_by_k) cudaFree(kv.second);
     cudaFree(slot->kband);
     cudaFree(slot->W);
     cudaFree(slot->ptx);
-    huv_launch::tc_release(slot->tc);
+    huv_launch::tc_release_all(slot->tc);
     *slot = DeviceSet();
   }
   const int h = ks->band_half_width();
@@ -244,7 +248,38 @@ DeviceSet& Engine::device_set(double z) {
   return *slot;
 }
 
+const float* Engine::flare_weights(DeviceSet& ds, int K) {
+  if (K <= 0 || K >= ds.K) return ds.W;
+  auto it = ds.W_by_k.find(K);
+  if (it != ds.W_by_k.end()) return it->second;
+  const int B = ds.B;
+  std::vector<float> w(static_cast<size_t>(B) * B, 0.f);
+  std::vector<double> wd(static_cast<size_t>(B) * B, 0.0);
+  for (int k = 0; k < K; ++k)
+    for (size_t i = 0; i < wd.size(); ++i) {
+      // |kappa_k|^2 = lambda_k |u_k|^2 / N^4 (the band kernels carry sqrt(lambda)/N^2)
+      const float2 v = ds.host_kband[static_cast<size_t>(k) * B * B + i];
+      wd[i] += static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y;
+    }
+  for (size_t i = 0; i < wd.size(); ++i) w[i] = static_cast<float>(wd[i]);
+  float* d = nullptr;
+  check_cuda(cudaMalloc(&d, sizeof(float) * w.size()), "cudaMalloc(W prefix)");
+  check_cuda(cudaMemcpy(d, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice), "upload W prefix");
+  ds.W_by_k[K] = d;
+  return d;
+}
+
+int Engine::kernel_count_for(const KernelSet& ks, int max_kernels) const {
+  const int k = select_kernel_count(ks.all_values.empty() ? ks.eigenvalues : ks.all_values, ks.trace, max_kernels,
+                                    settings.kernel_energy_fraction);
+  return std::min(k, ks.num_kernels());
+}
+
 void* Engine::workspace(size_t bytes) {
+  if (ws_override) {
+    if (bytes > ws_override_bytes) throw Error(HUV_ERR_OUT_OF_MEMORY, "plan workspace too small");
+    return ws_override;
+  }
   if (bytes > ws_bytes) {
     if (ws) cudaFree(ws);
     ws = nullptr;
@@ -270,9 +305,11 @@ int Engine::choose_eval_grid(const DeviceSet& ds, int requested) const {
 
 static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
-void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st) {
+void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use,
+                          const float* W_use) {
   const int lgn = ilog2(n), lgm = ilog2(M);
-  const int B = ds.B, K = ds.K, hb = ds.hb;
+  const int B = ds.B, K = K_use > 0 ? K_use : ds.K, hb = ds.hb;
+  const float* Wf = W_use ? W_use : ds.W;
   const bool coarse = M < n;
   const int h2 = 2 * hb, B2 = 2 * h2 + 1;
   const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
@@ -305,7 +342,7 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
     const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
     float* o = out + static_cast<size_t>(n) * n * c0;
     check_cuda(huv_launch::band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb,
-                                        b.pixel_transfer ? ds.ptx : nullptr, ds.W, mean, twn, st),
+                                        b.pixel_transfer ? ds.ptx : nullptr, Wf, mean, twn, st),
                "band_forward");
     prof.launches += 2;
     check_cuda(huv_launch::socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");

@@ -40,8 +40,9 @@ struct DeviceSet {
   float* W = nullptr;
   float* ptx = nullptr;
   std::vector<double> eig_scaled;
+  std::map<int, float*> W_by_k;  // flare weights of kernel-count prefixes
   std::vector<float2> host_kband;
-  TcState tc;
+  std::map<int, TcState> tc;  // per evaluation grid (log2 M); kept for the set's lifetime
 };
 
 // Launch accounting and live timing of the dominant kernel.  When `on`,
@@ -116,8 +117,15 @@ struct Engine {
   void* workspace(size_t bytes);
   int choose_eval_grid(const DeviceSet& ds, int requested) const;
   bool tc_supported(const DeviceSet& ds, int M) const;
-  void run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st);
-  void run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st);
+  // K_use / W_use: kernel count and flare weights to use (0 / nullptr = the whole set).
+  void run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use = 0,
+                    const float* W_use = nullptr);
+  void run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use = 0,
+                   const float* W_use = nullptr);
+  // Flare weights W = sum_{k < K} lambda_k |u_k|^2 / N^4 of the first K kernels (device, cached).
+  const float* flare_weights(DeviceSet& ds, int K);
+  // Kernel count for a budget of `max_kernels` under the reference's truncation rule.
+  int kernel_count_for(const KernelSet& ks, int max_kernels) const;
   // ILT (batched): cost and optional gradient; the optimizer.
   void ilt_eval(const huv_ilt_params& p, int masks, const float* theta, const float* target, float* grad,
                 double* cost_dev, cudaStream_t st);
@@ -144,6 +152,10 @@ struct Engine {
   DeviceSet focus_dev, scratch_dev;
   void* ws = nullptr;
   size_t ws_bytes = 0;
+  // When set, workspace() hands out this buffer (a captured plan's own
+  // workspace) and fails instead of reallocating.
+  void* ws_override = nullptr;
+  size_t ws_override_bytes = 0;
   int* dev_err = nullptr;
   void* io_in = nullptr;
   void* io_out = nullptr;

@@ -59,7 +59,8 @@ std::vector<SourcePoint> sample_source(const Fill& fill, int points_per_axis, do
 struct KernelSet {
   int n = 0;                       // grid size
   std::vector<int64_t> support;    // flat indices i*n + j (row i = y order)
-  std::vector<double> eigenvalues; // raw (absolute), decreasing
+  std::vector<double> eigenvalues; // raw (absolute), decreasing, retained
+  std::vector<double> all_values;  // every eigenvalue of the decomposition (re-truncation)
   std::vector<cd> values;          // K * S, kernel-major
   double trace = 0, clear_field = 0, pupil_peak = 0;
   int method = 0;                  // 0 dense_tcc, 1 dense_gram

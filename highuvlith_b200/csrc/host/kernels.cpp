@@ -385,6 +385,7 @@ KernelSet build_kernels(const std::vector<SourcePoint>& points, const Optics& op
     std::vector<cd> v = eig.vectors(k);
     ks.trace = trace;
     ks.eigenvalues.assign(eig.values().begin(), eig.values().begin() + k);
+    ks.all_values = eig.values();
     ks.values = std::move(v);  // k x m, kernel-major (columns of V)
     ks.support.resize(m);
     for (int64_t i = 0; i < m; ++i) ks.support[i] = cand[rows[i]].idx;
@@ -415,6 +416,7 @@ KernelSet build_kernels(const std::vector<SourcePoint>& points, const Optics& op
     std::vector<cd> v = eig.vectors(k);
     ks.trace = trace;
     ks.eigenvalues.assign(eig.values().begin(), eig.values().begin() + k);
+    ks.all_values = eig.values();
     // u_k = A v_k / sqrt(lambda_k) over every candidate.
     ks.values.assign(static_cast<size_t>(k) * n_cand, cd(0, 0));
     parallel_for(n_cand, [&](int64_t b, int64_t e) {

@@ -167,6 +167,33 @@ huv_status huv_image_batch(void* engine, const huv_batch* batch, float* out, voi
  * on `stream` and synchronises it (the reference-facing end-to-end call). */
 huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out_host, void* stream);
 
+/* Uneven batches (no counterpart in the reference, which images one clip per
+ * call): clips of different grids, sources and kernel budgets in one CUDA
+ * graph.  Each clip names the engine built for its source and grid and its
+ * own kernel budget; the kernel count is re-truncated from that engine's
+ * eigenvalues with the reference's rule (select_kernel_count,
+ * aerial.rs:992-1029).  Inputs/outputs are device buffers fixed at creation:
+ * write new rasters into the same buffers and launch again.  Engines must
+ * outlive the plan and must not be used concurrently with its launches. */
+typedef struct {
+  void* engine;        /* engine for this clip's source and grid (in-focus kernel set) */
+  int32_t max_kernels; /* this clip's kernel budget */
+  int32_t input_kind;  /* huv_input_kind */
+  const void* input;   /* device raster N*N */
+  float* out;          /* device image N*N */
+} huv_clip;
+
+/* Group, autotune (autotune != 0: time each candidate form and evaluation
+ * grid on the group's own clips; results cached per (N, h, K, kind)),
+ * pre-allocate, run once and capture the whole batch into one CUDA graph. */
+huv_status huv_plan_create(const huv_clip* clips, int32_t n_clips, int32_t pixel_transfer, int32_t autotune,
+                           void** plan_out);
+/* One cudaGraphLaunch of the whole uneven batch on `stream`. */
+huv_status huv_plan_launch(void* plan, void* stream);
+/* JSON description of the groups and the tuned choices. */
+huv_status huv_plan_describe(void* plan, char* buf, int32_t capacity);
+void huv_plan_destroy(void* plan);
+
 /* Pixel ILT (crates/highuvlith-core/src/ilt.rs).  One process condition
  * (focus, dose, weight); m = sigmoid(beta theta), t = a + (1 - a) m with a
  * real absorber amplitude a (0 = binary). */
