@@ -44,7 +44,8 @@ def test_plan_matches_per_clip_engines():
         plan.launch()
         torch.cuda.synchronize()
     groups = plan.describe()
-    assert len(groups) == 5 and sum(g["clips"] for g in groups) == len(spec)
+    # (arfi, 256) has only 8 kernels: budgets 16 and 48 share one group
+    assert len(groups) == 4 and sum(g["clips"] for g in groups) == len(spec)
     for (src, n, kmax, raster), (_, _, _, out) in zip(refs, clips):
         ref_eng = euv(n) if src == "euv" else arfi(n)
         ref_eng = HB.SimulationEngine(ref_eng.source, ref_eng.optics, grid=HB.GridConfig(n, 1.0), max_kernels=kmax)
