@@ -87,4 +87,13 @@ __device__ float2* block_fft(float2* src, float2* dst, int lg, int S, const floa
   return src;
 }
 
+// Largest power of two <= want whose `per_unit` bytes times it fit in the
+// dynamic shared-memory budget of the FFT kernels (192 KiB).
+inline int fit_units(int want, size_t per_unit) {
+  const size_t budget = size_t(192) << 10;
+  int u = 1;
+  while (u * 2 <= want && static_cast<size_t>(u * 2) * per_unit <= budget) u *= 2;
+  return u;
+}
+
 }  // namespace huv_dev

@@ -404,11 +404,11 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     sum_parts<<<(nc * 2 + 127) / 128, 128, 0, st>>>(pdata, kRedBlocks, 2, nc, sums);
     float* dcdm = nullptr;
     if (grad) {
-      const int Wc = lgn >= 11 ? 4 : 8;
+      const int Wc = fit_units(8, 2 * (sizeof(float2) << lgn) + (sizeof(float) << lgn));
       const size_t sm = 2 * (static_cast<size_t>(Wc) << lgn) * sizeof(float2) + (static_cast<size_t>(Wc) << lgn) * sizeof(float);
       ilt_cols_adj<<<dim3(n / Wc, nc), 256, sm, st>>>(T, img, K, hb, lgn, Wc, keep, sums,
                                                       flare / static_cast<float>(npix), V, tw);
-      const int S = lgn >= 11 ? 2 : 4;
+      const int S = fit_units(4, 2 * (sizeof(float2) << lgn));
       const size_t sm2 = 2 * (static_cast<size_t>(S) << lgn) * sizeof(float2);
       ilt_rows_adj<<<dim3(B, nc), 256, sm2, st>>>(V, ds.kband, K, hb, lgn, S, Q, tw);
       const float scale = static_cast<float>(2.0 * (1.0 - p.absorber) * p.weight);

@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "fft_block.cuh"
 
 namespace huv_dev {
@@ -247,8 +249,8 @@ static int pick_threads(int work) { return work >= 256 ? 256 : 128; }
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X,
                          float2* Mband, const float* ptx, const float* W, float* mean,
                          const float2* tw, cudaStream_t st) {
-  const int rows_per_block = (kind == 2) ? 2 : 4;
-  const int S = (kind == 2) ? rows_per_block : rows_per_block / 2;
+  const int S = fit_units(2, 2 * (sizeof(float2) << lg));
+  const int rows_per_block = (kind == 2) ? S : 2 * S;
   const size_t sm1 = 2 * (static_cast<size_t>(S) << lg) * sizeof(float2);
   dim3 g1(n / rows_per_block, clips);
   const int th = pick_threads(S << (lg - 2));
@@ -258,7 +260,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     default: band_rows_fwd<2><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
   }
   const int B = 2 * hb + 1;
-  const int cpb = 4;
+  const int cpb = fit_units(4, 2 * (sizeof(float2) << lg));
   const int nblk = (B + cpb - 1) / cpb;
   const size_t sm2 = 2 * (static_cast<size_t>(cpb) << lg) * sizeof(float2);
   float* parts = (W && mean) ? mean + clips : nullptr;
@@ -270,7 +272,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
 cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
                       float2* T, const float2* tw, cudaStream_t st) {
   const int B = 2 * hb + 1;
-  const int S = lgm >= 11 ? 2 : 4;
+  const int S = fit_units(4, 2 * (sizeof(float2) << lgm));
   const size_t sm3 = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
   dim3 g3((K * B + S - 1) / S, clips);
   socs_rows_inv<<<g3, 256, sm3, st>>>(kband, scale, Mband, K, hb, lgm, S, T, tw);
@@ -280,7 +282,7 @@ cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
                       const float* mean, float* out, int mode, const float2* tw, cudaStream_t st) {
   const int L = 1 << lgm;
-  const int Wc = lgm >= 11 ? 4 : (L >= 8 ? 8 : L);
+  const int Wc = std::min(L, fit_units(8, 2 * (sizeof(float2) << lgm) + (sizeof(float) << lgm)));
   const size_t sm4 = (2 * (static_cast<size_t>(Wc) << lgm)) * sizeof(float2) +
                      (static_cast<size_t>(Wc) << lgm) * sizeof(float);
   dim3 g4(L / Wc, clips);

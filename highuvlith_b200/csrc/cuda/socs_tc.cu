@@ -509,7 +509,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
                             mean, twn, st),
                "band_forward");
     {
-      const int S = 8;
+      const int S = fit_units(8, 2 * (sizeof(float2) << lgm));
       dim3 g((K * B + S - 1) / S, nc);
       const size_t sm = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
       socs_rows_tc<<<g, 256, sm, st>>>(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, S, kpE, kstE * 16, BE, twm);
@@ -544,7 +544,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st),
                "band_forward(interp)");
     {
-      const int S = 8;
+      const int S = fit_units(8, 2 * (sizeof(float2) << lgn));
       dim3 g((nrI + S - 1) / S, nc);
       const size_t sm = 2 * (static_cast<size_t>(S) << lgn) * sizeof(float2);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
