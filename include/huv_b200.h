@@ -234,6 +234,29 @@ huv_status huv_ilt_optimize(void* engine, const huv_ilt_params* params, const hu
                             float* theta, const float* target, double* final_cost, int32_t* iterations,
                             double* history, void* stream);
 
+/* Fourier-neural-operator surrogate of the image (no counterpart in the
+ * reference).  Maps a transmittance map (grid x grid floats, [y, x]) to the
+ * normalised aerial image.  Width 64, `modes` x `modes` retained Fourier modes
+ * (2 * modes along y), `layers` Fourier layers with GELU, projection 64 -> 128
+ * -> 1.  Activations are stored in BF16, arithmetic is FP32, parameters FP32
+ * (flat vector, seeded initialisation).  All array arguments are device
+ * pointers unless named *_host. */
+huv_status huv_fno_create(int32_t grid, int32_t width, int32_t modes, int32_t layers, int32_t proj, uint64_t seed,
+                          int32_t device, void** fno_out);
+void huv_fno_destroy(void* fno);
+/* Copy the parameters to the host (host = NULL: count only). */
+huv_status huv_fno_params(void* fno, float* host, int64_t capacity, int64_t* count);
+huv_status huv_fno_set_params(void* fno, const float* host, int64_t count);
+/* images = FNO(masks) for `batch` maps. */
+huv_status huv_fno_forward(void* fno, int32_t batch, const float* masks, float* images, void* stream);
+/* Gradient of the MSE to `targets` (or, targets = NULL, of sum(dout . FNO))
+ * with respect to the parameters (param_grad) and the input (dmask). */
+huv_status huv_fno_backward(void* fno, int32_t batch, const float* masks, const float* targets, const float* dout,
+                            float* param_grad, float* dmask, float* loss_host, void* stream);
+/* One Adam step on the MSE to `targets`. */
+huv_status huv_fno_train_step(void* fno, int32_t batch, const float* masks, const float* targets, float lr,
+                              float weight_decay, float* loss_host, void* stream);
+
 /* Allocation-free variant of huv_image_batch (no counterpart in the
  * reference, which has no device path).  For callers that cannot call
  * cudaMalloc: applications whose memory pool already owns the device, and
