@@ -214,9 +214,10 @@ __global__ void __launch_bounds__(256) fno_layer_bwd(const float* __restrict__ d
   float gw[16], gb = 0.f;
 #pragma unroll
   for (int q = 0; q < 16; ++q) gw[q] = 0.f;
-  for (int x0 = 0; x0 < S; x0 += XT) {
+  const int xt = min(XT, S);  // S is a power of two, so xt divides S
+  for (int x0 = 0; x0 < S; x0 += xt) {
     __syncthreads();
-    for (int t = threadIdx.x; t < XT * C; t += blockDim.x) {
+    for (int t = threadIdx.x; t < xt * C; t += blockDim.x) {
       const size_t g = row + static_cast<size_t>(x0) * C + t;
       const float gv = dvnext[g];
       const float d = act ? gv * gelu_grad(__bfloat162float(z[g])) : gv;
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(256) fno_layer_bwd(const float* __restrict__ d
       sv[t] = __bfloat162float(v[g]);
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < XT * C; t += blockDim.x) {
+    for (int t = threadIdx.x; t < xt * C; t += blockDim.x) {
       const int x = t / C, i = t - x * C;
       float acc = 0.f;
 #pragma unroll 8
@@ -237,11 +238,11 @@ __global__ void __launch_bounds__(256) fno_layer_bwd(const float* __restrict__ d
       const int pr = threadIdx.x + q * 256;  // (o, i) pair
       const int o = pr / C, i = pr - o * C;
       float acc = 0.f;
-      for (int x = 0; x < XT; ++x) acc += sdz[x * C + o] * sv[x * C + i];
+      for (int x = 0; x < xt; ++x) acc += sdz[x * C + o] * sv[x * C + i];
       gw[q] += acc;
     }
     if (threadIdx.x < C)
-      for (int x = 0; x < XT; ++x) gb += sdz[x * C + threadIdx.x];
+      for (int x = 0; x < xt; ++x) gb += sdz[x * C + threadIdx.x];
   }
 #pragma unroll
   for (int q = 0; q < 16; ++q) atomicAdd(dW + threadIdx.x + q * 256, gw[q]);
