@@ -27,9 +27,9 @@ def layout(C: int, m: int, L: int, P: int):
     take("Wl", C * 3)
     take("bl", C)
     for l in range(L):
-        take(f"R{l}", modes * C * C * 2)
-        take(f"W{l}", C * C)
-        take(f"b{l}", C)
+        take(f"R_{l}", modes * C * C * 2)
+        take(f"W_{l}", C * C)
+        take(f"b_{l}", C)
     take("Q1", P * C)
     take("b1", P)
     take("Q2", P)
@@ -63,13 +63,13 @@ def forward(params: np.ndarray, masks: np.ndarray, S: int, C: int = 64, m: int =
     w = torch.ones(m, dtype=torch.float64)
     w[1:] = 2.0
     for l in range(L):
-        R = g(f"R{l}", (J, m, C, C, 2))
+        R = g(f"R_{l}", (J, m, C, C, 2))
         Rc = torch.complex(R[..., 0], R[..., 1])
         vc = v.to(torch.complex128)
         X = torch.einsum("bysc,ks,jy->bjkc", vc, Ex, Ey)               # (B, J, m, C)
         Y = torch.einsum("bjki,jkio->bjko", X, Rc)
-        spec = torch.einsum("bjko,k,ks,jy->bysc", Y, w.to(torch.complex128), Ex.conj(), Ey.conj()).real / (S * S)
-        z = spec + v @ g(f"W{l}", (C, C)).T + g(f"b{l}", (C,))
+        spec = torch.einsum("bjko,k,ks,jy->byso", Y, w.to(torch.complex128), Ex.conj(), Ey.conj()).real / (S * S)
+        z = spec + v @ g(f"W_{l}", (C, C)).T + g(f"b_{l}", (C,))
         v = torch.nn.functional.gelu(z) if l < L - 1 else z
     h = torch.nn.functional.gelu(v @ g("Q1", (P, C)).T + g("b1", (P,)))
     out = h @ g("Q2", (P,)) + g("b2", (1,))
