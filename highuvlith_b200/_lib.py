@@ -76,6 +76,12 @@ class IltOpt(C.Structure):
     _fields_ = [("max_iterations", C.c_int32), ("learning_rate", C.c_double), ("convergence_tol", C.c_double)]
 
 
+class SurrogateIlt(C.Structure):
+    _fields_ = [("judge_every", C.c_int32), ("error_bound", C.c_double), ("surrogate_iterations", C.c_int32),
+                ("exact_iterations", C.c_int32), ("takeover_iteration", C.c_int32), ("n_judges", C.c_int32),
+                ("judge_errors", C.c_double * 64)]
+
+
 class Batch(C.Structure):
     _fields_ = [("n_clips", C.c_int32), ("input_kind", C.c_int32), ("input", C.c_void_p),
                 ("pixel_transfer", C.c_int32), ("defocus_nm", C.c_double), ("form", C.c_int32),
@@ -119,6 +125,9 @@ SIGNATURES = {
                                     C.c_void_p, C.c_void_p, C.c_void_p]),
     "huv_ilt_optimize": (C.c_int, [C.c_void_p, C.POINTER(IltParams), C.POINTER(IltOpt), C.c_int32, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "huv_ilt_optimize_surrogate": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(IltParams), C.POINTER(IltOpt),
+                                             C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(SurrogateIlt),
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "huv_image_batch_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),
     "huv_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
     "huv_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32),

@@ -160,11 +160,14 @@ class SimulationEngine:
         L.check(L.lib().huv_engine_create(C.byref(source._c()), C.byref(optics._c()), C.byref(g),
                                           C.byref(st), device, C.byref(h)))
         self._h = h
+        self._destroy = L.lib().huv_engine_destroy
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            L.lib().huv_engine_destroy(h)
+        # The destroy function is bound at construction: at interpreter exit
+        # module globals may already be gone.
+        h, destroy = getattr(self, "_h", None), getattr(self, "_destroy", None)
+        if h and destroy is not None:
+            destroy(h)
             self._h = None
 
     @property
@@ -342,6 +345,7 @@ class UnevenPlan:
         h = C.c_void_p()
         L.check(L.lib().huv_plan_create(arr, len(clips), int(pixel_transfer), int(autotune), C.byref(h)))
         self._h = h
+        self._destroy = L.lib().huv_plan_destroy
 
     def launch(self, stream=None):
         import torch
@@ -355,7 +359,9 @@ class UnevenPlan:
         return json.loads(buf.value.decode())
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            L.lib().huv_plan_destroy(h)
+        # The destroy function is bound at construction: at interpreter exit
+        # module globals may already be gone.
+        h, destroy = getattr(self, "_h", None), getattr(self, "_destroy", None)
+        if h and destroy is not None:
+            destroy(h)
             self._h = None

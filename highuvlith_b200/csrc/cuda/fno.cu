@@ -692,6 +692,20 @@ struct Fno {
 
 }  // namespace huv
 
+namespace huv {
+// The FNO as the image model of surrogate-assisted ILT.  input_grad reuses
+// the activations of the preceding forward on the same maps.
+struct FnoImageModel : Surrogate {
+  Fno* f;
+  explicit FnoImageModel(Fno* f_) : f(f_) {}
+  int grid() const override { return f->S; }
+  void forward(int B, const float* t, float* img, cudaStream_t st) override { f->forward(B, t, img, st); }
+  void input_grad(int B, const float* t, const float* dout, float* dt, cudaStream_t st) override {
+    f->backward(B, t, dout, dt, st);
+  }
+};
+}  // namespace huv
+
 using huv::Error;
 using huv::Fno;
 
@@ -796,6 +810,38 @@ huv_status huv_fno_train_step(void* fno, int32_t batch, const float* masks, cons
     if (loss_host) *loss_host = l;
     f->backward(batch, masks, f->dout, nullptr, st);
     f->adam(lr, weight_decay, st);
+  });
+}
+
+huv_status huv_ilt_optimize_surrogate(void* engine, void* fno, const huv_ilt_params* params, const huv_ilt_opt* opt,
+                                      int32_t n_masks, float* theta, const float* target, huv_surrogate_ilt* sur,
+                                      double* final_cost, int32_t* iterations, double* history, void* stream) {
+  return fno_guard([&] {
+    huv::Engine* e = static_cast<huv::Engine*>(engine);
+    Fno* f = as_fno(fno);
+    if (!e || !params || !opt || !theta || !target || !sur)
+      throw Error(HUV_ERR_INVALID_PARAMETER, "surrogate ilt: null argument");
+    if (opt->max_iterations < 0 || !(opt->learning_rate > 0) || !(opt->convergence_tol >= 0))
+      throw Error(HUV_ERR_INVALID_PARAMETER, "ilt optimizer: max_iterations >= 0, learning_rate > 0, tol >= 0");
+    if (sur->judge_every < 1 || !(sur->error_bound > 0))
+      throw Error(HUV_ERR_INVALID_PARAMETER, "surrogate ilt: judge_every >= 1, error_bound > 0");
+    if (f->S != e->n) throw Error(HUV_ERR_DIMENSION_MISMATCH, "surrogate ilt: FNO grid differs from the engine grid");
+    if (!(params->beta > 0) || !(params->absorber >= 0 && params->absorber < 1) || !(params->tv_epsilon > 0) ||
+        (params->cost_kind != 0 && params->cost_kind != 1))
+      throw Error(HUV_ERR_INVALID_PARAMETER, "ilt: invalid params");
+    if (n_masks <= 0) return;
+    std::lock_guard<std::mutex> lock(e->mu);
+    e->ensure_device();
+    huv::FnoImageModel model(f);
+    huv::SurrogateReport rep;
+    e->ilt_optimize(*params, *opt, n_masks, theta, target, final_cost, iterations, history,
+                    static_cast<cudaStream_t>(stream), &model, sur->judge_every, sur->error_bound, &rep);
+    sur->surrogate_iterations = rep.surrogate_iterations;
+    sur->exact_iterations = rep.exact_iterations;
+    sur->takeover_iteration = rep.takeover_iteration;
+    sur->n_judges = static_cast<int32_t>(rep.judge_errors.size());
+    for (int i = 0; i < 64; ++i)
+      sur->judge_errors[i] = i < static_cast<int>(rep.judge_errors.size()) ? rep.judge_errors[i] : 0.0;
   });
 }
 

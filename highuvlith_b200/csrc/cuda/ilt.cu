@@ -270,6 +270,44 @@ __global__ void batched_axpby(const float* __restrict__ x, float* __restrict__ y
     out[mask * n + i] = al * x[mask * n + i] + ga * y[mask * n + i];
 }
 
+__global__ void scale_inplace(float* __restrict__ x, size_t n, float s) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    x[i] *= s;
+}
+
+// parts[mask][block] = (max |a - b|, max |b|)
+__global__ void err_parts(const float* __restrict__ a, const float* __restrict__ b, size_t n,
+                          double* __restrict__ parts) {
+  __shared__ float re[32], rb[32];
+  const int mask = blockIdx.y;
+  float e = 0.f, m = 0.f;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    e = fmaxf(e, fabsf(a[mask * n + i] - b[mask * n + i]));
+    m = fmaxf(m, fabsf(b[mask * n + i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
+    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    re[threadIdx.x >> 5] = e;
+    rb[threadIdx.x >> 5] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float E = 0.f, Mx = 0.f;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+      E = fmaxf(E, re[w]);
+      Mx = fmaxf(Mx, rb[w]);
+    }
+    double* p = parts + (static_cast<size_t>(mask) * gridDim.x + blockIdx.x) * 2;
+    p[0] = E;
+    p[1] = Mx;
+  }
+}
+
 // cost[c] = weight * (sum r^2) / npix + reg[c]
 __global__ void ilt_combine(const double* __restrict__ data, const double* __restrict__ reg, int masks, double w,
                             double inv_npix, double* __restrict__ cost) {
@@ -428,6 +466,92 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   }
 }
 
+// Surrogate-based ILT cost and gradient: the transmittance's image comes
+// from `sur`, its adjoint through the surrogate's input gradient; data term,
+// regularisers and chain rule as in the exact path.
+void Engine::ilt_eval_surrogate(Surrogate* sur, const huv_ilt_params& p, int masks, const float* theta,
+                                const float* target, float* grad, double* cost_dev, cudaStream_t st) {
+  using namespace huv_dev;
+  const size_t npix = static_cast<size_t>(n) * n;
+  const size_t per = 3 * ((sizeof(float) * npix + 255) & ~size_t(255)) + 3 * 256 * 8 * 2;
+  char* base = static_cast<char*>(workspace(per * masks + 4096));
+  float* tbuf = reinterpret_cast<float*>(base);
+  float* img = tbuf + npix * masks;
+  float* dt = img + npix * masks;
+  double* pdata = reinterpret_cast<double*>(dt + npix * masks);
+  double* preg = pdata + static_cast<size_t>(masks) * kRedBlocks * 2;
+  double* sums = preg + static_cast<size_t>(masks) * kRedBlocks;
+  double* regsum = sums + 2 * masks;
+  ilt_transmittance<<<1184, 256, 0, st>>>(theta, npix * masks, static_cast<float>(p.beta),
+                                          static_cast<float>(p.absorber), tbuf);
+  sur->forward(masks, tbuf, img, st);
+  ilt_data<<<dim3(kRedBlocks, masks), 256, 0, st>>>(img, target, npix, p.cost_kind, static_cast<float>(p.threshold),
+                                                    static_cast<float>(p.steepness), static_cast<float>(p.dose), img,
+                                                    pdata);
+  sum_parts<<<(masks * 2 + 127) / 128, 128, 0, st>>>(pdata, kRedBlocks, 2, masks, sums);
+  float* dcdm = nullptr;
+  if (grad) {
+    sur->input_grad(masks, tbuf, img, dt, st);  // img now holds G = dC/dI
+    // dC/dm = weight (1 - a) dC/dt
+    const float sc = static_cast<float>(p.weight * (1.0 - p.absorber));
+    scale_inplace<<<1184, 256, 0, st>>>(dt, npix * masks, sc);
+    dcdm = dt;
+  }
+  ilt_finish<<<dim3(kRedBlocks, masks), 256, 0, st>>>(theta, dcdm, n, static_cast<float>(p.beta),
+                                                      static_cast<float>(p.tv_weight), static_cast<float>(p.tv_epsilon),
+                                                      static_cast<float>(p.binarization_weight), grad, preg);
+  sum_parts<<<(masks + 127) / 128, 128, 0, st>>>(preg, kRedBlocks, 1, masks, regsum);
+  ilt_combine<<<(masks + 127) / 128, 128, 0, st>>>(sums, regsum, masks, p.weight, 1.0 / static_cast<double>(npix),
+                                                   cost_dev);
+  check_cuda(cudaGetLastError(), "ilt surrogate kernels");
+}
+
+std::vector<double> Engine::surrogate_error(Surrogate* sur, const huv_ilt_params& p, int masks, const float* theta,
+                                            cudaStream_t st) {
+  using namespace huv_dev;
+  const size_t npix = static_cast<size_t>(n) * n;
+  float *t = nullptr, *a = nullptr, *b = nullptr;
+  double* parts = nullptr;
+  check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&t), sizeof(float) * npix * masks * 3, st), "cudaMallocAsync");
+  check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&parts), sizeof(double) * masks * kRedBlocks * 2, st),
+             "cudaMallocAsync");
+  a = t + npix * masks;
+  b = a + npix * masks;
+  ilt_transmittance<<<1184, 256, 0, st>>>(theta, npix * masks, static_cast<float>(p.beta),
+                                          static_cast<float>(p.absorber), t);
+  sur->forward(masks, t, a, st);
+  huv_batch bt{};
+  bt.n_clips = masks;
+  bt.input_kind = HUV_INPUT_RASTER_F32;
+  bt.input = t;
+  bt.pixel_transfer = 0;
+  bt.defocus_nm = p.defocus_nm;
+  bt.form = HUV_FORM_AUTO;
+  DeviceSet& ds = device_set(p.defocus_nm);
+  int M = choose_eval_grid(ds, 0);
+  if (tc_supported(ds, std::max(M, 128)) && n >= 128)
+    run_tc_form(bt, ds, std::max(M, 128), b, st);
+  else
+    run_fft_form(bt, ds, M, b, st);
+  // per mask: max |a - b| and max |b|
+  err_parts<<<dim3(kRedBlocks, masks), 256, 0, st>>>(a, b, npix, parts);
+  std::vector<double> h(static_cast<size_t>(masks) * kRedBlocks * 2);
+  check_cuda(cudaMemcpyAsync(h.data(), parts, h.size() * 8, cudaMemcpyDeviceToHost, st), "D2H err");
+  check_cuda(cudaFreeAsync(t, st), "cudaFreeAsync");
+  check_cuda(cudaFreeAsync(parts, st), "cudaFreeAsync");
+  check_cuda(cudaStreamSynchronize(st), "sync");
+  std::vector<double> out(masks);
+  for (int m2 = 0; m2 < masks; ++m2) {
+    double e = 0, r = 0;
+    for (int i = 0; i < kRedBlocks; ++i) {
+      e = std::max(e, h[(static_cast<size_t>(m2) * kRedBlocks + i) * 2]);
+      r = std::max(r, h[(static_cast<size_t>(m2) * kRedBlocks + i) * 2 + 1]);
+    }
+    out[m2] = r > 0 ? e / r : 0.0;
+  }
+  return out;
+}
+
 }  // namespace huv
 
 // ------------------------------------------------------------ optimizer
@@ -456,7 +580,8 @@ struct DevVec {
 }  // namespace
 
 void Engine::ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int masks, float* theta, const float* target,
-                          double* final_cost, int* iterations, double* history, cudaStream_t st) {
+                          double* final_cost, int* iterations, double* history, cudaStream_t st, Surrogate* sur,
+                          int judge_every, double error_bound, SurrogateReport* report) {
   using namespace huv_dev;
   const size_t npix = static_cast<size_t>(n) * n;
   const size_t blk = sizeof(float) * npix;
@@ -520,8 +645,12 @@ void Engine::ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int mas
     scatter_blocks<<<dim3(256, c), threads, 0, st>>>(idx.as<int>(), src, npix, dst);
     prof.launches += 1;
   };
+  bool use_sur = sur != nullptr;
   auto eval = [&](const float* th, const float* tg, int count, float* g) {
-    ilt_eval(p, count, th, tg, g, cost_d.as<double>(), st);
+    if (use_sur)
+      ilt_eval_surrogate(sur, p, count, th, tg, g, cost_d.as<double>(), st);
+    else
+      ilt_eval(p, count, th, tg, g, cost_d.as<double>(), st);
     std::vector<double> h(count);
     fetch(cost_d, h.data(), sizeof(double) * count);
     return h;
@@ -541,7 +670,39 @@ void Engine::ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int mas
     std::vector<int> act;
     for (int m = 0; m < masks; ++m)
       if (!done[m]) act.push_back(m);
+    if (use_sur && judge_every > 0 && ((it > 0 && it % judge_every == 0) || act.empty())) {
+      // Exact SOCS re-images every mask (also when the surrogate run has
+      // stopped) and judges the surrogate; past the bound it takes over for
+      // all masks, stopped ones included.
+      act = all;
+      const int ac0 = masks;
+      gaxpby(act, ones(ac0, 1.f), ones(ac0, 0.f), theta, nullptr, trial.as<float>());
+      const std::vector<double> err = surrogate_error(sur, p, ac0, trial.as<float>(), st);
+      const double worst = *std::max_element(err.begin(), err.end());
+      if (report) report->judge_errors.push_back(worst);
+      if (worst > error_bound) {
+        // Takeover: exact costs and gradients from here on.
+        use_sur = false;
+        if (report) report->takeover_iteration = it;
+        gaxpby(act, ones(ac0, 1.f), ones(ac0, 0.f), target, nullptr, tgt.as<float>());
+        const std::vector<double> ce = eval(trial.as<float>(), tgt.as<float>(), ac0, gnew.as<float>());
+        scatter(act, gnew.as<float>(), grad.as<float>());
+        gaxpby(act, ones(ac0, -1.f), ones(ac0, 0.f), grad.as<float>(), nullptr, gnew.as<float>());
+        scatter(act, gnew.as<float>(), dir.as<float>());
+        for (int j = 0; j < ac0; ++j) {
+          cost[act[j]] = ce[j];
+          small[act[j]] = 0;
+          done[act[j]] = 0;
+        }
+      }
+      if (use_sur) {
+        act.clear();
+        for (int m = 0; m < masks; ++m)
+          if (!done[m]) act.push_back(m);
+      }
+    }
     if (act.empty()) break;
+    if (report) (use_sur ? report->surrogate_iterations : report->exact_iterations) += 1;
     std::vector<double> acc_cost(masks, 0.0), acc_s(masks, 0.0);
     std::vector<char> accepted(masks, 0);
     std::vector<int> attempt_set = act;
@@ -649,6 +810,12 @@ void Engine::ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int mas
       small[m] = rel < tol ? small[m] + 1 : 0;
       if (small[m] >= 3 || cost[m] == 0.0) done[m] = 1;
     }
+  }
+  if (sur && use_sur) {
+    // Report exact costs at the final masks.
+    use_sur = false;
+    const std::vector<double> ce = eval(theta, target, masks, nullptr);
+    for (int m = 0; m < masks; ++m) cost[m] = ce[m];
   }
   for (int m = 0; m < masks; ++m) {
     if (final_cost) final_cost[m] = cost[m];

@@ -95,6 +95,24 @@ struct Prof {
   }
 };
 
+// A learned image model usable inside ILT in place of the exact SOCS image.
+struct Surrogate {
+  virtual ~Surrogate() = default;
+  virtual int grid() const = 0;
+  // img[b] = model(t[b]) for B maps of grid x grid.
+  virtual void forward(int B, const float* t, float* img, cudaStream_t st) = 0;
+  // dt[b] = d sum(dout . model(t)) / dt.
+  virtual void input_grad(int B, const float* t, const float* dout, float* dt, cudaStream_t st) = 0;
+};
+
+// Outcome of a surrogate-assisted ILT run.
+struct SurrogateReport {
+  int surrogate_iterations = 0;
+  int exact_iterations = 0;
+  int takeover_iteration = -1;       // iteration at which exact SOCS took over (-1: never)
+  std::vector<double> judge_errors;  // max relative image error at each judge
+};
+
 struct CacheEntry {
   double z = 0;
   std::shared_ptr<KernelSet> ks;
@@ -130,7 +148,15 @@ struct Engine {
   void ilt_eval(const huv_ilt_params& p, int masks, const float* theta, const float* target, float* grad,
                 double* cost_dev, cudaStream_t st);
   void ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int masks, float* theta, const float* target,
-                    double* final_cost, int* iterations, double* history, cudaStream_t st);
+                    double* final_cost, int* iterations, double* history, cudaStream_t st,
+                    Surrogate* sur = nullptr, int judge_every = 5, double error_bound = 0.05,
+                    SurrogateReport* report = nullptr);
+  // Cost (and gradient) with the image from `sur` instead of SOCS.
+  void ilt_eval_surrogate(Surrogate* sur, const huv_ilt_params& p, int masks, const float* theta,
+                          const float* target, float* grad, double* cost_dev, cudaStream_t st);
+  // Max relative image error of the surrogate against SOCS, per mask (host).
+  std::vector<double> surrogate_error(Surrogate* sur, const huv_ilt_params& p, int masks, const float* theta,
+                                      cudaStream_t st);
   // Device error flag written by bounded waits that gave up (0 = none).
   int read_device_error();
 

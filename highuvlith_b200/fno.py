@@ -20,11 +20,14 @@ class FnoSurrogate:
         h = C.c_void_p()
         L.check(L.lib().huv_fno_create(grid, width, modes, layers, proj, seed, device, C.byref(h)))
         self._h = h
+        self._destroy = L.lib().huv_fno_destroy
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            L.lib().huv_fno_destroy(h)
+        # The destroy function is bound at construction: at interpreter exit
+        # module globals may already be gone.
+        h, destroy = getattr(self, "_h", None), getattr(self, "_destroy", None)
+        if h and destroy is not None:
+            destroy(h)
             self._h = None
 
     @property

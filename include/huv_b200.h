@@ -234,6 +234,27 @@ huv_status huv_ilt_optimize(void* engine, const huv_ilt_params* params, const hu
                             float* theta, const float* target, double* final_cost, int32_t* iterations,
                             double* history, void* stream);
 
+/* Surrogate-assisted ILT: no reference counterpart (the reference's
+ * optimizer, run_stage in ilt.rs:755-866, images every iterate with SOCS).
+ * Costs and gradients come from an FNO image model (huv_fno_create, grid equal
+ * to the engine's); every judge_every iterations exact SOCS re-images all
+ * masks and, when the largest relative image error max|I_fno - I_socs| /
+ * max|I_socs| exceeds error_bound, SOCS takes over for the rest of the run.
+ * final_cost is always the exact SOCS cost. */
+typedef struct {
+  int32_t judge_every;         /* in: iterations between exact judges (5) */
+  double error_bound;          /* in: relative image error that triggers takeover */
+  int32_t surrogate_iterations;/* out: iterations costed by the surrogate */
+  int32_t exact_iterations;    /* out: iterations costed by SOCS */
+  int32_t takeover_iteration;  /* out: iteration SOCS took over at, -1 if never */
+  int32_t n_judges;            /* out: judges run (first 64 errors kept) */
+  double judge_errors[64];     /* out: worst relative error at each judge */
+} huv_surrogate_ilt;
+
+huv_status huv_ilt_optimize_surrogate(void* engine, void* fno, const huv_ilt_params* params, const huv_ilt_opt* opt,
+                                      int32_t n_masks, float* theta, const float* target, huv_surrogate_ilt* sur,
+                                      double* final_cost, int32_t* iterations, double* history, void* stream);
+
 /* Fourier-neural-operator surrogate of the image (no counterpart in the
  * reference).  Maps a transmittance map (grid x grid floats, [y, x]) to the
  * normalised aerial image.  Width 64, `modes` x `modes` retained Fourier modes
