@@ -49,53 +49,138 @@ __global__ void fno_lift(const float* __restrict__ a, int S, int C, const float*
   }
 }
 
+// ------------------------------------------------------------ register tiles
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+// acc[p][q] += a[p] w[q]
+__device__ __forceinline__ void fma44(float (&acc)[4][4], float4 a, float4 w) {
+  const float av[4] = {a.x, a.y, a.z, a.w}, wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[p][q] = fmaf(av[p], wv[q], acc[p][q]);
+}
+__device__ __forceinline__ void st_bf16x4(__nv_bfloat16* p, float a, float b, float c, float d) {
+  __nv_bfloat162 lo = __floats2bfloat162_rn(a, b), hi = __floats2bfloat162_rn(c, d);
+  uint2 u;
+  u.x = *reinterpret_cast<uint32_t*>(&lo);
+  u.y = *reinterpret_cast<uint32_t*>(&hi);
+  *reinterpret_cast<uint2*>(p) = u;
+}
+
 // ------------------------------------------------------------ DFT along x
-// out[b][y][kx][c] (complex) = sum_x in[b][y][x][c] e^{-2 pi i kx x / S}, kx < m.
-// grid: (S, B); block: C * ceil(...) threads, each (kx, c) pair strided.
+// out[r][kx][c] (complex) = sum_x in[r][x][c] e^{-2 pi i kx x / S} for rows r
+// (= (b, y)), kx < m <= 16, C = 64.  Rows are grid-strided; x runs in chunks
+// of up to 128 split over four thread groups; thread (kg, cg) of a group owns
+// kx 4kg..4kg+3 x c 4cg..4cg+3 (complex), the groups are summed at the end.
+// Dynamic shared memory: 48 KiB.
 template <typename T>
-__global__ void fno_dft_x(const T* __restrict__ in, int S, int C, int m, const float2* __restrict__ twx,
-                          float2* __restrict__ out) {
-  extern __shared__ float srow[];  // [S][C]
-  const int y = blockIdx.x, b = blockIdx.y;
-  const size_t row = (static_cast<size_t>(b) * S + y) * S * C;
-  for (int t = threadIdx.x; t < S * C; t += blockDim.x) srow[t] = ld(in, row + t);
-  __syncthreads();
-  for (int t = threadIdx.x; t < m * C; t += blockDim.x) {
-    const int kx = t / C, c = t - kx * C;
-    float re = 0.f, im = 0.f;
-    const float2* tw = twx + static_cast<size_t>(kx) * S;  // e^{-2 pi i kx x / S}
-    for (int x = 0; x < S; ++x) {
-      const float v = srow[x * C + c];
-      const float2 w = __ldg(tw + x);
-      re += v * w.x;
-      im += v * w.y;
+__global__ void __launch_bounds__(256) fno_dft_x(const T* __restrict__ in, int S, int m,
+                                                  const float2* __restrict__ twx, float2* __restrict__ out,
+                                                  int rows) {
+  constexpr int C = 64, XC = 128;
+  extern __shared__ __align__(16) float dsm[];
+  float* sIn = dsm;                                        // [XC][C]
+  float2* sTw = reinterpret_cast<float2*>(sIn + XC * C);   // [16][XC]
+  float2* red = reinterpret_cast<float2*>(sIn);            // [4][16][C], aliases sIn
+  const int t = threadIdx.x;
+  const int grp = t >> 6, kg = t & 3, cg = (t >> 2) & 15;
+  const int xc = min(XC, S), xs = xc >> 2;
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    float acc[4][4][2];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[q][c][0] = acc[q][c][1] = 0.f;
+    const size_t row = static_cast<size_t>(r) * S * C;
+    for (int x0 = 0; x0 < S; x0 += xc) {
+      __syncthreads();
+      for (int e = t; e < xc * C; e += 256) sIn[e] = ld(in, row + static_cast<size_t>(x0) * C + e);
+      for (int e = t; e < 16 * xc; e += 256) {
+        const int kx = e / xc, x = e - kx * xc;
+        sTw[e] = kx < m ? __ldg(twx + static_cast<size_t>(kx) * S + x0 + x) : make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+      for (int xx = 0; xx < xs; ++xx) {
+        const int x = grp * xs + xx;
+        const float4 a = ld4(sIn + x * C + cg * 4);
+        const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float2 w = sTw[(kg * 4 + q) * xc + x];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            acc[q][c][0] = fmaf(av[c], w.x, acc[q][c][0]);
+            acc[q][c][1] = fmaf(av[c], w.y, acc[q][c][1]);
+          }
+        }
+      }
     }
-    out[((static_cast<size_t>(b) * S + y) * m + kx) * C + c] = make_float2(re, im);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        red[(grp * 16 + kg * 4 + q) * C + cg * 4 + c] = make_float2(acc[q][c][0], acc[q][c][1]);
+    __syncthreads();
+    for (int e = t; e < m * C; e += 256) {
+      float2 sum = red[e];
+#pragma unroll
+      for (int g = 1; g < 4; ++g) {
+        const float2 v = red[g * 16 * C + e];
+        sum.x += v.x;
+        sum.y += v.y;
+      }
+      out[static_cast<size_t>(r) * m * C + e] = sum;
+    }
   }
 }
 
 // ------------------------------------------------------------ DFT along y
-// Forward (to modes): out[b][j][kx][c] = sum_y in[b][y][kx][c] e^{-2 pi i ky_j y / S}.
-// Inverse (from modes): out[b][y][kx][c] = sum_j in[b][j][kx][c] e^{+2 pi i ky_j y / S}.
-// twy[j][y] = e^{-2 pi i ky_j y / S}; grid: (rows_out, B).
+// Forward (to modes): out[b][j][col] = sum_y in[b][y][col] twy[j][y], col =
+// (kx, c) over m * C columns; grid (ceil(mC / 64), B), thread (col, j group
+// of 8), J = 2m <= 32.
+// Inverse (from modes): out[b][y][col] = sum_j in[b][j][col] conj(twy[j][y]);
+// grid (S, B).  twy[j][y] = e^{-2 pi i ky_j y / S}.
 template <bool INVERSE>
-__global__ void fno_dft_y(const float2* __restrict__ in, int S, int C, int m, const float2* __restrict__ twy,
-                          float2* __restrict__ out) {
-  const int r = blockIdx.x, b = blockIdx.y;
-  const int J = 2 * m;
-  const int rows_in = INVERSE ? J : S;
-  const int rows_out = INVERSE ? S : J;
-  (void)rows_out;
-  for (int t = threadIdx.x; t < m * C; t += blockDim.x) {
-    float re = 0.f, im = 0.f;
-    for (int q = 0; q < rows_in; ++q) {
-      const float2 v = in[((static_cast<size_t>(b) * rows_in + q) * m) * C + t];
-      float2 w = INVERSE ? __ldg(twy + static_cast<size_t>(q) * S + r) : __ldg(twy + static_cast<size_t>(r) * S + q);
-      if (INVERSE) w.y = -w.y;
-      re += v.x * w.x - v.y * w.y;
-      im += v.x * w.y + v.y * w.x;
+__global__ void __launch_bounds__(256) fno_dft_y(const float2* __restrict__ in, int S, int C, int m,
+                                                  const float2* __restrict__ twy, float2* __restrict__ out) {
+  const int J = 2 * m, mC = m * C;
+  if (!INVERSE) {
+    const int b = blockIdx.y;
+    const int col = blockIdx.x * 64 + (threadIdx.x & 63);
+    const int j0 = (threadIdx.x >> 6) * 8;
+    if (col >= mC || j0 >= J) return;
+    float2 acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = make_float2(0.f, 0.f);
+    const float2* src = in + static_cast<size_t>(b) * S * mC + col;
+    for (int y = 0; y < S; ++y) {
+      const float2 v = src[static_cast<size_t>(y) * mC];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        if (j0 + q < J) {
+          const float2 w = __ldg(twy + static_cast<size_t>(j0 + q) * S + y);
+          acc[q].x = fmaf(v.x, w.x, fmaf(-v.y, w.y, acc[q].x));
+          acc[q].y = fmaf(v.x, w.y, fmaf(v.y, w.x, acc[q].y));
+        }
+      }
     }
-    out[((static_cast<size_t>(b) * (INVERSE ? S : J) + r) * m) * C + t] = make_float2(re, im);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (j0 + q < J) out[(static_cast<size_t>(b) * J + j0 + q) * mC + col] = acc[q];
+  } else {
+    const int r = blockIdx.x, b = blockIdx.y;
+    for (int t = threadIdx.x; t < mC; t += blockDim.x) {
+      float re = 0.f, im = 0.f;
+      for (int q = 0; q < J; ++q) {
+        const float2 v = in[(static_cast<size_t>(b) * J + q) * mC + t];
+        float2 w = __ldg(twy + static_cast<size_t>(q) * S + r);
+        w.y = -w.y;
+        re += v.x * w.x - v.y * w.y;
+        im += v.x * w.y + v.y * w.x;
+      }
+      out[(static_cast<size_t>(b) * S + r) * mC + t] = make_float2(re, im);
+    }
   }
 }
 
@@ -159,114 +244,189 @@ __global__ void fno_mix_bwd(const float2* __restrict__ X, const float2* __restri
 }
 
 // ------------------------------------------------------------ layer output
-// z = S^-2 Re sum_kx w_kx Z[y][kx][o] e^{+i th} + sum_i W[o][i] v[i] + b[o];
-// v_next = GELU(z) (or z for the last layer).  grid: (S, B), block 256.
-__global__ void fno_layer_out(const float2* __restrict__ Z, const __nv_bfloat16* __restrict__ v,
-                              const float* __restrict__ W, const float* __restrict__ bias, int S, int C, int m,
-                              const float2* __restrict__ twx, int act, __nv_bfloat16* __restrict__ zsave,
-                              __nv_bfloat16* __restrict__ vnext) {
-  extern __shared__ float sm[];
-  float* sW = sm;                                           // [C][C]
-  float2* sZ = reinterpret_cast<float2*>(sW + C * C);       // [m][C]
-  const int y = blockIdx.x, b = blockIdx.y;
-  for (int t = threadIdx.x; t < C * C; t += blockDim.x) sW[t] = W[t];
-  const float2* Zr = Z + (static_cast<size_t>(b) * S + y) * m * C;
+// z = S^-2 Re sum_kx w_kx Z[r][kx][o] e^{+i th} + sum_i W[o][i] v[i] + b[o],
+// th = 2 pi kx x / S; v_next = GELU(z) (or z for the last layer).  Rows r =
+// (b, y) grid-strided; pixels in tiles of 64; thread (pg, og) owns pixels
+// 4pg..4pg+3 x outputs 4og..4og+3.  The spectral term is a K = 2m
+// contraction of cos/sin rows against (w Re Z, -w Im Z).
+// Dynamic shared memory: (2 * 64 * 68 + 2m * (64 + 68)) floats.
+__global__ void __launch_bounds__(256) fno_layer_out(const float2* __restrict__ Z, const __nv_bfloat16* __restrict__ v,
+                                                      const float* __restrict__ W, const float* __restrict__ bias,
+                                                      int S, int m, const float2* __restrict__ twx, int act,
+                                                      __nv_bfloat16* __restrict__ zsave,
+                                                      __nv_bfloat16* __restrict__ vnext, int rows) {
+  constexpr int C = 64, XT = 64, LD = 68;
+  extern __shared__ __align__(16) float dsm[];
+  float* sWT = dsm;             // [i][LD]: W transposed
+  float* sV = sWT + C * LD;     // [i][LD]: v tile transposed
+  float* sZ = sV + C * LD;      // [2m][C]
+  float* sT = sZ + 2 * m * C;   // [2m][LD]
+  const int t = threadIdx.x, og = t & 15, pg = t >> 4;
+  for (int e = t; e < C * C; e += 256) sWT[(e & 63) * LD + (e >> 6)] = W[e];
+  float b4[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) b4[q] = bias[og * 4 + q];
   const float inv = 1.f / (static_cast<float>(S) * S);
-  for (int t = threadIdx.x; t < m * C; t += blockDim.x) {
-    const float w = (t / C) == 0 ? inv : 2.f * inv;
-    sZ[t] = make_float2(Zr[t].x * w, Zr[t].y * w);
-  }
-  __syncthreads();
-  const size_t row = (static_cast<size_t>(b) * S + y) * S * C;
-  for (int t = threadIdx.x; t < S * C; t += blockDim.x) {
-    const int x = t / C, o = t - x * C;
-    float acc = bias[o];
-    for (int kx = 0; kx < m; ++kx) {
-      const float2 w = __ldg(twx + static_cast<size_t>(kx) * S + x);  // e^{-i th}: use conj
-      const float2 z = sZ[kx * C + o];
-      acc += z.x * w.x + z.y * w.y;  // Re(z e^{+i th})
+  const int xt = min(XT, S);
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    __syncthreads();
+    const float2* Zr = Z + static_cast<size_t>(r) * m * C;
+    for (int e = t; e < m * C; e += 256) {
+      const int kx = e / C, o = e - kx * C;
+      const float w = (kx == 0 ? 1.f : 2.f) * inv;
+      const float2 zz = Zr[e];
+      sZ[(2 * kx) * C + o] = w * zz.x;
+      sZ[(2 * kx + 1) * C + o] = -w * zz.y;
     }
-    const __nv_bfloat16* vp = v + row + static_cast<size_t>(x) * C;
-    const float* wr = sW + o * C;
-    for (int i = 0; i < C; ++i) acc += wr[i] * __bfloat162float(vp[i]);
-    zsave[row + t] = __float2bfloat16_rn(acc);
-    vnext[row + t] = __float2bfloat16_rn(act ? gelu(acc) : acc);
+    const size_t row = static_cast<size_t>(r) * S * C;
+    for (int x0 = 0; x0 < S; x0 += xt) {
+      __syncthreads();
+      for (int e = t; e < xt * C; e += 256)
+        sV[(e & 63) * LD + (e >> 6)] = __bfloat162float(v[row + static_cast<size_t>(x0) * C + e]);
+      for (int e = t; e < 2 * m * xt; e += 256) {
+        const int kk = e / xt, px = e - kk * xt;
+        const float2 w = __ldg(twx + static_cast<size_t>(kk >> 1) * S + x0 + px);  // (cos, -sin)
+        sT[kk * LD + px] = (kk & 1) ? -w.y : w.x;
+      }
+      __syncthreads();
+      if (pg * 4 < xt) {
+        float acc[4][4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[p][q] = b4[q];
+#pragma unroll 8
+        for (int i = 0; i < C; ++i) fma44(acc, ld4(sV + i * LD + pg * 4), ld4(sWT + i * LD + og * 4));
+        for (int kk = 0; kk < 2 * m; ++kk) fma44(acc, ld4(sT + kk * LD + pg * 4), ld4(sZ + kk * C + og * 4));
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          const size_t g = row + static_cast<size_t>(x0 + pg * 4 + p) * C + og * 4;
+          st_bf16x4(zsave + g, acc[p][0], acc[p][1], acc[p][2], acc[p][3]);
+          if (act)
+            st_bf16x4(vnext + g, gelu(acc[p][0]), gelu(acc[p][1]), gelu(acc[p][2]), gelu(acc[p][3]));
+          else
+            st_bf16x4(vnext + g, acc[p][0], acc[p][1], acc[p][2], acc[p][3]);
+        }
+      }
+    }
   }
 }
 
-// Backward of the layer output: dz = dvnext * GELU'(z) (or dvnext); writes dz
-// (f32), dv = W^T dz (f32, overwriting dv), dW += dz v^T, db += dz.
-// grid: (S, B), block 256; the row is walked in tiles of 64 pixels with the
-// weight-gradient partials in registers (C = 64: 16 (o, i) pairs per thread).
+// Backward of the layer output: dz = dvnext * GELU'(z) (or dvnext) -> dz
+// (f32); dv = W^T dz (f32, overwriting dv); dW += dz^T v; db += sum dz.  Rows
+// grid-strided, tiles of 64 pixels; weight-gradient partials stay in
+// registers (thread (og, ig) owns 4 x 4 of dW) until one atomic add per block.
+// Dynamic shared memory: (64 * 64 + 3 * 64 * 68) floats.
 __global__ void __launch_bounds__(256) fno_layer_bwd(const float* __restrict__ dvnext,
                                                       const __nv_bfloat16* __restrict__ z,
                                                       const __nv_bfloat16* __restrict__ v,
                                                       const float* __restrict__ W, int S, int act,
                                                       float* __restrict__ dz, float* __restrict__ dv,
-                                                      float* __restrict__ dW, float* __restrict__ db) {
-  constexpr int C = 64, XT = 64;
-  __shared__ float sW[C * C];
-  __shared__ float sdz[XT * C];
-  __shared__ float sv[XT * C];
-  const int y = blockIdx.x, b = blockIdx.y;
-  const size_t row = (static_cast<size_t>(b) * S + y) * S * C;
-  for (int t = threadIdx.x; t < C * C; t += blockDim.x) sW[t] = W[t];
-  float gw[16], gb = 0.f;
+                                                      float* __restrict__ dW, float* __restrict__ db, int rows) {
+  constexpr int C = 64, XT = 64, LD = 68;
+  extern __shared__ __align__(16) float dsm[];
+  float* sW = dsm;             // [o][C]
+  float* sD = sW + C * C;      // [px][LD]  dz
+  float* sDT = sD + XT * LD;   // [o][LD]   dz transposed
+  float* sV = sDT + C * LD;    // [px][LD]
+  const int t = threadIdx.x, hi = t >> 4, lo = t & 15;
+  for (int e = t; e < C * C; e += 256) sW[e] = W[e];
+  float gw[4][4], gb = 0.f;
 #pragma unroll
-  for (int q = 0; q < 16; ++q) gw[q] = 0.f;
-  const int xt = min(XT, S);  // S is a power of two, so xt divides S
-  for (int x0 = 0; x0 < S; x0 += xt) {
-    __syncthreads();
-    for (int t = threadIdx.x; t < xt * C; t += blockDim.x) {
-      const size_t g = row + static_cast<size_t>(x0) * C + t;
-      const float gv = dvnext[g];
-      const float d = act ? gv * gelu_grad(__bfloat162float(z[g])) : gv;
-      sdz[t] = d;
-      dz[g] = d;
-      sv[t] = __bfloat162float(v[g]);
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < xt * C; t += blockDim.x) {
-      const int x = t / C, i = t - x * C;
-      float acc = 0.f;
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) gw[p][q] = 0.f;
+  const int xt = min(XT, S);
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    const size_t row = static_cast<size_t>(r) * S * C;
+    for (int x0 = 0; x0 < S; x0 += xt) {
+      __syncthreads();
+      for (int e = t; e < xt * C; e += 256) {
+        const int px = e >> 6, o = e & 63;
+        const size_t g = row + static_cast<size_t>(x0) * C + e;
+        const float gv = dvnext[g];
+        const float d = act ? gv * gelu_grad(__bfloat162float(z[g])) : gv;
+        dz[g] = d;
+        sD[px * LD + o] = d;
+        sDT[o * LD + px] = d;
+        sV[px * LD + o] = __bfloat162float(v[g]);
+      }
+      __syncthreads();
+      if (hi * 4 < xt) {
+        float acc[4][4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[p][q] = 0.f;
 #pragma unroll 8
-      for (int o = 0; o < C; ++o) acc += sW[o * C + i] * sdz[x * C + o];
-      dv[row + static_cast<size_t>(x0) * C + t] = acc;
-    }
+        for (int o = 0; o < C; ++o) fma44(acc, ld4(sDT + o * LD + hi * 4), ld4(sW + o * C + lo * 4));
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int pr = threadIdx.x + q * 256;  // (o, i) pair
-      const int o = pr / C, i = pr - o * C;
-      float acc = 0.f;
-      for (int x = 0; x < xt; ++x) acc += sdz[x * C + o] * sv[x * C + i];
-      gw[q] += acc;
+        for (int p = 0; p < 4; ++p)
+          *reinterpret_cast<float4*>(dv + row + static_cast<size_t>(x0 + hi * 4 + p) * C + lo * 4) =
+              make_float4(acc[p][0], acc[p][1], acc[p][2], acc[p][3]);
+      }
+#pragma unroll 4
+      for (int px = 0; px < xt; ++px) fma44(gw, ld4(sD + px * LD + hi * 4), ld4(sV + px * LD + lo * 4));
+      if (t < C)
+        for (int px = 0; px < xt; ++px) gb += sD[px * LD + t];
     }
-    if (threadIdx.x < C)
-      for (int x = 0; x < xt; ++x) gb += sdz[x * C + threadIdx.x];
   }
 #pragma unroll
-  for (int q = 0; q < 16; ++q) atomicAdd(dW + threadIdx.x + q * 256, gw[q]);
-  if (threadIdx.x < C) atomicAdd(db + threadIdx.x, gb);
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) atomicAdd(dW + (hi * 4 + p) * C + lo * 4 + q, gw[p][q]);
+  if (t < C) atomicAdd(db + t, gb);
 }
 
-// dv[b][y][x][c] += Re sum_kx Z[b][y][kx][c] e^{+2 pi i kx x / S}  (weight 1).
-__global__ void fno_spec_to_dv(const float2* __restrict__ Z, int S, int C, int m, const float2* __restrict__ twx,
-                               float* __restrict__ dv) {
-  extern __shared__ float2 sZ[];
-  const int y = blockIdx.x, b = blockIdx.y;
-  const float2* Zr = Z + (static_cast<size_t>(b) * S + y) * m * C;
-  for (int t = threadIdx.x; t < m * C; t += blockDim.x) sZ[t] = Zr[t];
-  __syncthreads();
-  const size_t row = (static_cast<size_t>(b) * S + y) * S * C;
-  for (int t = threadIdx.x; t < S * C; t += blockDim.x) {
-    const int x = t / C, c = t - x * C;
-    float acc = 0.f;
-    for (int kx = 0; kx < m; ++kx) {
-      const float2 w = __ldg(twx + static_cast<size_t>(kx) * S + x);
-      const float2 z = sZ[kx * C + c];
-      acc += z.x * w.x + z.y * w.y;
+// dv[r][x][c] += Re sum_kx Z[r][kx][c] e^{+2 pi i kx x / S} (weight 1); rows
+// grid-strided, tiles of 64 pixels, thread (pg, cg) owns 4 x 4.
+// Dynamic shared memory: 2m * (64 + 68) floats.
+__global__ void __launch_bounds__(256) fno_spec_to_dv(const float2* __restrict__ Z, int S, int m,
+                                                       const float2* __restrict__ twx, float* __restrict__ dv,
+                                                       int rows) {
+  constexpr int C = 64, XT = 64, LD = 68;
+  extern __shared__ __align__(16) float dsm[];
+  float* sZ = dsm;              // [2m][C]
+  float* sT = sZ + 2 * m * C;   // [2m][LD]
+  const int t = threadIdx.x, cg = t & 15, pg = t >> 4;
+  const int xt = min(XT, S);
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    __syncthreads();
+    const float2* Zr = Z + static_cast<size_t>(r) * m * C;
+    for (int e = t; e < m * C; e += 256) {
+      const int kx = e / C, c = e - kx * C;
+      const float2 zz = Zr[e];
+      sZ[(2 * kx) * C + c] = zz.x;
+      sZ[(2 * kx + 1) * C + c] = -zz.y;
     }
-    dv[row + t] += acc;
+    const size_t row = static_cast<size_t>(r) * S * C;
+    for (int x0 = 0; x0 < S; x0 += xt) {
+      __syncthreads();
+      for (int e = t; e < 2 * m * xt; e += 256) {
+        const int kk = e / xt, px = e - kk * xt;
+        const float2 w = __ldg(twx + static_cast<size_t>(kk >> 1) * S + x0 + px);
+        sT[kk * LD + px] = (kk & 1) ? -w.y : w.x;
+      }
+      __syncthreads();
+      if (pg * 4 < xt) {
+        float acc[4][4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[p][q] = 0.f;
+        for (int kk = 0; kk < 2 * m; ++kk) fma44(acc, ld4(sT + kk * LD + pg * 4), ld4(sZ + kk * C + cg * 4));
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          float4* d = reinterpret_cast<float4*>(dv + row + static_cast<size_t>(x0 + pg * 4 + p) * C + cg * 4);
+          float4 cur = *d;
+          cur.x += acc[p][0];
+          cur.y += acc[p][1];
+          cur.z += acc[p][2];
+          cur.w += acc[p][3];
+          *d = cur;
+        }
+      }
+    }
   }
 }
 
@@ -283,108 +443,198 @@ __global__ void fno_scale_modes(float2* __restrict__ Y, int B, int J, int m, int
 }
 
 // ------------------------------------------------------------ projection
-// out[b][p] = sum_j Q2[j] GELU(sum_c Q1[j][c] v[p][c] + b1[j]) + b2.
-__global__ void fno_proj(const __nv_bfloat16* __restrict__ v, const float* __restrict__ Q1, const float* __restrict__ b1,
-                         const float* __restrict__ Q2, const float* __restrict__ b2, int C, int P, size_t npix,
-                         float* __restrict__ out) {
-  extern __shared__ float sm[];
-  float* sQ1 = sm;            // [P][C]
-  float* sb1 = sQ1 + P * C;   // [P]
-  float* sQ2 = sb1 + P;       // [P]
-  for (int t = threadIdx.x; t < P * C; t += blockDim.x) sQ1[t] = Q1[t];
-  for (int t = threadIdx.x; t < P; t += blockDim.x) {
-    sb1[t] = b1[t];
-    sQ2[t] = Q2[t];
+// out[p] = sum_j Q2[j] GELU(sum_c Q1[j][c] v[p][c] + b1[j]) + b2 (C = 64,
+// P = 128).  Tiles of 64 pixels grid-strided; thread (pg, jg) owns pixels
+// 4pg..4pg+3 x hidden units 8jg..8jg+7; the 16 j groups of a pixel quad sit
+// in adjacent lanes and are summed with shuffles.
+// Dynamic shared memory: (64 * 128 + 64 * 68) floats.
+__global__ void __launch_bounds__(256) fno_proj(const __nv_bfloat16* __restrict__ v, const float* __restrict__ Q1,
+                                                 const float* __restrict__ b1, const float* __restrict__ Q2,
+                                                 const float* __restrict__ b2, size_t npix, float* __restrict__ out) {
+  constexpr int C = 64, P = 128, PT = 64, LD = 68;
+  extern __shared__ __align__(16) float dsm[];
+  float* sQT = dsm;            // [c][P]
+  float* sVT = sQT + C * P;    // [c][LD]
+  const int t = threadIdx.x, jg = t & 15, pg = t >> 4;
+  for (int e = t; e < C * P; e += 256) sQT[e] = Q1[(e & (P - 1)) * C + (e >> 7)];
+  float bj[8], qj[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    bj[q] = b1[jg * 8 + q];
+    qj[q] = Q2[jg * 8 + q];
   }
-  __syncthreads();
-  for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < npix;
-       p += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    float vin[64];
-    for (int c = 0; c < C; ++c) vin[c] = __bfloat162float(v[p * C + c]);
-    float acc = b2[0];
-    for (int j = 0; j < P; ++j) {
-      float h = sb1[j];
-      const float* q = sQ1 + j * C;
-      for (int c = 0; c < C; ++c) h += q[c] * vin[c];
-      acc += sQ2[j] * gelu(h);
+  const float bias2 = b2[0];
+  const size_t tiles = (npix + PT - 1) / PT;
+  for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const size_t p0 = tile * PT;
+    __syncthreads();
+    for (int e = t; e < PT * C; e += 256) {
+      const int px = e >> 6, c = e & 63;
+      sVT[c * LD + px] = p0 + px < npix ? __bfloat162float(v[p0 * C + e]) : 0.f;
     }
-    out[p] = acc;
+    __syncthreads();
+    float h[4][8];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) h[p][q] = bj[q];
+#pragma unroll 4
+    for (int c = 0; c < C; ++c) {
+      const float4 a = ld4(sVT + c * LD + pg * 4);
+      const float4 w0 = ld4(sQT + c * P + jg * 8), w1 = ld4(sQT + c * P + jg * 8 + 4);
+      const float av[4] = {a.x, a.y, a.z, a.w};
+      const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[p][q] = fmaf(av[p], wv[q], h[p][q]);
+    }
+    float part[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      float sum = 0.f;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sum = fmaf(qj[q], gelu(h[p][q]), sum);
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      part[p] = sum;
+    }
+    if (jg == 0)
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+        if (p0 + pg * 4 + p < npix) out[p0 + pg * 4 + p] = part[p] + bias2;
   }
 }
 
 // Backward of the projection given dout: dv (f32) and dQ1, db1, dQ2, db2.
-// Tiles of 64 pixels; C = 64, P = 128; block 256.  Partials in registers.
+// Per tile of 64 pixels: the hidden layer is recomputed (thread (pg, jg) as
+// in the forward), dh = dout Q2 GELU'(h) is kept in shared memory in both
+// orientations, dv = Q1^T dh (thread (pg, cg), 4 x 4) and dQ1 += dh^T v
+// (thread (jg8, cg), 8 x 4 in registers across tiles).
+// Dynamic shared memory: (2 * 64 * 128 + 2 * 64 * 68 + 64 * 132 + 128 * 68 + 64) floats.
 __global__ void __launch_bounds__(256) fno_proj_bwd(const __nv_bfloat16* __restrict__ v,
                                                      const float* __restrict__ Q1, const float* __restrict__ b1,
                                                      const float* __restrict__ Q2, size_t npix,
                                                      const float* __restrict__ dout, float* __restrict__ dv,
                                                      float* __restrict__ dQ1, float* __restrict__ db1,
                                                      float* __restrict__ dQ2, float* __restrict__ db2) {
-  constexpr int C = 64, P = 128, PT = 64;
-  extern __shared__ float sm[];
-  float* sQ1 = sm;              // [P][C]
-  float* sv = sQ1 + P * C;      // [PT][C]
-  float* sdh = sv + PT * C;     // [PT][P]
-  float* sgh = sdh + PT * P;    // [PT][P]  dout * gelu(h)
-  float* sd = sgh + PT * P;     // [PT]
-  for (int t = threadIdx.x; t < P * C; t += blockDim.x) sQ1[t] = Q1[t];
-  float gq1[32], gbias1 = 0.f, gq2 = 0.f, gb2 = 0.f;
+  constexpr int C = 64, P = 128, PT = 64, LD = 68, LDP = 132;
+  extern __shared__ __align__(16) float dsm[];
+  float* sQT = dsm;              // [c][P]
+  float* sQ = sQT + C * P;       // [j][C]
+  float* sVT = sQ + P * C;       // [c][LD]
+  float* sV = sVT + C * LD;      // [px][LD]
+  float* sDh = sV + PT * LD;     // [px][LDP]
+  float* sDhT = sDh + PT * LDP;  // [j][LD]
+  float* sd = sDhT + P * LD;     // [PT]
+  const int t = threadIdx.x, hi = t >> 4, lo = t & 15;
+  for (int e = t; e < C * P; e += 256) {
+    sQT[e] = Q1[(e & (P - 1)) * C + (e >> 7)];
+    sQ[e] = Q1[e];
+  }
+  float bj[8], qj[8], gb1[8], gq2[8], gq1[8][4], gd2 = 0.f;
 #pragma unroll
-  for (int q = 0; q < 32; ++q) gq1[q] = 0.f;
+  for (int q = 0; q < 8; ++q) {
+    bj[q] = b1[lo * 8 + q];
+    qj[q] = Q2[lo * 8 + q];
+    gb1[q] = gq2[q] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) gq1[q][c] = 0.f;
+  }
   const size_t tiles = (npix + PT - 1) / PT;
   for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const size_t p0 = tile * PT;
-    const int np = static_cast<int>(min(static_cast<size_t>(PT), npix - p0));
     __syncthreads();
-    for (int t = threadIdx.x; t < PT * C; t += blockDim.x) {
-      const int pl = t / C;
-      sv[t] = pl < np ? __bfloat162float(v[(p0 + pl) * C + (t - pl * C)]) : 0.f;
+    for (int e = t; e < PT * C; e += 256) {
+      const int px = e >> 6, c = e & 63;
+      const float x = p0 + px < npix ? __bfloat162float(v[p0 * C + e]) : 0.f;
+      sVT[c * LD + px] = x;
+      sV[px * LD + c] = x;
     }
-    for (int t = threadIdx.x; t < PT; t += blockDim.x) sd[t] = t < np ? dout[p0 + t] : 0.f;
+    for (int e = t; e < PT; e += 256) sd[e] = p0 + e < npix ? dout[p0 + e] : 0.f;
     __syncthreads();
-    for (int t = threadIdx.x; t < PT * P; t += blockDim.x) {
-      const int pl = t / P, j = t - pl * P;
-      float h = b1[j];
-      const float* q = sQ1 + j * C;
-      const float* vv = sv + pl * C;
-#pragma unroll 8
-      for (int c = 0; c < C; ++c) h += q[c] * vv[c];
-      const float d = sd[pl];
-      sdh[t] = d * Q2[j] * gelu_grad(h);
-      sgh[t] = d * gelu(h);
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < PT * C; t += blockDim.x) {
-      const int pl = t / C, c = t - pl * C;
-      if (pl >= np) continue;
-      float acc = 0.f;
-#pragma unroll 8
-      for (int j = 0; j < P; ++j) acc += sQ1[j * C + c] * sdh[pl * P + j];
-      dv[(p0 + pl) * C + c] = acc;
-    }
+    {
+      // hidden layer: thread (pg = hi, jg = lo)
+      float h[4][8];
 #pragma unroll
-    for (int q = 0; q < 32; ++q) {
-      const int pr = threadIdx.x + q * 256;  // (j, c)
-      const int j = pr / C, c = pr - j * C;
-      float acc = 0.f;
-      for (int pl = 0; pl < PT; ++pl) acc += sdh[pl * P + j] * sv[pl * C + c];
-      gq1[q] += acc;
-    }
-    if (threadIdx.x < P)
-      for (int pl = 0; pl < PT; ++pl) {
-        gbias1 += sdh[pl * P + threadIdx.x];
-        gq2 += sgh[pl * P + threadIdx.x];
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[p][q] = bj[q];
+#pragma unroll 4
+      for (int c = 0; c < C; ++c) {
+        const float4 a = ld4(sVT + c * LD + hi * 4);
+        const float4 w0 = ld4(sQT + c * P + lo * 8), w1 = ld4(sQT + c * P + lo * 8 + 4);
+        const float av[4] = {a.x, a.y, a.z, a.w};
+        const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 8; ++q) h[p][q] = fmaf(av[p], wv[q], h[p][q]);
       }
-    if (threadIdx.x == 0)
-      for (int pl = 0; pl < PT; ++pl) gb2 += sd[pl];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const int px = hi * 4 + p;
+        const float d = sd[px];
+        if (lo == 0) gd2 += d;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float hh = h[p][q];
+          const float dh = d * qj[q] * gelu_grad(hh);
+          gq2[q] = fmaf(d, gelu(hh), gq2[q]);
+          gb1[q] += dh;
+          sDh[px * LDP + lo * 8 + q] = dh;
+          sDhT[(lo * 8 + q) * LD + px] = dh;
+        }
+      }
+    }
+    __syncthreads();
+    {
+      // dv: thread (pg = hi, cg = lo)
+      float acc[4][4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = 0.f;
+#pragma unroll 8
+      for (int j = 0; j < P; ++j) fma44(acc, ld4(sDhT + j * LD + hi * 4), ld4(sQ + j * C + lo * 4));
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+        if (p0 + hi * 4 + p < npix)
+          *reinterpret_cast<float4*>(dv + (p0 + hi * 4 + p) * C + lo * 4) =
+              make_float4(acc[p][0], acc[p][1], acc[p][2], acc[p][3]);
+    }
+    // dQ1: thread (jg8 = hi, cg = lo)
+#pragma unroll 2
+    for (int px = 0; px < PT; ++px) {
+      const float4 a0 = ld4(sDh + px * LDP + hi * 8), a1 = ld4(sDh + px * LDP + hi * 8 + 4);
+      const float4 b = ld4(sV + px * LD + lo * 4);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) gq1[q][c] = fmaf(av[q], bv[c], gq1[q][c]);
+    }
   }
 #pragma unroll
-  for (int q = 0; q < 32; ++q) atomicAdd(dQ1 + threadIdx.x + q * 256, gq1[q]);
-  if (threadIdx.x < P) {
-    atomicAdd(db1 + threadIdx.x, gbias1);
-    atomicAdd(dQ2 + threadIdx.x, gq2);
+  for (int q = 0; q < 8; ++q)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) atomicAdd(dQ1 + (hi * 8 + q) * C + lo * 4 + c, gq1[q][c]);
+  // gb1, gq2 (thread (pg = hi, jg = lo)): lanes l and l ^ 16 share jg.
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    gb1[q] += __shfl_xor_sync(0xffffffffu, gb1[q], 16);
+    gq2[q] += __shfl_xor_sync(0xffffffffu, gq2[q], 16);
   }
-  if (threadIdx.x == 0) atomicAdd(db2, gb2);
+  gd2 += __shfl_xor_sync(0xffffffffu, gd2, 16);
+  if ((t & 31) < 16) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      atomicAdd(db1 + lo * 8 + q, gb1[q]);
+      atomicAdd(dQ2 + lo * 8 + q, gq2[q]);
+    }
+    if (lo == 0) atomicAdd(db2, gd2);
+  }
 }
 
 // Lift backward: dWl, dbl and the input gradient da = sum_c Wl[c][0] dv0[c].
@@ -556,6 +806,8 @@ struct Fno {
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_proj, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_proj_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_layer_out, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+      check_cuda(cudaFuncSetAttribute(huv_dev::fno_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
+      check_cuda(cudaFuncSetAttribute(huv_dev::fno_spec_to_dv, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
       attr = true;
     }
   }
@@ -623,22 +875,34 @@ struct Fno {
     B_cap = B;
   }
 
+  // Launch shapes and dynamic shared memory of the tiled kernels.
+  static constexpr size_t kDftXSmem = (128 * 64 + 16 * 128 * 2) * 4;
+  static constexpr size_t kProjSmem = (64 * 128 + 64 * 68) * 4;
+  static constexpr size_t kProjBwdSmem = (2 * 64 * 128 + 2 * 64 * 68 + 64 * 132 + 128 * 68 + 64) * 4;
+  static constexpr size_t kLayerBwdSmem = (64 * 64 + 3 * 64 * 68) * 4;
+  size_t layer_out_smem() const { return (2 * 64 * 68 + 2 * static_cast<size_t>(m) * (64 + 68)) * 4; }
+  size_t spec_smem() const { return (2 * static_cast<size_t>(m) * (64 + 68)) * 4; }
+  static unsigned pgrid(size_t pix) { return static_cast<unsigned>(std::min<size_t>((pix + 63) / 64, 296)); }
+
   // images[b][S][S] = FNO(masks[b]); activations kept for backward.
   void forward(int B, const float* masks, float* images, cudaStream_t st) {
     using namespace huv_dev;
     ensure(B);
     const size_t pix = static_cast<size_t>(B) * S * S;
+    const int rows = B * S;
+    const dim3 rgrid(std::min(rows, 4096));
+    const dim3 ygrid((m * C + 63) / 64, B);
     fno_lift<<<2048, 256, 0, st>>>(masks, S, C, par + oWl, par + obl, v[0], pix * C);
     for (int l = 0; l < L; ++l) {
-      fno_dft_x<__nv_bfloat16><<<dim3(S, B), 256, static_cast<size_t>(S) * C * 4, st>>>(v[l], S, C, m, twx, Xa);
-      fno_dft_y<false><<<dim3(J, B), 256, 0, st>>>(Xa, S, C, m, twy, Xl[l]);
+      fno_dft_x<__nv_bfloat16><<<rgrid, 256, kDftXSmem, st>>>(v[l], S, m, twx, Xa, rows);
+      fno_dft_y<false><<<ygrid, 256, 0, st>>>(Xa, S, C, m, twy, Xl[l]);
       fno_mix<<<dim3(modes, B), C, C * 8, st>>>(Xl[l], reinterpret_cast<const float2*>(par + oR[l]), C, modes, Y);
       fno_dft_y<true><<<dim3(S, B), 256, 0, st>>>(Y, S, C, m, twy, Za);
-      fno_layer_out<<<dim3(S, B), 256, static_cast<size_t>(C) * C * 4 + static_cast<size_t>(m) * C * 8, st>>>(
-          Za, v[l], par + oW[l], par + ob[l], S, C, m, twx, l < L - 1 ? 1 : 0, z[l], v[l + 1]);
+      fno_layer_out<<<rgrid, 256, layer_out_smem(), st>>>(
+          Za, v[l], par + oW[l], par + ob[l], S, m, twx, l < L - 1 ? 1 : 0, z[l], v[l + 1], rows);
     }
-    fno_proj<<<1184, 256, (static_cast<size_t>(P) * C + 2 * P) * 4, st>>>(v[L], par + oQ1, par + ob1, par + oQ2,
-                                                                         par + ob2, C, P, pix, images ? images : out);
+    fno_proj<<<pgrid(pix), 256, kProjSmem, st>>>(v[L], par + oQ1, par + ob1, par + oQ2, par + ob2, pix,
+                                                 images ? images : out);
     check_cuda(cudaGetLastError(), "fno forward");
   }
 
@@ -647,23 +911,25 @@ struct Fno {
   void backward(int B, const float* masks, const float* dOut, float* dmask, cudaStream_t st) {
     using namespace huv_dev;
     const size_t pix = static_cast<size_t>(B) * S * S;
+    const int rows = B * S;
+    const dim3 rgrid(std::min(rows, 4096));
+    const dim3 ygrid((m * C + 63) / 64, B);
     check_cuda(cudaMemsetAsync(grad, 0, npar * 4, st), "memset grad");
-    const size_t smp = (static_cast<size_t>(P) * C + static_cast<size_t>(64) * C + 2 * static_cast<size_t>(64) * P + 64) * 4;
-    fno_proj_bwd<<<1184, 256, smp, st>>>(v[L], par + oQ1, par + ob1, par + oQ2, pix, dOut, dvA, grad + oQ1,
-                                         grad + ob1, grad + oQ2, grad + ob2);
+    fno_proj_bwd<<<std::min<size_t>((pix + 63) / 64, 148), 256, kProjBwdSmem, st>>>(
+        v[L], par + oQ1, par + ob1, par + oQ2, pix, dOut, dvA, grad + oQ1, grad + ob1, grad + oQ2, grad + ob2);
     float* dnext = dvA;
     float* dcur = dvB;
     for (int l = L - 1; l >= 0; --l) {
-      fno_layer_bwd<<<dim3(S, B), 256, 0, st>>>(dnext, z[l], v[l], par + oW[l], S, l < L - 1 ? 1 : 0, dz, dcur,
-                                                 grad + oW[l], grad + ob[l]);
-      fno_dft_x<float><<<dim3(S, B), 256, static_cast<size_t>(S) * C * 4, st>>>(dz, S, C, m, twx, Xa);
-      fno_dft_y<false><<<dim3(J, B), 256, 0, st>>>(Xa, S, C, m, twy, Y);
+      fno_layer_bwd<<<std::min(rows, 296), 256, kLayerBwdSmem, st>>>(
+          dnext, z[l], v[l], par + oW[l], S, l < L - 1 ? 1 : 0, dz, dcur, grad + oW[l], grad + ob[l], rows);
+      fno_dft_x<float><<<rgrid, 256, kDftXSmem, st>>>(dz, S, m, twx, Xa, rows);
+      fno_dft_y<false><<<ygrid, 256, 0, st>>>(Xa, S, C, m, twy, Y);
       fno_scale_modes<<<256, 256, 0, st>>>(Y, B, J, m, C, 1.f / (static_cast<float>(S) * S));
       fno_mix_bwd<<<modes, 256, static_cast<size_t>(2) * B * C * 8, st>>>(
           Xl[l], Y, reinterpret_cast<const float2*>(par + oR[l]), C, modes, B, dX,
           reinterpret_cast<float2*>(grad + oR[l]));
       fno_dft_y<true><<<dim3(S, B), 256, 0, st>>>(dX, S, C, m, twy, Za);
-      fno_spec_to_dv<<<dim3(S, B), 256, static_cast<size_t>(m) * C * 8, st>>>(Za, S, C, m, twx, dcur);
+      fno_spec_to_dv<<<rgrid, 256, spec_smem(), st>>>(Za, S, m, twx, dcur, rows);
       std::swap(dnext, dcur);
     }
     fno_lift_bwd<<<1184, 256, 0, st>>>(masks, dnext, S, par + oWl, pix, grad + oWl, grad + obl, dmask);
@@ -738,6 +1004,8 @@ huv_status huv_fno_create(int32_t grid, int32_t width, int32_t modes, int32_t la
     if (!fno_out) throw Error(HUV_ERR_INVALID_PARAMETER, "fno_out: null");
     if (width != 64 || proj != 128)
       throw Error(HUV_ERR_UNSUPPORTED, "fno: this build's kernels are specialised to width 64, projection 128");
+    if (modes > 16)
+      throw Error(HUV_ERR_UNSUPPORTED, "fno: this build's DFT tiles hold at most 16 retained modes per axis");
     if (grid < 8 || (grid & (grid - 1)) || modes < 1 || 2 * modes > grid || layers < 1)
       throw Error(HUV_ERR_INVALID_PARAMETER, "fno: grid power of two >= 8, 1 <= modes <= grid/2, layers >= 1");
     *fno_out = new Fno(grid, width, modes, layers, proj, seed, device);

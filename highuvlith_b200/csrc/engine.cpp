@@ -119,6 +119,12 @@ Engine::~Engine() {
     cudaFree(ws);
     cudaFree(io_in);
     cudaFree(io_out);
+    if (io_h2d) {
+      cudaStreamDestroy(io_h2d);
+      cudaStreamDestroy(io_d2h);
+      for (auto& row : io_ev)
+        for (auto e : row) cudaEventDestroy(e);
+    }
   }
 }
 
@@ -388,19 +394,27 @@ void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
   }
 }
 
+// Host buffers in, host buffers out.  The batch is cut into chunks that
+// flow through a ring of three device slots: copy-in on one internal stream,
+// the imaging on `st`, copy-out on another, ordered by events, so that the
+// host->device copy of chunk i+1 and the device->host copy of chunk i-1
+// overlap the imaging of chunk i (PCIe is full duplex).
 void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t st) {
   std::lock_guard<std::mutex> host_lock(host_mu);
   if (b.n_clips <= 0) return;
   if (!b.input || !out_host) throw Error(HUV_ERR_INVALID_PARAMETER, "input/out: null pointer");
+  if (b.input_kind < 0 || b.input_kind > 2) throw Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
+  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
+  const size_t in_per = in_elem * static_cast<size_t>(n) * n;
+  const size_t out_per = sizeof(float) * static_cast<size_t>(n) * n;
+  const int by_bytes = static_cast<int>(std::max<size_t>(1, (size_t(128) << 20) / out_per));
+  const int chunk = std::max(1, std::min((b.n_clips + 3) / 4, by_bytes));
+  const int nchunks = (b.n_clips + chunk - 1) / chunk;
+  const int ring = std::min(nchunks, 3);
   {
     std::lock_guard<std::mutex> lock(mu);
     ensure_device();
-  }
-  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
-  const size_t in_bytes = in_elem * static_cast<size_t>(n) * n * b.n_clips;
-  const size_t out_bytes = sizeof(float) * static_cast<size_t>(n) * n * b.n_clips;
-  {
-    std::lock_guard<std::mutex> lock(mu);
+    const size_t in_bytes = in_per * chunk * ring, out_bytes = out_per * chunk * ring;
     if (in_bytes > io_in_bytes) {
       if (io_in) cudaFree(io_in);
       io_in = nullptr;
@@ -415,12 +429,46 @@ void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t 
       check_cuda(cudaMalloc(&io_out, out_bytes), "cudaMalloc(io_out)");
       io_out_bytes = out_bytes;
     }
-    check_cuda(cudaMemcpyAsync(io_in, b.input, in_bytes, cudaMemcpyHostToDevice, st), "H2D input");
+    if (!io_h2d) {
+      check_cuda(cudaStreamCreateWithFlags(&io_h2d, cudaStreamNonBlocking), "cudaStreamCreate(h2d)");
+      check_cuda(cudaStreamCreateWithFlags(&io_d2h, cudaStreamNonBlocking), "cudaStreamCreate(d2h)");
+      for (int r = 0; r < 3; ++r) {
+        check_cuda(cudaEventCreateWithFlags(&io_ev[0][r], cudaEventDisableTiming), "cudaEventCreate");
+        check_cuda(cudaEventCreateWithFlags(&io_ev[1][r], cudaEventDisableTiming), "cudaEventCreate");
+        check_cuda(cudaEventCreateWithFlags(&io_ev[2][r], cudaEventDisableTiming), "cudaEventCreate");
+      }
+    }
   }
-  huv_batch d = b;
-  d.input = io_in;
-  image_batch(d, static_cast<float*>(io_out), st);
-  check_cuda(cudaMemcpyAsync(out_host, io_out, out_bytes, cudaMemcpyDeviceToHost, st), "D2H images");
+  cudaEvent_t* in_done = io_ev[0];
+  cudaEvent_t* img_done = io_ev[1];
+  cudaEvent_t* out_done = io_ev[2];
+  for (int i = 0; i < nchunks; ++i) {
+    const int slot = i % ring;
+    const int c0 = i * chunk, nc = std::min(chunk, b.n_clips - c0);
+    char* din = static_cast<char*>(io_in) + in_per * chunk * slot;
+    float* dout = reinterpret_cast<float*>(static_cast<char*>(io_out) + out_per * chunk * slot);
+    // the input slot is free once the imaging of chunk i - ring has run
+    if (i >= ring) check_cuda(cudaStreamWaitEvent(io_h2d, img_done[slot], 0), "wait(img)");
+    check_cuda(cudaMemcpyAsync(din, static_cast<const char*>(b.input) + in_per * c0, in_per * nc,
+                               cudaMemcpyHostToDevice, io_h2d),
+               "H2D input");
+    check_cuda(cudaEventRecord(in_done[slot], io_h2d), "record(in)");
+    check_cuda(cudaStreamWaitEvent(st, in_done[slot], 0), "wait(in)");
+    // the output slot is free once chunk i - ring has been copied out
+    if (i >= ring) check_cuda(cudaStreamWaitEvent(st, out_done[slot], 0), "wait(out)");
+    huv_batch d = b;
+    d.n_clips = nc;
+    d.input = din;
+    image_batch(d, dout, st);
+    check_cuda(cudaEventRecord(img_done[slot], st), "record(img)");
+    check_cuda(cudaStreamWaitEvent(io_d2h, img_done[slot], 0), "wait(img)");
+    check_cuda(cudaMemcpyAsync(out_host + static_cast<size_t>(n) * n * c0, dout, out_per * nc,
+                               cudaMemcpyDeviceToHost, io_d2h),
+               "D2H images");
+    check_cuda(cudaEventRecord(out_done[slot], io_d2h), "record(out)");
+  }
+  check_cuda(cudaStreamSynchronize(io_d2h), "cudaStreamSynchronize(d2h)");
+  check_cuda(cudaStreamSynchronize(io_h2d), "cudaStreamSynchronize(h2d)");
   check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   std::lock_guard<std::mutex> lock(mu);
   if (read_device_error() != 0)

@@ -186,6 +186,8 @@ struct Engine {
   void* io_in = nullptr;
   void* io_out = nullptr;
   size_t io_in_bytes = 0, io_out_bytes = 0;
+  cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
+  cudaEvent_t io_ev[3][3] = {};  // [copy-in done, imaging done, copy-out done][ring slot]
 };
 
 }  // namespace huv

@@ -12,7 +12,10 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def test_fno_forward_and_gradients_match_fp64_reference():
+@pytest.mark.parametrize("S,M,LAYERS", [(S, M, LAYERS), (128, 16, 2)])
+def test_fno_forward_and_gradients_match_fp64_reference(S, M, LAYERS):
+    """Small grid (one partial pixel tile per row) and a grid with several
+    64-pixel tiles per row and the full 16 retained modes."""
     import torch
     from highuvlith_b200.fno import FnoSurrogate
     from oracle import fno_ref
