@@ -41,7 +41,11 @@ constexpr int kTcStages = 3;
 constexpr int kTcBN = 128;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s per wait
 constexpr uint32_t kABox = 128 * 128;             // 128 rows x 64 bf16
-constexpr uint32_t kBBox = kTcBN * 128;           // BN rows x 64 bf16
+// B box of BN rows x 64 bf16
+__host__ __device__ constexpr uint32_t b_box_bytes(int bn) { return static_cast<uint32_t>(bn) * 128; }
+// Row-transform GEMM (MODE 2): N = band rows padded to a multiple of 16.
+constexpr int kRowBN = 80;
+constexpr int kStageWords = 2 * 16 * 81;  // per epilogue warp: [plane][16 x][80 (+1 pad) my] bf16x2
 
 struct TcGemmParams {
   int kboxes;       // 64-wide K boxes loaded
@@ -57,20 +61,37 @@ struct TcGemmParams {
   const float* mean;
   float* out;
   int* err;
+  // MODE 2 output: split-BF16 operand rows, Bop[g][plane][x][2 my + re/im]
+  __nv_bfloat16* bop;
+  long long bop_g;      // elements between steps (kernels)
+  long long bop_prob;   // elements between problems
+  long long bop_plane;  // elements between the hi and lo planes
+  int bop_ld;           // row stride (elements)
 };
 
-__host__ __device__ constexpr size_t tc_smem_bytes(int kboxes) {
-  return 1024 + 2 * static_cast<size_t>(kboxes) * kABox + kTcStages * 2 * static_cast<size_t>(kBBox) + 256;
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(v);
+  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+__host__ __device__ constexpr size_t tc_smem_bytes(int kboxes, int bn = kTcBN, bool stage = false) {
+  return 1024 + 2 * static_cast<size_t>(kboxes) * kABox + kTcStages * 2 * static_cast<size_t>(b_box_bytes(bn)) +
+         256 + (stage ? 4 * kStageWords * sizeof(uint32_t) : 0);
 }
 
 // MODE 0: sum over G steps (kernels) of |E|^2 with (re, im) in adjacent
 // accumulator rows; out(y, x) = keep * sum + flare * mean[problem];
 // grid: (x tiles, a_rows / 128, problems).  MODE 1: step g is x tile g of the
 // same rows (the A tile stays resident), out(y, g * BN + j) = accumulator;
-// grid: (1, a_rows / 128, problems).
-template <int MODE>
+// grid: (1, a_rows / 128, problems).  MODE 2: step g is kernel g; the
+// accumulator rows are (x, re/im), its columns band rows my; the tile is
+// split into BF16 hi/lo and written, through shared memory, as rows x of the
+// next GEMM's operand: bop[g][plane][x][2 my + re/im]; grid as MODE 1.
+template <int MODE, int BN = kTcBN>
 __global__ void __launch_bounds__(192, 1)
     tc_dft_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcGemmParams p) {
+  constexpr uint32_t kBBox = b_box_bytes(BN);
+  constexpr uint32_t kTmemCols = 2 * BN <= 128 ? 128 : 256;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
@@ -104,7 +125,7 @@ __global__ void __launch_bounds__(192, 1)
     fence_barrier_init();
   }
   if (warp == 0) {
-    tmem_alloc(tmem_slot, 2 * kTcBN);
+    tmem_alloc(tmem_slot, kTmemCols);
     tmem_relinquish();
   }
   tc_fence_before();
@@ -135,7 +156,7 @@ __global__ void __launch_bounds__(192, 1)
             break;
           }
           mbar_arrive_expect_tx(&full[s], 2u * kBBox);
-          const int row = prob * p.b_prob + g * p.b_step + n_tile * kTcBN;
+          const int row = prob * p.b_prob + g * p.b_step + n_tile * BN;
           tma_load_2d(sB + (s * 2 + 0) * kBBox, &tmB, kb * 64, row, &full[s]);
           tma_load_2d(sB + (s * 2 + 1) * kBBox, &tmB, kb * 64, row + p.b_plane, &full[s]);
         }
@@ -147,7 +168,7 @@ __global__ void __launch_bounds__(192, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = idesc_bf16(128, kTcBN);
+      const uint32_t idesc = idesc_bf16(128, BN);
       bool ok = mbar_wait(a_full, 0, kWaitLimitNs);
       if (!ok) fail(2);
       tc_fence_after();
@@ -159,7 +180,7 @@ __global__ void __launch_bounds__(192, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t d = tmem_base + buf * kTcBN;
+        const uint32_t d = tmem_base + buf * BN;
         for (int kb = 0; kb < p.kboxes; ++kb, ++it) {
           const int s = it % kTcStages;
           if (!mbar_wait(&full[s], (it / kTcStages) & 1, kWaitLimitNs)) {
@@ -195,7 +216,9 @@ __global__ void __launch_bounds__(192, 1)
     // Epilogue warps 2..5: TMEM lane quadrant = warp % 4.
     const int quad = warp & 3;
     const int row = quad * 32 + lane;  // accumulator row within the tile
-    constexpr int HALF = kTcBN / 2;
+    constexpr int HALF = BN / 2;
+    // MODE 2 staging: after the 256 bytes of barriers, kStageWords per warp
+    uint32_t* stage = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(bars) + 256) + quad * kStageWords;
     float acc[MODE == 0 ? HALF : 1];
 #pragma unroll
     for (int i = 0; i < (MODE == 0 ? HALF : 1); ++i) acc[i] = 0.f;
@@ -211,9 +234,41 @@ __global__ void __launch_bounds__(192, 1)
         break;
       }
       tc_fence_after();
-      const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + buf * kTcBN;
+      const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + buf * BN;
+      if (MODE == 2) {
+        // rows (x, re/im) in adjacent lanes: even lanes keep the hi pair of
+        // (re, im), odd lanes the lo pair; staged as [plane][x][my].
+        const int xl = lane >> 1;
 #pragma unroll
-      for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+          float v[16];
+          tmem_ld16(taddr + c0, v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const float other = __shfl_xor_sync(0xffffffffu, v[i], 1);
+            const float re = odd ? other : v[i], im = odd ? v[i] : other;
+            __nv_bfloat16 rh, rl, ih, il;
+            split_bf16(re, rh, rl);
+            split_bf16(im, ih, il);
+            __nv_bfloat162 pr;
+            pr.x = odd ? rl : rh;
+            pr.y = odd ? il : ih;
+            stage[(odd * 16 + xl) * 81 + c0 + i] = *reinterpret_cast<uint32_t*>(&pr);
+          }
+        }
+        __syncwarp();
+        // coalesced copy-out: 32 rows (2 planes x 16 x) of BN bf16 pairs
+        const int x0 = (m_tile * 128 + quad * 32) >> 1;
+        uint32_t* base_out = reinterpret_cast<uint32_t*>(p.bop + prob * p.bop_prob + g * p.bop_g);
+        for (int w = lane; w < 32 * BN; w += 32) {
+          const int r = w / BN, my = w - r * BN;
+          const int pl = r >> 4, x = x0 + (r & 15);
+          base_out[(pl * p.bop_plane + static_cast<long long>(x) * p.bop_ld) / 2 + my] = stage[r * 81 + my];
+        }
+        __syncwarp();
+      }
+#pragma unroll
+      for (int c0 = 0; c0 < (MODE == 2 ? 0 : BN); c0 += 32) {
         float v[32];
         tmem_ld32(taddr + c0, v);
         if (MODE == 0) {
@@ -226,7 +281,7 @@ __global__ void __launch_bounds__(192, 1)
           }
         } else {
           const int y = m_tile * 128 + row;
-          float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + g * kTcBN + c0;
+          float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + g * BN + c0;
 #pragma unroll
           for (int i = 0; i < 32; i += 4)
             *reinterpret_cast<float4*>(o + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
@@ -239,7 +294,7 @@ __global__ void __launch_bounds__(192, 1)
     if (MODE == 0 && ok) {
       const int y = (m_tile * 128 + row) >> 1;
       const float add = p.mean ? p.flare * p.mean[prob] : 0.f;
-      float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + n_tile * kTcBN + odd * HALF;
+      float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + n_tile * BN + odd * HALF;
 #pragma unroll
       for (int i = 0; i < HALF; i += 4)
         *reinterpret_cast<float4*>(o + i) = make_float4(p.keep * acc[i] + add, p.keep * acc[i + 1] + add,
@@ -249,12 +304,7 @@ __global__ void __launch_bounds__(192, 1)
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tmem_dealloc(tmem_base, 2 * kTcBN);
-}
-
-__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-  hi = __float2bfloat16_rn(v);
-  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+  if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
 }
 
 // Row transform along x of the band products, written as the tensor-core
@@ -311,6 +361,33 @@ __global__ void socs_rows_tc(const float2* __restrict__ kband, float scale, cons
         lo[kk] = z;
       }
     }
+  }
+}
+
+// Band products of every kernel with the mask band, split into BF16 planes as
+// the B operand of the row-transform GEMM: P[prob][k][plane][my][kk], rows my
+// padded to rows_pad, kk = 2 mx + re/im padded to kp; zero outside my < B,
+// mx < B.  grid (K, problems).
+__global__ void band_products(const float2* __restrict__ kband, const float2* __restrict__ Mband, int K, int B,
+                              int rows_pad, int kp, __nv_bfloat16* __restrict__ P) {
+  const int k = blockIdx.x, prob = blockIdx.y;
+  const float2* Mc = Mband + static_cast<size_t>(prob) * B * B;
+  const float2* u = kband + static_cast<size_t>(k) * B * B;
+  const size_t plane = static_cast<size_t>(rows_pad) * kp;
+  __nv_bfloat162* hi = reinterpret_cast<__nv_bfloat162*>(P + (static_cast<size_t>(prob) * K + k) * 2 * plane);
+  __nv_bfloat162* lo = hi + plane / 2;
+  const int pairs = kp / 2;
+  for (int e = threadIdx.x; e < rows_pad * pairs; e += blockDim.x) {
+    const int my = e / pairs, mx = e - my * pairs;
+    __nv_bfloat162 h, l;
+    h.x = h.y = l.x = l.y = __float2bfloat16_rn(0.f);
+    if (my < B && mx < B) {
+      const float2 v = cmul(u[my * B + mx], Mc[my * B + mx]);
+      split_bf16(v.x, h.x, l.x);
+      split_bf16(v.y, h.y, l.y);
+    }
+    hi[e] = h;
+    lo[e] = l;
   }
 }
 
@@ -386,6 +463,9 @@ cudaError_t tc_set_smem() {
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<2, kRowBN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, kRowBN, true)))))
+    return e;
   if ((e = cudaFuncSetAttribute(socs_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   return cudaSuccess;
 }
@@ -474,12 +554,13 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const size_t per_x = align256(sizeof(float2) * n * B);
   const size_t per_m = align256(sizeof(float2) * B * B);
   const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kpE * 2);
+  const size_t per_p = align256(static_cast<size_t>(K) * 2 * kRowBN * kpE * 2);
   const size_t per_i = align256(sizeof(float) * M * M);
   const size_t per_x2 = align256(sizeof(float2) * M * B2);
   const size_t per_c = align256(sizeof(float2) * B2 * B2);
   const size_t per_bi = align256(static_cast<size_t>(2) * n * kpI * 2);
   const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
-  const size_t per_clip = per_x + per_m + per_be + per_i + per_x2 + per_c + per_bi + per_mean;
+  const size_t per_clip = per_x + per_m + per_be + per_p + per_i + per_x2 + per_c + per_bi + per_mean;
   const size_t budget = size_t(1) << 30;
   int chunk = static_cast<int>(std::max<size_t>(1, budget / per_clip));
   chunk = std::min(chunk, b.n_clips);
@@ -493,6 +574,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   float2* X = reinterpret_cast<float2*>(take(per_x));
   float2* Mb = reinterpret_cast<float2*>(take(per_m));
   __nv_bfloat16* BE = reinterpret_cast<__nv_bfloat16*>(take(per_be));
+  __nv_bfloat16* P = reinterpret_cast<__nv_bfloat16*>(take(per_p));
   float* IM = reinterpret_cast<float*>(take(per_i));
   float2* X2 = reinterpret_cast<float2*>(take(per_x2));
   float2* C = reinterpret_cast<float2*>(take(per_c));
@@ -508,17 +590,35 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     check_cuda(band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb, b.pixel_transfer ? ds.ptx : nullptr, Wf,
                             mean, twn, st),
                "band_forward");
-    {
-      const int S = fit_units(8, 2 * (sizeof(float2) << lgm));
-      dim3 g((K * B + S - 1) / S, nc);
-      const size_t sm = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
-      socs_rows_tc<<<g, 256, sm, st>>>(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, S, kpE, kstE * 16, BE, twm);
-      check_cuda(cudaGetLastError(), "socs_rows_tc");
-    }
-    CUtensorMap mbE, mbI;
+    CUtensorMap mbE, mbI, mbP;
     if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kpE, kTcBN) ||
-        !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kpI, kTcBN))
+        !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kpI, kTcBN) ||
+        !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * kRowBN, kpE, kRowBN))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
+    {
+      // Row transforms of every kernel's band product on tensor cores: the
+      // same M-point inverse DFT operand (A_E) against the split products,
+      // written straight as the next GEMM's split operand.
+      band_products<<<dim3(K, nc), 256, 0, st>>>(ds.kband, Mb, K, B, kRowBN, kpE, P);
+      check_cuda(cudaGetLastError(), "band_products");
+      TcGemmParams p{};
+      p.kboxes = kpE / 64;
+      p.ksteps = kstE;
+      p.G = K;
+      p.a_rows = 2 * M;
+      p.b_prob = K * 2 * kRowBN;
+      p.b_step = 2 * kRowBN;
+      p.b_plane = kRowBN;
+      p.err = dev_err;
+      p.bop = BE;
+      p.bop_g = 2ll * M * kpE;
+      p.bop_prob = static_cast<long long>(K) * 2 * M * kpE;
+      p.bop_plane = static_cast<long long>(M) * kpE;
+      p.bop_ld = kpE;
+      dim3 g(1, 2 * M / 128, nc);
+      tc_dft_gemm<2, kRowBN><<<g, 192, tc_smem_bytes(3, kRowBN, true), st>>>(tc.map_ae, mbP, p);
+      check_cuda(cudaGetLastError(), "tc_dft_gemm<2>");
+    }
     {
       TcGemmParams p{};
       p.kboxes = kpE / 64;
@@ -571,7 +671,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       tc_dft_gemm<1><<<g, 192, smem_tc, st>>>(tc.map_ai, mbI, p);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
     }
-    prof.launches += 7;
+    prof.launches += 8;
   }
 }
 

@@ -12,6 +12,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 
 #include "host.hpp"
@@ -29,20 +31,111 @@ int host_threads() {
   return n;
 }
 
+namespace {
+// Persistent worker pool: parallel_for is called thousands of times per
+// eigensolve (twice per Householder step), so threads are started once.
+// A parallel_for issued from inside a worker runs serially.
+class Pool {
+ public:
+  explicit Pool(int n) {
+    for (int i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+  }
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> l(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+  int size() const { return static_cast<int>(workers_.size()); }
+  // Runs body(b, e) over chunks of [0, n); the caller works too.  Returns
+  // once every chunk has run and no worker is inside the region.
+  void run(int64_t n, int chunks, const std::function<void(int64_t, int64_t)>& body) {
+    std::lock_guard<std::mutex> region(run_mu_);
+    const int64_t chunk = (n + chunks - 1) / chunks;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      body_ = &body;
+      n_ = n;
+      chunk_ = chunk;
+      next_.store(0);
+      pending_ = (n + chunk - 1) / chunk;
+      ++generation_;
+    }
+    cv_.notify_all();
+    work(body, n, chunk);
+    std::unique_lock<std::mutex> g(mu_);
+    done_cv_.wait(g, [this] { return pending_ == 0 && active_ == 0; });
+    body_ = nullptr;
+  }
+  static bool& in_worker() {
+    static thread_local bool w = false;
+    return w;
+  }
+
+ private:
+  void work(const std::function<void(int64_t, int64_t)>& body, int64_t n, int64_t chunk) {
+    for (;;) {
+      const int64_t b = next_.fetch_add(1) * chunk;
+      if (b >= n) break;
+      body(b, std::min(n, b + chunk));
+      std::lock_guard<std::mutex> g(mu_);
+      if (--pending_ == 0) done_cv_.notify_all();
+    }
+  }
+  void loop() {
+    in_worker() = true;
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(int64_t, int64_t)>* body;
+      int64_t n, chunk;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return stop_ || (generation_ != seen && body_ != nullptr); });
+        if (stop_) return;
+        seen = generation_;
+        body = body_;
+        n = n_;
+        chunk = chunk_;
+        ++active_;
+      }
+      work(*body, n, chunk);
+      std::lock_guard<std::mutex> g(mu_);
+      if (--active_ == 0 && pending_ == 0) done_cv_.notify_all();
+    }
+  }
+
+  std::vector<std::thread> workers_;
+  std::mutex mu_, run_mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(int64_t, int64_t)>* body_ = nullptr;
+  int64_t n_ = 0, chunk_ = 1;
+  std::atomic<int64_t> next_{0};
+  int64_t pending_ = 0;
+  int active_ = 0;
+  uint64_t generation_ = 0;
+  bool stop_ = false;
+};
+
+Pool& pool() {
+  static Pool p(std::max(host_threads() - 1, 0));
+  return p;
+}
+}  // namespace
+
 void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)>& body) {
-  const int t = std::min<int64_t>(host_threads(), std::max<int64_t>(n / 64, 1));
-  if (t <= 1 || n < 128) {
+  const int t = static_cast<int>(std::min<int64_t>(host_threads(), std::max<int64_t>(n / 64, 1)));
+  if (t <= 1 || n < 128 || Pool::in_worker()) {
     body(0, n);
     return;
   }
-  std::vector<std::thread> pool;
-  const int64_t chunk = (n + t - 1) / t;
-  for (int i = 0; i < t; ++i) {
-    const int64_t b = i * chunk, e = std::min(n, b + chunk);
-    if (b >= e) break;
-    pool.emplace_back([&body, b, e] { body(b, e); });
+  Pool& p = pool();
+  if (p.size() == 0) {
+    body(0, n);
+    return;
   }
-  for (auto& th : pool) th.join();
+  p.run(n, t, body);
 }
 
 // ----------------------------------------------------------- selection
@@ -97,17 +190,20 @@ class HermitianEigen {
 
  private:
   void decompose(std::vector<cd> a);
+  std::vector<double> tridiag_vectors(int count) const;
   int n_;
+  double scale_ = 1.0;
   std::vector<double> values_;
   std::vector<std::vector<cd>> refl_;  // unit Householder vectors acting on rows k+1..n-1
   std::vector<cd> phase_;
-  std::vector<double> z_;              // tridiagonal eigenvectors, column-major
-  std::vector<int> order_;
+  std::vector<double> td_, te_;        // the real tridiagonal (scaled): diagonal, off-diagonal
+  std::vector<double> tvals_;          // its eigenvalues, decreasing (scaled)
 };
 
 // Implicit symmetric QL on (d, e); e[i] couples d[i], d[i+1].  Accumulates
-// rotations into z (column-major n x n).
+// rotations into z (column-major n x n) unless z is empty (eigenvalues only).
 bool tridiag_ql(int n, std::vector<double>& d, std::vector<double>& e, std::vector<double>& z) {
+  const bool vecs = !z.empty();
   if (n == 0) return true;
   double dmax = 0, emax = 0;
   for (int i = 0; i < n; ++i) dmax = std::max(dmax, std::fabs(d[i]));
@@ -147,12 +243,14 @@ bool tridiag_ql(int n, std::vector<double>& d, std::vector<double>& e, std::vect
         p = s * r;
         d[i + 1] = g + p;
         g = c * r - b;
-        double* zi = &z[static_cast<size_t>(i) * n];
-        double* zj = &z[static_cast<size_t>(i + 1) * n];
-        for (int q = 0; q < n; ++q) {
-          const double t = zj[q];
-          zj[q] = s * zi[q] + c * t;
-          zi[q] = c * zi[q] - s * t;
+        if (vecs) {
+          double* zi = &z[static_cast<size_t>(i) * n];
+          double* zj = &z[static_cast<size_t>(i + 1) * n];
+          for (int q = 0; q < n; ++q) {
+            const double t = zj[q];
+            zj[q] = s * zi[q] + c * t;
+            zi[q] = c * zi[q] - s * t;
+          }
         }
       }
       if (early) continue;
@@ -195,10 +293,14 @@ void HermitianEigen::decompose(std::vector<cd> a) {
     parallel_for(m, [&](int64_t b, int64_t e2) {
       for (int64_t i = b; i < e2; ++i) {
         // (A22 u)_i = sum_j A[i][j] u_j = sum_j conj(A[j][i]) u_j; column i is contiguous.
-        const cd* col = &a[static_cast<size_t>(k + 1 + i) * n + (k + 1)];
-        cd acc(0, 0);
-        for (int j = 0; j < m; ++j) acc += std::conj(col[j]) * u[j];
-        p[i] = 2.0 * acc;
+        const double* col = reinterpret_cast<const double*>(&a[static_cast<size_t>(k + 1 + i) * n + (k + 1)]);
+        const double* uu = reinterpret_cast<const double*>(u.data());
+        double re = 0.0, im = 0.0;
+        for (int j = 0; j < m; ++j) {
+          re += col[2 * j] * uu[2 * j] + col[2 * j + 1] * uu[2 * j + 1];
+          im += col[2 * j] * uu[2 * j + 1] - col[2 * j + 1] * uu[2 * j];
+        }
+        p[i] = cd(2.0 * re, 2.0 * im);
       }
     });
     cd kk(0, 0);
@@ -207,9 +309,16 @@ void HermitianEigen::decompose(std::vector<cd> a) {
     for (int i = 0; i < m; ++i) p[i] -= kr * u[i];
     parallel_for(m, [&](int64_t b, int64_t e2) {
       for (int64_t j = b; j < e2; ++j) {
-        const cd qj = std::conj(p[j]), uj = std::conj(u[j]);
-        cd* col = &a[static_cast<size_t>(k + 1 + j) * n + (k + 1)];
-        for (int i = 0; i < m; ++i) col[i] -= u[i] * qj + p[i] * uj;
+        // col -= u conj(p_j) + p conj(u_j)
+        const double qr = p[j].real(), qi = -p[j].imag(), vr = u[j].real(), vi = -u[j].imag();
+        double* col = reinterpret_cast<double*>(&a[static_cast<size_t>(k + 1 + j) * n + (k + 1)]);
+        const double* uu = reinterpret_cast<const double*>(u.data());
+        const double* pp = reinterpret_cast<const double*>(p.data());
+        for (int i = 0; i < m; ++i) {
+          const double ur = uu[2 * i], ui = uu[2 * i + 1], pr = pp[2 * i], pi = pp[2 * i + 1];
+          col[2 * i] -= ur * qr - ui * qi + pr * vr - pi * vi;
+          col[2 * i + 1] -= ur * qi + ui * qr + pr * vi + pi * vr;
+        }
       }
     });
     sub[k] = beta;
@@ -224,24 +333,122 @@ void HermitianEigen::decompose(std::vector<cd> a) {
     const double r = std::abs(sub[k]);
     phase_[k + 1] = r > 0 ? phase_[k] * (sub[k] / r) : phase_[k];
   }
-  z_.assign(static_cast<size_t>(n) * n, 0.0);
-  for (int i = 0; i < n; ++i) z_[static_cast<size_t>(i) * n + i] = 1.0;
-  if (!tridiag_ql(n, d, e, z_))
+  td_ = d;
+  te_ = e;
+  // Eigenvalues by implicit QL without vectors (O(n^2)); eigenvectors are
+  // computed on demand for the retained kernels only (tridiag_vectors).
+  std::vector<double> none;
+  if (!tridiag_ql(n, d, e, none))
     throw Error(HUV_ERR_TCC_DECOMPOSITION, "Hermitian eigensolver: QL iteration did not converge");
-  order_.resize(n);
-  std::iota(order_.begin(), order_.end(), 0);
-  std::stable_sort(order_.begin(), order_.end(), [&](int x, int y) { return d[x] > d[y]; });
+  std::sort(d.begin(), d.end(), [](double x, double y) { return x > y; });
+  tvals_ = d;
+  scale_ = scale;
   values_.resize(n);
-  for (int i = 0; i < n; ++i) values_[i] = d[order_[i]] * scale;
+  for (int i = 0; i < n; ++i) values_[i] = d[i] * scale;
+}
+
+// Eigenvectors of the real symmetric tridiagonal (td_, te_) for its `count`
+// largest eigenvalues, by inverse iteration: LU with partial pivoting of
+// T - lambda I (the tridiagonal form of LAPACK's gttrf/gttrs), three solves
+// from a fixed start vector, each followed by modified Gram-Schmidt against
+// the vectors already found for eigenvalues within 1e-3 ||T|| (a cluster:
+// equal eigenvalues get an orthonormal basis of their eigenspace).  Returns
+// column-major n x count.
+std::vector<double> HermitianEigen::tridiag_vectors(int count) const {
+  const int n = n_;
+  std::vector<double> z(static_cast<size_t>(n) * count, 0.0);
+  if (n == 1) {
+    for (int c = 0; c < count; ++c) z[c] = 1.0;
+    return z;
+  }
+  double tnorm = 0.0;
+  for (int i = 0; i < n; ++i)
+    tnorm = std::max(tnorm, std::fabs(td_[i]) + (i > 0 ? std::fabs(te_[i - 1]) : 0.0) + std::fabs(te_[i]));
+  if (tnorm == 0.0) tnorm = 1.0;
+  const double eps = std::numeric_limits<double>::epsilon();
+  const double pivmin = eps * tnorm;
+  const double ortol = 1e-3 * tnorm;
+  std::vector<double> dl(n), dd(n), du(n), du2(n), x(n);
+  std::vector<int> ipiv(n);
+  int cluster_start = 0;
+  double lam_prev = 0.0;
+  for (int c = 0; c < count; ++c) {
+    double lam = tvals_[c];
+    if (c > 0 && lam_prev - lam > ortol) cluster_start = c;
+    // separate equal eigenvalues slightly so each solve stays well posed
+    if (c > cluster_start && lam >= lam_prev - 10.0 * eps * tnorm) lam = lam_prev - 10.0 * eps * tnorm;
+    lam_prev = lam;
+    // LU of T - lam I with partial pivoting
+    for (int i = 0; i < n; ++i) dd[i] = td_[i] - lam;
+    for (int i = 0; i + 1 < n; ++i) {
+      dl[i] = te_[i];
+      du[i] = te_[i];
+    }
+    for (int i = 0; i + 1 < n; ++i) {
+      if (std::fabs(dd[i]) >= std::fabs(dl[i])) {
+        if (dd[i] == 0.0) dd[i] = pivmin;
+        const double f = dl[i] / dd[i];
+        dl[i] = f;
+        dd[i + 1] -= f * du[i];
+        du2[i] = 0.0;
+        ipiv[i] = i;
+      } else {
+        const double f = dd[i] / dl[i];
+        dd[i] = dl[i];
+        dl[i] = f;
+        const double t = du[i];
+        du[i] = dd[i + 1];
+        dd[i + 1] = t - f * dd[i + 1];
+        if (i + 2 < n) {
+          du2[i] = du[i + 1];
+          du[i + 1] = -f * du[i + 1];
+        } else {
+          du2[i] = 0.0;
+        }
+        ipiv[i] = i + 1;
+      }
+    }
+    if (dd[n - 1] == 0.0) dd[n - 1] = pivmin;
+    // fixed, non-degenerate start vector
+    for (int i = 0; i < n; ++i) x[i] = 1.0 + 0.5 * std::sin(1.0 + 0.7 * i + 0.37 * c);
+    for (int it = 0; it < 3; ++it) {
+      for (int i = 0; i + 1 < n; ++i) {
+        if (ipiv[i] == i) {
+          x[i + 1] -= dl[i] * x[i];
+        } else {
+          const double t = x[i];
+          x[i] = x[i + 1];
+          x[i + 1] = t - dl[i] * x[i];
+        }
+      }
+      x[n - 1] /= dd[n - 1];
+      x[n - 2] = (x[n - 2] - du[n - 2] * x[n - 1]) / dd[n - 2];
+      for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - du[i] * x[i + 1] - du2[i] * x[i + 2]) / dd[i];
+      for (int q = cluster_start; q < c; ++q) {
+        const double* zq = &z[static_cast<size_t>(q) * n];
+        double dot = 0.0;
+        for (int i = 0; i < n; ++i) dot += zq[i] * x[i];
+        for (int i = 0; i < n; ++i) x[i] -= dot * zq[i];
+      }
+      double nrm = 0.0;
+      for (int i = 0; i < n; ++i) nrm += x[i] * x[i];
+      nrm = std::sqrt(nrm);
+      if (!(nrm > 0.0) || !std::isfinite(nrm))
+        throw Error(HUV_ERR_TCC_DECOMPOSITION, "Hermitian eigensolver: inverse iteration broke down");
+      for (int i = 0; i < n; ++i) x[i] /= nrm;
+    }
+    std::copy(x.begin(), x.end(), z.begin() + static_cast<size_t>(c) * n);
+  }
+  return z;
 }
 
 std::vector<cd> HermitianEigen::vectors(int count) const {
   const int n = n_;
   count = std::min(count, n);
+  const std::vector<double> z = tridiag_vectors(count);
   std::vector<cd> w(static_cast<size_t>(n) * count);
   for (int c = 0; c < count; ++c)
-    for (int i = 0; i < n; ++i)
-      w[static_cast<size_t>(c) * n + i] = phase_[i] * z_[static_cast<size_t>(order_[c]) * n + i];
+    for (int i = 0; i < n; ++i) w[static_cast<size_t>(c) * n + i] = phase_[i] * z[static_cast<size_t>(c) * n + i];
   for (int k = static_cast<int>(refl_.size()) - 1; k >= 0; --k) {
     const auto& u = refl_[k];
     if (u.empty()) continue;
@@ -369,16 +576,31 @@ KernelSet build_kernels(const std::vector<SourcePoint>& points, const Optics& op
     double trace = 0.0;
     for (int64_t r : rows)
       for (int64_t c : keep_cols) trace += std::norm(a[static_cast<size_t>(c * n_cand + r)]);
-    // TCC[f, f'] = sum_s A[f, s] conj(A[f', s]), column-major m x m.
+    // TCC[f, f'] = sum_s A[f, s] conj(A[f', s]), column-major m x m, from a
+    // row-major copy of the used rows (contiguous dot products, one triangle).
+    const int64_t nk = static_cast<int64_t>(keep_cols.size());
+    std::vector<cd> yr(static_cast<size_t>(m * nk));
+    parallel_for(m, [&](int64_t b, int64_t e) {
+      for (int64_t i = b; i < e; ++i)
+        for (int64_t c = 0; c < nk; ++c)
+          yr[static_cast<size_t>(i * nk + c)] = a[static_cast<size_t>(keep_cols[c] * n_cand + rows[i])];
+    });
     std::vector<cd> tcc(static_cast<size_t>(m * m));
     parallel_for(m, [&](int64_t b, int64_t e) {
-      for (int64_t jj = b; jj < e; ++jj)
-        for (int64_t ii = 0; ii < m; ++ii) {
-          cd acc(0, 0);
-          for (int64_t c : keep_cols)
-            acc += a[static_cast<size_t>(c * n_cand + rows[ii])] * std::conj(a[static_cast<size_t>(c * n_cand + rows[jj])]);
-          tcc[static_cast<size_t>(jj * m + ii)] = acc;
+      for (int64_t jj = b; jj < e; ++jj) {
+        const cd* yj = &yr[static_cast<size_t>(jj * nk)];
+        for (int64_t ii = jj; ii < m; ++ii) {
+          const cd* yi = &yr[static_cast<size_t>(ii * nk)];
+          double re = 0, im = 0;
+          for (int64_t c = 0; c < nk; ++c) {
+            // yi[c] * conj(yj[c])
+            re += yi[c].real() * yj[c].real() + yi[c].imag() * yj[c].imag();
+            im += yi[c].imag() * yj[c].real() - yi[c].real() * yj[c].imag();
+          }
+          tcc[static_cast<size_t>(jj * m + ii)] = cd(re, im);
+          tcc[static_cast<size_t>(ii * m + jj)] = cd(re, -im);
         }
+      }
     });
     HermitianEigen eig(static_cast<int>(m), std::move(tcc));
     const int k = select_kernel_count(eig.values(), trace, max_kernels, fraction);
@@ -417,17 +639,19 @@ KernelSet build_kernels(const std::vector<SourcePoint>& points, const Optics& op
     ks.trace = trace;
     ks.eigenvalues.assign(eig.values().begin(), eig.values().begin() + k);
     ks.all_values = eig.values();
-    // u_k = A v_k / sqrt(lambda_k) over every candidate.
+    // u_k = A v_k / sqrt(lambda_k) over every candidate (columns of A are
+    // contiguous: accumulate column by column over a block of rows).
     ks.values.assign(static_cast<size_t>(k) * n_cand, cd(0, 0));
     parallel_for(n_cand, [&](int64_t b, int64_t e) {
       for (int q = 0; q < k; ++q) {
-        const double inv = 1.0 / std::sqrt(ks.eigenvalues[q]);
-        for (int64_t r = b; r < e; ++r) {
-          cd acc(0, 0);
-          for (int64_t j = 0; j < n_eff; ++j)
-            acc += a[static_cast<size_t>(keep_cols[j] * n_cand + r)] * v[static_cast<size_t>(q * n_eff + j)];
-          ks.values[static_cast<size_t>(q * n_cand + r)] = acc * inv;
+        cd* out = &ks.values[static_cast<size_t>(q * n_cand)];
+        for (int64_t j = 0; j < n_eff; ++j) {
+          const cd vj = v[static_cast<size_t>(q * n_eff + j)];
+          const cd* col = &a[static_cast<size_t>(keep_cols[j] * n_cand)];
+          for (int64_t r = b; r < e; ++r) out[r] += col[r] * vj;
         }
+        const double inv = 1.0 / std::sqrt(ks.eigenvalues[q]);
+        for (int64_t r = b; r < e; ++r) out[r] *= inv;
       }
     });
     ks.support.resize(n_cand);
