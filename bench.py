@@ -253,6 +253,54 @@ def ilt_leg(eng, stream, masks=64, iterations=3):
             "mean_cost_start": float(np.mean(costs)), "mean_cost_end": float(np.mean(res["final_cost"]))}
 
 
+def focus_sweep_leg(reps=3):
+    """21-plane focus sweeps with kernels built per plane, the reference's
+    focus_sweep_21 benchmark scenes (benches/aerial_benchmark.rs:120-165):
+    VUV F2 157.63 nm sigma 0.7, NA 0.75, 256^2 at 2 nm, K=20, focus -200..200
+    step 20, 65 nm lines on a 180 nm pitch; EUV 13.5 nm sigma 0.7 through the
+    Schwarzschild objective (NA 0.33, obscuration 0.25, mirror amplitude 0.67,
+    flare 0.03), 256^2 at 1 nm, K=20, focus -100..100 step 10, 16 nm lines on
+    a 32 nm pitch.  A fresh engine per repetition (creation untimed, its
+    in-focus set reused for the z = 0 plane): the 20 other planes are built on
+    the host (one plane per thread, FP64) and all 21 imaged on the device."""
+    import torch
+    import highuvlith_b200 as HB
+    scenes = {
+        "vuv_2nm_256": (HB.SourceConfig.f2_laser(0.7), HB.OpticsConfig(0.75), HB.GridConfig(256, 2.0),
+                        [-200.0 + 20.0 * i for i in range(21)], 65.0 / 2.0, 180.0 / 2.0),
+        "euv_1nm_256": (HB.SourceConfig.euv(0.7), HB.OpticsConfig(0.33, 0.03, 1.0, "euv", 0.25, 0.67 ** 2),
+                        HB.GridConfig(256, 1.0), [-100.0 + 10.0 * i for i in range(21)], 16.0, 32.0),
+    }
+    out = {"published_reference_ms": {"vuv_2nm_256": 34.0, "euv_1nm_256": 307.0},
+           "published_reference_hw": "Apple M3 Pro, 11 cores (README.md:518)", "host_threads": os.cpu_count()}
+    for name, (src, opt, grid, focus, line_px, pitch_px) in scenes.items():
+        n = grid.size
+        x = np.arange(n)
+        row = ((x % pitch_px) >= line_px).astype(np.uint8)  # opaque lines on a clear field
+        d = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(row, (1, n, n)))).cuda()
+        res = {}
+        for build in ("host", "device_reference_rule"):
+            times, creates = [], []
+            for r in range(reps + 1):
+                t0 = time.perf_counter()
+                eng = HB.SimulationEngine(src, opt, grid=grid, max_kernels=20, kernel_build=build)
+                t1 = time.perf_counter()
+                imgs = eng.compute_batch_through_focus(d, focus)
+                torch.cuda.synchronize()
+                t2 = time.perf_counter()
+                if r > 0:  # the first repetition warms up the device path
+                    creates.append((t1 - t0) * 1e3)
+                    times.append((t2 - t1) * 1e3)
+                method = eng.imaging_diagnostics()["method"]
+                del eng
+            res[build] = {"planes": len(focus), "sweep_ms": float(np.median(times)),
+                          "engine_create_ms": float(np.median(creates)),
+                          "create_plus_sweep_ms": float(np.median(np.add(times, creates))), "method": method,
+                          "image_check_max": float(imgs.max().item())}
+        out[name] = res
+    return out
+
+
 def uneven_leg(stream, n_clips=2048, steps=3):
     """C3: an uneven batch in one graph launch: sides from {256, 512, 1024,
     2048} at 1 nm, kernel budgets from {16, 32, 48, 64}, sources alternating
@@ -401,6 +449,7 @@ def run_ours(args):
         extra["forms"] = forms
         extra["ilt"] = ilt_leg(eng, stream)
         extra["uneven_batch"] = uneven_leg(stream, n_clips=args.uneven_clips)
+        extra["focus_sweep"] = focus_sweep_leg()
         step(args.form, args.eval_grid)
         torch.cuda.synchronize()
         extra["accuracy"] = accuracy(d_out[0].cpu().numpy(), rasters[0])

@@ -49,7 +49,7 @@ class Grid(C.Structure):
 class Settings(C.Structure):
     _fields_ = [("max_kernels", C.c_int32), ("kernel_energy_fraction", C.c_double),
                 ("source_points_per_axis", C.c_int32), ("normalization", C.c_int32),
-                ("kernel_cache_capacity", C.c_int32)]
+                ("kernel_cache_capacity", C.c_int32), ("kernel_build", C.c_int32)]
 
 
 class Diagnostics(C.Structure):
@@ -128,6 +128,8 @@ SIGNATURES = {
     "huv_ilt_optimize_surrogate": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(IltParams), C.POINTER(IltOpt),
                                              C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(SurrogateIlt),
                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "huv_image_focus_sweep": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_int32, C.c_void_p,
+                                        C.c_void_p]),
     "huv_image_batch_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),
     "huv_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
     "huv_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32),

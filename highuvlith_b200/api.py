@@ -12,7 +12,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass, field, replace
-from typing import Optional, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -129,6 +129,10 @@ class MaskConfig:
 
 
 _NORMALIZATION = {"clear_field": 0, "absolute": 1}
+# Where the FP64 kernel set is built: host C++ (dense), the GPU (dense), or the
+# GPU with the reference's solver rule (randomized subspace iteration for
+# large problems, aerial.rs:1116-1128).
+_KERNEL_BUILD = {"host": 0, "device": 1, "device_reference_rule": 2}
 
 
 class SimulationEngine:
@@ -140,7 +144,8 @@ class SimulationEngine:
     def __init__(self, source: SourceConfig, optics: OpticsConfig, mask: Optional[MaskConfig] = None,
                  grid: Optional[GridConfig] = None, max_kernels: int = 30,
                  kernel_energy_fraction: float = 1.0, source_points_per_axis: Optional[int] = None,
-                 normalization: str = "clear_field", kernel_cache_capacity: int = 32, device: int = 0):
+                 normalization: str = "clear_field", kernel_cache_capacity: int = 32, device: int = 0,
+                 kernel_build: str = "host"):
         if normalization not in _NORMALIZATION:
             raise ValueError(f"normalization must be one of {sorted(_NORMALIZATION)}")
         if source_points_per_axis is not None and source_points_per_axis < 1:
@@ -155,6 +160,9 @@ class SimulationEngine:
         st.source_points_per_axis = source_points_per_axis or 0
         st.normalization = _NORMALIZATION[normalization]
         st.kernel_cache_capacity = kernel_cache_capacity
+        if kernel_build not in _KERNEL_BUILD:
+            raise ValueError(f"kernel_build must be one of {sorted(_KERNEL_BUILD)}")
+        st.kernel_build = _KERNEL_BUILD[kernel_build]
         g = L.Grid(self.grid.size, self.grid.pixel_nm)
         h = C.c_void_p()
         L.check(L.lib().huv_engine_create(C.byref(source._c()), C.byref(optics._c()), C.byref(g),
@@ -188,7 +196,7 @@ class SimulationEngine:
         return {
             "num_kernels": d.num_kernels, "captured_energy_fraction": d.captured_energy_fraction,
             "num_frequencies": d.num_frequencies, "num_columns": d.num_columns,
-            "method": ["dense_tcc", "dense_gram"][d.method],
+            "method": ["dense_tcc", "dense_gram", "randomized"][d.method],
             "support_exceeds_nyquist": bool(d.support_exceeds_nyquist),
             "clear_field_intensity": d.clear_field_intensity, "normalized": bool(d.normalized),
             "band_half_width": d.band_half_width, "num_source_points": d.num_source_points,
@@ -301,6 +309,37 @@ class SimulationEngine:
         if m is None:
             raise ValueError("no mask given")
         return self.compute_batch_host(m.rasterize(self.grid), focus_nm, pixel_transfer=True)[0]
+
+    def compute_through_focus(self, focus_nm: Sequence[float], mask: Optional[MaskConfig] = None) -> List[np.ndarray]:
+        """Images of ``mask`` at several focus planes (py_simulation.rs:319-330,
+        aerial.rs:1820-1825): kernels of uncached planes built concurrently,
+        every plane imaged on the device (huv_image_focus_sweep)."""
+        import torch
+        m = mask or self.mask
+        if m is None:
+            raise ValueError("no mask given")
+        r = torch.from_numpy(np.ascontiguousarray(m.rasterize(self.grid))[None]).to(f"cuda:{self.device}")
+        return [img[0] for img in self.compute_batch_through_focus(r, focus_nm).cpu().numpy()]
+
+    def compute_batch_through_focus(self, rasters, focus_nm: Sequence[float], pixel_transfer: bool = True,
+                                    form: str = "auto", eval_grid: int = 0, out=None, stream=None):
+        """process::batch_defocus (process.rs:1303-1313) for a batch of device
+        rasters: returns float32 (planes, B, N, N) on the device."""
+        import torch
+        n = self.grid.size
+        if rasters.dim() == 2:
+            rasters = rasters.unsqueeze(0)
+        if not rasters.is_cuda or rasters.shape[-2:] != (n, n):
+            raise ValueError(f"rasters must be (B, {n}, {n}) on the CUDA device")
+        rasters = rasters.contiguous()
+        z = np.ascontiguousarray(np.asarray(focus_nm, dtype=np.float64).reshape(-1))
+        if out is None:
+            out = torch.empty((len(z), rasters.shape[0], n, n), dtype=torch.float32, device=rasters.device)
+        b = L.Batch(rasters.shape[0], self._kind(rasters), rasters.data_ptr(), int(pixel_transfer), 0.0,
+                    L.FORM[form], int(eval_grid))
+        st = (stream or torch.cuda.current_stream(rasters.device)).cuda_stream
+        L.check(L.lib().huv_image_focus_sweep(self._h, C.byref(b), z.ctypes.data, len(z), out.data_ptr(), st))
+        return out
 
     def compute_from_transmittance(self, transmittance, focus_nm: float = 0.0) -> np.ndarray:
         """Image of a complex transmittance map (n, n) [y, x]

@@ -175,6 +175,15 @@ huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out
   });
 }
 
+huv_status huv_image_focus_sweep(void* engine, const huv_batch* batch, const double* focus_nm, int32_t n_planes,
+                                 float* out, void* stream) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!batch) throw Error(HUV_ERR_INVALID_PARAMETER, "batch: null");
+    e->image_focus_sweep(*batch, focus_nm, n_planes, out, static_cast<cudaStream_t>(stream));
+  });
+}
+
 huv_status huv_ilt_cost_grad(void* engine, const huv_ilt_params* params, int32_t n_masks, const float* theta,
                              const float* target, double* cost_host, float* grad, void* stream) {
   return guarded([&] {

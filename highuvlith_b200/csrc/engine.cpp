@@ -17,6 +17,10 @@
 #include <vector>
 
 #include "engine.hpp"
+
+#include <atomic>
+#include <exception>
+#include <thread>
 #include "host/host.hpp"
 
 namespace huv_launch {
@@ -97,8 +101,9 @@ Engine::Engine(const huv_source& s, const huv_optics& o, const huv_grid& g, cons
   const double cutoff = optics.cutoff(lambda);
   const double df_sigma = (1.0 / (n * pixel_nm)) / cutoff;
   points = sample_source(fill, st.source_points_per_axis, df_sigma);
-  focus = std::make_shared<KernelSet>(build_kernels(points, optics, n, pixel_nm, lambda, st.max_kernels,
-                                                    st.kernel_energy_fraction, 0.0));
+  if (st.kernel_build < HUV_BUILD_HOST || st.kernel_build > HUV_BUILD_DEVICE_RULE)
+    throw Error(HUV_ERR_INVALID_PARAMETER, "kernel_build: unknown");
+  focus = std::make_shared<KernelSet>(build_set(0.0));
 }
 
 Engine::~Engine() {
@@ -128,6 +133,14 @@ Engine::~Engine() {
   }
 }
 
+KernelSet Engine::build_set(double z) {
+  if (settings.kernel_build == HUV_BUILD_HOST)
+    return build_kernels(points, optics, n, pixel_nm, lambda, settings.max_kernels, settings.kernel_energy_fraction, z);
+  return build_kernels_device(points, optics, n, pixel_nm, lambda, settings.max_kernels,
+                              settings.kernel_energy_fraction, z, device,
+                              settings.kernel_build == HUV_BUILD_DEVICE_RULE);
+}
+
 std::shared_ptr<KernelSet> Engine::kernel_set(double z) {
   if (z == 0.0) return focus;
   for (auto& e : cache)
@@ -135,11 +148,15 @@ std::shared_ptr<KernelSet> Engine::kernel_set(double z) {
       e.last_used = ++clock;
       return e.ks;
     }
-  auto ks = std::make_shared<KernelSet>(build_kernels(points, optics, n, pixel_nm, lambda, settings.max_kernels,
-                                                      settings.kernel_energy_fraction, z));
+  auto ks = std::make_shared<KernelSet>(build_set(z));
+  cache_insert(z, ks);
+  return ks;
+}
+
+void Engine::cache_insert(double z, std::shared_ptr<KernelSet> ks) {
   if (settings.kernel_cache_capacity <= 0) {
     scratch_set = ks;
-    return ks;
+    return;
   }
   if (static_cast<int>(cache.size()) >= settings.kernel_cache_capacity) {
     auto it = std::min_element(cache.begin(), cache.end(),
@@ -158,7 +175,64 @@ std::shared_ptr<KernelSet> Engine::kernel_set(double z) {
   e.ks = ks;
   e.last_used = ++clock;
   cache.push_back(e);
-  return ks;
+}
+
+void Engine::prebuild_planes(const double* z, int planes) {
+  std::vector<double> todo;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    for (int p = 0; p < planes; ++p) {
+      const double zz = z[p];
+      if (zz == 0.0 || std::find(todo.begin(), todo.end(), zz) != todo.end()) continue;
+      bool have = false;
+      for (const auto& e : cache) have = have || e.z == zz;
+      if (!have) todo.push_back(zz);
+    }
+    const size_t cap = static_cast<size_t>(std::max(settings.kernel_cache_capacity, 0));
+    if (todo.size() > cap) todo.resize(cap);  // the rest is built on demand
+  }
+  if (todo.empty()) return;
+  std::vector<std::shared_ptr<KernelSet>> built(todo.size());
+  std::vector<std::exception_ptr> errs(todo.size());
+  std::atomic<size_t> next{0};
+  auto worker = [&] {
+    SerialHostScope serial;
+    for (size_t i; (i = next.fetch_add(1)) < todo.size();) {
+      try {
+        built[i] = std::make_shared<KernelSet>(build_set(todo[i]));
+      } catch (...) {
+        errs[i] = std::current_exception();
+      }
+    }
+  };
+  const int nt = static_cast<int>(std::min<size_t>(todo.size(), static_cast<size_t>(host_threads())));
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(worker);
+  worker();
+  for (auto& t : th) t.join();
+  for (auto& e : errs)
+    if (e) std::rethrow_exception(e);
+  std::lock_guard<std::mutex> lock(mu);
+  for (size_t i = 0; i < todo.size(); ++i) {
+    bool have = false;
+    for (const auto& e : cache) have = have || e.z == todo[i];
+    if (!have) cache_insert(todo[i], built[i]);
+  }
+}
+
+void Engine::image_focus_sweep(const huv_batch& b, const double* z, int planes, float* out, cudaStream_t st) {
+  if (planes < 0) throw Error(HUV_ERR_INVALID_PARAMETER, "n_planes: must be >= 0");
+  if (planes == 0 || b.n_clips == 0) return;
+  if (!z || !out) throw Error(HUV_ERR_INVALID_PARAMETER, "focus/out: null pointer");
+  for (int p = 0; p < planes; ++p)
+    if (!std::isfinite(z[p])) throw Error(HUV_ERR_INVALID_PARAMETER, "focus_nm: must be finite");
+  prebuild_planes(z, planes);
+  const size_t plane = static_cast<size_t>(b.n_clips) * n * n;
+  for (int p = 0; p < planes; ++p) {
+    huv_batch bp = b;
+    bp.defocus_nm = z[p];
+    image_batch(bp, out + plane * p, st);
+  }
 }
 
 // ------------------------------------------------------------ device side

@@ -125,8 +125,16 @@ struct Engine {
   ~Engine();
 
   std::shared_ptr<KernelSet> kernel_set(double z);
+  void cache_insert(double z, std::shared_ptr<KernelSet> ks);
+  // The kernel set of focus plane z, built where settings.kernel_build says.
+  KernelSet build_set(double z);
   void image_batch(const huv_batch& b, float* out, cudaStream_t st);
   void image_batch_host(const huv_batch& b, float* out_host, cudaStream_t st);
+  // Kernel sets of the focus planes not cached yet, built concurrently (one
+  // plane per host thread) and cached.
+  void prebuild_planes(const double* z, int planes);
+  // out[plane][clip][y][x]: the batch imaged at every focus plane.
+  void image_focus_sweep(const huv_batch& b, const double* z, int planes, float* out, cudaStream_t st);
 
   // device helpers
   void ensure_device();

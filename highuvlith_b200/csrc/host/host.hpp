@@ -79,6 +79,13 @@ KernelSet build_kernels(const std::vector<SourcePoint>& points, const Optics& op
                         double pixel_nm, double lambda, int max_kernels, double fraction,
                         double defocus_nm, int force_method = -1);
 
+// The same kernel set built with the A matrix and its products on GPU
+// `device` in FP64 (csrc/cuda/kbuild.cu); reference_rule selects the
+// reference's solver rule (randomized subspace iteration for large problems).
+KernelSet build_kernels_device(const std::vector<SourcePoint>& points, const Optics& optics, int n,
+                               double pixel_nm, double lambda, int max_kernels, double fraction,
+                               double defocus_nm, int device, bool reference_rule);
+
 // Hermitian eigensolver (column-major n x n input, both triangles read).
 // Returns eigenvalues in decreasing order and the first `count` eigenvectors
 // (column-major n x count).
@@ -88,5 +95,12 @@ void hermitian_eigen(int n, const std::vector<cd>& h, std::vector<double>& value
 // Worker count for host-parallel loops.
 int host_threads();
 void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)>& body);
+// While alive, parallel_for on this thread runs serially (for callers that
+// parallelise at a coarser grain themselves).
+struct SerialHostScope {
+  SerialHostScope();
+  ~SerialHostScope();
+  bool prev;
+};
 
 }  // namespace huv

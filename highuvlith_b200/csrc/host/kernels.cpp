@@ -124,6 +124,9 @@ Pool& pool() {
 }
 }  // namespace
 
+SerialHostScope::SerialHostScope() : prev(Pool::in_worker()) { Pool::in_worker() = true; }
+SerialHostScope::~SerialHostScope() { Pool::in_worker() = prev; }
+
 void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)>& body) {
   const int t = static_cast<int>(std::min<int64_t>(host_threads(), std::max<int64_t>(n / 64, 1)));
   if (t <= 1 || n < 128 || Pool::in_worker()) {

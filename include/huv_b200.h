@@ -86,7 +86,16 @@ typedef struct {
   int32_t source_points_per_axis; /* 0 = adaptive sampling, n >= 1 = n x n grid */
   int32_t normalization;          /* 0 = clear field (relative), 1 = absolute */
   int32_t kernel_cache_capacity;  /* kernel sets kept per engine (focus planes) */
+  int32_t kernel_build;           /* huv_kernel_build: where the FP64 kernel set is built */
 } huv_settings;
+
+/* Where the FP64 SOCS kernel set is built (KernelBuilder::build, aerial.rs:1041-1317). */
+typedef enum {
+  HUV_BUILD_HOST = 0,          /* host C++, dense Hermitian eigensolve */
+  HUV_BUILD_DEVICE = 1,        /* A matrix and its products on the GPU (FP64), dense eigensolve */
+  HUV_BUILD_DEVICE_RULE = 2    /* as 1, with the reference's solver rule (aerial.rs:1116-1128):
+                                  randomized subspace iteration when the problem is large */
+} huv_kernel_build;
 
 /* KernelDiagnostics (aerial.rs:254-276). method: 0 dense_tcc, 1 dense_gram. */
 typedef struct {
@@ -166,6 +175,15 @@ huv_status huv_image_batch(void* engine, const huv_batch* batch, float* out, voi
 /* Same call with HOST input and output buffers: copies in, images, copies out
  * on `stream` and synchronises it (the reference-facing end-to-end call). */
 huv_status huv_image_batch_host(void* engine, const huv_batch* batch, float* out_host, void* stream);
+
+/* Through-focus imaging: compute_through_focus (aerial.rs:1820-1825) and
+ * process::batch_defocus (process.rs:1303-1313) for a batch of clips.
+ * out (device) is n_planes*n_clips*N*N floats, [plane][clip][y][x]; the
+ * batch's own defocus_nm is ignored.  Kernel sets of planes not yet cached
+ * are built concurrently on the host (one plane per thread, FP64), then every
+ * plane is imaged on `stream`. */
+huv_status huv_image_focus_sweep(void* engine, const huv_batch* batch, const double* focus_nm, int32_t n_planes,
+                                 float* out, void* stream);
 
 /* Uneven batches (no counterpart in the reference, which images one clip per
  * call): clips of different grids, sources and kernel budgets in one CUDA
