@@ -43,9 +43,12 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s per wait
 constexpr uint32_t kABox = 128 * 128;             // 128 rows x 64 bf16
 // B box of BN rows x 64 bf16
 __host__ __device__ constexpr uint32_t b_box_bytes(int bn) { return static_cast<uint32_t>(bn) * 128; }
-// Row-transform GEMM (MODE 2): N = band rows padded to a multiple of 16.
+// Row-transform GEMM (MODE 2): N = band rows padded to 80 (B <= 80) or 96
+// (B <= 96, the largest band whose operand rows fit K = 192).
 constexpr int kRowBN = 80;
-constexpr int kStageWords = 2 * 16 * 81;  // per epilogue warp: [plane][16 x][80 (+1 pad) my] bf16x2
+constexpr int kRowBNWide = 96;
+// per epilogue warp: [plane][16 x][BN (+1 pad) my] bf16x2
+__host__ __device__ constexpr int stage_words(int bn) { return 2 * 16 * (bn + 1); }
 
 struct TcGemmParams {
   int kboxes;       // 64-wide K boxes loaded
@@ -67,6 +70,7 @@ struct TcGemmParams {
   long long bop_prob;   // elements between problems
   long long bop_plane;  // elements between the hi and lo planes
   int bop_ld;           // row stride (elements)
+  int bop_cols;         // band rows my written (2 bop_cols <= bop_ld)
 };
 
 __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
@@ -76,7 +80,7 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bflo
 
 __host__ __device__ constexpr size_t tc_smem_bytes(int kboxes, int bn = kTcBN, bool stage = false) {
   return 1024 + 2 * static_cast<size_t>(kboxes) * kABox + kTcStages * 2 * static_cast<size_t>(b_box_bytes(bn)) +
-         256 + (stage ? 4 * kStageWords * sizeof(uint32_t) : 0);
+         256 + (stage ? 4 * static_cast<size_t>(stage_words(bn)) * sizeof(uint32_t) : 0);
 }
 
 // MODE 0: sum over G steps (kernels) of |E|^2 with (re, im) in adjacent
@@ -218,7 +222,8 @@ __global__ void __launch_bounds__(192, 1)
     const int row = quad * 32 + lane;  // accumulator row within the tile
     constexpr int HALF = BN / 2;
     // MODE 2 staging: after the 256 bytes of barriers, kStageWords per warp
-    uint32_t* stage = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(bars) + 256) + quad * kStageWords;
+    constexpr int SLD = BN + 1;  // staging row stride (words)
+    uint32_t* stage = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(bars) + 256) + quad * stage_words(BN);
     float acc[MODE == 0 ? HALF : 1];
 #pragma unroll
     for (int i = 0; i < (MODE == 0 ? HALF : 1); ++i) acc[i] = 0.f;
@@ -253,17 +258,18 @@ __global__ void __launch_bounds__(192, 1)
             __nv_bfloat162 pr;
             pr.x = odd ? rl : rh;
             pr.y = odd ? il : ih;
-            stage[(odd * 16 + xl) * 81 + c0 + i] = *reinterpret_cast<uint32_t*>(&pr);
+            stage[(odd * 16 + xl) * SLD + c0 + i] = *reinterpret_cast<uint32_t*>(&pr);
           }
         }
         __syncwarp();
-        // coalesced copy-out: 32 rows (2 planes x 16 x) of BN bf16 pairs
+        // coalesced copy-out: 32 rows (2 planes x 16 x) of bop_cols bf16 pairs
         const int x0 = (m_tile * 128 + quad * 32) >> 1;
+        const int nc = p.bop_cols;
         uint32_t* base_out = reinterpret_cast<uint32_t*>(p.bop + prob * p.bop_prob + g * p.bop_g);
-        for (int w = lane; w < 32 * BN; w += 32) {
-          const int r = w / BN, my = w - r * BN;
+        for (int w = lane; w < 32 * nc; w += 32) {
+          const int r = w / nc, my = w - r * nc;
           const int pl = r >> 4, x = x0 + (r & 15);
-          base_out[(pl * p.bop_plane + static_cast<long long>(x) * p.bop_ld) / 2 + my] = stage[r * 81 + my];
+          base_out[(pl * p.bop_plane + static_cast<long long>(x) * p.bop_ld) / 2 + my] = stage[r * SLD + my];
         }
         __syncwarp();
       }
@@ -466,6 +472,9 @@ cudaError_t tc_set_smem() {
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<2, kRowBN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, kRowBN, true)))))
     return e;
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<2, kRowBNWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, kRowBNWide, true)))))
+    return e;
   if ((e = cudaFuncSetAttribute(socs_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   return cudaSuccess;
 }
@@ -554,7 +563,9 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const size_t per_x = align256(sizeof(float2) * n * B);
   const size_t per_m = align256(sizeof(float2) * B * B);
   const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kpE * 2);
-  const size_t per_p = align256(static_cast<size_t>(K) * 2 * kRowBN * kpE * 2);
+  const int rbn = B <= kRowBN ? kRowBN : kRowBNWide;  // rows of P (band rows my, padded)
+  if (B > kRowBNWide) throw Error(HUV_ERR_UNSUPPORTED, "TC form: band wider than 96 orders");
+  const size_t per_p = align256(static_cast<size_t>(K) * 2 * rbn * kpE * 2);
   const size_t per_i = align256(sizeof(float) * M * M);
   const size_t per_x2 = align256(sizeof(float2) * M * B2);
   const size_t per_c = align256(sizeof(float2) * B2 * B2);
@@ -593,30 +604,34 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     CUtensorMap mbE, mbI, mbP;
     if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kpE, kTcBN) ||
         !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kpI, kTcBN) ||
-        !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * kRowBN, kpE, kRowBN))
+        !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * rbn, kpE, rbn))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
     {
       // Row transforms of every kernel's band product on tensor cores: the
       // same M-point inverse DFT operand (A_E) against the split products,
       // written straight as the next GEMM's split operand.
-      band_products<<<dim3(K, nc), 256, 0, st>>>(ds.kband, Mb, K, B, kRowBN, kpE, P);
+      band_products<<<dim3(K, nc), 256, 0, st>>>(ds.kband, Mb, K, B, rbn, kpE, P);
       check_cuda(cudaGetLastError(), "band_products");
       TcGemmParams p{};
       p.kboxes = kpE / 64;
       p.ksteps = kstE;
       p.G = K;
       p.a_rows = 2 * M;
-      p.b_prob = K * 2 * kRowBN;
-      p.b_step = 2 * kRowBN;
-      p.b_plane = kRowBN;
+      p.b_prob = K * 2 * rbn;
+      p.b_step = 2 * rbn;
+      p.b_plane = rbn;
       p.err = dev_err;
       p.bop = BE;
       p.bop_g = 2ll * M * kpE;
       p.bop_prob = static_cast<long long>(K) * 2 * M * kpE;
       p.bop_plane = static_cast<long long>(M) * kpE;
       p.bop_ld = kpE;
+      p.bop_cols = std::min(kstE * 8, rbn);  // the K columns GEMM0 reads: 2 my + re/im < 16 kstE
       dim3 g(1, 2 * M / 128, nc);
-      tc_dft_gemm<2, kRowBN><<<g, 192, tc_smem_bytes(3, kRowBN, true), st>>>(tc.map_ae, mbP, p);
+      if (rbn == kRowBN)
+        tc_dft_gemm<2, kRowBN><<<g, 192, tc_smem_bytes(3, kRowBN, true), st>>>(tc.map_ae, mbP, p);
+      else
+        tc_dft_gemm<2, kRowBNWide><<<g, 192, tc_smem_bytes(3, kRowBNWide, true), st>>>(tc.map_ae, mbP, p);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<2>");
     }
     {

@@ -49,23 +49,31 @@ def test_device_build_matches_host_build(case, z):
 
 @pytest.mark.parametrize("z", [0.0, 90.0])
 def test_randomized_rule_matches_dense_within_reference_bounds(z):
-    """EUV 256^2 at 1 nm, sigma 0.7, K = 20: 349 orders > 320 and 3 (20 + 16)
-    < 349, so the reference's rule takes the randomized solver."""
+    """EUV 256^2 at 1 nm, sigma 0.7: 349 orders > 320 and 3 (6 + 16) < 349, so
+    the reference's rule takes the randomized solver.  Six kernels, as in the
+    reference's own test (aerial.rs:2650-2675): each eigenvalue within 10 x
+    (lambda_{l+1} / lambda_k)^(2q+1) of the dense one, images within 1e-5."""
     src, opt, grid = HB.SourceConfig.euv(0.7), HB.OpticsConfig.euv_nxe_033(), HB.GridConfig(256, 1.0)
-    dense = HB.SimulationEngine(src, opt, grid=grid, max_kernels=20)
-    rnd = HB.SimulationEngine(src, opt, grid=grid, max_kernels=20, kernel_build="device_reference_rule")
+    dense = HB.SimulationEngine(src, opt, grid=grid, max_kernels=6)
+    rnd = HB.SimulationEngine(src, opt, grid=grid, max_kernels=6, kernel_build="device_reference_rule")
     assert rnd.imaging_diagnostics(z)["method"] == "randomized"
     assert dense.imaging_diagnostics(z)["method"] == "dense_tcc"
     ev_d, _ = dense.kernels(z)
     ev_r, _ = rnd.kernels(z)
-    assert len(ev_r) == len(ev_d)
-    # all eigenvalues of the dense TCC for the bound (lambda_{l+1} / lambda_k)^(2q+1)
+    assert len(ev_r) == len(ev_d) == 6
     full = HB.SimulationEngine(src, opt, grid=grid, max_kernels=1000)
     ev_all, _ = full.kernels(z)
-    l = 20 + 16
-    for k in range(len(ev_d)):
-        bound = max((ev_all[l] / ev_all[k]) ** 7, 1e-13) if l < len(ev_all) else 1e-13
-        assert abs(ev_r[k] / ev_d[k] - 1.0) <= 10.0 * bound + 1e-12, (k, ev_r[k], ev_d[k])
+    l = 6 + 16
+    for k in range(6):
+        bound = max((ev_all[l] / ev_all[k]) ** 7, 1e-13)
+        assert abs(ev_r[k] / ev_d[k] - 1.0) <= 10.0 * bound, (k, ev_r[k], ev_d[k], bound)
     _, rasters = gen_batch(2, 256, base_seed=9, wmin=8, wmax=40, dmin=0.2, dmax=0.6)
     a, b = _images(dense, rasters, z), _images(rnd, rasters, z)
     assert np.max(np.abs(a - b)) < 1e-5
+
+
+def test_reference_rule_keeps_dense_for_small_problems():
+    """min(orders, columns) <= 320: the rule solves densely (as the host)."""
+    src, opt, grid = HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(), HB.GridConfig(128, 1.0)
+    eng = HB.SimulationEngine(src, opt, grid=grid, max_kernels=16, kernel_build="device_reference_rule")
+    assert eng.imaging_diagnostics()["method"] in ("dense_tcc", "dense_gram")
