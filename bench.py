@@ -432,7 +432,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.quick:
         # other device forms on the same batch (fewer steps), for the TC-vs-plain factor
         forms = {}
-        for name, form, eg in (("fft_full_grid", "fft", N_GRID), ("fft_coarse_grid", "fft", 0), ("tc", "tc", 0)):
+        for name, form, eg in (("fft_full_grid", "fft", N_GRID), ("fft_coarse_grid", "fft", 0), ("tc", "tc", 0),
+                               ("tc_gemm_rows", "tc_rows", 0)):
             try:
                 step(form, eg)
                 torch.cuda.synchronize()
@@ -495,7 +496,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="auto", choices=["auto", "fft", "tc"])
+    ap.add_argument("--form", default="auto", choices=["auto", "fft", "tc", "tc_rows"])
     ap.add_argument("--eval-grid", dest="eval_grid", type=int, default=0)
     ap.add_argument("--quick", action="store_true", help="skip the extra forms, accuracy and CPU baseline")
     ap.add_argument("--uneven-clips", dest="uneven_clips", type=int, default=2048)

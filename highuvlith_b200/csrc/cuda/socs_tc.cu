@@ -512,7 +512,7 @@ bool Engine::tc_supported(const DeviceSet& ds, int M) const {
 }
 
 void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use,
-                         const float* W_use) {
+                         const float* W_use, bool gemm_rows) {
   using namespace huv_launch;
   static bool smem_set = false;
   if (!smem_set) {
@@ -565,7 +565,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kpE * 2);
   const int rbn = B <= kRowBN ? kRowBN : kRowBNWide;  // rows of P (band rows my, padded)
   if (B > kRowBNWide) throw Error(HUV_ERR_UNSUPPORTED, "TC form: band wider than 96 orders");
-  const size_t per_p = align256(static_cast<size_t>(K) * 2 * rbn * kpE * 2);
+  const size_t per_p = gemm_rows ? align256(static_cast<size_t>(K) * 2 * rbn * kpE * 2) : 0;
   const size_t per_i = align256(sizeof(float) * M * M);
   const size_t per_x2 = align256(sizeof(float2) * M * B2);
   const size_t per_c = align256(sizeof(float2) * B2 * B2);
@@ -604,9 +604,16 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     CUtensorMap mbE, mbI, mbP;
     if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kpE, kTcBN) ||
         !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kpI, kTcBN) ||
-        !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * rbn, kpE, rbn))
+        (gemm_rows && !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * rbn, kpE, rbn)))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
-    {
+    if (!gemm_rows) {
+      // Row transforms as FP32 shared-memory FFTs, emitting the split operand.
+      const int S = fit_units(8, 2 * (sizeof(float2) << lgm));
+      dim3 g((K * B + S - 1) / S, nc);
+      const size_t sm = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
+      socs_rows_tc<<<g, 256, sm, st>>>(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, S, kpE, kstE * 16, BE, twm);
+      check_cuda(cudaGetLastError(), "socs_rows_tc");
+    } else {
       // Row transforms of every kernel's band product on tensor cores: the
       // same M-point inverse DFT operand (A_E) against the split products,
       // written straight as the next GEMM's split operand.
@@ -686,7 +693,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       tc_dft_gemm<1><<<g, 192, smem_tc, st>>>(tc.map_ai, mbI, p);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
     }
-    prof.launches += 8;
+    prof.launches += gemm_rows ? 8 : 7;
   }
 }
 

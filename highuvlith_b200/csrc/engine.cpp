@@ -458,9 +458,9 @@ void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
   const int Mtc = (b.eval_grid == 0 && M < 128 && n >= 128) ? 128 : M;
   int form = b.form;
   if (form == HUV_FORM_AUTO) form = tc_supported(ds, Mtc) ? HUV_FORM_TC : HUV_FORM_FFT;
-  if (form == HUV_FORM_TC) {
+  if (form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS) {
     if (!tc_supported(ds, Mtc)) throw Error(HUV_ERR_UNSUPPORTED, "TC form: unsupported band/grid for this build");
-    run_tc_form(b, ds, Mtc, out, st);
+    run_tc_form(b, ds, Mtc, out, st, 0, nullptr, form == HUV_FORM_TC_ROWS);
   } else if (form == HUV_FORM_FFT) {
     run_fft_form(b, ds, M, out, st);
   } else {

@@ -147,7 +147,7 @@ struct Engine {
   void run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use = 0,
                     const float* W_use = nullptr);
   void run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use = 0,
-                   const float* W_use = nullptr);
+                   const float* W_use = nullptr, bool gemm_rows = false);
   // Flare weights W = sum_{k < K} lambda_k |u_k|^2 / N^4 of the first K kernels (device, cached).
   const float* flare_weights(DeviceSet& ds, int K);
   // Kernel count for a budget of `max_kernels` under the reference's truncation rule.

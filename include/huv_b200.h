@@ -122,7 +122,8 @@ typedef enum {
 typedef enum {
   HUV_FORM_AUTO = 0, /* autotuned choice */
   HUV_FORM_FFT = 1,  /* plain FP32 FFT form */
-  HUV_FORM_TC = 2    /* split-BF16x3 tcgen05 DFT-GEMM form */
+  HUV_FORM_TC = 2,   /* split-BF16x3 tcgen05 DFT-GEMM form (row transforms as FP32 FFTs) */
+  HUV_FORM_TC_ROWS = 3 /* the same with the row transforms as tcgen05 DFT-GEMMs too */
 } huv_form;
 
 typedef struct {

@@ -148,10 +148,12 @@ def test_c2_clips_full_size_parity_and_cd():
 TC_CASES = [c for c in SMALL if c[3].size >= 128]
 
 
+@pytest.mark.parametrize("form", ["tc", "tc_rows"])
 @pytest.mark.parametrize("case", TC_CASES, ids=[c[0] for c in TC_CASES])
-def test_tc_form_matches_oracle(case):
+def test_tc_form_matches_oracle(case, form):
     """Split-BF16x3 tcgen05 form vs the FP64 oracle (tolerance 1e-3; the
-    split products carry ~2^-16 relative precision)."""
+    split products carry ~2^-16 relative precision); row transforms as FFTs
+    ("tc") or as tensor-core DFT-GEMMs too ("tc_rows")."""
     torch = _torch()
     _, src, opt, grid, kmax, fill, oopt = case
     eng = HB.SimulationEngine(src, opt, grid=grid, max_kernels=kmax)
@@ -159,7 +161,7 @@ def test_tc_form_matches_oracle(case):
     n = grid.size
     _, rasters = gen_batch(3, n, base_seed=13, wmin=max(2, n // 40), wmax=max(4, n // 8), dmin=0.2, dmax=0.6)
     d = torch.from_numpy(rasters).cuda()
-    out = eng.compute_batch(d, form="tc").cpu().numpy()
+    out = eng.compute_batch(d, form=form).cpu().numpy()
     eng.device_status()
     for c in range(3):
         ref = oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[c]))
