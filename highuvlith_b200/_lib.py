@@ -20,7 +20,7 @@ STATUS_NAMES = {
 
 FILL = {"conventional": 0, "annular": 1, "quadrupole": 2, "dipole": 3, "gaussian": 4, "quasar": 5}
 OPTICS_PROJECTION, OPTICS_EUV = 0, 1
-INPUT_U8, INPUT_F32, INPUT_C64 = 0, 1, 2
+INPUT_U8, INPUT_F32, INPUT_C64, INPUT_RECTS = 0, 1, 2, 3
 FORM = {"auto": 0, "fft": 1, "tc": 2, "tc_rows": 3}
 
 
@@ -80,6 +80,15 @@ class SurrogateIlt(C.Structure):
     _fields_ = [("judge_every", C.c_int32), ("error_bound", C.c_double), ("surrogate_iterations", C.c_int32),
                 ("exact_iterations", C.c_int32), ("takeover_iteration", C.c_int32), ("n_judges", C.c_int32),
                 ("judge_errors", C.c_double * 64)]
+
+
+class Rect(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("w", C.c_double), ("h", C.c_double)]
+
+
+class RectClips(C.Structure):
+    _fields_ = [("rects", C.c_void_p), ("offsets", C.c_void_p), ("feature_re", C.c_double),
+                ("feature_im", C.c_double), ("background_re", C.c_double), ("background_im", C.c_double)]
 
 
 class Batch(C.Structure):

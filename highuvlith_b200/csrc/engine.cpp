@@ -124,6 +124,10 @@ Engine::~Engine() {
     cudaFree(ws);
     cudaFree(io_in);
     cudaFree(io_out);
+    cudaFree(rect.clip_rows);
+    cudaFree(rect.rows);
+    cudaFree(rect.runs);
+    cudaFree(rect.coef);
     if (io_h2d) {
       cudaStreamDestroy(io_h2d);
       cudaStreamDestroy(io_d2h);
@@ -392,7 +396,9 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
   const float* Wf = W_use ? W_use : ds.W;
   const bool coarse = M < n;
   const int h2 = 2 * hb, B2 = 2 * h2 + 1;
-  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
+  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8
+                             ? 1
+                             : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : (b.input_kind == HUV_INPUT_RECTS ? 0 : 8));
   // Per-clip workspace.
   const size_t per_x = align256(sizeof(float2) * n * B);
   const size_t per_m = align256(sizeof(float2) * B * B);
@@ -421,9 +427,12 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
     const int nc = std::min(chunk, b.n_clips - c0);
     const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
     float* o = out + static_cast<size_t>(n) * n * c0;
-    check_cuda(huv_launch::band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb,
-                                        b.pixel_transfer ? ds.ptx : nullptr, Wf, mean, twn, st),
-               "band_forward");
+    if (b.input_kind == HUV_INPUT_RECTS)
+      rect_band(c0, nc, hb, Wf, Mb, mean, st);
+    else
+      check_cuda(huv_launch::band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb,
+                                          b.pixel_transfer ? ds.ptx : nullptr, Wf, mean, twn, st),
+                 "band_forward");
     prof.launches += 2;
     check_cuda(huv_launch::socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");
     prof.begin("socs_cols_inv", st);
@@ -448,9 +457,10 @@ void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
   if (b.n_clips < 0) throw Error(HUV_ERR_INVALID_PARAMETER, "n_clips: must be >= 0");
   if (b.n_clips == 0) return;
   if (!b.input || !out) throw Error(HUV_ERR_INVALID_PARAMETER, "input/out: null pointer");
-  if (b.input_kind < 0 || b.input_kind > 2) throw Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
+  if (b.input_kind < 0 || b.input_kind > 3) throw Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
   if (!std::isfinite(b.defocus_nm)) throw Error(HUV_ERR_INVALID_PARAMETER, "defocus_nm: must be finite");
   ensure_device();
+  if (b.input_kind == HUV_INPUT_RECTS) upload_rects(b);
   DeviceSet& ds = device_set(b.defocus_nm == 0.0 ? 0.0 : b.defocus_nm);
   const int M = choose_eval_grid(ds, b.eval_grid);
   // The tensor-core form tiles the evaluation grid by 128; an automatically
@@ -477,8 +487,13 @@ void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t 
   std::lock_guard<std::mutex> host_lock(host_mu);
   if (b.n_clips <= 0) return;
   if (!b.input || !out_host) throw Error(HUV_ERR_INVALID_PARAMETER, "input/out: null pointer");
-  if (b.input_kind < 0 || b.input_kind > 2) throw Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
-  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
+  if (b.input_kind < 0 || b.input_kind > 3) throw Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
+  // Rectangle clips are read on the host (their tables are built there):
+  // nothing to copy in, each chunk views its slice of the offsets.
+  const bool rects = b.input_kind == HUV_INPUT_RECTS;
+  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8
+                             ? 1
+                             : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : (rects ? 0 : 8));
   const size_t in_per = in_elem * static_cast<size_t>(n) * n;
   const size_t out_per = sizeof(float) * static_cast<size_t>(n) * n;
   const int by_bytes = static_cast<int>(std::max<size_t>(1, (size_t(128) << 20) / out_per));
@@ -523,9 +538,10 @@ void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t 
     float* dout = reinterpret_cast<float*>(static_cast<char*>(io_out) + out_per * chunk * slot);
     // the input slot is free once the imaging of chunk i - ring has run
     if (i >= ring) check_cuda(cudaStreamWaitEvent(io_h2d, img_done[slot], 0), "wait(img)");
-    check_cuda(cudaMemcpyAsync(din, static_cast<const char*>(b.input) + in_per * c0, in_per * nc,
-                               cudaMemcpyHostToDevice, io_h2d),
-               "H2D input");
+    if (!rects)
+      check_cuda(cudaMemcpyAsync(din, static_cast<const char*>(b.input) + in_per * c0, in_per * nc,
+                                 cudaMemcpyHostToDevice, io_h2d),
+                 "H2D input");
     check_cuda(cudaEventRecord(in_done[slot], io_h2d), "record(in)");
     check_cuda(cudaStreamWaitEvent(st, in_done[slot], 0), "wait(in)");
     // the output slot is free once chunk i - ring has been copied out
@@ -533,6 +549,12 @@ void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t 
     huv_batch d = b;
     d.n_clips = nc;
     d.input = din;
+    huv_rect_clips view{};
+    if (rects) {
+      view = *static_cast<const huv_rect_clips*>(b.input);
+      view.offsets += c0;
+      d.input = &view;
+    }
     image_batch(d, dout, st);
     check_cuda(cudaEventRecord(img_done[slot], st), "record(img)");
     check_cuda(cudaStreamWaitEvent(io_d2h, img_done[slot], 0), "wait(img)");

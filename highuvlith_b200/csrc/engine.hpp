@@ -130,6 +130,10 @@ struct Engine {
   KernelSet build_set(double z);
   void image_batch(const huv_batch& b, float* out, cudaStream_t st);
   void image_batch_host(const huv_batch& b, float* out_host, cudaStream_t st);
+  // Rectangle clips (HUV_INPUT_RECTS): the batch's row/run table on the
+  // device, then the exact band spectrum of clips [c0, c0 + nc).
+  void upload_rects(const huv_batch& b);
+  void rect_band(int c0, int nc, int hb, const float* W, float2* Mband, float* mean, cudaStream_t st);
   // Kernel sets of the focus planes not cached yet, built concurrently (one
   // plane per host thread) and cached.
   void prebuild_planes(const double* z, int planes);
@@ -194,6 +198,12 @@ struct Engine {
   void* io_in = nullptr;
   void* io_out = nullptr;
   size_t io_in_bytes = 0, io_out_bytes = 0;
+  struct RectTable {
+    void *clip_rows = nullptr, *rows = nullptr, *runs = nullptr, *coef = nullptr;
+    size_t clip_rows_cap = 0, rows_cap = 0, runs_cap = 0, coef_cap = 0;
+    int n_rows = 0;
+    double2 dv{0, 0}, bg{0, 0};
+  } rect;
   cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
   cudaEvent_t io_ev[3][3] = {};  // [copy-in done, imaging done, copy-out done][ring slot]
 };

@@ -115,8 +115,31 @@ typedef struct {
 typedef enum {
   HUV_INPUT_RASTER_U8 = 0,       /* N*N uint8 transmittance 0/1 (binary mask raster) */
   HUV_INPUT_RASTER_F32 = 1,      /* N*N float real transmittance */
-  HUV_INPUT_TRANSMITTANCE_C64 = 2/* N*N interleaved (re, im) float complex transmittance */
+  HUV_INPUT_TRANSMITTANCE_C64 = 2,/* N*N interleaved (re, im) float complex transmittance */
+  HUV_INPUT_RECTS = 3            /* huv_rect_clips (host memory): exact analytic spectrum */
 } huv_input_kind;
+
+/* A rectangle feature (mask.rs Feature::Rect): centre (x, y) and size (w, h)
+ * in nm, field coordinates centred on the grid (pixel centres at
+ * -L/2 + (j + 1/2) p).  Sub-pixel positions and overlaps are allowed. */
+typedef struct {
+  double x, y, w, h;
+} huv_rect;
+
+/* Rectangle clips for HUV_INPUT_RECTS: clip c is the union of
+ * rects[offsets[c] .. offsets[c + 1]) with amplitude `feature` on a field of
+ * amplitude `background` (binary dark field: feature 1, background 0; clear
+ * field with opaque features: feature 0, background 1; an attenuated PSM puts
+ * its complex absorber amplitude on either).  The spectrum is Mask::spectrum's
+ * closed form (mask.rs:616-657, 1439-1503) over the disjoint cells of the
+ * union (mask.rs:1365-1437), evaluated on the band on the GPU; pixel_transfer
+ * is ignored (the spectrum is exact). */
+typedef struct {
+  const huv_rect* rects;
+  const int32_t* offsets;   /* n_clips + 1 non-decreasing indexes into rects */
+  double feature_re, feature_im;
+  double background_re, background_im;
+} huv_rect_clips;
 
 /* Which device form evaluates the SOCS sum. */
 typedef enum {
