@@ -116,7 +116,7 @@ typedef enum {
   HUV_INPUT_RASTER_U8 = 0,       /* N*N uint8 transmittance 0/1 (binary mask raster) */
   HUV_INPUT_RASTER_F32 = 1,      /* N*N float real transmittance */
   HUV_INPUT_TRANSMITTANCE_C64 = 2,/* N*N interleaved (re, im) float complex transmittance */
-  HUV_INPUT_RECTS = 3            /* huv_rect_clips (host memory): exact analytic spectrum */
+  HUV_INPUT_RECTS = 3            /* a huv_rect_clips in host memory: exact analytic spectrum */
 } huv_input_kind;
 
 /* A rectangle feature (mask.rs Feature::Rect): centre (x, y) and size (w, h)
