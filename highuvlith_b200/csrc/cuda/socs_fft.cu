@@ -254,10 +254,12 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   const size_t sm1 = 2 * (static_cast<size_t>(S) << lg) * sizeof(float2);
   dim3 g1(n / rows_per_block, clips);
   const int th = pick_threads(S << (lg - 2));
+  // Only device rasters come here (rectangle clips take the analytic path).
   switch (kind) {
     case 0: band_rows_fwd<0><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
     case 1: band_rows_fwd<1><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
-    default: band_rows_fwd<2><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
+    case 2: band_rows_fwd<2><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
+    default: return cudaErrorInvalidValue;
   }
   const int B = 2 * hb + 1;
   const int cpb = fit_units(4, 2 * (sizeof(float2) << lg));

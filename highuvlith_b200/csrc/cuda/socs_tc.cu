@@ -559,7 +559,9 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the DFT operands");
     tc.lgm = lgm;
   }
-  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8 ? 1 : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : 8);
+  const size_t in_elem = b.input_kind == HUV_INPUT_RASTER_U8
+                             ? 1
+                             : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : (b.input_kind == HUV_INPUT_RECTS ? 0 : 8));
   const size_t per_x = align256(sizeof(float2) * n * B);
   const size_t per_m = align256(sizeof(float2) * B * B);
   const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kpE * 2);
@@ -598,9 +600,12 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     const int nc = std::min(chunk, b.n_clips - c0);
     const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
     float* o = out + static_cast<size_t>(n) * n * c0;
-    check_cuda(band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb, b.pixel_transfer ? ds.ptx : nullptr, Wf,
-                            mean, twn, st),
-               "band_forward");
+    if (b.input_kind == HUV_INPUT_RECTS)
+      rect_band(c0, nc, hb, Wf, Mb, mean, st);  // host-side table, exact spectrum on the device
+    else
+      check_cuda(band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb, b.pixel_transfer ? ds.ptx : nullptr, Wf,
+                              mean, twn, st),
+                 "band_forward");
     CUtensorMap mbE, mbI, mbP;
     if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kpE, kTcBN) ||
         !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kpI, kTcBN) ||
