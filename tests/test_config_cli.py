@@ -1,0 +1,122 @@
+"""TOML front end (the reference CLI's simulate configuration) and profile
+metrics: parsing and grid snapping on the CPU; the published example results
+through the device path on the GPU."""
+import json
+import math
+
+import numpy as np
+import pytest
+
+from highuvlith_b200 import config as C
+from highuvlith_b200 import metrics as PM
+from oracle import metrics as M
+
+# Imaging sections of the reference's examples/sim_arf.toml and of the F2
+# scene behind README.md:106,132,338-340 (the values, restated).
+ARF = """
+[source]
+type = "vuv"
+preset = "arf"
+sigma = 0.7
+[optics]
+na = 0.93
+flare_fraction = 0.02
+[mask]
+cd_nm = 80.0
+pitch_nm = 160.0
+[grid]
+size = 128
+pixel_nm = 2.5
+[process]
+dose_mj_cm2 = 30.0
+focus_nm = 0.0
+"""
+
+F2 = """
+[source]
+wavelength_nm = 157.63
+sigma = 0.7
+bandwidth_pm = 1.1
+[optics]
+na = 0.75
+flare_fraction = 0.02
+[mask]
+cd_nm = 65.0
+pitch_nm = 180.0
+[grid]
+size = 256
+pixel_nm = 1.0
+[process]
+dose_mj_cm2 = 30.0
+focus_nm = 0.0
+"""
+
+
+def test_parse_and_commensurate_grid():
+    a = C.load(ARF, is_text=True)
+    assert a.source.wavelength_nm == pytest.approx(193.368)
+    assert a.grid.pixel_nm == 2.5 and not a.notes  # 320 nm = 2 pitches already
+    assert a.tone == "dark" and a.feature == 0 and a.background == 1
+    f = C.load(F2, is_text=True)
+    assert f.grid.pixel_nm == pytest.approx(180.0 / 256)  # snapped to one 180 nm period
+    assert f.notes
+    # lines cover the field periodically: total clear width per period = pitch - cd
+    field = f.grid.field_nm
+    xs = np.linspace(-field / 2, field / 2, 20001)[:-1]
+    opaque = np.zeros_like(xs, dtype=bool)
+    for x, _, w, _ in f.rects:
+        opaque |= np.abs(xs - x) <= w / 2
+    assert abs(opaque.mean() - 65.0 / 180.0) < 1e-3
+
+
+def test_unsupported_sections_raise():
+    with pytest.raises(C.ConfigError):
+        C.load(ARF + '[imaging]\nspectrum = "narrow_band"\n', is_text=True)
+    with pytest.raises(C.ConfigError):
+        C.load(ARF.replace('type = "vuv"', 'type = "synchrotron"'), is_text=True)
+
+
+def test_metrics_match_oracle_on_random_profiles():
+    rng = np.random.default_rng(4)
+    n = 256
+    x = -64.0 + (np.arange(n) + 0.5) * 0.5
+    t = np.linspace(0, 2 * np.pi, n, endpoint=False)
+    for _ in range(20):
+        prof = 0.5 + 0.3 * np.cos(t * rng.integers(1, 4) + rng.uniform(0, 6)) + 0.05 * np.cos(5 * t)
+        for tone in ("dark", "bright"):
+            a = PM.printed_cd(prof, x, 0.45, tone)
+            b = M.measure_cd_periodic(list(prof), list(x), 0.45, tone)
+            assert (a is None) == (b is None)
+            if a is not None:
+                assert abs(a - b) < 1e-9
+                assert abs(PM.nils(prof, x, 0.45, tone) - M.nils_periodic(list(prof), list(x), 0.45, tone)) < 1e-9
+    img = rng.random((8, 8))
+    assert PM.image_contrast(img) == pytest.approx(M.image_contrast(img))
+    np.testing.assert_allclose(PM.centre_profile(img), M.centre_profile(img))
+
+
+@pytest.mark.gpu
+def test_published_example_results_on_the_device():
+    a = C.simulate(C.load(ARF, is_text=True))
+    assert round(a["printed_cd_nm"], 1) == 85.7
+    assert round(a["nils"], 2) == 1.32
+    assert abs(a["contrast"] - 0.412) < 1e-3
+    f = C.simulate(C.load(F2, is_text=True))
+    assert round(f["contrast"], 4) == 0.4545
+    assert round(f["printed_cd_nm"], 2) == 41.20
+    assert round(f["nils"], 3) == 0.654
+
+
+@pytest.mark.gpu
+def test_cli_simulate_json(tmp_path, capsys):
+    from highuvlith_b200 import cli
+    p = tmp_path / "arf.toml"
+    p.write_text(ARF)
+    assert cli.main(["simulate", "--config", str(p), "--image", str(tmp_path / "img.npy")]) == 0
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert round(out["printed_cd_nm"], 1) == 85.7
+    assert np.load(tmp_path / "img.npy").shape == (128, 128)
+    # a dose override moves the printing threshold as I = 0.3 * nominal / dose
+    assert cli.main(["simulate", "--config", str(p), "--dose", "33"]) == 0
+    out2 = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert math.isclose(out2["threshold"], 0.3 * 30 / 33)
