@@ -406,10 +406,26 @@ def run_ours(args):
     per_launch_s = prof["ms"] / launches / 1e3
     images_per_launch = N_CLIPS * args.steps / launches
     achieved = bytes_per_image * images_per_launch / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+    total_ms = ms * args.steps
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": None, "kernel": prof["kernel"], "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
                 "algorithmic_bytes_per_image": bytes_per_image,
-                "kernel_share_of_step": prof["ms"] / (ms * args.steps) if ms > 0 else None}
+                "kernel_share_of_step": prof["ms"] / total_ms if ms > 0 else None,
+                "note": "achieved = SURVEY 8(d) algorithmic bytes per image x images per launch / the dominant "
+                        "region's mean launch time (CUDA events on the launching stream)",
+                "regions": {k: {"launches": v[0], "ms": v[1], "share": v[1] / total_ms if total_ms > 0 else None}
+                            for k, v in prof["regions"].items()}}
+    g = prof["regions"].get("tc_dft_gemm<sumsq>")
+    if g and g[1] > 0:
+        # the |E|^2 contraction on tensor cores: 8 B M^2 K FLOP per image (complex MAC = 8,
+        # split products counted once), against the measured bf16 peak
+        B = 2 * diag["band_half_width"] + 1
+        M_eval = 256
+        flop = 8.0 * B * M_eval * M_eval * K * N_CLIPS * args.steps
+        roofline["tensor_gemm"] = {"kernel": "tc_dft_gemm<sumsq>", "achieved": flop / (g[1] / 1e3) / 1e12,
+                                   "peak": tc_burst, "unit": "TFLOP/s",
+                                   "frac": flop / (g[1] / 1e3) / 1e12 / tc_burst if tc_burst else None,
+                                   "issued_products_per_algorithmic": 3}
 
     # end to end through the host-buffer C ABI call (pinned buffers)
     h_in = torch.from_numpy(rasters).pin_memory()

@@ -141,6 +141,7 @@ SIGNATURES = {
                                         C.c_void_p]),
     "huv_image_batch_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),
     "huv_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
+    "huv_profile_regions": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "huv_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32),
                                    C.POINTER(C.c_int64), C.c_char_p, C.c_int32]),
 }

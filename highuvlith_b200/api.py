@@ -232,12 +232,18 @@ class SimulationEngine:
         L.check(L.lib().huv_profile_enable(self._h, int(on)))
 
     def profile_read(self) -> dict:
-        """{'kernel', 'ms', 'launches', 'total_launches'} since the last read."""
+        """{'kernel', 'ms', 'launches', 'total_launches', 'regions'} since the
+        last read; 'kernel' is the region with the largest total time and
+        'regions' maps every timed region to (launches, total ms)."""
+        import json as _json
+        buf = C.create_string_buffer(8192)
+        L.check(L.lib().huv_profile_regions(self._h, buf, 8192))
+        regions = {k: tuple(v) for k, v in _json.loads(buf.value.decode()).items()}
         ms, nl, tot = C.c_double(), C.c_int32(), C.c_int64()
         name = C.create_string_buffer(64)
         L.check(L.lib().huv_profile_read(self._h, C.byref(ms), C.byref(nl), C.byref(tot), name, 64))
         return {"kernel": name.value.decode(), "ms": ms.value, "launches": nl.value,
-                "total_launches": tot.value}
+                "total_launches": tot.value, "regions": regions}
 
     # ---------------------------------------------------------- device calls
     @staticmethod

@@ -241,14 +241,42 @@ huv_status huv_profile_read(void* engine, double* dominant_ms, int32_t* dominant
   return guarded([&] {
     Engine* e = as_engine(engine);
     std::lock_guard<std::mutex> lock(e->mu);
-    if (dominant_ms) *dominant_ms = e->prof.total_ms();
-    if (dominant_launches) *dominant_launches = static_cast<int32_t>(e->prof.used);
+    const auto regions = e->prof.regions();
+    std::string best;
+    double best_ms = 0.0;
+    int best_n = 0;
+    for (const auto& kv : regions)
+      if (kv.second.second > best_ms) {
+        best = kv.first;
+        best_ms = kv.second.second;
+        best_n = kv.second.first;
+      }
+    if (dominant_ms) *dominant_ms = best_ms;
+    if (dominant_launches) *dominant_launches = best_n;
     if (total_launches) *total_launches = e->prof.launches;
     if (dominant_name && name_capacity > 0) {
-      std::strncpy(dominant_name, e->prof.name.c_str(), static_cast<size_t>(name_capacity) - 1);
+      std::strncpy(dominant_name, best.c_str(), static_cast<size_t>(name_capacity) - 1);
       dominant_name[name_capacity - 1] = 0;
     }
     e->prof.reset();
+  });
+}
+
+huv_status huv_profile_regions(void* engine, char* json, int32_t capacity) {
+  return guarded([&] {
+    Engine* e = as_engine(engine);
+    if (!json || capacity <= 0) throw Error(HUV_ERR_INVALID_PARAMETER, "profile regions: buffer");
+    std::lock_guard<std::mutex> lock(e->mu);
+    std::string out = "{";
+    bool first = true;
+    for (const auto& kv : e->prof.regions()) {
+      out += (first ? "\"" : ",\"") + kv.first + "\":[" + std::to_string(kv.second.first) + "," +
+             std::to_string(kv.second.second) + "]";
+      first = false;
+    }
+    out += "}";
+    if (static_cast<int32_t>(out.size()) >= capacity) throw Error(HUV_ERR_DIMENSION_MISMATCH, "profile regions: capacity");
+    std::memcpy(json, out.c_str(), out.size() + 1);
   });
 }
 

@@ -600,17 +600,20 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     const int nc = std::min(chunk, b.n_clips - c0);
     const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
     float* o = out + static_cast<size_t>(n) * n * c0;
+    prof.begin("mask_band", st);
     if (b.input_kind == HUV_INPUT_RECTS)
       rect_band(c0, nc, hb, Wf, Mb, mean, st);  // host-side table, exact spectrum on the device
     else
       check_cuda(band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb, b.pixel_transfer ? ds.ptx : nullptr, Wf,
                               mean, twn, st),
                  "band_forward");
+    prof.end(st);
     CUtensorMap mbE, mbI, mbP;
     if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kpE, kTcBN) ||
         !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kpI, kTcBN) ||
         (gemm_rows && !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * rbn, kpE, rbn)))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
+    prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
     if (!gemm_rows) {
       // Row transforms as FP32 shared-memory FFTs, emitting the split operand.
       const int S = fit_units(8, 2 * (sizeof(float2) << lgm));
@@ -646,6 +649,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
         tc_dft_gemm<2, kRowBNWide><<<g, 192, tc_smem_bytes(3, kRowBNWide, true), st>>>(tc.map_ae, mbP, p);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<2>");
     }
+    prof.end(st);
     {
       TcGemmParams p{};
       p.kboxes = kpE / 64;
@@ -668,15 +672,19 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       prof.end(st);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<0>");
     }
+    prof.begin("interp_band", st);
     check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st),
                "band_forward(interp)");
+    prof.end(st);
     {
+      prof.begin("socs_rows_tc<interp>", st);
       const int S = fit_units(8, 2 * (sizeof(float2) << lgn));
       dim3 g((nrI + S - 1) / S, nc);
       const size_t sm = 2 * (static_cast<size_t>(S) << lgn) * sizeof(float2);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
       socs_rows_tc<<<g, 256, sm, st>>>(nullptr, scale, C, 1, h2, h2, nrI, lgn, S, kpI, kstI * 16, BI, twn);
       check_cuda(cudaGetLastError(), "socs_rows_tc(interp)");
+      prof.end(st);
     }
     {
       TcGemmParams p{};
@@ -695,7 +703,9 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.out = o;
       p.err = dev_err;
       dim3 g(1, n / 128, nc);
+      prof.begin("tc_dft_gemm<interp>", st);
       tc_dft_gemm<1><<<g, 192, smem_tc, st>>>(tc.map_ai, mbI, p);
+      prof.end(st);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
     }
     prof.launches += gemm_rows ? 8 : 7;

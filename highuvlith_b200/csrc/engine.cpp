@@ -427,26 +427,34 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
     const int nc = std::min(chunk, b.n_clips - c0);
     const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
     float* o = out + static_cast<size_t>(n) * n * c0;
+    prof.begin("mask_band", st);
     if (b.input_kind == HUV_INPUT_RECTS)
       rect_band(c0, nc, hb, Wf, Mb, mean, st);
     else
       check_cuda(huv_launch::band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb,
                                           b.pixel_transfer ? ds.ptx : nullptr, Wf, mean, twn, st),
                  "band_forward");
+    prof.end(st);
     prof.launches += 2;
+    prof.begin("socs_rows_inv", st);
     check_cuda(huv_launch::socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");
+    prof.end(st);
     prof.begin("socs_cols_inv", st);
     check_cuda(huv_launch::socs_cols(T, K, hb, lgm, nc, ds.keep, ds.flare, mean, coarse ? IM : o, 0, twm, st),
                "socs_cols");
     prof.end(st);
     prof.launches += 2;
     if (coarse) {
+      prof.begin("interp_band", st);
       check_cuda(huv_launch::band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr,
                                           nullptr, twm, st),
                  "band_forward(interp)");
+      prof.end(st);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
+      prof.begin("interp_rows_cols", st);
       check_cuda(huv_launch::socs_rows(nullptr, scale, C, 1, h2, lgn, nc, T2, twn, st), "socs_rows(interp)");
       check_cuda(huv_launch::socs_cols(T2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, o, 1, twn, st), "socs_cols(interp)");
+      prof.end(st);
       prof.launches += 4;
     }
   }

@@ -51,19 +51,20 @@ struct DeviceSet {
 // library's kernels.
 struct Prof {
   bool on = false;
-  std::string name;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+  std::vector<std::string> names;  // region name of each used event pair
   size_t used = 0;
   int64_t launches = 0;
   void begin(const char* nm, cudaStream_t st) {
     if (!on) return;
-    name = nm;
     if (used == pool.size()) {
       cudaEvent_t a, b;
       check_cuda(cudaEventCreate(&a), "cudaEventCreate");
       check_cuda(cudaEventCreate(&b), "cudaEventCreate");
       pool.emplace_back(a, b);
     }
+    if (names.size() <= used) names.resize(used + 1);
+    names[used] = nm;
     check_cuda(cudaEventRecord(pool[used].first, st), "cudaEventRecord");
   }
   void end(cudaStream_t st) {
@@ -71,15 +72,18 @@ struct Prof {
     check_cuda(cudaEventRecord(pool[used].second, st), "cudaEventRecord");
     ++used;
   }
-  double total_ms() {
-    double t = 0;
+  // name -> (launches, total ms) over the recorded regions
+  std::map<std::string, std::pair<int, double>> regions() {
+    std::map<std::string, std::pair<int, double>> out;
     for (size_t i = 0; i < used; ++i) {
       check_cuda(cudaEventSynchronize(pool[i].second), "cudaEventSynchronize");
       float ms = 0;
       check_cuda(cudaEventElapsedTime(&ms, pool[i].first, pool[i].second), "cudaEventElapsedTime");
-      t += ms;
+      auto& r = out[names[i]];
+      r.first += 1;
+      r.second += ms;
     }
-    return t;
+    return out;
   }
   void reset() {
     used = 0;
@@ -91,6 +95,7 @@ struct Prof {
       cudaEventDestroy(pr.second);
     }
     pool.clear();
+    names.clear();
     used = 0;
   }
 };

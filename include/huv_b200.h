@@ -357,6 +357,9 @@ huv_status huv_rasterize_rects(int32_t n, int32_t n_clips, const int32_t* rects_
 huv_status huv_profile_enable(void* engine, int32_t on);
 huv_status huv_profile_read(void* engine, double* dominant_ms, int32_t* dominant_launches,
                             int64_t* total_launches, char* dominant_name, int32_t name_capacity);
+/* Every timed region since the last huv_profile_read as JSON
+ * {"name": [launches, total_ms], ...} (does not reset; measurement hook). */
+huv_status huv_profile_regions(void* engine, char* json, int32_t capacity);
 
 #ifdef __cplusplus
 }
