@@ -97,3 +97,25 @@ def test_rect_input_rejects_bad_tables():
     import torch
     out = torch.empty((2, 64, 64), device="cuda")
     assert L.lib().huv_image_batch(eng.handle, C.byref(b), out.data_ptr(), None) == 1
+
+
+@pytest.mark.parametrize("form,tol", [("fft", 1e-5), ("tc", 1e-3)])
+def test_c1_line_space_on_incommensurate_field(form, tol):
+    """C1: ArF dry 193.368 nm, NA 0.93, annular 0.60/0.85, K = 24, 256^2 at
+    2 nm, 65 nm opaque lines on a 130 nm pitch (512 / 130 = 3.94 periods, so
+    the grating is truncated at the field edge) -- exact spectrum vs the
+    oracle's Mask.line_space, and the printed CD."""
+    from oracle import metrics as M
+    n, p = 256, 2.0
+    eng = HB.SimulationEngine(HB.SourceConfig.arf_laser(0.7).with_illumination("annular", 0.6, 0.85),
+                              HB.OpticsConfig(0.93), grid=HB.GridConfig(n, p), max_kernels=24)
+    oeng = H.Engine(H.fill_annular(0.6, 0.85), H.ProjectionOptics(0.93), H.Grid(n, p), 193.368, max_kernels=24)
+    half = n * p / 2
+    lines = [(c, 0.0, 65.0, 2 * n * p) for c in np.arange(-130.0 * 3, 130.0 * 4, 130.0) if abs(c) < half + 65]
+    img = eng.compute_batch_rects([lines], feature=0.0, background=1.0, form=form).cpu().numpy()[0]
+    ref = oeng.compute(H.Mask.line_space(65.0, 130.0))
+    assert _rel(img, ref) < tol, _rel(img, ref)
+    x = -half + (np.arange(n) + 0.5) * p
+    cd = M.measure_cd_periodic(list(M.centre_profile(img)), list(x), 0.3, "dark")
+    cd_ref = M.measure_cd_periodic(list(M.centre_profile(ref)), list(x), 0.3, "dark")
+    assert cd is not None and abs(cd - cd_ref) < 0.2
