@@ -374,6 +374,17 @@ constexpr int kRedBlocks = 64;  // blocks per mask for reductions
 
 // Cost (and gradient when grad != nullptr) for `masks` masks on the device.
 // cost_dev: masks doubles on the device.
+//
+// Every per-kernel field is evaluated on the coarse grid M > 4h (the
+// smallest power of two, as for the image): the intensity is band-limited to
+// 2h, so its exact N x N samples come from the M x M ones by band
+// interpolation; the adjoint needs only the band h of G0 . E_k, which depends
+// only on the band 2h of G0 = dC/dI, and the product of a band-2h and a
+// band-h function is alias-free on M > 4h.  Hence
+//   Q(f) = sum_k conj(kappa_k(f)) sum_{x in N^2} G0 E_k e^{-2 pi i f x / N}
+//        = (N / M)^2 sum_k conj(kappa_k(f)) sum_{x' in M^2} G0' E_k e^{-2 pi i f x' / M},
+// G0' the band-2h part of G0 sampled on the M grid.  Only the transmittance,
+// the data term, G's band, dC/dm and the regularisers touch N x N.
 void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, const float* target, float* grad,
                       double* cost_dev, cudaStream_t st) {
   using namespace huv_dev;
@@ -385,22 +396,31 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   }
   DeviceSet& ds = device_set(p.defocus_nm == 0.0 ? 0.0 : p.defocus_nm);
   const int K = ds.K, hb = ds.hb, B = ds.B;
-  const int lg = ilog2i(n);
-  const size_t npix = static_cast<size_t>(n) * n;
-  const float2* tw = twiddle(lg);
+  const int h2 = 2 * hb, B2 = 2 * h2 + 1;
+  const int lgn = ilog2i(n);
+  const int M = choose_eval_grid(ds, 0);
+  const int lgm = ilog2i(M);
+  const bool coarse = M < n;
+  const size_t npix = static_cast<size_t>(n) * n, mpix = static_cast<size_t>(M) * M;
+  const float2* twn = twiddle(lgn);
+  const float2* twm = twiddle(lgm);
   const float flare = ds.flare, keep = ds.keep;
   // Per-mask workspace.
   const size_t s_t = a256(sizeof(float) * npix);           // transmittance, then dC/dm
-  const size_t s_x = a256(sizeof(float2) * n * B);
+  const size_t s_x = a256(sizeof(float2) * n * B2);        // row transforms of N x N inputs (band <= 2h)
   const size_t s_m = a256(sizeof(float2) * B * B);
-  const size_t s_mean = a256(sizeof(float) * (1 + (B + 3) / 4));
-  const size_t s_T = a256(sizeof(float2) * static_cast<size_t>(K) * B * n);
-  const size_t s_img = a256(sizeof(float) * npix);         // image, then G
-  const size_t s_V = grad ? a256(sizeof(float2) * static_cast<size_t>(K) * B * n) : 0;
+  const size_t s_mean = a256(sizeof(float) * (1 + (B2 + 3) / 4));
+  const size_t s_T = a256(sizeof(float2) * static_cast<size_t>(K) * B * M);
+  const size_t s_im = coarse ? a256(sizeof(float) * mpix) : 0;  // I on M, then G' on M
+  const size_t s_c = coarse ? a256(sizeof(float2) * B2 * B2) : 0;
+  const size_t s_x2 = coarse ? a256(sizeof(float2) * static_cast<size_t>(std::max(M, n)) * B2) : 0;
+  const size_t s_img = a256(sizeof(float) * npix);         // image on N, then G
+  const size_t s_V = grad ? a256(sizeof(float2) * static_cast<size_t>(K) * B * M) : 0;
   const size_t s_q = grad ? a256(sizeof(float2) * B * B) : 0;
   const size_t s_t2 = grad ? a256(sizeof(float2) * static_cast<size_t>(B) * n) : 0;
   const size_t s_parts = a256(sizeof(double) * kRedBlocks * 2);
-  const size_t per = s_t + s_x + s_m + s_mean + s_T + s_img + s_V + s_q + s_t2 + 3 * s_parts + a256(sizeof(double) * 4);
+  const size_t per = s_t + s_x + s_m + s_mean + s_T + s_im + s_c + s_x2 + s_img + s_V + s_q + s_t2 + 3 * s_parts +
+                     a256(sizeof(double) * 4);
   const size_t budget = size_t(2) << 30;
   int chunk = static_cast<int>(std::max<size_t>(1, budget / per));
   chunk = std::min(chunk, masks);
@@ -416,6 +436,9 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   float2* Mb = reinterpret_cast<float2*>(take(s_m));
   float* mean = reinterpret_cast<float*>(take(s_mean));
   float2* T = reinterpret_cast<float2*>(take(s_T));
+  float* IM = reinterpret_cast<float*>(take(s_im));
+  float2* C = reinterpret_cast<float2*>(take(s_c));
+  float2* X2 = reinterpret_cast<float2*>(take(s_x2));
   float* img = reinterpret_cast<float*>(take(s_img));
   float2* V = reinterpret_cast<float2*>(take(s_V));
   float2* Q = reinterpret_cast<float2*>(take(s_q));
@@ -424,35 +447,53 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   double* preg = reinterpret_cast<double*>(take(s_parts));
   double* sums = reinterpret_cast<double*>(take(s_parts));
   double* regsum = reinterpret_cast<double*>(take(a256(sizeof(double) * 4)));
-  const int lgn = lg;
-  const dim3 red_grid(kRedBlocks, 1);
   for (int c0 = 0; c0 < masks; c0 += chunk) {
     const int nc = std::min(chunk, masks - c0);
     const float* th = theta + npix * c0;
     const float* tg = target + npix * c0;
     ilt_transmittance<<<1184, 256, 0, st>>>(th, npix * nc, static_cast<float>(p.beta),
                                             static_cast<float>(p.absorber), tbuf);
-    check_cuda(band_forward(tbuf, HUV_INPUT_RASTER_F32, n, lgn, hb, nc, X, Mb, nullptr, ds.W, mean, tw, st),
+    check_cuda(band_forward(tbuf, HUV_INPUT_RASTER_F32, n, lgn, hb, nc, X, Mb, nullptr, ds.W, mean, twn, st),
                "ilt band_forward");
-    check_cuda(socs_rows(ds.kband, 0.f, Mb, K, hb, lgn, nc, T, tw, st), "ilt socs_rows");
-    check_cuda(socs_cols(T, K, hb, lgn, nc, keep, flare, mean, img, 0, tw, st), "ilt socs_cols");
+    // fields of every kernel on the evaluation grid, the image on it, then on N x N
+    check_cuda(socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "ilt socs_rows");
+    check_cuda(socs_cols(T, K, hb, lgm, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
+    if (coarse) {
+      check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st),
+                 "ilt band(I)");
+      const float scale = 1.0f / static_cast<float>(mpix);
+      check_cuda(socs_rows(nullptr, scale, C, 1, h2, lgn, nc, X2, twn, st), "ilt interp rows");
+      check_cuda(socs_cols(X2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, img, 1, twn, st), "ilt interp cols");
+    }
     ilt_data<<<dim3(kRedBlocks, nc), 256, 0, st>>>(img, tg, npix, p.cost_kind, static_cast<float>(p.threshold),
                                                    static_cast<float>(p.steepness), static_cast<float>(p.dose),
                                                    img, pdata);
     sum_parts<<<(nc * 2 + 127) / 128, 128, 0, st>>>(pdata, kRedBlocks, 2, nc, sums);
     float* dcdm = nullptr;
     if (grad) {
-      const int Wc = fit_units(8, 2 * (sizeof(float2) << lgn) + (sizeof(float) << lgn));
-      const size_t sm = 2 * (static_cast<size_t>(Wc) << lgn) * sizeof(float2) + (static_cast<size_t>(Wc) << lgn) * sizeof(float);
-      ilt_cols_adj<<<dim3(n / Wc, nc), 256, sm, st>>>(T, img, K, hb, lgn, Wc, keep, sums,
-                                                      flare / static_cast<float>(npix), V, tw);
-      const int S = fit_units(4, 2 * (sizeof(float2) << lgn));
-      const size_t sm2 = 2 * (static_cast<size_t>(S) << lgn) * sizeof(float2);
-      ilt_rows_adj<<<dim3(B, nc), 256, sm2, st>>>(V, ds.kband, K, hb, lgn, S, Q, tw);
-      const float scale = static_cast<float>(2.0 * (1.0 - p.absorber) * p.weight);
-      check_cuda(socs_rows(nullptr, scale, Q, 1, hb, lgn, nc, T2, tw, st), "ilt grad rows");
+      // G' = the band-2h part of G = dC/dI, sampled on the evaluation grid
+      const float* Gm = img;
+      float grid_scale = 1.f;
+      if (coarse) {
+        check_cuda(band_forward(img, HUV_INPUT_RASTER_F32, n, lgn, h2, nc, X, C, nullptr, nullptr, nullptr, twn, st),
+                   "ilt band(G)");
+        check_cuda(socs_rows(nullptr, 1.0f / static_cast<float>(npix), C, 1, h2, lgm, nc, X2, twm, st),
+                   "ilt G rows");
+        check_cuda(socs_cols(X2, 1, h2, lgm, nc, 1.f, 0.f, nullptr, IM, 1, twm, st), "ilt G cols");
+        Gm = IM;
+        grid_scale = static_cast<float>(static_cast<double>(npix) / static_cast<double>(mpix));
+      }
+      const int Wc = fit_units(8, 2 * (sizeof(float2) << lgm) + (sizeof(float) << lgm));
+      const size_t sm = 2 * (static_cast<size_t>(Wc) << lgm) * sizeof(float2) + (static_cast<size_t>(Wc) << lgm) * sizeof(float);
+      ilt_cols_adj<<<dim3(M / Wc, nc), 256, sm, st>>>(T, Gm, K, hb, lgm, Wc, keep, sums,
+                                                      flare / static_cast<float>(npix), V, twm);
+      const int S = fit_units(4, 2 * (sizeof(float2) << lgm));
+      const size_t sm2 = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
+      ilt_rows_adj<<<dim3(B, nc), 256, sm2, st>>>(V, ds.kband, K, hb, lgm, S, Q, twm);
+      const float scale = static_cast<float>(2.0 * (1.0 - p.absorber) * p.weight) * grid_scale;
+      check_cuda(socs_rows(nullptr, scale, Q, 1, hb, lgn, nc, T2, twn, st), "ilt grad rows");
       dcdm = tbuf;  // the transmittance is no longer needed
-      check_cuda(socs_cols(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, tw, st), "ilt grad cols");
+      check_cuda(socs_cols(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, twn, st), "ilt grad cols");
     }
     ilt_finish<<<dim3(kRedBlocks, nc), 256, 0, st>>>(th, dcdm, n, static_cast<float>(p.beta),
                                                      static_cast<float>(p.tv_weight), static_cast<float>(p.tv_epsilon),
@@ -462,7 +503,7 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     ilt_combine<<<(nc + 127) / 128, 128, 0, st>>>(sums, regsum, nc, p.weight, 1.0 / static_cast<double>(npix),
                                                   cost_dev + c0);
     check_cuda(cudaGetLastError(), "ilt kernels");
-    prof.launches += grad ? 16 : 10;
+    prof.launches += (grad ? 16 : 10) + (coarse ? (grad ? 9 : 4) : 0);
   }
 }
 

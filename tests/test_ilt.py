@@ -39,20 +39,29 @@ def test_contact_target_area():
 
 
 # ----------------------------------------------------------------- device
-def _device_case(n=128, kmax=16):
-    grid = HB.GridConfig(n, 1.0)
-    eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(), grid=grid, max_kernels=kmax)
+def _device_case(n=128, kmax=16, scene="euv"):
+    if scene == "euv":
+        grid = HB.GridConfig(n, 1.0)
+        eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(), grid=grid,
+                                  max_kernels=kmax)
+    else:  # ArF dry with the default 2 % flare, 4 nm pixels
+        grid = HB.GridConfig(n, 4.0)
+        eng = HB.SimulationEngine(HB.SourceConfig.arf_laser(0.7), HB.OpticsConfig(0.93), grid=grid,
+                                  max_kernels=kmax)
     ev, ker = eng.kernels(0.0)
     return eng, ev, ker
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("scene,flare", [("euv", 0.0), ("arf", 0.02)])
 @pytest.mark.parametrize("cost", ["resist", "image"])
-def test_device_cost_and_gradient_match_oracle(cost):
+def test_device_cost_and_gradient_match_oracle(cost, scene, flare):
+    """The device evaluates fields and adjoint on the coarse grid M > 4h
+    (exact for band-limited kernels) and the data term on N x N."""
     import torch
     from highuvlith_b200 import ilt
     n = 128
-    eng, ev, ker = _device_case(n)
+    eng, ev, ker = _device_case(n, scene=scene)
     rng = np.random.default_rng(7)
     targets = np.stack([OI.contact_array_target(n, 1.0, s, p, p, c, c)
                         for s, p, c in ((18.0, 36.0, 2), (22.0, 44.0, 3))])
@@ -62,7 +71,7 @@ def test_device_cost_and_gradient_match_oracle(cost):
                                          torch.from_numpy(targets.astype(np.float32)).cuda(), st)
     g_dev = g_dev.cpu().numpy()
     for i in range(2):
-        cfg = OI.IltConfig(cost=cost, threshold=0.25, steepness=50.0, flare=0.0, tv_weight=0.01,
+        cfg = OI.IltConfig(cost=cost, threshold=0.25, steepness=50.0, flare=flare, tv_weight=0.01,
                            bin_weight=0.02)
         prob = OI.IltProblem(ev, ker, targets[i], cfg)
         c_ref, g_ref = prob.cost_and_gradient(theta[i].astype(np.float64))
