@@ -520,10 +520,24 @@ def main():
     ap.add_argument("--uneven-clips", dest="uneven_clips", type=int, default=2048)
     ap.add_argument("--clips", type=int, default=N_CLIPS,
                     help="clips per GPU (default 256, the workload; smaller only for profiler captures)")
+    ap.add_argument("--leg", default=None, choices=["ilt", "uneven", "focus_sweep"],
+                    help="run one extra leg alone and print its JSON (for profiler captures)")
     args = ap.parse_args()
     N_CLIPS = args.clips
     if args.impl == "reference":
         return run_reference(args)
+    if args.leg:
+        import torch
+        torch.cuda.set_device(0)
+        stream = torch.cuda.current_stream()
+        if args.leg == "ilt":
+            out = ilt_leg(c2_engine(0), stream)
+        elif args.leg == "uneven":
+            out = uneven_leg(stream, n_clips=args.uneven_clips)
+        else:
+            out = focus_sweep_leg()
+        print(json.dumps({args.leg: out}))
+        return 0
     return run_ours(args)
 
 
