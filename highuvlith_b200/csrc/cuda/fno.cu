@@ -24,6 +24,19 @@
 #include "../../../include/huv_b200.h"
 #include "../engine.hpp"
 
+namespace huv_launch {
+// tensor-core forward of the FNO (csrc/cuda/fno_tc.cu)
+cudaError_t fno_tc_set_smem();
+bool fno_tc_layer(int B, int S, int m, const __nv_bfloat16* v, const __nv_bfloat16* Wb, const __nv_bfloat16* Tw,
+                  const __nv_bfloat16* Zs, const float* bias, int act, __nv_bfloat16* zsave, __nv_bfloat16* vnext,
+                  int* err, cudaStream_t st);
+bool fno_tc_proj(int B, int S, const __nv_bfloat16* v, const __nv_bfloat16* Q1b, const float* b1, const float* q2,
+                 const float* b2, float* out, int* err, cudaStream_t st);
+void fno_tc_to_bf16(const float* a, int n, __nv_bfloat16* b, cudaStream_t st);
+void fno_tc_pack_zs(const float2* Z, int rows, int m, int S, __nv_bfloat16* Zs, cudaStream_t st);
+void fno_tc_tw_table(const float2* twx, int S, int m, __nv_bfloat16* Tw, cudaStream_t st);
+}  // namespace huv_launch
+
 namespace huv_dev {
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
@@ -733,6 +746,11 @@ struct Fno {
   float *par = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
   float2 *twx = nullptr, *twy = nullptr;
   int64_t adam_t = 0;
+  // tensor-core forward (grids of at least 128): bf16 weights, twiddle table,
+  // packed spectral operand, device error flag
+  bool tc = false;
+  __nv_bfloat16 *wb = nullptr, *q1b = nullptr, *tw_tab = nullptr, *zs = nullptr;
+  int* tc_err = nullptr;
   // activations
   std::vector<__nv_bfloat16*> v, z;
   std::vector<float2*> Xl;
@@ -810,6 +828,17 @@ struct Fno {
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_spec_to_dv, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
       attr = true;
     }
+    tc = S >= 128 && S % 128 == 0 && C == 64 && P == 128 && m <= 16;
+    if (tc) {
+      check_cuda(huv_launch::fno_tc_set_smem(), "cudaFuncSetAttribute(fno tc)");
+      check_cuda(cudaMalloc(&wb, static_cast<size_t>(L) * C * C * 2), "cudaMalloc(fno wb)");
+      check_cuda(cudaMalloc(&q1b, static_cast<size_t>(P) * C * 2), "cudaMalloc(fno q1b)");
+      check_cuda(cudaMalloc(&tw_tab, static_cast<size_t>(S) * 64 * 2), "cudaMalloc(fno tw)");
+      check_cuda(cudaMalloc(&tc_err, sizeof(int)), "cudaMalloc(fno err)");
+      check_cuda(cudaMemset(tc_err, 0, sizeof(int)), "memset");
+      huv_launch::fno_tc_tw_table(twx, S, m, tw_tab, nullptr);
+      check_cuda(cudaDeviceSynchronize(), "fno_tw_table");
+    }
   }
 
   void free_acts() {
@@ -829,6 +858,8 @@ struct Fno {
     cudaFree(dvB);
     cudaFree(dz);
     cudaFree(loss);
+    cudaFree(zs);
+    zs = nullptr;
     Xa = Y = Za = dX = nullptr;
     out = dout = dvA = dvB = dz = loss = nullptr;
   }
@@ -836,6 +867,10 @@ struct Fno {
   ~Fno() {
     cudaSetDevice(device);
     free_acts();
+    cudaFree(wb);
+    cudaFree(q1b);
+    cudaFree(tw_tab);
+    cudaFree(tc_err);
     cudaFree(par);
     cudaFree(grad);
     cudaFree(m1);
@@ -872,6 +907,7 @@ struct Fno {
     al(reinterpret_cast<void**>(&dvB), pix * C * 4);
     al(reinterpret_cast<void**>(&dz), pix * C * 4);
     al(reinterpret_cast<void**>(&loss), 4);
+    if (tc) al(reinterpret_cast<void**>(&zs), static_cast<size_t>(B) * S * 64 * 64 * 2);
     B_cap = B;
   }
 
@@ -898,11 +934,25 @@ struct Fno {
       fno_dft_y<false><<<ygrid, 256, 0, st>>>(Xa, S, C, m, twy, Xl[l]);
       fno_mix<<<dim3(modes, B), C, C * 8, st>>>(Xl[l], reinterpret_cast<const float2*>(par + oR[l]), C, modes, Y);
       fno_dft_y<true><<<dim3(S, B), 256, 0, st>>>(Y, S, C, m, twy, Za);
-      fno_layer_out<<<rgrid, 256, layer_out_smem(), st>>>(
-          Za, v[l], par + oW[l], par + ob[l], S, m, twx, l < L - 1 ? 1 : 0, z[l], v[l + 1], rows);
+      if (tc) {
+        huv_launch::fno_tc_to_bf16(par + oW[l], C * C, wb + static_cast<size_t>(l) * C * C, st);
+        huv_launch::fno_tc_pack_zs(Za, rows, m, S, zs, st);
+        if (!huv_launch::fno_tc_layer(B, S, m, v[l], wb + static_cast<size_t>(l) * C * C, tw_tab, zs, par + ob[l],
+                                      l < L - 1 ? 1 : 0, z[l], v[l + 1], tc_err, st))
+          throw Error(HUV_ERR_CUDA, "fno: tensor-core layer launch failed");
+      } else {
+        fno_layer_out<<<rgrid, 256, layer_out_smem(), st>>>(
+            Za, v[l], par + oW[l], par + ob[l], S, m, twx, l < L - 1 ? 1 : 0, z[l], v[l + 1], rows);
+      }
     }
-    fno_proj<<<pgrid(pix), 256, kProjSmem, st>>>(v[L], par + oQ1, par + ob1, par + oQ2, par + ob2, pix,
-                                                 images ? images : out);
+    if (tc) {
+      huv_launch::fno_tc_to_bf16(par + oQ1, P * C, q1b, st);
+      if (!huv_launch::fno_tc_proj(B, S, v[L], q1b, par + ob1, par + oQ2, par + ob2, images ? images : out, tc_err, st))
+        throw Error(HUV_ERR_CUDA, "fno: tensor-core projection launch failed");
+    } else {
+      fno_proj<<<pgrid(pix), 256, kProjSmem, st>>>(v[L], par + oQ1, par + ob1, par + oQ2, par + ob2, pix,
+                                                   images ? images : out);
+    }
     check_cuda(cudaGetLastError(), "fno forward");
   }
 

@@ -464,6 +464,11 @@ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 }  // namespace
 
+// 2-D bf16 tensor map (box 64 x box_rows, 128B swizzle) for other files' kernels.
+bool tc_map_bf16(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_rows) {
+  return make_map(map, ptr, rows, kp, box_rows);
+}
+
 cudaError_t tc_set_smem() {
   const int bytes = static_cast<int>(tc_smem_bytes(3));
   cudaError_t e;
