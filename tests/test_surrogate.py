@@ -63,7 +63,7 @@ def test_surrogate_ilt_gain_and_judge(trained):
     np.testing.assert_allclose(r_tr.final_cost, ce, rtol=1e-6)
 
     # Judge every 5th iterate with a bound below the surrogate's error: SOCS
-    # takes over at iteration 5 and the run ends near the exact-only result.
+    # takes over at iteration 5 and exact iterations finish the run.
     th_j = th0.clone()
     r_j = S.optimize_with_surrogate(eng, fno, th_j, tg, st, judge_every=5, error_bound=0.05)
     assert r_j.takeover_iteration == 5
