@@ -16,8 +16,8 @@
 // out[p] = sum_j Q2[j] GELU(D[p][j] + b1[j]) + b2, one pixel per thread.
 //
 // Warp roles: 0 TMA producer (no multicast), 1 MMA issuer (one thread),
-// 2..5 epilogue (one tensor-memory lane quadrant each).  Three shared-memory
-// stages, tensor memory double-buffered.  Every mbarrier wait is bounded
+// 2..5 epilogue (one tensor-memory lane quadrant each).  Two shared-memory
+// stages, tensor memory double-buffered, two CTAs per SM.  Every mbarrier wait is bounded
 // (2 s); a timeout sets *err and unwinds.  Operands BF16, accumulation FP32.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -29,7 +29,7 @@
 
 namespace huv_dev {
 
-constexpr int kFnoStages = 3;
+constexpr int kFnoStages = 2;  // two stages keep two CTAs (8 epilogue warps) per SM
 constexpr uint64_t kFnoWaitNs = 2000000000ull;
 constexpr uint32_t kTile = 128 * 128;  // 128 rows x 64 bf16
 
@@ -50,7 +50,7 @@ struct FnoTcParams {
 __device__ __forceinline__ float tc_gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
 
 template <int MODE>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(192, 2)
     fno_tc_pw(const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmW,
               const __grid_constant__ CUtensorMap tmTw, const __grid_constant__ CUtensorMap tmZ, FnoTcParams p) {
   constexpr int N = MODE == 0 ? 64 : 128;
@@ -300,7 +300,7 @@ bool fno_tc_layer(int B, int S, int m, const __nv_bfloat16* v, const __nv_bfloat
   p.vnext = vnext;
   p.act = act;
   p.err = err;
-  const int grid = std::min(p.tiles, 148);
+  const int grid = std::min(p.tiles, 2 * 148);
   huv_dev::fno_tc_pw<0><<<grid, 192, fno_tc_smem(0), st>>>(mv, mw, mt, mz, p);
   return cudaGetLastError() == cudaSuccess;
 }
@@ -319,7 +319,7 @@ bool fno_tc_proj(int B, int S, const __nv_bfloat16* v, const __nv_bfloat16* Q1b,
   p.b2 = b2;
   p.out = out;
   p.err = err;
-  const int grid = std::min(p.tiles, 148);
+  const int grid = std::min(p.tiles, 2 * 148);
   huv_dev::fno_tc_pw<1><<<grid, 192, fno_tc_smem(1), st>>>(mv, mq, mq, mq, p);
   return cudaGetLastError() == cudaSuccess;
 }
