@@ -220,6 +220,61 @@ __global__ void ilt_finish(const float* __restrict__ theta, const float* __restr
   if (threadIdx.x == 0) parts[static_cast<size_t>(mask) * gridDim.x + blockIdx.x] = c;
 }
 
+// The same as ilt_finish for grids that are multiples of 32: a block takes a
+// 32 x 32 tile, computes m = sigmoid(beta theta) once for the tile and its
+// 1-pixel periodic halo in shared memory (instead of up to nine sigmoids per
+// pixel), and writes its share of the regulariser cost to parts[mask][tile].
+// grid: ((n / 32)^2, masks), block 256.
+__global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict__ theta,
+                                                         const float* __restrict__ dcdm, int n, float beta,
+                                                         float tv_w, float tv_eps, float bin_w,
+                                                         float* __restrict__ grad, double* __restrict__ parts) {
+  __shared__ float sm[34][35];
+  __shared__ double red[32];
+  const int mask = blockIdx.y;
+  const size_t npix = static_cast<size_t>(n) * n;
+  const int tiles_x = n >> 5;
+  const int ti = blockIdx.x / tiles_x, tj = blockIdx.x - ti * tiles_x;
+  const float* th = theta + mask * npix;
+  const float inv_n = 1.f / static_cast<float>(npix);
+  for (int e = threadIdx.x; e < 34 * 34; e += blockDim.x) {
+    const int r = e / 34, c = e - r * 34;
+    const int i = (ti * 32 - 1 + r + n) % n, j = (tj * 32 - 1 + c + n) % n;
+    sm[r][c] = 1.f / (1.f + __expf(-beta * th[static_cast<size_t>(i) * n + j]));
+  }
+  __syncthreads();
+  double cost = 0.0;
+  for (int q = 0; q < 4; ++q) {
+    const int pidx = threadIdx.x + 256 * q;
+    const int r = (pidx >> 5) + 1, c = (pidx & 31) + 1;
+    const float m = sm[r][c];
+    float g = 0.f;
+    if (tv_w > 0.f) {
+      const float gx = sm[r][c + 1] - m, gy = sm[r + 1][c] - m;
+      const float sv = sqrtf(gx * gx + gy * gy + tv_eps * tv_eps);
+      cost += static_cast<double>(tv_w) * (sv - tv_eps) * inv_n;
+      if (grad) {
+        const float ml = sm[r][c - 1], mu = sm[r - 1][c];
+        const float gxl = m - ml, gyl = sm[r + 1][c - 1] - ml;
+        const float sl = sqrtf(gxl * gxl + gyl * gyl + tv_eps * tv_eps);
+        const float gxu = sm[r - 1][c + 1] - mu, gyu = m - mu;
+        const float su = sqrtf(gxu * gxu + gyu * gyu + tv_eps * tv_eps);
+        g += tv_w * inv_n * (-(gx + gy) / sv + gxl / sl + gyu / su);
+      }
+    }
+    if (bin_w > 0.f) {
+      cost += static_cast<double>(bin_w) * 4.0 * m * (1.0 - m) * inv_n;
+      g += bin_w * 4.f * (1.f - 2.f * m) * inv_n;
+    }
+    if (grad) {
+      const size_t gp = mask * npix + static_cast<size_t>(ti * 32 + r - 1) * n + tj * 32 + c - 1;
+      grad[gp] = ((dcdm ? dcdm[gp] : 0.f) + g) * beta * m * (1.f - m);
+    }
+  }
+  const double cs = block_sum_double(cost, red);
+  if (threadIdx.x == 0) parts[static_cast<size_t>(mask) * gridDim.x + blockIdx.x] = cs;
+}
+
 // ------------------------------------------------------------ optimizer algebra
 // Per-mask reductions over n elements: out[mask] = sum a*b (dot) or max |a|.
 __global__ void batched_dot(const float* __restrict__ a, const float* __restrict__ b, size_t n,
@@ -419,8 +474,11 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   const size_t s_q = grad ? a256(sizeof(float2) * B * B) : 0;
   const size_t s_t2 = grad ? a256(sizeof(float2) * static_cast<size_t>(B) * n) : 0;
   const size_t s_parts = a256(sizeof(double) * kRedBlocks * 2);
-  const size_t per = s_t + s_x + s_m + s_mean + s_T + s_im + s_c + s_x2 + s_img + s_V + s_q + s_t2 + 3 * s_parts +
-                     a256(sizeof(double) * 4);
+  const bool tiled = n % 32 == 0;
+  const int reg_parts = tiled ? (n / 32) * (n / 32) : kRedBlocks;
+  const size_t s_preg = a256(sizeof(double) * std::max(reg_parts, 2 * kRedBlocks));
+  const size_t per = s_t + s_x + s_m + s_mean + s_T + s_im + s_c + s_x2 + s_img + s_V + s_q + s_t2 + 2 * s_parts +
+                     s_preg + a256(sizeof(double) * 4);
   const size_t budget = size_t(2) << 30;
   int chunk = static_cast<int>(std::max<size_t>(1, budget / per));
   chunk = std::min(chunk, masks);
@@ -444,7 +502,7 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   float2* Q = reinterpret_cast<float2*>(take(s_q));
   float2* T2 = reinterpret_cast<float2*>(take(s_t2));
   double* pdata = reinterpret_cast<double*>(take(s_parts));
-  double* preg = reinterpret_cast<double*>(take(s_parts));
+  double* preg = reinterpret_cast<double*>(take(s_preg));
   double* sums = reinterpret_cast<double*>(take(s_parts));
   double* regsum = reinterpret_cast<double*>(take(a256(sizeof(double) * 4)));
   for (int c0 = 0; c0 < masks; c0 += chunk) {
@@ -495,11 +553,18 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
       dcdm = tbuf;  // the transmittance is no longer needed
       check_cuda(socs_cols(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, twn, st), "ilt grad cols");
     }
-    ilt_finish<<<dim3(kRedBlocks, nc), 256, 0, st>>>(th, dcdm, n, static_cast<float>(p.beta),
-                                                     static_cast<float>(p.tv_weight), static_cast<float>(p.tv_epsilon),
-                                                     static_cast<float>(p.binarization_weight),
-                                                     grad ? grad + npix * c0 : nullptr, preg);
-    sum_parts<<<(nc + 127) / 128, 128, 0, st>>>(preg, kRedBlocks, 1, nc, regsum);
+    if (tiled)
+      ilt_finish_tiled<<<dim3(reg_parts, nc), 256, 0, st>>>(
+          th, dcdm, n, static_cast<float>(p.beta), static_cast<float>(p.tv_weight),
+          static_cast<float>(p.tv_epsilon), static_cast<float>(p.binarization_weight),
+          grad ? grad + npix * c0 : nullptr, preg);
+    else
+      ilt_finish<<<dim3(kRedBlocks, nc), 256, 0, st>>>(th, dcdm, n, static_cast<float>(p.beta),
+                                                       static_cast<float>(p.tv_weight),
+                                                       static_cast<float>(p.tv_epsilon),
+                                                       static_cast<float>(p.binarization_weight),
+                                                       grad ? grad + npix * c0 : nullptr, preg);
+    sum_parts<<<(nc + 127) / 128, 128, 0, st>>>(preg, reg_parts, 1, nc, regsum);
     ilt_combine<<<(nc + 127) / 128, 128, 0, st>>>(sums, regsum, nc, p.weight, 1.0 / static_cast<double>(npix),
                                                   cost_dev + c0);
     check_cuda(cudaGetLastError(), "ilt kernels");
