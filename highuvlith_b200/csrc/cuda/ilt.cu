@@ -400,7 +400,8 @@ __global__ void scatter_blocks(const int* __restrict__ idx, const float* __restr
 // ================================================================== host
 namespace huv_launch {
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
-                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st);
+                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
+                         const uint8_t* row_digits, int* err);
 cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
                       float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
@@ -511,13 +512,14 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     const float* tg = target + npix * c0;
     ilt_transmittance<<<1184, 256, 0, st>>>(th, npix * nc, static_cast<float>(p.beta),
                                             static_cast<float>(p.absorber), tbuf);
-    check_cuda(band_forward(tbuf, HUV_INPUT_RASTER_F32, n, lgn, hb, nc, X, Mb, nullptr, ds.W, mean, twn, st),
+    check_cuda(band_forward(tbuf, HUV_INPUT_RASTER_F32, n, lgn, hb, nc, X, Mb, nullptr, ds.W, mean, twn, st, nullptr, nullptr),
                "ilt band_forward");
     // fields of every kernel on the evaluation grid, the image on it, then on N x N
     check_cuda(socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "ilt socs_rows");
     check_cuda(socs_cols(T, K, hb, lgm, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
     if (coarse) {
-      check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st),
+      check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st, nullptr,
+                              nullptr),
                  "ilt band(I)");
       const float scale = 1.0f / static_cast<float>(mpix);
       check_cuda(socs_rows(nullptr, scale, C, 1, h2, lgn, nc, X2, twn, st), "ilt interp rows");
@@ -533,7 +535,8 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
       const float* Gm = img;
       float grid_scale = 1.f;
       if (coarse) {
-        check_cuda(band_forward(img, HUV_INPUT_RASTER_F32, n, lgn, h2, nc, X, C, nullptr, nullptr, nullptr, twn, st),
+        check_cuda(band_forward(img, HUV_INPUT_RASTER_F32, n, lgn, h2, nc, X, C, nullptr, nullptr, nullptr, twn, st, nullptr,
+                                nullptr),
                    "ilt band(G)");
         check_cuda(socs_rows(nullptr, 1.0f / static_cast<float>(npix), C, 1, h2, lgm, nc, X2, twm, st),
                    "ilt G rows");

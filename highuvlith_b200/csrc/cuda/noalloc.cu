@@ -31,7 +31,8 @@
 
 namespace huv_launch {
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
-                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st);
+                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
+                         const uint8_t* row_digits, int* err);
 cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
                       float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
@@ -193,14 +194,15 @@ extern "C" huv_status huv_image_batch_noalloc(void* engine, const huv_batch* bat
       const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
       float* o = out + static_cast<size_t>(n) * n * c0;
       huv::check_cuda(huv_launch::band_forward(in, b.input_kind, n, lgn, h, nc, X, Mb,
-                                               b.pixel_transfer ? d_ptx : nullptr, d_w, mean, d_twn, st),
+                                               b.pixel_transfer ? d_ptx : nullptr, d_w, mean, d_twn, st, nullptr,
+                                               nullptr),
                       "band_forward");
       huv::check_cuda(huv_launch::socs_rows(d_kb, 0.f, Mb, K, h, lgm, nc, T, d_twm, st), "socs_rows");
       huv::check_cuda(huv_launch::socs_cols(T, K, h, lgm, nc, keep, flare, mean, coarse ? IM : o, 0, d_twm, st),
                       "socs_cols");
       if (coarse) {
         huv::check_cuda(huv_launch::band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr,
-                                                 nullptr, d_twm, st),
+                                                 nullptr, d_twm, st, nullptr, nullptr),
                         "band_forward(interp)");
         const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
         huv::check_cuda(huv_launch::socs_rows(nullptr, scale, C, 1, h2, lgn, nc, T2, d_twn, st), "socs_rows(interp)");

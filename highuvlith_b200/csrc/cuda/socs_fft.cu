@@ -243,20 +243,34 @@ using namespace huv_dev;
 
 static int pick_threads(int work) { return work >= 256 ? 256 : 128; }
 
+cudaError_t mask_rows_tc(const void* in, int n, int hb, int clips, float2* X, const uint8_t* digits, int* err,
+                         cudaStream_t st);
+
 // Mask (or image) band: rows then columns.  When W is given, `mean` must hold
 // clips + clips * ceil(B / 4) floats: the first `clips` receive the flare
-// means, the rest holds the per-block parts.
+// means, the rest holds the per-block parts.  `row_digits` (may be NULL) is
+// the device digit table of the tensor-core row band for u8 rasters; `err`
+// receives that kernel's timeout code.
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X,
                          float2* Mband, const float* ptx, const float* W, float* mean,
-                         const float2* tw, cudaStream_t st) {
+                         const float2* tw, cudaStream_t st, const uint8_t* row_digits, int* err) {
   const int S = fit_units(2, 2 * (sizeof(float2) << lg));
   const int rows_per_block = (kind == 2) ? S : 2 * S;
   const size_t sm1 = 2 * (static_cast<size_t>(S) << lg) * sizeof(float2);
   dim3 g1(n / rows_per_block, clips);
   const int th = pick_threads(S << (lg - 2));
+  // u8 rasters take the exact integer tensor-core row band when the shape
+  // and the input's alignment allow it.
+  cudaError_t rows_tc = cudaErrorNotSupported;
+  if (kind == 0 && row_digits) {
+    rows_tc = mask_rows_tc(in, n, hb, clips, X, row_digits, err, st);
+    if (rows_tc != cudaSuccess && rows_tc != cudaErrorNotSupported) return rows_tc;
+  }
   // Only device rasters come here (rectangle clips take the analytic path).
   switch (kind) {
-    case 0: band_rows_fwd<0><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
+    case 0:
+      if (rows_tc != cudaSuccess) band_rows_fwd<0><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw);
+      break;
     case 1: band_rows_fwd<1><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
     case 2: band_rows_fwd<2><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
     default: return cudaErrorInvalidValue;

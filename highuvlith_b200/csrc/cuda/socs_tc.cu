@@ -404,7 +404,8 @@ namespace huv_launch {
 
 using namespace huv_dev;
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
-                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st);
+                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
+                         const uint8_t* row_digits, int* err);
 
 namespace {
 
@@ -610,7 +611,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       rect_band(c0, nc, hb, Wf, Mb, mean, st);  // host-side table, exact spectrum on the device
     else
       check_cuda(band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb, b.pixel_transfer ? ds.ptx : nullptr, Wf,
-                              mean, twn, st),
+                              mean, twn, st, row_digit_table(hb), dev_err),
                  "band_forward");
     prof.end(st);
     CUtensorMap mbE, mbI, mbP;
@@ -678,7 +679,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       check_cuda(cudaGetLastError(), "tc_dft_gemm<0>");
     }
     prof.begin("interp_band", st);
-    check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st),
+    check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st, nullptr,
+                            nullptr),
                "band_forward(interp)");
     prof.end(st);
     {

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -24,9 +25,9 @@
 #include "host/host.hpp"
 
 namespace huv_launch {
-cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X,
-                         float2* Mband, const float* ptx, const float* W, float* mean,
-                         const float2* tw, cudaStream_t st);
+cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
+                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
+                         const uint8_t* row_digits, int* err);
 cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
                       float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
@@ -34,6 +35,8 @@ cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float 
 cudaError_t set_smem_limits();
 void tc_release(huv::TcState& tc);
 void tc_release_all(std::map<int, huv::TcState>& m);
+bool mask_rows_tc_supported(int n, int hb);
+std::vector<uint8_t> mask_rows_tc_digits(int n, int hb);
 }  // namespace huv_launch
 
 namespace huv {
@@ -110,6 +113,7 @@ Engine::~Engine() {
   if (device_ready) {
     cudaSetDevice(device);
     for (auto& kv : twiddles) cudaFree(kv.second);
+    for (auto& kv : row_digits) cudaFree(kv.second);
     auto free_set = [](DeviceSet& d) {
       for (auto& kv : d.W_by_k) cudaFree(kv.second);
       cudaFree(d.kband);
@@ -262,6 +266,20 @@ const float2* Engine::twiddle(int lg) {
   check_cuda(cudaMalloc(&d, sizeof(float2) * L), "cudaMalloc(twiddle)");
   check_cuda(cudaMemcpy(d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice), "cudaMemcpy(twiddle)");
   twiddles[lg] = d;
+  return d;
+}
+
+const uint8_t* Engine::row_digit_table(int hb) {
+  auto it = row_digits.find(hb);
+  if (it != row_digits.end()) return it->second;
+  const char* env = std::getenv("HUV_MASK_ROWS");
+  uint8_t* d = nullptr;
+  if (!(env && std::string(env) == "fft") && huv_launch::mask_rows_tc_supported(n, hb)) {
+    const std::vector<uint8_t> h = huv_launch::mask_rows_tc_digits(n, hb);
+    check_cuda(cudaMalloc(&d, h.size()), "cudaMalloc(row digits)");
+    check_cuda(cudaMemcpy(d, h.data(), h.size(), cudaMemcpyHostToDevice), "cudaMemcpy(row digits)");
+  }
+  row_digits[hb] = d;
   return d;
 }
 
@@ -432,7 +450,8 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
       rect_band(c0, nc, hb, Wf, Mb, mean, st);
     else
       check_cuda(huv_launch::band_forward(in, b.input_kind, n, lgn, hb, nc, X, Mb,
-                                          b.pixel_transfer ? ds.ptx : nullptr, Wf, mean, twn, st),
+                                          b.pixel_transfer ? ds.ptx : nullptr, Wf, mean, twn, st,
+                                          row_digit_table(hb), dev_err),
                  "band_forward");
     prof.end(st);
     prof.launches += 2;
@@ -447,7 +466,7 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
     if (coarse) {
       prof.begin("interp_band", st);
       check_cuda(huv_launch::band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr,
-                                          nullptr, twm, st),
+                                          nullptr, twm, st, nullptr, nullptr),
                  "band_forward(interp)");
       prof.end(st);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));

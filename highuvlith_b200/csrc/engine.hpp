@@ -148,6 +148,10 @@ struct Engine {
   // device helpers
   void ensure_device();
   const float2* twiddle(int lg);
+  // Digit planes of the tensor-core row band of u8 rasters for band
+  // half-width hb (NULL when that path does not apply to this grid, or when
+  // HUV_MASK_ROWS=fft in the environment selects the FFT rows).
+  const uint8_t* row_digit_table(int hb);
   DeviceSet& device_set(double z);
   void* workspace(size_t bytes);
   int choose_eval_grid(const DeviceSet& ds, int requested) const;
@@ -192,6 +196,7 @@ struct Engine {
   std::mutex mu, host_mu;
   bool device_ready = false;
   std::map<int, float2*> twiddles;
+  std::map<int, uint8_t*> row_digits;
   DeviceSet focus_dev, scratch_dev;
   void* ws = nullptr;
   size_t ws_bytes = 0;
