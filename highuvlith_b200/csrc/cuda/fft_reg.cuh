@@ -1,0 +1,204 @@
+// Register-radix Stockham FFT over S interleaved sequences (FP32 complex).
+//
+// Each pass of radix R (16, 8, 4) loads R points of one butterfly into
+// registers, applies the Stockham twiddles w^{r k}, does the R-point DFT in
+// registers (16 = 4 x 4 and 8 = 4 x 2 with the internal twiddles W16^e) and
+// stores R points; a length L = 2^LG takes 2 or 3 passes instead of log4(L)
+// shared-memory round trips.  Data sit in shared memory sequence-minor:
+// element i of sequence s at ((i + pad(i)) * S + s), pad(i) = i / 16 when
+// S < 16, so that the lanes of a half-warp (consecutive s, then consecutive
+// butterflies) touch distinct banks in every pass, including the strided
+// writes of the first one.
+//
+// The phase functions are __host__ __device__ so that a host harness can run
+// them thread by thread; a kernel calls them with a barrier between phases.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace huv_dev {
+
+// W16^e = exp(DIR * 2 pi i e / 16), e in [0, 16): cos / sin of e pi / 8.
+template <int DIR>
+__host__ __device__ __forceinline__ float2 w16(int e) {
+  constexpr float c[16] = {1.0f,
+                           0.92387953251128674f,
+                           0.70710678118654752f,
+                           0.38268343236508977f,
+                           0.0f,
+                           -0.38268343236508977f,
+                           -0.70710678118654752f,
+                           -0.92387953251128674f,
+                           -1.0f,
+                           -0.92387953251128674f,
+                           -0.70710678118654752f,
+                           -0.38268343236508977f,
+                           0.0f,
+                           0.38268343236508977f,
+                           0.70710678118654752f,
+                           0.92387953251128674f};
+  const float s = c[(e + 12) & 15];  // sin(x) = cos(x - pi/2)
+  return make_float2(c[e & 15], DIR > 0 ? s : -s);
+}
+
+__host__ __device__ __forceinline__ float2 fr_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 fr_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 fr_mul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// multiply by exp(DIR * i pi / 2): +i (DIR > 0) or -i
+template <int DIR>
+__host__ __device__ __forceinline__ float2 fr_rot90(float2 a) {
+  return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// 4-point DFT of (a0, a1, a2, a3) in place.
+template <int DIR>
+__host__ __device__ __forceinline__ void fr_dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
+  const float2 s02 = fr_add(a0, a2), d02 = fr_sub(a0, a2);
+  const float2 s13 = fr_add(a1, a3), d13 = fr_rot90<DIR>(fr_sub(a1, a3));
+  a0 = fr_add(s02, s13);
+  a2 = fr_sub(s02, s13);
+  a1 = fr_add(d02, d13);
+  a3 = fr_sub(d02, d13);
+}
+
+// R-point DFT of v in place, natural order in and out.
+template <int R, int DIR>
+__host__ __device__ __forceinline__ void fr_dft(float2 (&v)[R]) {
+  if constexpr (R == 4) {
+    fr_dft4<DIR>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 8) {
+    // n = q + 2 m, k = p + 4 q': X = sum_q W2^{q q'} W8^{q p} [sum_m v W4^{m p}]
+    float2 u[2][4];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      u[q][0] = v[q];
+      u[q][1] = v[q + 2];
+      u[q][2] = v[q + 4];
+      u[q][3] = v[q + 6];
+      fr_dft4<DIR>(u[q][0], u[q][1], u[q][2], u[q][3]);
+    }
+#pragma unroll
+    for (int p = 1; p < 4; ++p) u[1][p] = fr_mul(u[1][p], w16<DIR>(2 * p));
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      v[p] = fr_add(u[0][p], u[1][p]);
+      v[p + 4] = fr_sub(u[0][p], u[1][p]);
+    }
+  } else if constexpr (R == 16) {
+    // n = q + 4 m, k = p + 4 q': X = sum_q W4^{q q'} W16^{q p} [sum_m v W4^{m p}]
+    float2 u[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      u[q][0] = v[q];
+      u[q][1] = v[q + 4];
+      u[q][2] = v[q + 8];
+      u[q][3] = v[q + 12];
+      fr_dft4<DIR>(u[q][0], u[q][1], u[q][2], u[q][3]);
+    }
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+#pragma unroll
+      for (int p = 1; p < 4; ++p) u[q][p] = fr_mul(u[q][p], w16<DIR>(q * p));
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      fr_dft4<DIR>(u[0][p], u[1][p], u[2][p], u[3][p]);
+      v[p] = u[0][p];
+      v[p + 4] = u[1][p];
+      v[p + 8] = u[2][p];
+      v[p + 12] = u[3][p];
+    }
+  }
+}
+
+// Radix plan: LG 7 = 16 x 8, 8 = 16 x 16, 9 = 16 x 8 x 4, 10 = 16 x 16 x 4.
+__host__ __device__ constexpr int fr_passes(int LG) { return LG <= 8 ? 2 : 3; }
+__host__ __device__ constexpr int fr_radix(int LG, int pass) {
+  return pass == 0 ? 16 : (LG == 7 ? 8 : (LG == 8 ? 16 : (LG == 9 ? (pass == 1 ? 8 : 4) : (pass == 1 ? 16 : 4))));
+}
+// Stockham sub-transform size before pass `pass`.
+__host__ __device__ constexpr int fr_ns(int LG, int pass) {
+  return pass == 0 ? 1 : fr_ns(LG, pass - 1) * fr_radix(LG, pass - 1);
+}
+
+// Shared-memory index of element i of sequence s.
+template <int S>
+__host__ __device__ __forceinline__ int fr_idx(int i, int s) {
+  return (S < 16 ? i + (i >> 4) : i) * S + s;
+}
+// Buffer length (float2) for S sequences of length L.
+__host__ __device__ constexpr int fr_buf(int L, int S) { return (S < 16 ? L + L / 16 : L) * S; }
+
+// Threads of one block: one radix-16 butterfly per thread per pass.
+__host__ __device__ constexpr int fr_threads(int LG, int S) { return S * (1 << LG) / 16; }
+
+// First pass (radix 16, no twiddles) for thread t, reading a zero-padded
+// band: position i of sequence s holds P[s][mx] for the order mx - hb = i
+// (i <= hb) or i - L (i >= L - hb), and zero elsewhere.  Requires 2 hb < L.
+template <int LG, int S, int DIR>
+__host__ __device__ __forceinline__ void fr_first_pass_band(int t, const float2* P, int B, int hb, float2* dst) {
+  constexpr int L = 1 << LG;
+  const int s = t % S, j = t / S;
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const int i = j + r * (L / 16);
+    const int mx = i <= hb ? i + hb : (i >= L - hb ? i - L + hb : -1);
+    v[r] = mx >= 0 ? P[s * B + mx] : make_float2(0.f, 0.f);
+  }
+  fr_dft<16, DIR>(v);
+#pragma unroll
+  for (int r = 0; r < 16; ++r) dst[fr_idx<S>(j * 16 + r, s)] = v[r];
+}
+
+// Middle pass `pass` (not the first, not the last) for thread t: src -> dst.
+template <int LG, int S, int DIR, int PASS>
+__host__ __device__ __forceinline__ void fr_mid_pass(int t, const float2* src, float2* dst, const float2* tw) {
+  constexpr int L = 1 << LG;
+  constexpr int R = fr_radix(LG, PASS), Ns = fr_ns(LG, PASS), T = fr_threads(LG, S);
+  constexpr int stride = L / (Ns * R);
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    const int u = t + b * T;
+    const int s = u % S, j = u / S;
+    const int k = j & (Ns - 1);
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[fr_idx<S>(j + r * (L / R), s)];
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      float2 w = tw[r * k * stride];
+      if (DIR > 0) w.y = -w.y;
+      v[r] = fr_mul(v[r], w);
+    }
+    fr_dft<R, DIR>(v);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[fr_idx<S>(base + r * Ns, s)] = v[r];
+  }
+}
+
+// Last pass for butterfly u: loads, twiddles and transforms; returns the
+// sequence s and j; v[p] is output element x = j + p * (L / R).
+template <int LG, int S, int DIR>
+__host__ __device__ __forceinline__ void fr_last_pass(int u, const float2* src, const float2* tw, int& s, int& j,
+                                                      float2 (&v)[fr_radix(LG, fr_passes(LG) - 1)]) {
+  constexpr int L = 1 << LG;
+  constexpr int P = fr_passes(LG) - 1;
+  constexpr int R = fr_radix(LG, P), Ns = fr_ns(LG, P);
+  constexpr int stride = L / (Ns * R);  // 1
+  s = u % S;
+  j = u / S;
+  const int k = j;  // j < L / R = Ns
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = src[fr_idx<S>(j + r * (L / R), s)];
+#pragma unroll
+  for (int r = 1; r < R; ++r) {
+    float2 w = tw[r * k * stride];
+    if (DIR > 0) w.y = -w.y;
+    v[r] = fr_mul(v[r], w);
+  }
+  fr_dft<R, DIR>(v);
+}
+
+}  // namespace huv_dev

@@ -33,6 +33,7 @@
 
 #include "../engine.hpp"
 #include "fft_block.cuh"
+#include "fft_reg.cuh"
 #include "tc_ptx.cuh"
 
 namespace huv_dev {
@@ -370,6 +371,91 @@ __global__ void socs_rows_tc(const float2* __restrict__ kband, float scale, cons
   }
 }
 
+// socs_rows_tc with register-radix passes (fft_reg.cuh): S sequences of
+// length L = 2^LG per block, one radix-16 butterfly per thread per pass.  The
+// band products are read once into a compact [S][B] array, the first pass
+// reads them as the zero-padded band, and the last pass writes the split
+// operand straight from registers (consecutive lanes = consecutive band rows
+// of one x, so each store covers contiguous words).
+// grid: (ceil(K * nrows / S), problems); block fr_threads(LG, S).
+template <int LG, int S>
+__global__ void __launch_bounds__(fr_threads(LG, S))
+    socs_rows_reg(const float2* __restrict__ kband, float scale, const float2* __restrict__ Mband, int K, int hb,
+                  int row_off, int nrows, int kp, int zero_to, __nv_bfloat16* __restrict__ Bop,
+                  const float2* __restrict__ tw) {
+  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
+  constexpr int R = fr_radix(LG, NP - 1);
+  extern __shared__ float2 smem[];
+  const int B = 2 * hb + 1;
+  const int prob = blockIdx.y;
+  const int seq0 = blockIdx.x * S;
+  const int nseq = min(S, K * nrows - seq0);
+  const int t = threadIdx.x;
+  float2* P = smem;  // [S][B]
+  float2* b0 = smem + S * B;
+  float2* b1 = b0 + fr_buf(L, S);
+  const float2* Mc = Mband + static_cast<size_t>(prob) * B * B;
+  for (int e = t; e < S * B; e += T) {
+    const int s = e / B, mx = e - s * B;
+    float2 val = make_float2(0.f, 0.f);
+    if (s < nseq) {
+      const int seq = seq0 + s;
+      const int k = seq / nrows, my = row_off + (seq - k * nrows);
+      const float2 m = Mc[static_cast<size_t>(my) * B + mx];
+      const float2 u = kband ? kband[(static_cast<size_t>(k) * B + my) * B + mx] : make_float2(scale, 0.f);
+      val = cmul(u, m);
+    }
+    P[e] = val;
+  }
+  __syncthreads();
+  fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
+  __syncthreads();
+  const float2* src = b0;
+  if constexpr (NP == 3) {
+    fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
+    __syncthreads();
+    src = b1;
+  }
+  const size_t plane = static_cast<size_t>(L) * kp;
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    int s, j;
+    float2 v[R];
+    fr_last_pass<LG, S, +1>(t + b * T, src, tw, s, j, v);
+    if (s >= nseq) continue;
+    const int seq = seq0 + s;
+    const int k = seq / nrows, myr = seq - k * nrows;
+    __nv_bfloat16* hi = Bop + (static_cast<size_t>(prob) * K + k) * 2 * plane + 2 * myr;
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      const size_t x = static_cast<size_t>(j + p * (L / R));
+      __nv_bfloat162 hv, lv;
+      split_bf16(v[p].x, hv.x, lv.x);
+      split_bf16(v[p].y, hv.y, lv.y);
+      *reinterpret_cast<__nv_bfloat162*>(hi + x * kp) = hv;
+      *reinterpret_cast<__nv_bfloat162*>(hi + plane + x * kp) = lv;
+    }
+    if (myr == nrows - 1) {
+      const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
+      for (int p = 0; p < R; ++p) {
+        __nv_bfloat16* row = hi - 2 * myr + static_cast<size_t>(j + p * (L / R)) * kp;
+        for (int kk = 2 * nrows; kk < zero_to; ++kk) {
+          row[kk] = z;
+          row[plane + kk] = z;
+        }
+      }
+    }
+  }
+}
+
+// Sequences per block of socs_rows_reg for L = 2^lg (0: no instance).
+constexpr int rows_reg_S(int lg) { return lg == 7 ? 32 : lg == 8 ? 16 : lg == 9 ? 8 : lg == 10 ? 4 : 0; }
+constexpr size_t rows_reg_smem(int lg, int B) {
+  return (static_cast<size_t>(rows_reg_S(lg)) * B +
+          (fr_passes(lg) - 1) * static_cast<size_t>(fr_buf(1 << lg, rows_reg_S(lg)))) *
+         sizeof(float2);
+}
+
 // Band products of every kernel with the mask band, split into BF16 planes as
 // the B operand of the row-transform GEMM: P[prob][k][plane][my][kk], rows my
 // padded to rows_pad, kk = 2 mx + re/im padded to kp; zero outside my < B,
@@ -463,6 +549,31 @@ std::vector<uint16_t> split_planes(const std::vector<double>& v, int rows, int k
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
+// Row transforms into the split operand: register-radix kernel for
+// L = 128 .. 1024 (band within 110 KiB of shared memory), else the
+// shared-memory radix-4 kernel.
+void launch_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int row_off, int nrows,
+                 int lg, int kp, int zero_to, __nv_bfloat16* Bop, const float2* tw, int problems, cudaStream_t st) {
+  const int B = 2 * hb + 1;
+  const int S = rows_reg_S(lg);
+  if (S > 0 && 2 * hb < (1 << lg) && rows_reg_smem(lg, B) <= 110 * 1024) {
+    const dim3 g((K * nrows + S - 1) / S, problems);
+    const size_t sm = rows_reg_smem(lg, B);
+    const int th = fr_threads(lg, S);
+    switch (lg) {
+      case 7: socs_rows_reg<7, 32><<<g, th, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      case 8: socs_rows_reg<8, 16><<<g, th, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      case 9: socs_rows_reg<9, 8><<<g, th, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      default: socs_rows_reg<10, 4><<<g, th, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+    }
+    return;
+  }
+  const int S8 = fit_units(8, 2 * (sizeof(float2) << lg));
+  const dim3 g((K * nrows + S8 - 1) / S8, problems);
+  const size_t sm = 2 * (static_cast<size_t>(S8) << lg) * sizeof(float2);
+  socs_rows_tc<<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, lg, S8, kp, zero_to, Bop, tw);
+}
+
 }  // namespace
 
 // 2-D bf16 tensor map (box 64 x box_rows, 128B swizzle) for other files' kernels.
@@ -482,6 +593,15 @@ cudaError_t tc_set_smem() {
                                 static_cast<int>(tc_smem_bytes(3, kRowBNWide, true)))))
     return e;
   if ((e = cudaFuncSetAttribute(socs_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+  const int reg_bytes = 110 * 1024;
+  if ((e = cudaFuncSetAttribute(socs_rows_reg<7, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes)))
+    return e;
+  if ((e = cudaFuncSetAttribute(socs_rows_reg<8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes)))
+    return e;
+  if ((e = cudaFuncSetAttribute(socs_rows_reg<9, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes)))
+    return e;
+  if ((e = cudaFuncSetAttribute(socs_rows_reg<10, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes)))
+    return e;
   return cudaSuccess;
 }
 
@@ -621,11 +741,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
     prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
     if (!gemm_rows) {
-      // Row transforms as FP32 shared-memory FFTs, emitting the split operand.
-      const int S = fit_units(8, 2 * (sizeof(float2) << lgm));
-      dim3 g((K * B + S - 1) / S, nc);
-      const size_t sm = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
-      socs_rows_tc<<<g, 256, sm, st>>>(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, S, kpE, kstE * 16, BE, twm);
+      // Row transforms as FP32 register-radix FFTs, emitting the split operand.
+      launch_rows(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, kpE, kstE * 16, BE, twm, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc");
     } else {
       // Row transforms of every kernel's band product on tensor cores: the
@@ -685,11 +802,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     prof.end(st);
     {
       prof.begin("socs_rows_tc<interp>", st);
-      const int S = fit_units(8, 2 * (sizeof(float2) << lgn));
-      dim3 g((nrI + S - 1) / S, nc);
-      const size_t sm = 2 * (static_cast<size_t>(S) << lgn) * sizeof(float2);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
-      socs_rows_tc<<<g, 256, sm, st>>>(nullptr, scale, C, 1, h2, h2, nrI, lgn, S, kpI, kstI * 16, BI, twn);
+      launch_rows(nullptr, scale, C, 1, h2, h2, nrI, lgn, kpI, kstI * 16, BI, twn, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc(interp)");
       prof.end(st);
     }

@@ -112,8 +112,11 @@ def test_u8_levels_tensor_rows_match_fft_rows_and_oracle(form, monkeypatch):
         monkeypatch.delenv("HUV_MASK_ROWS")
         a, b = a.cpu().numpy(), b.cpu().numpy()
         oeng = _oracle_engine(H.fill_conventional(0.5), H.euv_nxe_033(), grid, 13.5, kmax)
+        # the TC form's split-BF16 GEMMs round at ~1e-5, so a 1e-7 change of
+        # the mask band moves its image by up to that much
+        tol_ab = 5e-6 if form == "fft" else 3e-5
         for c in range(3):
-            assert rel_err(a[c], b[c]) < 5e-6, (n, c, rel_err(a[c], b[c]))
+            assert rel_err(a[c], b[c]) < tol_ab, (n, c, rel_err(a[c], b[c]))
             if n <= 256:
                 ref = oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[c]), 0.0)
                 tol = 1e-5 if form == "fft" else 5e-5
