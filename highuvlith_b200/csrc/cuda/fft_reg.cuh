@@ -151,6 +151,16 @@ __host__ __device__ __forceinline__ void fr_first_pass_band(int t, const float2*
   for (int r = 0; r < 16; ++r) dst[fr_idx<S>(j * 16 + r, s)] = v[r];
 }
 
+// First pass (radix 16, no twiddles) for thread t given its 16 inputs
+// v[r] = element j + r L / 16 of sequence s (s = t % S, j = t / S).
+template <int LG, int S, int DIR>
+__host__ __device__ __forceinline__ void fr_first_pass_vals(int t, float2 (&v)[16], float2* dst) {
+  const int s = t % S, j = t / S;
+  fr_dft<16, DIR>(v);
+#pragma unroll
+  for (int r = 0; r < 16; ++r) dst[fr_idx<S>(j * 16 + r, s)] = v[r];
+}
+
 // Middle pass `pass` (not the first, not the last) for thread t: src -> dst.
 template <int LG, int S, int DIR, int PASS>
 __host__ __device__ __forceinline__ void fr_mid_pass(int t, const float2* src, float2* dst, const float2* tw) {

@@ -406,6 +406,10 @@ cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int
                       float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
                       const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
+cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                        float2* T, const float2* tw, cudaStream_t st);
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+                        const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 
 cudaError_t ilt_set_smem() {
   const int big = 200 * 1024;
@@ -522,8 +526,8 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
                               nullptr),
                  "ilt band(I)");
       const float scale = 1.0f / static_cast<float>(mpix);
-      check_cuda(socs_rows(nullptr, scale, C, 1, h2, lgn, nc, X2, twn, st), "ilt interp rows");
-      check_cuda(socs_cols(X2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, img, 1, twn, st), "ilt interp cols");
+      check_cuda(socs_rows_x(nullptr, scale, C, 1, h2, lgn, nc, X2, twn, st), "ilt interp rows");
+      check_cuda(socs_cols_x(X2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, img, 1, twn, st), "ilt interp cols");
     }
     ilt_data<<<dim3(kRedBlocks, nc), 256, 0, st>>>(img, tg, npix, p.cost_kind, static_cast<float>(p.threshold),
                                                    static_cast<float>(p.steepness), static_cast<float>(p.dose),
@@ -538,9 +542,9 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
         check_cuda(band_forward(img, HUV_INPUT_RASTER_F32, n, lgn, h2, nc, X, C, nullptr, nullptr, nullptr, twn, st, nullptr,
                                 nullptr),
                    "ilt band(G)");
-        check_cuda(socs_rows(nullptr, 1.0f / static_cast<float>(npix), C, 1, h2, lgm, nc, X2, twm, st),
+        check_cuda(socs_rows_x(nullptr, 1.0f / static_cast<float>(npix), C, 1, h2, lgm, nc, X2, twm, st),
                    "ilt G rows");
-        check_cuda(socs_cols(X2, 1, h2, lgm, nc, 1.f, 0.f, nullptr, IM, 1, twm, st), "ilt G cols");
+        check_cuda(socs_cols_x(X2, 1, h2, lgm, nc, 1.f, 0.f, nullptr, IM, 1, twm, st), "ilt G cols");
         Gm = IM;
         grid_scale = static_cast<float>(static_cast<double>(npix) / static_cast<double>(mpix));
       }
@@ -552,6 +556,7 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
       const size_t sm2 = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
       ilt_rows_adj<<<dim3(B, nc), 256, sm2, st>>>(V, ds.kband, K, hb, lgm, S, Q, twm);
       const float scale = static_cast<float>(2.0 * (1.0 - p.absorber) * p.weight) * grid_scale;
+      // Q is not Hermitian: the unpaired synthesis takes Re of the complex field
       check_cuda(socs_rows(nullptr, scale, Q, 1, hb, lgn, nc, T2, twn, st), "ilt grad rows");
       dcdm = tbuf;  // the transmittance is no longer needed
       check_cuda(socs_cols(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, twn, st), "ilt grad cols");

@@ -22,6 +22,7 @@
 #include <algorithm>
 
 #include "fft_block.cuh"
+#include "fft_reg.cuh"
 
 namespace huv_dev {
 
@@ -234,6 +235,223 @@ __global__ void socs_cols_inv(const float2* __restrict__ T, int K, int hb, int l
   }
 }
 
+// ------------------------------------------- register-radix (fft_reg.cuh)
+// x-major band layout of the row transforms: Tt[clip][k][x][my], B values
+// per x, so that the row kernel's stores and the column kernel's loads are
+// both contiguous.  Used for L = 128 .. 1024 with 2 hb < L.
+
+// Inverse transform along x of every (kernel, band row) product; S sequences
+// per block.  grid: (ceil(K * B / S), clips).
+template <int LG, int S>
+__global__ void __launch_bounds__(fr_threads(LG, S))
+    socs_rows_xt(const float2* __restrict__ kband, float scale, const float2* __restrict__ Mband, int K, int hb,
+                 float2* __restrict__ Tt, const float2* __restrict__ tw) {
+  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
+  constexpr int R = fr_radix(LG, NP - 1);
+  extern __shared__ float2 smem[];
+  const int B = 2 * hb + 1;
+  const int clip = blockIdx.y;
+  const int seq0 = blockIdx.x * S;
+  const int nseq = min(S, K * B - seq0);
+  const int t = threadIdx.x;
+  float2* P = smem;  // [S][B] band products
+  float2* b0 = smem + S * B;
+  float2* b1 = b0 + fr_buf(L, S);
+  const float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
+  for (int e = t; e < S * B; e += T) {
+    const int s = e / B, mx = e - s * B;
+    float2 val = make_float2(0.f, 0.f);
+    if (s < nseq) {
+      const int seq = seq0 + s;
+      const int k = seq / B, my = seq - k * B;
+      const float2 m = Mc[static_cast<size_t>(my) * B + mx];
+      const float2 u = kband ? kband[(static_cast<size_t>(k) * B + my) * B + mx] : make_float2(scale, 0.f);
+      val = cmul(u, m);
+    }
+    P[e] = val;
+  }
+  __syncthreads();
+  fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
+  __syncthreads();
+  const float2* src = b0;
+  if constexpr (NP == 3) {
+    fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
+    __syncthreads();
+    src = b1;
+  }
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    int s, j;
+    float2 v[R];
+    fr_last_pass<LG, S, +1>(t + b * T, src, tw, s, j, v);
+    if (s >= nseq) continue;
+    const int seq = seq0 + s;
+    const int k = seq / B, my = seq - k * B;
+    float2* o = Tt + (static_cast<size_t>(clip) * K + k) * L * B + my;
+#pragma unroll
+    for (int p = 0; p < R; ++p) o[static_cast<size_t>(j + p * (L / R)) * B] = v[p];
+  }
+}
+
+// Column pass over Tt + accumulation, S sequences per block.  MODE 0: columns
+// x0 + s; out = keep * sum_k |E_k|^2 + flare * mean, with the sum held in
+// registers across k.  MODE 1 (band synthesis of a real image, K = 1): two
+// columns per sequence, z = T(., x0 + 2s) + i T(., x0 + 2s + 1); each column
+// is Hermitian in my, so Re and Im of the transform are the two real
+// columns.  grid: (L / (S or 2 S), clips); out: [clip][L][L].
+template <int LG, int S, int MODE>
+__global__ void __launch_bounds__(fr_threads(LG, S))
+    socs_cols_xt(const float2* __restrict__ Tt, int K, int hb, float keep, float flare,
+                 const float* __restrict__ mean, float* __restrict__ out, const float2* __restrict__ tw) {
+  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
+  constexpr int R = fr_radix(LG, NP - 1);
+  constexpr int XS = MODE == 1 ? 2 * S : S;
+  extern __shared__ float2 smem[];
+  const int B = 2 * hb + 1;
+  const int clip = blockIdx.y;
+  const int x0 = blockIdx.x * XS;
+  const int t = threadIdx.x;
+  float2* P = smem;  // [S][B]
+  float2* b0 = smem + S * B;
+  float2* b1 = b0 + fr_buf(L, S);
+  float acc[16];
+  float2 res[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    acc[i] = 0.f;
+    res[i] = make_float2(0.f, 0.f);
+  }
+  for (int k = 0; k < K; ++k) {
+    const float2* src = Tt + ((static_cast<size_t>(clip) * K + k) * L + x0) * B;
+    if (MODE == 0) {
+      for (int e = t; e < S * B; e += T) P[e] = src[e];
+    } else {
+      for (int e = t; e < S * B; e += T) {
+        const int s = e / B, my = e - s * B;
+        const float2 a = src[static_cast<size_t>(2 * s) * B + my];
+        const float2 c = src[static_cast<size_t>(2 * s + 1) * B + my];
+        P[e] = make_float2(a.x - c.y, a.y + c.x);
+      }
+    }
+    __syncthreads();
+    fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
+    __syncthreads();
+    const float2* cur = b0;
+    if constexpr (NP == 3) {
+      fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
+      __syncthreads();
+      cur = b1;
+    }
+#pragma unroll
+    for (int b = 0; b < 16 / R; ++b) {
+      int s, j;
+      float2 v[R];
+      fr_last_pass<LG, S, +1>(t + b * T, cur, tw, s, j, v);
+#pragma unroll
+      for (int p = 0; p < R; ++p) {
+        if (MODE == 0)
+          acc[b * R + p] += v[p].x * v[p].x + v[p].y * v[p].y;
+        else
+          res[b * R + p] = v[p];
+      }
+    }
+    __syncthreads();
+  }
+  const float add = (MODE == 0 && mean) ? flare * mean[clip] : 0.f;
+  float* oc = out + static_cast<size_t>(clip) * L * L;
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    const int u = t + b * T;
+    const int s = u % S, j = u / S;
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      const size_t y = static_cast<size_t>(j + p * (L / R));
+      if (MODE == 0)
+        oc[y * L + x0 + s] = keep * acc[b * R + p] + add;
+      else
+        *reinterpret_cast<float2*>(oc + y * L + x0 + 2 * s) = res[b * R + p];
+    }
+  }
+}
+
+// band_cols_fwd with register-radix passes: forward FFT along y of S band
+// columns of X[clip][y][B] per block, the first pass reading X directly.
+// grid: (ceil(B / S), clips).
+template <int LG, int S>
+__global__ void __launch_bounds__(fr_threads(LG, S))
+    band_cols_reg(const float2* __restrict__ X, int hb, const float* __restrict__ ptx,
+                  const float* __restrict__ W, float2* __restrict__ Mband, float* __restrict__ parts,
+                  const float2* __restrict__ tw) {
+  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
+  constexpr int R = fr_radix(LG, NP - 1);
+  extern __shared__ float2 smem[];
+  __shared__ float red[T / 32];
+  const int B = 2 * hb + 1;
+  const int clip = blockIdx.y;
+  const int c0 = blockIdx.x * S;
+  const int t = threadIdx.x;
+  float2* b0 = smem;
+  float2* b1 = b0 + fr_buf(L, S);
+  const float2* Xc = X + static_cast<size_t>(clip) * L * B;
+  {
+    const int s = t % S, j = t / S;
+    const bool live = c0 + s < B;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+      v[r] = live ? Xc[static_cast<size_t>(j + r * (L / 16)) * B + c0 + s] : make_float2(0.f, 0.f);
+    fr_first_pass_vals<LG, S, -1>(t, v, b0);
+  }
+  __syncthreads();
+  const float2* cur = b0;
+  if constexpr (NP == 3) {
+    fr_mid_pass<LG, S, -1, 1>(t, b0, b1, tw);
+    __syncthreads();
+    cur = b1;
+  }
+  float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
+  float part = 0.f;
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    int s, j;
+    float2 v[R];
+    fr_last_pass<LG, S, -1>(t + b * T, cur, tw, s, j, v);
+    const int mx = c0 + s;
+    if (mx >= B) continue;
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      const int idx = j + p * (L / R);
+      const int mi = idx <= hb ? idx + hb : (idx >= L - hb ? idx - L + hb : -1);
+      if (mi < 0) continue;
+      float2 val = v[p];
+      if (ptx) {
+        const float f = ptx[mi] * ptx[mx];
+        val.x *= f;
+        val.y *= f;
+      }
+      Mc[static_cast<size_t>(mi) * B + mx] = val;
+      if (W) part += W[mi * B + mx] * (val.x * val.x + val.y * val.y);
+    }
+  }
+  if (parts) {
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if ((t & 31) == 0) red[t >> 5] = part;
+    __syncthreads();
+    if (t == 0) {
+      float sum = 0.f;
+      for (int w = 0; w < T / 32; ++w) sum += red[w];
+      parts[static_cast<size_t>(clip) * gridDim.x + blockIdx.x] = sum;
+    }
+  }
+}
+
+// Sequences per block of the register-radix kernels for L = 2^lg.
+constexpr int xt_S(int lg) { return lg == 7 ? 32 : lg == 8 ? 16 : lg == 9 ? 8 : lg == 10 ? 4 : 0; }
+constexpr size_t xt_buf_bytes(int lg) {
+  return (fr_passes(lg) - 1) * static_cast<size_t>(fr_buf(1 << lg, xt_S(lg))) * sizeof(float2);
+}
+constexpr int kXtSmemMax = 110 * 1024;
+
 }  // namespace huv_dev
 
 // ------------------------------------------------------------ launchers
@@ -245,6 +463,11 @@ static int pick_threads(int work) { return work >= 256 ? 256 : 128; }
 
 cudaError_t mask_rows_tc(const void* in, int n, int hb, int clips, float2* X, const uint8_t* digits, int* err,
                          cudaStream_t st);
+bool xt_ok(int lg, int hb);
+cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                      float2* T, const float2* tw, cudaStream_t st);
+cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+                      const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 
 // Mask (or image) band: rows then columns.  When W is given, `mean` must hold
 // clips + clips * ceil(B / 4) floats: the first `clips` receive the flare
@@ -276,12 +499,78 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     default: return cudaErrorInvalidValue;
   }
   const int B = 2 * hb + 1;
-  const int cpb = fit_units(4, 2 * (sizeof(float2) << lg));
-  const int nblk = (B + cpb - 1) / cpb;
-  const size_t sm2 = 2 * (static_cast<size_t>(cpb) << lg) * sizeof(float2);
   float* parts = (W && mean) ? mean + clips : nullptr;
-  band_cols_fwd<<<dim3(nblk, clips), 256, sm2, st>>>(X, lg, hb, cpb, ptx, W, Mband, parts, tw);
+  int nblk;
+  if (xt_ok(lg, hb)) {
+    // register-radix columns: S <= 4 ... 32 columns per block, at most
+    // ceil(B / 4) parts per clip as the callers size them
+    const int S = xt_S(lg);
+    nblk = (B + S - 1) / S;
+    const dim3 g(nblk, clips);
+    const size_t sm = xt_buf_bytes(lg);
+    switch (lg) {
+      case 7: band_cols_reg<7, 32><<<g, 256, sm, st>>>(X, hb, ptx, W, Mband, parts, tw); break;
+      case 8: band_cols_reg<8, 16><<<g, 256, sm, st>>>(X, hb, ptx, W, Mband, parts, tw); break;
+      case 9: band_cols_reg<9, 8><<<g, 256, sm, st>>>(X, hb, ptx, W, Mband, parts, tw); break;
+      default: band_cols_reg<10, 4><<<g, 256, sm, st>>>(X, hb, ptx, W, Mband, parts, tw); break;
+    }
+  } else {
+    const int cpb = fit_units(4, 2 * (sizeof(float2) << lg));
+    nblk = (B + cpb - 1) / cpb;
+    const size_t sm2 = 2 * (static_cast<size_t>(cpb) << lg) * sizeof(float2);
+    band_cols_fwd<<<dim3(nblk, clips), 256, sm2, st>>>(X, lg, hb, cpb, ptx, W, Mband, parts, tw);
+  }
   if (parts) mean_reduce<<<(clips + 127) / 128, 128, 0, st>>>(parts, nblk, clips, mean);
+  return cudaGetLastError();
+}
+
+// Whether the register-radix kernels (x-major band layout) apply to L = 2^lg
+// and band half-width hb: the larger band (the interpolation's 4 hb + 1
+// columns included) within their shared-memory budget.
+bool xt_ok(int lg, int hb) {
+  const int S = xt_S(lg);
+  if (S == 0 || 2 * hb >= (1 << lg)) return false;
+  return static_cast<size_t>(S) * (2 * hb + 1) * sizeof(float2) + xt_buf_bytes(lg) <= static_cast<size_t>(kXtSmemMax);
+}
+
+// Rows of every (kernel, band row) product into T, x-major when xt_ok (the
+// layout socs_cols_x reads), else the [k][my][x] layout of socs_rows.
+cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                        float2* T, const float2* tw, cudaStream_t st) {
+  if (!xt_ok(lgm, hb)) return socs_rows(kband, scale, Mband, K, hb, lgm, clips, T, tw, st);
+  const int B = 2 * hb + 1, S = xt_S(lgm);
+  const dim3 g((K * B + S - 1) / S, clips);
+  const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) + xt_buf_bytes(lgm);
+  switch (lgm) {
+    case 7: socs_rows_xt<7, 32><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 8: socs_rows_xt<8, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 9: socs_rows_xt<9, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    default: socs_rows_xt<10, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+  }
+  return cudaGetLastError();
+}
+
+// Column pass over socs_rows_x's T (same lgm and hb).  mode 0: sum of |E_k|^2;
+// mode 1: synthesis of a real image from a Hermitian band (K = 1), two
+// columns per transform when xt_ok.
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+                        const float* mean, float* out, int mode, const float2* tw, cudaStream_t st) {
+  if (!xt_ok(lgm, hb)) return socs_cols(T, K, hb, lgm, clips, keep, flare, mean, out, mode, tw, st);
+  const int B = 2 * hb + 1, S = xt_S(lgm), L = 1 << lgm;
+  const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) + xt_buf_bytes(lgm);
+  const dim3 g(L / (mode == 0 ? S : 2 * S), clips);
+#define HUV_COLS_XT(LG, SS)                                                                                   \
+  if (mode == 0)                                                                                            \
+    socs_cols_xt<LG, SS, 0><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw);                      \
+  else                                                                                                      \
+    socs_cols_xt<LG, SS, 1><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw);
+  switch (lgm) {
+    case 7: HUV_COLS_XT(7, 32) break;
+    case 8: HUV_COLS_XT(8, 16) break;
+    case 9: HUV_COLS_XT(9, 8) break;
+    default: HUV_COLS_XT(10, 4) break;
+  }
+#undef HUV_COLS_XT
   return cudaGetLastError();
 }
 
@@ -319,6 +608,18 @@ cudaError_t set_smem_limits() {
   if ((e = cudaFuncSetAttribute(socs_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
   if ((e = cudaFuncSetAttribute(socs_cols_inv<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
   if ((e = cudaFuncSetAttribute(socs_cols_inv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  const int xt = kXtSmemMax;
+#define HUV_XT_ATTR(K)                                                                    \
+  if ((e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, xt))) return e;
+  HUV_XT_ATTR((socs_rows_xt<7, 32>)) HUV_XT_ATTR((socs_rows_xt<8, 16>))
+  HUV_XT_ATTR((socs_rows_xt<9, 8>)) HUV_XT_ATTR((socs_rows_xt<10, 4>))
+  HUV_XT_ATTR((socs_cols_xt<7, 32, 0>)) HUV_XT_ATTR((socs_cols_xt<8, 16, 0>))
+  HUV_XT_ATTR((socs_cols_xt<9, 8, 0>)) HUV_XT_ATTR((socs_cols_xt<10, 4, 0>))
+  HUV_XT_ATTR((socs_cols_xt<7, 32, 1>)) HUV_XT_ATTR((socs_cols_xt<8, 16, 1>))
+  HUV_XT_ATTR((socs_cols_xt<9, 8, 1>)) HUV_XT_ATTR((socs_cols_xt<10, 4, 1>))
+  HUV_XT_ATTR((band_cols_reg<7, 32>)) HUV_XT_ATTR((band_cols_reg<8, 16>))
+  HUV_XT_ATTR((band_cols_reg<9, 8>)) HUV_XT_ATTR((band_cols_reg<10, 4>))
+#undef HUV_XT_ATTR
   return cudaSuccess;
 }
 

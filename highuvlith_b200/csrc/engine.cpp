@@ -32,6 +32,10 @@ cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int
                       float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
                       const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
+cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                        float2* T, const float2* tw, cudaStream_t st);
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+                        const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 cudaError_t set_smem_limits();
 void tc_release(huv::TcState& tc);
 void tc_release_all(std::map<int, huv::TcState>& m);
@@ -456,10 +460,10 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
     prof.end(st);
     prof.launches += 2;
     prof.begin("socs_rows_inv", st);
-    check_cuda(huv_launch::socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");
+    check_cuda(huv_launch::socs_rows_x(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");
     prof.end(st);
     prof.begin("socs_cols_inv", st);
-    check_cuda(huv_launch::socs_cols(T, K, hb, lgm, nc, ds.keep, ds.flare, mean, coarse ? IM : o, 0, twm, st),
+    check_cuda(huv_launch::socs_cols_x(T, K, hb, lgm, nc, ds.keep, ds.flare, mean, coarse ? IM : o, 0, twm, st),
                "socs_cols");
     prof.end(st);
     prof.launches += 2;
@@ -471,8 +475,8 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
       prof.end(st);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
       prof.begin("interp_rows_cols", st);
-      check_cuda(huv_launch::socs_rows(nullptr, scale, C, 1, h2, lgn, nc, T2, twn, st), "socs_rows(interp)");
-      check_cuda(huv_launch::socs_cols(T2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, o, 1, twn, st), "socs_cols(interp)");
+      check_cuda(huv_launch::socs_rows_x(nullptr, scale, C, 1, h2, lgn, nc, T2, twn, st), "socs_rows(interp)");
+      check_cuda(huv_launch::socs_cols_x(T2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, o, 1, twn, st), "socs_cols(interp)");
       prof.end(st);
       prof.launches += 4;
     }
