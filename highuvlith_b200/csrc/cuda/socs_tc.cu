@@ -72,6 +72,8 @@ struct TcGemmParams {
   long long bop_plane;  // elements between the hi and lo planes
   int bop_ld;           // row stride (elements)
   int bop_cols;         // band rows my written (2 bop_cols <= bop_ld)
+  // MODE 1: 1 = store the output tiles with TMA (tmO) through shared memory
+  int out_tma;
 };
 
 __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
@@ -79,9 +81,14 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bflo
   lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
-__host__ __device__ constexpr size_t tc_smem_bytes(int kboxes, int bn = kTcBN, bool stage = false) {
+// MODE 1 output staging: per epilogue warp two 32 x 32 f32 tiles (128B swizzle).
+constexpr uint32_t kOutTile = 32 * 32 * 4;
+constexpr uint32_t kOutStage = 4 * 2 * kOutTile;
+
+__host__ __device__ constexpr size_t tc_smem_bytes(int kboxes, int bn = kTcBN, bool stage = false,
+                                                   bool out_stage = false) {
   return 1024 + 2 * static_cast<size_t>(kboxes) * kABox + kTcStages * 2 * static_cast<size_t>(b_box_bytes(bn)) +
-         256 + (stage ? 4 * static_cast<size_t>(stage_words(bn)) * sizeof(uint32_t) : 0);
+         (out_stage ? kOutStage : 0) + 256 + (stage ? 4 * static_cast<size_t>(stage_words(bn)) * sizeof(uint32_t) : 0);
 }
 
 // MODE 0: sum over G steps (kernels) of |E|^2 with (re, im) in adjacent
@@ -92,9 +99,13 @@ __host__ __device__ constexpr size_t tc_smem_bytes(int kboxes, int bn = kTcBN, b
 // accumulator rows are (x, re/im), its columns band rows my; the tile is
 // split into BF16 hi/lo and written, through shared memory, as rows x of the
 // next GEMM's operand: bop[g][plane][x][2 my + re/im]; grid as MODE 1.
+// MODE 1 with p.out_tma: each epilogue warp stages 32 x 32 tiles in shared
+// memory (128B swizzle, double-buffered) and stores them with TMA through
+// tmO, a [problems * a_rows][out_ld] f32 map with 32 x 32 boxes.
 template <int MODE, int BN = kTcBN>
 __global__ void __launch_bounds__(192, 1)
-    tc_dft_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcGemmParams p) {
+    tc_dft_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                const __grid_constant__ CUtensorMap tmO, TcGemmParams p) {
   constexpr uint32_t kBBox = b_box_bytes(BN);
   constexpr uint32_t kTmemCols = 2 * BN <= 128 ? 128 : 256;
   extern __shared__ uint8_t smem_raw[];
@@ -102,7 +113,8 @@ __global__ void __launch_bounds__(192, 1)
   uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   uint8_t* sA = base;
   uint8_t* sB = base + 2 * p.kboxes * kABox;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + kTcStages * 2 * kBBox);
+  uint8_t* sO = sB + kTcStages * 2 * kBBox;  // MODE 1 output staging (1024-aligned)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sO + (MODE == 1 ? kOutStage : 0));
   uint64_t* full = bars;
   uint64_t* empty = bars + kTcStages;
   uint64_t* a_full = bars + 2 * kTcStages;
@@ -230,6 +242,7 @@ __global__ void __launch_bounds__(192, 1)
     for (int i = 0; i < (MODE == 0 ? HALF : 1); ++i) acc[i] = 0.f;
     const int odd = lane & 1;
     bool ok = true;
+    int nst = 0;  // MODE 1 TMA-store tiles issued by this warp
     for (int g = 0; g < p.G; ++g) {
       const int buf = g & 1;
       // Warp-uniform outcome: tcgen05.ld below is .sync.aligned.
@@ -286,6 +299,23 @@ __global__ void __launch_bounds__(192, 1)
             const int j = c0 + i;
             if ((j / HALF) == odd) acc[j % HALF] += e;
           }
+        } else if (p.out_tma) {
+          // buffer `sb` was last read by the store issued two tiles ago
+          const int sbuf = nst & 1;
+          if (lane == 0 && nst >= 2) bulk_wait_read<1>();
+          __syncwarp();
+          uint8_t* sb = sO + (quad * 2 + sbuf) * kOutTile;
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            *reinterpret_cast<float4*>(sb + lane * 128 + ((q ^ (lane & 7)) << 4)) =
+                make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) {
+            tma_store_2d(&tmO, sb, g * BN + c0, prob * p.a_rows + m_tile * 128 + quad * 32);
+            bulk_commit();
+          }
+          ++nst;
         } else {
           const int y = m_tile * 128 + row;
           float* o = p.out + prob * p.out_plane + static_cast<long long>(y) * p.out_ld + g * BN + c0;
@@ -298,6 +328,9 @@ __global__ void __launch_bounds__(192, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty[buf]);
     }
+    // Every TMA store must have finished before the CTA's shared memory goes.
+    if (MODE == 1 && lane == 0 && nst > 0) bulk_wait<0>();
+    __syncwarp();
     if (MODE == 0 && ok) {
       const int y = (m_tile * 128 + row) >> 1;
       const float add = p.mean ? p.flare * p.mean[prob] : 0.f;
@@ -520,6 +553,20 @@ bool make_map(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2-D f32 tensor map over [rows][cols] (row stride cols floats), 32 x 32
+// boxes with 128B swizzle: the TMA-store target of the interpolation GEMM.
+bool make_out_map(CUtensorMap* map, void* ptr, uint64_t rows, uint64_t cols) {
+  auto fn = encode_fn();
+  if (!fn || (reinterpret_cast<uintptr_t>(ptr) & 15u) != 0 || (cols * 4) % 16 != 0) return false;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols) * 4};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 uint16_t host_bf16(float f) {
   uint32_t u;
   std::memcpy(&u, &f, 4);
@@ -585,7 +632,9 @@ cudaError_t tc_set_smem() {
   const int bytes = static_cast<int>(tc_smem_bytes(3));
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
-  if ((e = cudaFuncSetAttribute(tc_dft_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, kTcBN, false, true)))))
+    return e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<2, kRowBN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, kRowBN, true)))))
     return e;
@@ -651,6 +700,11 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const int h2 = 2 * hb, B2 = 2 * h2 + 1;
   const int kcE = 2 * B, kpE = round_up(kcE, 64), kstE = (kcE + 15) / 16;
   const int nrI = h2 + 1, kcI = 2 * nrI, kpI = round_up(kcI, 64), kstI = (kcI + 15) / 16;
+  // The split operands written per chunk keep only the K columns the MMAs
+  // read (16 ksteps); their tensor maps end there, so the last 64-wide box
+  // of a row is partly out of bounds and TMA fills that part with zeros
+  // instead of reading padding from memory.
+  const int kbE = kstE * 16, kbI = kstI * 16;
   TcState& tc = ds.tc[lgm];
   if (!tc.gy) {
     // A_E: rows (y, re/im) over the M grid, K = (my, re/im).
@@ -690,14 +744,14 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
                              : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : (b.input_kind == HUV_INPUT_RECTS ? 0 : 8));
   const size_t per_x = align256(sizeof(float2) * n * B);
   const size_t per_m = align256(sizeof(float2) * B * B);
-  const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kpE * 2);
+  const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kbE * 2);
   const int rbn = B <= kRowBN ? kRowBN : kRowBNWide;  // rows of P (band rows my, padded)
   if (B > kRowBNWide) throw Error(HUV_ERR_UNSUPPORTED, "TC form: band wider than 96 orders");
   const size_t per_p = gemm_rows ? align256(static_cast<size_t>(K) * 2 * rbn * kpE * 2) : 0;
   const size_t per_i = align256(sizeof(float) * M * M);
   const size_t per_x2 = align256(sizeof(float2) * M * B2);
   const size_t per_c = align256(sizeof(float2) * B2 * B2);
-  const size_t per_bi = align256(static_cast<size_t>(2) * n * kpI * 2);
+  const size_t per_bi = align256(static_cast<size_t>(2) * n * kbI * 2);
   const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
   const size_t per_clip = per_x + per_m + per_be + per_p + per_i + per_x2 + per_c + per_bi + per_mean;
   const size_t budget = size_t(1) << 30;
@@ -735,14 +789,14 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
                  "band_forward");
     prof.end(st);
     CUtensorMap mbE, mbI, mbP;
-    if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kpE, kTcBN) ||
-        !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kpI, kTcBN) ||
+    if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kbE, kTcBN) ||
+        !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kbI, kTcBN) ||
         (gemm_rows && !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * rbn, kpE, rbn)))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
     prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
     if (!gemm_rows) {
       // Row transforms as FP32 register-radix FFTs, emitting the split operand.
-      launch_rows(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, kpE, kstE * 16, BE, twm, nc, st);
+      launch_rows(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, kbE, kbE, BE, twm, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc");
     } else {
       // Row transforms of every kernel's band product on tensor cores: the
@@ -760,16 +814,17 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.b_plane = rbn;
       p.err = dev_err;
       p.bop = BE;
-      p.bop_g = 2ll * M * kpE;
-      p.bop_prob = static_cast<long long>(K) * 2 * M * kpE;
-      p.bop_plane = static_cast<long long>(M) * kpE;
-      p.bop_ld = kpE;
+      p.bop_g = 2ll * M * kbE;
+      p.bop_prob = static_cast<long long>(K) * 2 * M * kbE;
+      p.bop_plane = static_cast<long long>(M) * kbE;
+      p.bop_ld = kbE;
       p.bop_cols = std::min(kstE * 8, rbn);  // the K columns GEMM0 reads: 2 my + re/im < 16 kstE
       dim3 g(1, 2 * M / 128, nc);
       if (rbn == kRowBN)
-        tc_dft_gemm<2, kRowBN><<<g, 192, tc_smem_bytes(3, kRowBN, true), st>>>(tc.map_ae, mbP, p);
+        tc_dft_gemm<2, kRowBN><<<g, 192, tc_smem_bytes(3, kRowBN, true), st>>>(tc.map_ae, mbP, tc.map_ae, p);
       else
-        tc_dft_gemm<2, kRowBNWide><<<g, 192, tc_smem_bytes(3, kRowBNWide, true), st>>>(tc.map_ae, mbP, p);
+        tc_dft_gemm<2, kRowBNWide>
+            <<<g, 192, tc_smem_bytes(3, kRowBNWide, true), st>>>(tc.map_ae, mbP, tc.map_ae, p);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<2>");
     }
     prof.end(st);
@@ -791,7 +846,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.err = dev_err;
       dim3 g(M / kTcBN, 2 * M / 128, nc);
       prof.begin("tc_dft_gemm<sumsq>", st);
-      tc_dft_gemm<0><<<g, 192, smem_tc, st>>>(tc.map_ae, mbE, p);
+      tc_dft_gemm<0><<<g, 192, smem_tc, st>>>(tc.map_ae, mbE, tc.map_ae, p);
       prof.end(st);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<0>");
     }
@@ -803,7 +858,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     {
       prof.begin("socs_rows_tc<interp>", st);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
-      launch_rows(nullptr, scale, C, 1, h2, h2, nrI, lgn, kpI, kstI * 16, BI, twn, nc, st);
+      launch_rows(nullptr, scale, C, 1, h2, h2, nrI, lgn, kbI, kbI, BI, twn, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc(interp)");
       prof.end(st);
     }
@@ -823,9 +878,12 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.mean = nullptr;
       p.out = o;
       p.err = dev_err;
+      CUtensorMap mo;
+      p.out_tma = make_out_map(&mo, o, static_cast<uint64_t>(nc) * n, n) ? 1 : 0;
+      if (!p.out_tma) mo = tc.map_ai;  // unused
       dim3 g(1, n / 128, nc);
       prof.begin("tc_dft_gemm<interp>", st);
-      tc_dft_gemm<1><<<g, 192, smem_tc, st>>>(tc.map_ai, mbI, p);
+      tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_ai, mbI, mo, p);
       prof.end(st);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
     }
