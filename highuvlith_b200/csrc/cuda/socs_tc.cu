@@ -541,10 +541,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // 2-D bf16 tensor map over a K-major [rows][kp] array, box 64 x box_rows, 128B swizzle.
-bool make_map(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_rows) {
+// With cols > 0 the map ends at column cols (< kp): TMA fills the columns
+// beyond it with zeros instead of reading them.
+bool make_map(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_rows, int cols = 0) {
   auto fn = encode_fn();
   if (!fn) return false;
-  cuuint64_t dims[2] = {static_cast<cuuint64_t>(kp), rows};
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols > 0 ? cols : kp), rows};
   cuuint64_t strides[1] = {static_cast<cuuint64_t>(kp) * 2};
   cuuint32_t box[2] = {64, static_cast<cuuint32_t>(box_rows)};
   cuuint32_t estr[2] = {1, 1};
@@ -700,10 +702,10 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const int h2 = 2 * hb, B2 = 2 * h2 + 1;
   const int kcE = 2 * B, kpE = round_up(kcE, 64), kstE = (kcE + 15) / 16;
   const int nrI = h2 + 1, kcI = 2 * nrI, kpI = round_up(kcI, 64), kstI = (kcI + 15) / 16;
-  // The split operands written per chunk keep only the K columns the MMAs
-  // read (16 ksteps); their tensor maps end there, so the last 64-wide box
-  // of a row is partly out of bounds and TMA fills that part with zeros
-  // instead of reading padding from memory.
+  // The split operands written per chunk are laid out with rows of the K
+  // extent the MMAs read (16 ksteps) and written only up to the band's
+  // 2 B columns: their tensor maps end at column 2 B, so TMA fills the rest
+  // of the last 64-wide box with zeros instead of reading padding.
   const int kbE = kstE * 16, kbI = kstI * 16;
   TcState& tc = ds.tc[lgm];
   if (!tc.gy) {
@@ -789,14 +791,14 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
                  "band_forward");
     prof.end(st);
     CUtensorMap mbE, mbI, mbP;
-    if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kbE, kTcBN) ||
-        !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kbI, kTcBN) ||
+    if (!make_map(&mbE, BE, static_cast<uint64_t>(nc) * K * 2 * M, kbE, kTcBN, kcE) ||
+        !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kbI, kTcBN, kcI) ||
         (gemm_rows && !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * rbn, kpE, rbn)))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
     prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
     if (!gemm_rows) {
       // Row transforms as FP32 register-radix FFTs, emitting the split operand.
-      launch_rows(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, kbE, kbE, BE, twm, nc, st);
+      launch_rows(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, kbE, 0, BE, twm, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc");
     } else {
       // Row transforms of every kernel's band product on tensor cores: the
@@ -858,7 +860,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     {
       prof.begin("socs_rows_tc<interp>", st);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
-      launch_rows(nullptr, scale, C, 1, h2, h2, nrI, lgn, kbI, kbI, BI, twn, nc, st);
+      launch_rows(nullptr, scale, C, 1, h2, h2, nrI, lgn, kbI, 0, BI, twn, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc(interp)");
       prof.end(st);
     }
