@@ -194,11 +194,9 @@ huv_status huv_ilt_cost_grad(void* engine, const huv_ilt_params* params, int32_t
     std::lock_guard<std::mutex> lock(e->mu);
     e->ensure_device();
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    double* d = nullptr;
-    huv::check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(double) * n_masks, st), "cudaMallocAsync");
+    double* d = e->ilt_cost_buffer(n_masks);
     e->ilt_eval(*params, n_masks, theta, target, grad, d, st);
     huv::check_cuda(cudaMemcpyAsync(cost_host, d, sizeof(double) * n_masks, cudaMemcpyDeviceToHost, st), "D2H cost");
-    huv::check_cuda(cudaFreeAsync(d, st), "cudaFreeAsync");
     huv::check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   });
 }

@@ -132,6 +132,17 @@ __host__ __device__ constexpr int fr_buf(int L, int S) { return (S < 16 ? L + L 
 // Threads of one block: one radix-16 butterfly per thread per pass.
 __host__ __device__ constexpr int fr_threads(int LG, int S) { return S * (1 << LG) / 16; }
 
+// Sequences per block of the register-radix kernels for L = 2^lg (256
+// threads each), 0 where no instance exists; shared-memory bytes of the
+// ping-pong buffers of one block and the kernels' shared-memory ceiling.
+__host__ __device__ constexpr int xt_S(int lg) {
+  return lg == 7 ? 32 : lg == 8 ? 16 : lg == 9 ? 8 : lg == 10 ? 4 : 0;
+}
+__host__ __device__ constexpr size_t xt_buf_bytes(int lg) {
+  return (fr_passes(lg) - 1) * static_cast<size_t>(fr_buf(1 << lg, xt_S(lg))) * sizeof(float2);
+}
+constexpr int kXtSmemMax = 110 * 1024;
+
 // First pass (radix 16, no twiddles) for thread t, reading a zero-padded
 // band: position i of sequence s holds P[s][mx] for the order mx - hb = i
 // (i <= hb) or i - L (i >= L - hb), and zero elsewhere.  Requires 2 hb < L.

@@ -19,6 +19,7 @@
 
 #include "../engine.hpp"
 #include "fft_block.cuh"
+#include "fft_reg.cuh"
 
 namespace huv_dev {
 
@@ -136,6 +137,110 @@ __global__ void ilt_cols_adj(const float2* __restrict__ T, const float* __restri
       Vm[((static_cast<size_t>(k) * B + my) << lg) + x0 + w] = f[(w << lg) + ((my - hb) & (L - 1))];
     }
     __syncthreads();
+  }
+}
+
+// ilt_cols_adj with register-radix passes (fft_reg.cuh), reading the x-major
+// row transforms Tt[mask][k][x][my] of socs_rows_x.  CTA per (mask, S
+// columns); each thread keeps G0 at its own (column, y) positions in
+// registers across all kernels.  Per kernel: inverse FFT_y of the band column
+// (P -> b0 [-> b1]), times G0, natural order into the other buffer, forward
+// FFT_y, band rows [-hb, hb] kept: V[mask][k][my'][x] (the layout of
+// ilt_rows_adj).  grid: (L / S, masks); shared: S B + 2 buffers.
+template <int LG, int S>
+__global__ void __launch_bounds__(fr_threads(LG, S))
+    ilt_cols_adj_xt(const float2* __restrict__ Tt, const float* __restrict__ G, int K, int hb, float keep,
+                    const double* __restrict__ sums, float flare_over_n, float2* __restrict__ V,
+                    const float2* __restrict__ tw) {
+  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
+  constexpr int R = fr_radix(LG, NP - 1);
+  extern __shared__ float2 smem[];
+  const int B = 2 * hb + 1;
+  const int mask = blockIdx.y;
+  const int x0 = blockIdx.x * S;
+  const int t = threadIdx.x;
+  float2* P = smem;  // [S][B]
+  float2* b0 = smem + S * B;
+  float2* b1 = b0 + fr_buf(L, S);
+  // the inverse transform ends in `inv`, the weighted field goes to `oth`
+  float2* inv = NP == 3 ? b1 : b0;
+  float2* oth = NP == 3 ? b0 : b1;
+  const float add = sums ? flare_over_n * static_cast<float>(sums[mask * 2 + 1]) : 0.f;
+  const float* Gm = G + static_cast<size_t>(mask) * L * L;
+  float g[16];
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    const int u = t + b * T;
+    const int s = u % S, j = u / S;
+#pragma unroll
+    for (int p = 0; p < R; ++p)
+      g[b * R + p] = keep * Gm[static_cast<size_t>(j + p * (L / R)) * L + x0 + s] + add;
+  }
+  for (int k = 0; k < K; ++k) {
+    const float2* src = Tt + ((static_cast<size_t>(mask) * K + k) * L + x0) * B;
+    for (int e = t; e < S * B; e += T) P[e] = src[e];
+    __syncthreads();
+    fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
+    __syncthreads();
+    if constexpr (NP == 3) {
+      fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
+      __syncthreads();
+    }
+#pragma unroll
+    for (int b = 0; b < 16 / R; ++b) {
+      int s, j;
+      float2 v[R];
+      fr_last_pass<LG, S, +1>(t + b * T, inv, tw, s, j, v);
+#pragma unroll
+      for (int p = 0; p < R; ++p) {
+        const float w = g[b * R + p];
+        oth[fr_idx<S>(j + p * (L / R), s)] = make_float2(v[p].x * w, v[p].y * w);
+      }
+    }
+    __syncthreads();
+    {
+      const int s = t % S, j = t / S;
+      float2 v[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = oth[fr_idx<S>(j + r * (L / 16), s)];
+      fr_first_pass_vals<LG, S, -1>(t, v, inv);
+    }
+    __syncthreads();
+    const float2* cur = inv;
+    if constexpr (NP == 3) {
+      fr_mid_pass<LG, S, -1, 1>(t, inv, oth, tw);
+      __syncthreads();
+      cur = oth;
+    }
+    float2* Vk = V + (static_cast<size_t>(mask) * K + k) * B * L + x0;
+#pragma unroll
+    for (int b = 0; b < 16 / R; ++b) {
+      int s, j;
+      float2 v[R];
+      fr_last_pass<LG, S, -1>(t + b * T, cur, tw, s, j, v);
+#pragma unroll
+      for (int p = 0; p < R; ++p) {
+        const int idx = j + p * (L / R);
+        const int mi = idx <= hb ? idx + hb : (idx >= L - hb ? idx - L + hb : -1);
+        if (mi >= 0) Vk[static_cast<size_t>(mi) * L + s] = v[p];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// In place: Q <- its Hermitian part (Q(f) + conj(Q(-f))) / 2 on each mask's
+// B x B band, so that IFFT(Q) is real and equals Re IFFT of the original.
+__global__ void hermitian_part(float2* __restrict__ Q, int B, int masks) {
+  const int half = (B * B + 1) / 2;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < half * masks; e += gridDim.x * blockDim.x) {
+    const int mask = e / half, i = e - mask * half;
+    float2* q = Q + static_cast<size_t>(mask) * B * B;
+    const int j = B * B - 1 - i;
+    const float2 a = q[i], c = q[j];
+    const float2 h = make_float2(0.5f * (a.x + c.x), 0.5f * (a.y - c.y));
+    q[i] = h;
+    q[j] = make_float2(h.x, -h.y);
   }
 }
 
@@ -411,12 +516,30 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
 cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 
+bool xt_ok(int lg, int hb);
+
 cudaError_t ilt_set_smem() {
   const int big = 200 * 1024;
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
   if ((e = cudaFuncSetAttribute(huv_dev::ilt_rows_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+  const int xt = huv_dev::kXtSmemMax;
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<7, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+    return e;
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+    return e;
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<9, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+    return e;
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<10, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+    return e;
   return cudaSuccess;
+}
+
+// Shared memory of ilt_cols_adj_xt: the band columns and two buffers.
+size_t ilt_adj_xt_smem(int lg, int hb) {
+  const int S = huv_dev::xt_S(lg);
+  return (static_cast<size_t>(S) * (2 * hb + 1) + 2 * static_cast<size_t>(huv_dev::fr_buf(1 << lg, S))) *
+         sizeof(float2);
 }
 }  // namespace huv_launch
 
@@ -510,6 +633,7 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   double* preg = reinterpret_cast<double*>(take(s_preg));
   double* sums = reinterpret_cast<double*>(take(s_parts));
   double* regsum = reinterpret_cast<double*>(take(a256(sizeof(double) * 4)));
+  prof.begin(grad ? "ilt_cost_grad" : "ilt_cost", st);
   for (int c0 = 0; c0 < masks; c0 += chunk) {
     const int nc = std::min(chunk, masks - c0);
     const float* th = theta + npix * c0;
@@ -519,8 +643,16 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     check_cuda(band_forward(tbuf, HUV_INPUT_RASTER_F32, n, lgn, hb, nc, X, Mb, nullptr, ds.W, mean, twn, st, nullptr, nullptr),
                "ilt band_forward");
     // fields of every kernel on the evaluation grid, the image on it, then on N x N
-    check_cuda(socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "ilt socs_rows");
-    check_cuda(socs_cols(T, K, hb, lgm, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
+    // x-major row transforms (register-radix kernels) when the adjoint's
+    // register-radix column pass fits too, else the [k][my][x] layout
+    const bool xt = xt_ok(lgm, hb) && ilt_adj_xt_smem(lgm, hb) <= static_cast<size_t>(kXtSmemMax);
+    if (xt) {
+      check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "ilt socs_rows");
+      check_cuda(socs_cols_x(T, K, hb, lgm, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
+    } else {
+      check_cuda(socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "ilt socs_rows");
+      check_cuda(socs_cols(T, K, hb, lgm, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
+    }
     if (coarse) {
       check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st, nullptr,
                               nullptr),
@@ -548,18 +680,33 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
         Gm = IM;
         grid_scale = static_cast<float>(static_cast<double>(npix) / static_cast<double>(mpix));
       }
-      const int Wc = fit_units(8, 2 * (sizeof(float2) << lgm) + (sizeof(float) << lgm));
-      const size_t sm = 2 * (static_cast<size_t>(Wc) << lgm) * sizeof(float2) + (static_cast<size_t>(Wc) << lgm) * sizeof(float);
-      ilt_cols_adj<<<dim3(M / Wc, nc), 256, sm, st>>>(T, Gm, K, hb, lgm, Wc, keep, sums,
-                                                      flare / static_cast<float>(npix), V, twm);
+      if (xt) {
+        const dim3 ga(M / xt_S(lgm), nc);
+        const size_t sm = ilt_adj_xt_smem(lgm, hb);
+        const float fo = flare / static_cast<float>(npix);
+        switch (lgm) {
+          case 7: ilt_cols_adj_xt<7, 32><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+          case 8: ilt_cols_adj_xt<8, 16><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+          case 9: ilt_cols_adj_xt<9, 8><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+          default: ilt_cols_adj_xt<10, 4><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+        }
+      } else {
+        const int Wc = fit_units(8, 2 * (sizeof(float2) << lgm) + (sizeof(float) << lgm));
+        const size_t sm = 2 * (static_cast<size_t>(Wc) << lgm) * sizeof(float2) +
+                          (static_cast<size_t>(Wc) << lgm) * sizeof(float);
+        ilt_cols_adj<<<dim3(M / Wc, nc), 256, sm, st>>>(T, Gm, K, hb, lgm, Wc, keep, sums,
+                                                        flare / static_cast<float>(npix), V, twm);
+      }
       const int S = fit_units(4, 2 * (sizeof(float2) << lgm));
       const size_t sm2 = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
       ilt_rows_adj<<<dim3(B, nc), 256, sm2, st>>>(V, ds.kband, K, hb, lgm, S, Q, twm);
       const float scale = static_cast<float>(2.0 * (1.0 - p.absorber) * p.weight) * grid_scale;
-      // Q is not Hermitian: the unpaired synthesis takes Re of the complex field
-      check_cuda(socs_rows(nullptr, scale, Q, 1, hb, lgn, nc, T2, twn, st), "ilt grad rows");
+      // Re IFFT(Q) = IFFT(Hermitian part of Q): a real synthesis, two
+      // columns per transform on the register-radix path
+      hermitian_part<<<(nc * ((B * B + 1) / 2) + 255) / 256, 256, 0, st>>>(Q, B, nc);
+      check_cuda(socs_rows_x(nullptr, scale, Q, 1, hb, lgn, nc, T2, twn, st), "ilt grad rows");
       dcdm = tbuf;  // the transmittance is no longer needed
-      check_cuda(socs_cols(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, twn, st), "ilt grad cols");
+      check_cuda(socs_cols_x(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, twn, st), "ilt grad cols");
     }
     if (tiled)
       ilt_finish_tiled<<<dim3(reg_parts, nc), 256, 0, st>>>(
@@ -576,8 +723,9 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     ilt_combine<<<(nc + 127) / 128, 128, 0, st>>>(sums, regsum, nc, p.weight, 1.0 / static_cast<double>(npix),
                                                   cost_dev + c0);
     check_cuda(cudaGetLastError(), "ilt kernels");
-    prof.launches += (grad ? 16 : 10) + (coarse ? (grad ? 9 : 4) : 0);
+    prof.launches += (grad ? 17 : 10) + (coarse ? (grad ? 9 : 4) : 0);
   }
+  prof.end(st);
 }
 
 // Surrogate-based ILT cost and gradient: the transmittance's image comes

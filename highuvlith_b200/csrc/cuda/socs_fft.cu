@@ -445,13 +445,6 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
   }
 }
 
-// Sequences per block of the register-radix kernels for L = 2^lg.
-constexpr int xt_S(int lg) { return lg == 7 ? 32 : lg == 8 ? 16 : lg == 9 ? 8 : lg == 10 ? 4 : 0; }
-constexpr size_t xt_buf_bytes(int lg) {
-  return (fr_passes(lg) - 1) * static_cast<size_t>(fr_buf(1 << lg, xt_S(lg))) * sizeof(float2);
-}
-constexpr int kXtSmemMax = 110 * 1024;
-
 }  // namespace huv_dev
 
 // ------------------------------------------------------------ launchers

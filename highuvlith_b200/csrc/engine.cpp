@@ -129,6 +129,7 @@ Engine::~Engine() {
     for (auto& e : cache) free_set(e.dev);
     prof.release();
     cudaFree(dev_err);
+    cudaFree(ilt_cost_dev);
     cudaFree(ws);
     cudaFree(io_in);
     cudaFree(io_out);
@@ -379,6 +380,17 @@ int Engine::kernel_count_for(const KernelSet& ks, int max_kernels) const {
   const int k = select_kernel_count(ks.all_values.empty() ? ks.eigenvalues : ks.all_values, ks.trace, max_kernels,
                                     settings.kernel_energy_fraction);
   return std::min(k, ks.num_kernels());
+}
+
+double* Engine::ilt_cost_buffer(int n_masks) {
+  if (n_masks > ilt_cost_cap) {
+    cudaFree(ilt_cost_dev);
+    ilt_cost_dev = nullptr;
+    ilt_cost_cap = 0;
+    check_cuda(cudaMalloc(&ilt_cost_dev, sizeof(double) * n_masks), "cudaMalloc(ilt costs)");
+    ilt_cost_cap = n_masks;
+  }
+  return ilt_cost_dev;
 }
 
 void* Engine::workspace(size_t bytes) {

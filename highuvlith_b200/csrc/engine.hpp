@@ -154,6 +154,11 @@ struct Engine {
   const uint8_t* row_digit_table(int hb);
   DeviceSet& device_set(double z);
   void* workspace(size_t bytes);
+  // Device buffer of at least n doubles for per-mask ILT costs, kept (and
+  // grown) for the engine's lifetime.
+  double* ilt_cost_buffer(int n);
+  double* ilt_cost_dev = nullptr;
+  int ilt_cost_cap = 0;
   int choose_eval_grid(const DeviceSet& ds, int requested) const;
   bool tc_supported(const DeviceSet& ds, int M) const;
   // K_use / W_use: kernel count and flare weights to use (0 / nullptr = the whole set).
