@@ -407,6 +407,17 @@ def run_ours(args):
 
     # roofline of the dominant kernel
     hbm, tc_burst, tc_sus, peak_kind = peaks()
+    # DRAM bytes (read + write) per clip of each timed region, from ncu
+    # captures of this workload at 32 clips (cold cache, serialised;
+    # profiles/socs_tc_and_fft_c2_traffic_32clips.md), scaled to a launch by
+    # its clips
+    traffic_per_clip = {"tc_dft_gemm<sumsq>": (166.38e6 + 6.65e6) / 32,
+                        "socs_rows_tc": (19.29e6 + 110.03e6) / 32,
+                        "tc_dft_gemm<interp>": (22.77e6 + 71.55e6) / 32,
+                        "mask_band": (33.82e6 + 19.74e6 + 0.01e6) / 32,
+                        "socs_cols_inv": (152.44e6 + 0.22e6) / 32,
+                        "socs_rows_inv": (2.91e6 + 90.31e6) / 32,
+                        "interp_rows_cols": (5.93e6 + 0.21e6 + 39.12e6 + 77.20e6) / 32}
     K, S = diag["num_kernels"], diag["num_frequencies"]
     bytes_per_image = 4 * N_GRID ** 2 + 4 * N_GRID ** 2 + 8 * K * S
     launches = max(prof["launches"], 1)
@@ -415,7 +426,11 @@ def run_ours(args):
     achieved = bytes_per_image * images_per_launch / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
     total_ms = ms * args.steps
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "kernel": prof["kernel"], "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                "traffic": (traffic_per_clip[prof["kernel"]] * images_per_launch
+                            if prof["kernel"] in traffic_per_clip else None),
+                "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum per clip "
+                                "at 32 clips, x clips per launch)",
+                "kernel": prof["kernel"], "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
                 "algorithmic_bytes_per_image": bytes_per_image,
                 "kernel_share_of_step": prof["ms"] / total_ms if ms > 0 else None,
                 "note": "achieved = SURVEY 8(d) algorithmic bytes per image x images per launch / the dominant "
