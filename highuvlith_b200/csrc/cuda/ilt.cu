@@ -27,11 +27,20 @@ namespace huv_dev {
 // t = a + (1 - a) sigmoid(beta theta) (the transmittance fed to the band FFT).
 __global__ void ilt_transmittance(const float* __restrict__ theta, size_t n, float beta, float absorber,
                                   float* __restrict__ t) {
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+  // float4 body when both arrays are 16-byte aligned, scalar tail
+  const bool vec = ((reinterpret_cast<uintptr_t>(theta) | reinterpret_cast<uintptr_t>(t)) & 15u) == 0;
+  const size_t n4 = vec ? n / 4 : 0;
+  const float4* th4 = reinterpret_cast<const float4*>(theta);
+  float4* t4 = reinterpret_cast<float4*>(t);
+  auto f = [&](float v) { return absorber + (1.f - absorber) / (1.f + __expf(-beta * v)); };
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n4;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const float m = 1.f / (1.f + __expf(-beta * theta[i]));
-    t[i] = absorber + (1.f - absorber) * m;
+    const float4 v = th4[i];
+    t4[i] = make_float4(f(v.x), f(v.y), f(v.z), f(v.w));
   }
+  for (size_t i = 4 * n4 + blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    t[i] = f(theta[i]);
 }
 
 __device__ __forceinline__ double block_sum_double(double v, double* red) {
@@ -57,21 +66,41 @@ __global__ void ilt_data(const float* __restrict__ img, const float* __restrict_
   float* g = G + mask * npix;
   const float inv_n = 1.f / static_cast<float>(npix);
   double sr = 0.0, sg = 0.0;
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < npix;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const float I = im[i];
-    float r, gv;
+  auto term = [&](float I, float T, float& gv) {
+    float r;
     if (kind == 0) {
-      r = dose * I - tg[i];
+      r = dose * I - T;
       gv = 2.f * r * dose * inv_n;
     } else {
       const float R = 1.f / (1.f + __expf(-steep * (dose * I - thr)));
-      r = R - tg[i];
+      r = R - T;
       gv = 2.f * r * steep * R * (1.f - R) * dose * inv_n;
     }
-    g[i] = gv;
     sr += static_cast<double>(r) * r;
     sg += gv;
+  };
+  // float4 body when the three planes are 16-byte aligned, scalar tail
+  const bool vec =
+      ((reinterpret_cast<uintptr_t>(im) | reinterpret_cast<uintptr_t>(tg) | reinterpret_cast<uintptr_t>(g)) & 15u) == 0;
+  const size_t n4 = vec ? npix / 4 : 0;
+  const float4* im4 = reinterpret_cast<const float4*>(im);
+  const float4* tg4 = reinterpret_cast<const float4*>(tg);
+  float4* g4 = reinterpret_cast<float4*>(g);
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n4;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float4 I = im4[i], T = tg4[i];
+    float4 o;
+    term(I.x, T.x, o.x);
+    term(I.y, T.y, o.y);
+    term(I.z, T.z, o.z);
+    term(I.w, T.w, o.w);
+    g4[i] = o;
+  }
+  for (size_t i = 4 * n4 + blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < npix;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    float gv;
+    term(im[i], tg[i], gv);
+    g[i] = gv;
   }
   const double a = block_sum_double(sr, red);
   const double b = block_sum_double(sg, red);
@@ -344,11 +373,15 @@ __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict_
   const float inv_n = 1.f / static_cast<float>(npix);
   for (int e = threadIdx.x; e < 34 * 34; e += blockDim.x) {
     const int r = e / 34, c = e - r * 34;
-    const int i = (ti * 32 - 1 + r + n) % n, j = (tj * 32 - 1 + c + n) % n;
+    int i = ti * 32 - 1 + r, j = tj * 32 - 1 + c;
+    i = i < 0 ? i + n : (i >= n ? i - n : i);
+    j = j < 0 ? j + n : (j >= n ? j - n : j);
     sm[r][c] = 1.f / (1.f + __expf(-beta * th[static_cast<size_t>(i) * n + j]));
   }
   __syncthreads();
-  double cost = 0.0;
+  // per-thread partials of the 4 pixels in FP32, the block sum in FP64
+  float tv_part = 0.f, bin_part = 0.f;
+  const float eps2 = tv_eps * tv_eps;
   for (int q = 0; q < 4; ++q) {
     const int pidx = threadIdx.x + 256 * q;
     const int r = (pidx >> 5) + 1, c = (pidx & 31) + 1;
@@ -356,19 +389,20 @@ __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict_
     float g = 0.f;
     if (tv_w > 0.f) {
       const float gx = sm[r][c + 1] - m, gy = sm[r + 1][c] - m;
-      const float sv = sqrtf(gx * gx + gy * gy + tv_eps * tv_eps);
-      cost += static_cast<double>(tv_w) * (sv - tv_eps) * inv_n;
+      const float qv = gx * gx + gy * gy + eps2;
+      const float iv = rsqrtf(qv);
+      tv_part += qv * iv - tv_eps;
       if (grad) {
         const float ml = sm[r][c - 1], mu = sm[r - 1][c];
         const float gxl = m - ml, gyl = sm[r + 1][c - 1] - ml;
-        const float sl = sqrtf(gxl * gxl + gyl * gyl + tv_eps * tv_eps);
+        const float il = rsqrtf(gxl * gxl + gyl * gyl + eps2);
         const float gxu = sm[r - 1][c + 1] - mu, gyu = m - mu;
-        const float su = sqrtf(gxu * gxu + gyu * gyu + tv_eps * tv_eps);
-        g += tv_w * inv_n * (-(gx + gy) / sv + gxl / sl + gyu / su);
+        const float iu = rsqrtf(gxu * gxu + gyu * gyu + eps2);
+        g += tv_w * inv_n * (-(gx + gy) * iv + gxl * il + gyu * iu);
       }
     }
     if (bin_w > 0.f) {
-      cost += static_cast<double>(bin_w) * 4.0 * m * (1.0 - m) * inv_n;
+      bin_part += m * (1.f - m);
       g += bin_w * 4.f * (1.f - 2.f * m) * inv_n;
     }
     if (grad) {
@@ -376,6 +410,7 @@ __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict_
       grad[gp] = ((dcdm ? dcdm[gp] : 0.f) + g) * beta * m * (1.f - m);
     }
   }
+  const double cost = (static_cast<double>(tv_w) * tv_part + 4.0 * static_cast<double>(bin_w) * bin_part) * inv_n;
   const double cs = block_sum_double(cost, red);
   if (threadIdx.x == 0) parts[static_cast<size_t>(mask) * gridDim.x + blockIdx.x] = cs;
 }

@@ -374,6 +374,53 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
   }
 }
 
+// band_rows_fwd<1> (f32 rasters) with register-radix passes: S complex
+// sequences per block, sequence s packing rows (2s, 2s+1) as re / im; the
+// last pass leaves the spectra in natural order in shared memory, and the
+// two real rows' bands are split from Z(m) and conj Z(-m).
+// grid: (clips * L / (2 S)); X: [clip][y][B].
+template <int LG, int S>
+__global__ void __launch_bounds__(fr_threads(LG, S))
+    band_rows_reg(const float* __restrict__ in, int hb, float2* __restrict__ X, const float2* __restrict__ tw) {
+  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
+  extern __shared__ float2 smem[];
+  const int B = 2 * hb + 1;
+  const size_t row0 = static_cast<size_t>(blockIdx.x) * 2 * S;
+  const int t = threadIdx.x;
+  float2* b0 = smem;
+  float2* b1 = b0 + fr_buf(L, S);
+  {
+    const int s = t % S, j = t / S;
+    const float* ra = in + (row0 + 2 * s) * L + j;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = make_float2(ra[r * (L / 16)], ra[L + r * (L / 16)]);
+    fr_first_pass_vals<LG, S, -1>(t, v, b0);
+  }
+  __syncthreads();
+  float2* cur = b0;
+  if constexpr (NP == 3) {
+    fr_mid_pass<LG, S, -1, 1>(t, b0, b1, tw);
+    __syncthreads();
+    fr_mid_pass<LG, S, -1, 2>(t, b1, b0, tw);
+  } else {
+    fr_mid_pass<LG, S, -1, 1>(t, b0, b1, tw);
+    cur = b1;
+  }
+  __syncthreads();
+  for (int e = t; e < S * B; e += T) {
+    const int s = e / B, mi = e - s * B;
+    const int idx = (mi - hb) & (L - 1);
+    const float2 z = cur[fr_idx<S>(idx, s)];
+    const float2 zc = cconj(cur[fr_idx<S>((L - idx) & (L - 1), s)]);
+    const float2 xa = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y + zc.y));
+    const float2 d = csub(z, zc);
+    const float2 xb = make_float2(0.5f * d.y, -0.5f * d.x);
+    X[(row0 + 2 * s) * B + mi] = xa;
+    X[(row0 + 2 * s + 1) * B + mi] = xb;
+  }
+}
+
 // band_cols_fwd with register-radix passes: forward FFT along y of S band
 // columns of X[clip][y][B] per block, the first pass reading X directly.
 // grid: (ceil(B / S), clips).
@@ -476,18 +523,33 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   dim3 g1(n / rows_per_block, clips);
   const int th = pick_threads(S << (lg - 2));
   // u8 rasters take the exact integer tensor-core row band when the shape
-  // and the input's alignment allow it.
+  // and the input's alignment allow it; f32 rasters the register-radix rows.
   cudaError_t rows_tc = cudaErrorNotSupported;
   if (kind == 0 && row_digits) {
     rows_tc = mask_rows_tc(in, n, hb, clips, X, row_digits, err, st);
     if (rows_tc != cudaSuccess && rows_tc != cudaErrorNotSupported) return rows_tc;
+  }
+  if (kind == 1 && xt_ok(lg, hb)) {
+    const int Sr = xt_S(lg);
+    const dim3 gr(static_cast<unsigned>(static_cast<size_t>(clips) * n / (2 * Sr)));
+    const size_t smr = 2 * static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
+    const float* fin = static_cast<const float*>(in);
+    switch (lg) {
+      case 7: band_rows_reg<7, 32><<<gr, 256, smr, st>>>(fin, hb, X, tw); break;
+      case 8: band_rows_reg<8, 16><<<gr, 256, smr, st>>>(fin, hb, X, tw); break;
+      case 9: band_rows_reg<9, 8><<<gr, 256, smr, st>>>(fin, hb, X, tw); break;
+      default: band_rows_reg<10, 4><<<gr, 256, smr, st>>>(fin, hb, X, tw); break;
+    }
+    rows_tc = cudaSuccess;
   }
   // Only device rasters come here (rectangle clips take the analytic path).
   switch (kind) {
     case 0:
       if (rows_tc != cudaSuccess) band_rows_fwd<0><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw);
       break;
-    case 1: band_rows_fwd<1><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
+    case 1:
+      if (rows_tc != cudaSuccess) band_rows_fwd<1><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw);
+      break;
     case 2: band_rows_fwd<2><<<g1, th, sm1, st>>>(in, lg, rows_per_block, hb, X, tw); break;
     default: return cudaErrorInvalidValue;
   }
@@ -612,6 +674,8 @@ cudaError_t set_smem_limits() {
   HUV_XT_ATTR((socs_cols_xt<9, 8, 1>)) HUV_XT_ATTR((socs_cols_xt<10, 4, 1>))
   HUV_XT_ATTR((band_cols_reg<7, 32>)) HUV_XT_ATTR((band_cols_reg<8, 16>))
   HUV_XT_ATTR((band_cols_reg<9, 8>)) HUV_XT_ATTR((band_cols_reg<10, 4>))
+  HUV_XT_ATTR((band_rows_reg<7, 32>)) HUV_XT_ATTR((band_rows_reg<8, 16>))
+  HUV_XT_ATTR((band_rows_reg<9, 8>)) HUV_XT_ATTR((band_rows_reg<10, 4>))
 #undef HUV_XT_ATTR
   return cudaSuccess;
 }
