@@ -485,6 +485,28 @@ def run_ours(args):
                 forms[name] = {"ms_per_step": fms, "images_per_s": N_CLIPS / (fms / 1e3)}
             except Exception as exc:  # report, do not hide
                 forms[name] = {"unavailable": str(exc)[:200]}
+        # SURVEY 8(d) whole-path work per image: the reference's FFT FLOPs
+        # (5 N^2 log2 N^2 + K (5 B N log2 N + 5 N^2 log2 N)) for the FFT forms,
+        # the split-BF16 DFT-GEMM FLOPs of the coarse-grid formulation (band
+        # forward 4 B N^2 + 8 B^2 N, inverse K 8 (B^2 M + B M^2), interpolation
+        # 8 (M^2 N + M N^2), split products counted once) for the TC form
+        Bw = 2 * diag["band_half_width"] + 1
+        M_eval = 256
+        lgN = math.log2(N_GRID)
+        f_fft = 5 * N_GRID ** 2 * 2 * lgN + K * (5 * Bw * N_GRID * lgN + 5 * N_GRID ** 2 * lgN)
+        f_tc = (4 * Bw * N_GRID ** 2 + 8 * Bw * Bw * N_GRID + K * 8 * (Bw * Bw * M_eval + Bw * M_eval ** 2)
+                + 8 * (M_eval ** 2 * N_GRID + M_eval * N_GRID ** 2))
+        for name, f, peak in (("fft_full_grid", f_fft, None), ("fft_coarse_grid", f_fft, None),
+                              ("tc", f_tc, tc_sus), ("tc_gemm_rows", f_tc, tc_sus)):
+            r = forms.get(name, {})
+            if "images_per_s" in r:
+                r["algorithmic_gflop_per_image"] = f / 1e9
+                r["algorithmic_tflops"] = f * r["images_per_s"] / 1e12
+                if peak:
+                    r["frac_of_bf16_sustained"] = r["algorithmic_tflops"] / peak
+        if "images_per_s" in forms.get("tc", {}) and "images_per_s" in forms.get("fft_coarse_grid", {}):
+            forms["tc_over_fft_coarse_grid"] = forms["tc"]["images_per_s"] / forms["fft_coarse_grid"]["images_per_s"]
+            forms["tc_over_fft_full_grid"] = forms["tc"]["images_per_s"] / forms["fft_full_grid"]["images_per_s"]
         extra["forms"] = forms
         extra["ilt"] = ilt_leg(eng, stream)
         extra["uneven_batch"] = uneven_leg(stream, n_clips=args.uneven_clips)

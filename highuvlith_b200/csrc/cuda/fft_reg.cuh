@@ -132,6 +132,20 @@ __host__ __device__ constexpr int fr_buf(int L, int S) { return (S < 16 ? L + L 
 // Threads of one block: one radix-16 butterfly per thread per pass.
 __host__ __device__ constexpr int fr_threads(int LG, int S) { return S * (1 << LG) / 16; }
 
+// Asynchronous 8-byte global -> shared copies (cp.async, L1-allocating) for
+// prefetching the next kernel's band columns while the current one is
+// transformed.
+__device__ __forceinline__ void fr_cp_async8(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem_dst))),
+               "l"(gmem_src)
+               : "memory");
+}
+__device__ __forceinline__ void fr_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void fr_cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Sequences per block of the register-radix kernels for L = 2^lg (256
 // threads each), 0 where no instance exists; shared-memory bytes of the
 // ping-pong buffers of one block and the kernels' shared-memory ceiling.

@@ -175,7 +175,8 @@ __global__ void ilt_cols_adj(const float2* __restrict__ T, const float* __restri
 // registers across all kernels.  Per kernel: inverse FFT_y of the band column
 // (P -> b0 [-> b1]), times G0, natural order into the other buffer, forward
 // FFT_y, band rows [-hb, hb] kept: V[mask][k][my'][x] (the layout of
-// ilt_rows_adj).  grid: (L / S, masks); shared: S B + 2 buffers.
+// ilt_rows_adj).  grid: (L / S, masks); shared: P (S B), two FFT buffers,
+// a second band buffer P2 (S B).
 template <int LG, int S>
 __global__ void __launch_bounds__(fr_threads(LG, S))
     ilt_cols_adj_xt(const float2* __restrict__ Tt, const float* __restrict__ G, int K, int hb, float keep,
@@ -205,11 +206,25 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
     for (int p = 0; p < R; ++p)
       g[b * R + p] = keep * Gm[static_cast<size_t>(j + p * (L / R)) * L + x0 + s] + add;
   }
-  for (int k = 0; k < K; ++k) {
+  // kernel k's band columns arrive by cp.async in P[k & 1] while kernel
+  // k - 1 is transformed
+  float2* P2 = b1 + fr_buf(L, S);
+  auto prefetch = [&](int k) {
     const float2* src = Tt + ((static_cast<size_t>(mask) * K + k) * L + x0) * B;
-    for (int e = t; e < S * B; e += T) P[e] = src[e];
+    float2* dst = (k & 1) ? P2 : P;
+    for (int e = t; e < S * B; e += T) fr_cp_async8(dst + e, src + e);
+    fr_cp_commit();
+  };
+  prefetch(0);
+  for (int k = 0; k < K; ++k) {
+    if (k + 1 < K) {
+      prefetch(k + 1);  // its buffer was last read before the previous iteration's final barrier
+      fr_cp_wait<1>();
+    } else {
+      fr_cp_wait<0>();
+    }
     __syncthreads();
-    fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
+    fr_first_pass_band<LG, S, +1>(t, (k & 1) ? P2 : P, B, hb, b0);
     __syncthreads();
     if constexpr (NP == 3) {
       fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
@@ -570,10 +585,10 @@ cudaError_t ilt_set_smem() {
   return cudaSuccess;
 }
 
-// Shared memory of ilt_cols_adj_xt: the band columns and two buffers.
+// Shared memory of ilt_cols_adj_xt: two band-column buffers and two FFT buffers.
 size_t ilt_adj_xt_smem(int lg, int hb) {
   const int S = huv_dev::xt_S(lg);
-  return (static_cast<size_t>(S) * (2 * hb + 1) + 2 * static_cast<size_t>(huv_dev::fr_buf(1 << lg, S))) *
+  return (2 * static_cast<size_t>(S) * (2 * hb + 1) + 2 * static_cast<size_t>(huv_dev::fr_buf(1 << lg, S))) *
          sizeof(float2);
 }
 }  // namespace huv_launch

@@ -258,17 +258,19 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
   float2* b0 = smem + S * B;
   float2* b1 = b0 + fr_buf(L, S);
   const float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
-  for (int e = t; e < S * B; e += T) {
-    const int s = e / B, mx = e - s * B;
-    float2 val = make_float2(0.f, 0.f);
+  // one warp per sequence: (k, my) once per row, lanes along mx (no divisions)
+  for (int s = t >> 5; s < S; s += T / 32) {
+    float2* Ps = P + s * B;
     if (s < nseq) {
       const int seq = seq0 + s;
       const int k = seq / B, my = seq - k * B;
-      const float2 m = Mc[static_cast<size_t>(my) * B + mx];
-      const float2 u = kband ? kband[(static_cast<size_t>(k) * B + my) * B + mx] : make_float2(scale, 0.f);
-      val = cmul(u, m);
+      const float2* mrow = Mc + static_cast<size_t>(my) * B;
+      const float2* urow = kband ? kband + (static_cast<size_t>(k) * B + my) * B : nullptr;
+      for (int mx = t & 31; mx < B; mx += 32)
+        Ps[mx] = cmul(urow ? urow[mx] : make_float2(scale, 0.f), mrow[mx]);
+    } else {
+      for (int mx = t & 31; mx < B; mx += 32) Ps[mx] = make_float2(0.f, 0.f);
     }
-    P[e] = val;
   }
   __syncthreads();
   fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
@@ -321,11 +323,28 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
     acc[i] = 0.f;
     res[i] = make_float2(0.f, 0.f);
   }
-  for (int k = 0; k < K; ++k) {
+  // MODE 0: kernel k's band columns (one contiguous block of S B values)
+  // arrive by cp.async in P[k & 1] while kernel k - 1 is transformed.
+  float2* P2 = b1 + fr_buf(L, S);  // second band buffer (MODE 0)
+  auto prefetch = [&](int k) {
     const float2* src = Tt + ((static_cast<size_t>(clip) * K + k) * L + x0) * B;
+    float2* dst = (k & 1) ? P2 : P;
+    for (int e = t; e < S * B; e += T) fr_cp_async8(dst + e, src + e);
+    fr_cp_commit();
+  };
+  if (MODE == 0) prefetch(0);
+  for (int k = 0; k < K; ++k) {
+    const float2* Pk = P;
     if (MODE == 0) {
-      for (int e = t; e < S * B; e += T) P[e] = src[e];
+      if (k + 1 < K) {
+        prefetch(k + 1);  // its buffer was last read before the previous iteration's final barrier
+        fr_cp_wait<1>();
+      } else {
+        fr_cp_wait<0>();
+      }
+      Pk = (k & 1) ? P2 : P;
     } else {
+      const float2* src = Tt + ((static_cast<size_t>(clip) * K + k) * L + x0) * B;
       for (int e = t; e < S * B; e += T) {
         const int s = e / B, my = e - s * B;
         const float2 a = src[static_cast<size_t>(2 * s) * B + my];
@@ -334,7 +353,7 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
       }
     }
     __syncthreads();
-    fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
+    fr_first_pass_band<LG, S, +1>(t, Pk, B, hb, b0);
     __syncthreads();
     const float2* cur = b0;
     if constexpr (NP == 3) {
@@ -523,23 +542,21 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   dim3 g1(n / rows_per_block, clips);
   const int th = pick_threads(S << (lg - 2));
   // u8 rasters take the exact integer tensor-core row band when the shape
-  // and the input's alignment allow it; f32 rasters the register-radix rows.
+  // and the input's alignment allow it; f32 rasters of 1024-point rows the
+  // register-radix rows (4 sequences per block read 32-byte row segments;
+  // with more, shorter rows per block the radix-4 kernel's coalesced loads
+  // win).
   cudaError_t rows_tc = cudaErrorNotSupported;
   if (kind == 0 && row_digits) {
     rows_tc = mask_rows_tc(in, n, hb, clips, X, row_digits, err, st);
     if (rows_tc != cudaSuccess && rows_tc != cudaErrorNotSupported) return rows_tc;
   }
-  if (kind == 1 && xt_ok(lg, hb)) {
+  if (kind == 1 && lg == 10 && xt_ok(lg, hb)) {
     const int Sr = xt_S(lg);
     const dim3 gr(static_cast<unsigned>(static_cast<size_t>(clips) * n / (2 * Sr)));
     const size_t smr = 2 * static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
     const float* fin = static_cast<const float*>(in);
-    switch (lg) {
-      case 7: band_rows_reg<7, 32><<<gr, 256, smr, st>>>(fin, hb, X, tw); break;
-      case 8: band_rows_reg<8, 16><<<gr, 256, smr, st>>>(fin, hb, X, tw); break;
-      case 9: band_rows_reg<9, 8><<<gr, 256, smr, st>>>(fin, hb, X, tw); break;
-      default: band_rows_reg<10, 4><<<gr, 256, smr, st>>>(fin, hb, X, tw); break;
-    }
+    band_rows_reg<10, 4><<<gr, 256, smr, st>>>(fin, hb, X, tw);
     rows_tc = cudaSuccess;
   }
   // Only device rasters come here (rectangle clips take the analytic path).
@@ -580,12 +597,14 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
 }
 
 // Whether the register-radix kernels (x-major band layout) apply to L = 2^lg
-// and band half-width hb: the larger band (the interpolation's 4 hb + 1
-// columns included) within their shared-memory budget.
+// and band half-width hb: every one of them within the shared-memory budget.
 bool xt_ok(int lg, int hb) {
   const int S = xt_S(lg);
   if (S == 0 || 2 * hb >= (1 << lg)) return false;
-  return static_cast<size_t>(S) * (2 * hb + 1) * sizeof(float2) + xt_buf_bytes(lg) <= static_cast<size_t>(kXtSmemMax);
+  // the largest user: the column pass with two band buffers and two FFT buffers
+  const size_t cols = 2 * static_cast<size_t>(S) * (2 * hb + 1) * sizeof(float2) +
+                      2 * static_cast<size_t>(fr_buf(1 << lg, S)) * sizeof(float2);
+  return cols <= static_cast<size_t>(kXtSmemMax);
 }
 
 // Rows of every (kernel, band row) product into T, x-major when xt_ok (the
@@ -612,7 +631,10 @@ cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, floa
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st) {
   if (!xt_ok(lgm, hb)) return socs_cols(T, K, hb, lgm, clips, keep, flare, mean, out, mode, tw, st);
   const int B = 2 * hb + 1, S = xt_S(lgm), L = 1 << lgm;
-  const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) + xt_buf_bytes(lgm);
+  // the column pass always places its second band buffer after two FFT
+  // buffers (mode 0 double-buffers the band columns)
+  const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) * (mode == 0 ? 2 : 1) +
+                    2 * static_cast<size_t>(fr_buf(L, S)) * sizeof(float2);
   const dim3 g(L / (mode == 0 ? S : 2 * S), clips);
 #define HUV_COLS_XT(LG, SS)                                                                                   \
   if (mode == 0)                                                                                            \
@@ -674,8 +696,7 @@ cudaError_t set_smem_limits() {
   HUV_XT_ATTR((socs_cols_xt<9, 8, 1>)) HUV_XT_ATTR((socs_cols_xt<10, 4, 1>))
   HUV_XT_ATTR((band_cols_reg<7, 32>)) HUV_XT_ATTR((band_cols_reg<8, 16>))
   HUV_XT_ATTR((band_cols_reg<9, 8>)) HUV_XT_ATTR((band_cols_reg<10, 4>))
-  HUV_XT_ATTR((band_rows_reg<7, 32>)) HUV_XT_ATTR((band_rows_reg<8, 16>))
-  HUV_XT_ATTR((band_rows_reg<9, 8>)) HUV_XT_ATTR((band_rows_reg<10, 4>))
+  HUV_XT_ATTR((band_rows_reg<10, 4>))
 #undef HUV_XT_ATTR
   return cudaSuccess;
 }

@@ -428,17 +428,19 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
   float2* b0 = smem + S * B;
   float2* b1 = b0 + fr_buf(L, S);
   const float2* Mc = Mband + static_cast<size_t>(prob) * B * B;
-  for (int e = t; e < S * B; e += T) {
-    const int s = e / B, mx = e - s * B;
-    float2 val = make_float2(0.f, 0.f);
+  // one warp per sequence: (k, my) once per row, lanes along mx (no divisions)
+  for (int s = t >> 5; s < S; s += T / 32) {
+    float2* Ps = P + s * B;
     if (s < nseq) {
       const int seq = seq0 + s;
       const int k = seq / nrows, my = row_off + (seq - k * nrows);
-      const float2 m = Mc[static_cast<size_t>(my) * B + mx];
-      const float2 u = kband ? kband[(static_cast<size_t>(k) * B + my) * B + mx] : make_float2(scale, 0.f);
-      val = cmul(u, m);
+      const float2* mrow = Mc + static_cast<size_t>(my) * B;
+      const float2* urow = kband ? kband + (static_cast<size_t>(k) * B + my) * B : nullptr;
+      for (int mx = t & 31; mx < B; mx += 32)
+        Ps[mx] = cmul(urow ? urow[mx] : make_float2(scale, 0.f), mrow[mx]);
+    } else {
+      for (int mx = t & 31; mx < B; mx += 32) Ps[mx] = make_float2(0.f, 0.f);
     }
-    P[e] = val;
   }
   __syncthreads();
   fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
@@ -462,9 +464,10 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
 #pragma unroll
     for (int p = 0; p < R; ++p) {
       const size_t x = static_cast<size_t>(j + p * (L / R));
-      __nv_bfloat162 hv, lv;
-      split_bf16(v[p].x, hv.x, lv.x);
-      split_bf16(v[p].y, hv.y, lv.y);
+      // (re, im) -> bf16x2 hi, then the packed residual as lo
+      const __nv_bfloat162 hv = __float22bfloat162_rn(v[p]);
+      const float2 hf = __bfloat1622float2(hv);
+      const __nv_bfloat162 lv = __float22bfloat162_rn(make_float2(v[p].x - hf.x, v[p].y - hf.y));
       *reinterpret_cast<__nv_bfloat162*>(hi + x * kp) = hv;
       *reinterpret_cast<__nv_bfloat162*>(hi + plane + x * kp) = lv;
     }
