@@ -437,6 +437,16 @@ def run_ours(args):
                         "region's mean launch time (CUDA events on the launching stream)",
                 "regions": {k: {"launches": v[0], "ms": v[1], "share": v[1] / total_ms if total_ms > 0 else None}
                             for k, v in prof["regions"].items()}}
+    gi = prof["regions"].get("tc_dft_gemm<interp>")
+    if gi and gi[1] > 0:
+        # the band interpolation on tensor cores: a real N x N x 2(2h2+1)
+        # GEMM per image (2 N^2 (2 (4h + 1)) FLOP, split products counted once)
+        kc = 2 * (4 * diag["band_half_width"] + 1)
+        flop_i = 2.0 * N_GRID * N_GRID * kc * N_CLIPS * args.steps
+        roofline["tensor_interp"] = {"kernel": "tc_dft_gemm<interp>", "achieved": flop_i / (gi[1] / 1e3) / 1e12,
+                                     "peak": tc_burst, "unit": "TFLOP/s",
+                                     "frac": flop_i / (gi[1] / 1e3) / 1e12 / tc_burst if tc_burst else None,
+                                     "issued_products_per_algorithmic": 3}
     g = prof["regions"].get("tc_dft_gemm<sumsq>")
     if g and g[1] > 0:
         # the |E|^2 contraction on tensor cores: 8 B M^2 K FLOP per image (complex MAC = 8,
@@ -471,7 +481,7 @@ def run_ours(args):
         # other device forms on the same batch (fewer steps), for the TC-vs-plain factor
         forms = {}
         for name, form, eg in (("fft_full_grid", "fft", N_GRID), ("fft_coarse_grid", "fft", 0), ("tc", "tc", 0),
-                               ("tc_gemm_rows", "tc_rows", 0)):
+                               ("tc_gemm_rows", "tc_rows", 0), ("hybrid", "hybrid", 0)):
             try:
                 step(form, eg)
                 torch.cuda.synchronize()
@@ -507,6 +517,9 @@ def run_ours(args):
         if "images_per_s" in forms.get("tc", {}) and "images_per_s" in forms.get("fft_coarse_grid", {}):
             forms["tc_over_fft_coarse_grid"] = forms["tc"]["images_per_s"] / forms["fft_coarse_grid"]["images_per_s"]
             forms["tc_over_fft_full_grid"] = forms["tc"]["images_per_s"] / forms["fft_full_grid"]["images_per_s"]
+        if "images_per_s" in forms.get("hybrid", {}) and "images_per_s" in forms.get("fft_coarse_grid", {}):
+            forms["hybrid_over_fft_coarse_grid"] = (forms["hybrid"]["images_per_s"]
+                                                    / forms["fft_coarse_grid"]["images_per_s"])
         extra["forms"] = forms
         extra["ilt"] = ilt_leg(eng, stream)
         extra["uneven_batch"] = uneven_leg(stream, n_clips=args.uneven_clips)
@@ -556,7 +569,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="auto", choices=["auto", "fft", "tc", "tc_rows"])
+    ap.add_argument("--form", default="auto", choices=["auto", "fft", "tc", "tc_rows", "hybrid"])
     ap.add_argument("--eval-grid", dest="eval_grid", type=int, default=0)
     ap.add_argument("--quick", action="store_true", help="skip the extra forms, accuracy and CPU baseline")
     ap.add_argument("--uneven-clips", dest="uneven_clips", type=int, default=2048)

@@ -21,7 +21,7 @@ STATUS_NAMES = {
 FILL = {"conventional": 0, "annular": 1, "quadrupole": 2, "dipole": 3, "gaussian": 4, "quasar": 5}
 OPTICS_PROJECTION, OPTICS_EUV = 0, 1
 INPUT_U8, INPUT_F32, INPUT_C64, INPUT_RECTS = 0, 1, 2, 3
-FORM = {"auto": 0, "fft": 1, "tc": 2, "tc_rows": 3}
+FORM = {"auto": 0, "fft": 1, "tc": 2, "tc_rows": 3, "hybrid": 4}
 
 
 class HuvError(RuntimeError):

@@ -86,7 +86,7 @@ extern "C" huv_status huv_image_batch_noalloc(void* engine, const huv_batch* bat
     }
     if (!b.input || !out) throw huv::Error(HUV_ERR_INVALID_PARAMETER, "input/out: null pointer");
     if (b.input_kind < 0 || b.input_kind > 2) throw huv::Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
-    if (b.form == HUV_FORM_TC)
+    if (b.form != HUV_FORM_AUTO && b.form != HUV_FORM_FFT)
       throw huv::Error(HUV_ERR_UNSUPPORTED, "the allocation-free path runs the FP32 FFT form only");
     if (!std::isfinite(b.defocus_nm)) throw huv::Error(HUV_ERR_INVALID_PARAMETER, "defocus_nm: must be finite");
     cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -528,6 +528,10 @@ using namespace huv_dev;
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
                          const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
                          const uint8_t* row_digits, int* err);
+cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+                        float2* T, const float2* tw, cudaStream_t st);
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+                        const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 
 namespace {
 
@@ -692,7 +696,8 @@ bool Engine::tc_supported(const DeviceSet& ds, int M) const {
 }
 
 void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use,
-                         const float* W_use, bool gemm_rows) {
+                         const float* W_use, int core) {
+  const bool gemm_rows = core == kTcCoreGemmRows, fft_field = core == kTcCoreFftField;
   using namespace huv_launch;
   static bool smem_set = false;
   if (!smem_set) {
@@ -798,8 +803,21 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
         !make_map(&mbI, BI, static_cast<uint64_t>(nc) * 2 * n, kbI, kTcBN, kcI) ||
         (gemm_rows && !make_map(&mbP, P, static_cast<uint64_t>(nc) * K * 2 * rbn, kpE, rbn)))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the band operands");
-    prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
-    if (!gemm_rows) {
+    if (fft_field) {
+      // FP32 register-radix field pass: rows x-major into the operand
+      // buffer (K B M complex fits in its K 2 M kbE bf16), columns with
+      // sum lambda |E|^2 in registers, normalisation and flare -> IM
+      float2* T = reinterpret_cast<float2*>(BE);
+      prof.begin("socs_rows_inv", st);
+      check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");
+      prof.end(st);
+      prof.begin("socs_cols_inv", st);
+      check_cuda(socs_cols_x(T, K, hb, lgm, nc, ds.keep, ds.flare, mean, IM, 0, twm, st), "socs_cols");
+      prof.end(st);
+    }
+    if (!fft_field) prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
+    if (fft_field) {
+    } else if (!gemm_rows) {
       // Row transforms as FP32 register-radix FFTs, emitting the split operand.
       launch_rows(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, kbE, 0, BE, twm, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc");
@@ -832,8 +850,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
             <<<g, 192, tc_smem_bytes(3, kRowBNWide, true), st>>>(tc.map_ae, mbP, tc.map_ae, p);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<2>");
     }
-    prof.end(st);
-    {
+    if (!fft_field) prof.end(st);
+    if (!fft_field) {
       TcGemmParams p{};
       p.kboxes = kpE / 64;
       p.ksteps = kstE;

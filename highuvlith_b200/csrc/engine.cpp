@@ -510,10 +510,11 @@ void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
   // chosen grid below that is raised to 128 (still exact: any M > 4h is).
   const int Mtc = (b.eval_grid == 0 && M < 128 && n >= 128) ? 128 : M;
   int form = b.form;
-  if (form == HUV_FORM_AUTO) form = tc_supported(ds, Mtc) ? HUV_FORM_TC : HUV_FORM_FFT;
-  if (form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS) {
+  if (form == HUV_FORM_AUTO) form = tc_supported(ds, Mtc) ? HUV_FORM_HYBRID : HUV_FORM_FFT;
+  if (form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS || form == HUV_FORM_HYBRID) {
     if (!tc_supported(ds, Mtc)) throw Error(HUV_ERR_UNSUPPORTED, "TC form: unsupported band/grid for this build");
-    run_tc_form(b, ds, Mtc, out, st, 0, nullptr, form == HUV_FORM_TC_ROWS);
+    run_tc_form(b, ds, Mtc, out, st, 0, nullptr,
+                form == HUV_FORM_TC_ROWS ? kTcCoreGemmRows : (form == HUV_FORM_HYBRID ? kTcCoreFftField : kTcCoreFftRows));
   } else if (form == HUV_FORM_FFT) {
     run_fft_form(b, ds, M, out, st);
   } else {

@@ -22,6 +22,13 @@ void check_cuda(cudaError_t e, const char* what);
 // Device-side state of the tensor-core form for one kernel set: the split
 // BF16 DFT operands (A_E over the evaluation grid, A_I for the interpolation
 // to the output grid) and their TMA descriptors.
+// How the tensor-core form evaluates sum lambda |E|^2 on the evaluation
+// grid before its tcgen05 band interpolation: FP32 FFT row transforms into
+// the split operand + the tcgen05 y-contraction (HUV_FORM_TC), both on
+// tcgen05 (HUV_FORM_TC_ROWS), or the FP32 register-radix FFT field pass
+// (HUV_FORM_HYBRID).
+constexpr int kTcCoreFftRows = 0, kTcCoreGemmRows = 1, kTcCoreFftField = 2;
+
 struct TcState {
   int lgm = 0;          // evaluation grid the state was built for (log2)
   void* gy = nullptr;   // A_E planes [2][2M][kpE] bf16
@@ -165,7 +172,7 @@ struct Engine {
   void run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use = 0,
                     const float* W_use = nullptr);
   void run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use = 0,
-                   const float* W_use = nullptr, bool gemm_rows = false);
+                   const float* W_use = nullptr, int core = kTcCoreFftRows);
   // Flare weights W = sum_{k < K} lambda_k |u_k|^2 / N^4 of the first K kernels (device, cached).
   const float* flare_weights(DeviceSet& ds, int K);
   // Kernel count for a budget of `max_kernels` under the reference's truncation rule.

@@ -101,6 +101,8 @@ struct Plan {
     DeviceSet& ds = g.e->device_set(0.0);
     if (c.form == HUV_FORM_TC)
       g.e->run_tc_form(b, ds, c.M, out, st, g.K, g.W);
+    else if (c.form == HUV_FORM_HYBRID)
+      g.e->run_tc_form(b, ds, c.M, out, st, g.K, g.W, kTcCoreFftField);
     else
       g.e->run_fft_form(b, ds, c.M, out, st, g.K, g.W);
     if (!g.contiguous)
@@ -120,7 +122,10 @@ std::vector<Choice> candidates(Engine* e, DeviceSet& ds) {
   while (m < 4 * ds.hb + 1) m <<= 1;
   m = std::min(m, n);
   const int mtc = std::max(m, 128);
-  if (mtc <= n && e->tc_supported(ds, mtc)) out.push_back(Choice{HUV_FORM_TC, mtc, 0});
+  if (mtc <= n && e->tc_supported(ds, mtc)) {
+    out.push_back(Choice{HUV_FORM_TC, mtc, 0});
+    out.push_back(Choice{HUV_FORM_HYBRID, mtc, 0});
+  }
   out.push_back(Choice{HUV_FORM_FFT, m, 0});
   if (2 * m <= n && m < n) out.push_back(Choice{HUV_FORM_FFT, 2 * m, 0});
   if (m < n && out.size() < 4) out.push_back(Choice{HUV_FORM_FFT, n, 0});
@@ -247,7 +252,7 @@ huv_status huv_plan_create(const huv_clip* clips, int32_t n_clips, int32_t pixel
         huv::g_tuned[key] = g.choice;
       }
       rep << (gi ? "," : "") << "{\"n\":" << g.n << ",\"h\":" << g.h << ",\"K\":" << g.K << ",\"clips\":"
-          << g.clips.size() << ",\"form\":\"" << (g.choice.form == HUV_FORM_TC ? "tc" : "fft") << "\",\"eval_grid\":"
+          << g.clips.size() << ",\"form\":\"" << (g.choice.form == HUV_FORM_TC ? "tc" : (g.choice.form == HUV_FORM_HYBRID ? "hybrid" : "fft")) << "\",\"eval_grid\":"
           << g.choice.M << ",\"ms_per_clip\":" << g.choice.ms_per_clip << ",\"contiguous\":" << (g.contiguous ? 1 : 0)
           << "}";
     }

@@ -181,12 +181,13 @@ def test_c2_clips_full_size_parity_and_cd():
 TC_CASES = [c for c in SMALL if c[3].size >= 128]
 
 
-@pytest.mark.parametrize("form", ["tc", "tc_rows"])
+@pytest.mark.parametrize("form", ["tc", "tc_rows", "hybrid"])
 @pytest.mark.parametrize("case", TC_CASES, ids=[c[0] for c in TC_CASES])
 def test_tc_form_matches_oracle(case, form):
     """Split-BF16x3 tcgen05 form vs the FP64 oracle (tolerance 1e-3; the
     split products carry ~2^-16 relative precision); row transforms as FFTs
-    ("tc") or as tensor-core DFT-GEMMs too ("tc_rows")."""
+    ("tc"), as tensor-core DFT-GEMMs too ("tc_rows"), or the FP32 FFT field
+    pass with only the band interpolation on tensor cores ("hybrid")."""
     torch = _torch()
     _, src, opt, grid, kmax, fill, oopt = case
     eng = HB.SimulationEngine(src, opt, grid=grid, max_kernels=kmax)
@@ -212,10 +213,12 @@ def test_tc_form_c2_full_size():
     out = eng.compute_batch(d, form="tc").cpu().numpy()
     eng.device_status()
     fft = eng.compute_batch(d, form="fft").cpu().numpy()
+    hyb = eng.compute_batch(d).cpu().numpy()  # auto: the hybrid form
     x = grid.pixel_centres()
     for c in range(3):
         ref = oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[c]))
         assert rel_err(out[c], ref) < REL_TOL
         assert rel_err(out[c], fft[c]) < REL_TOL
+        assert rel_err(hyb[c], ref) < 1e-4, rel_err(hyb[c], ref)
     worst, unmatched = M.max_edge_error(out[0], oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[0])), x, 0.3)
     assert unmatched == 0 and worst < CD_TOL_NM, (worst, unmatched)

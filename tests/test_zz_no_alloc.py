@@ -21,9 +21,9 @@ from highuvlith_b200.clips import gen_batch
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(eng, rasters, out, eval_grid=0):
+def _noalloc(eng, rasters, out, eval_grid=0, form="fft"):
     import torch
-    b = L.Batch(rasters.shape[0], L.INPUT_U8, rasters.data_ptr(), 1, 0.0, L.FORM["fft"], eval_grid)
+    b = L.Batch(rasters.shape[0], L.INPUT_U8, rasters.data_ptr(), 1, 0.0, L.FORM[form], eval_grid)
     st = torch.cuda.current_stream().cuda_stream
     return L.lib().huv_image_batch_noalloc(eng.handle, C.byref(b), out.data_ptr(), st)
 
@@ -54,3 +54,14 @@ def test_noalloc_rejects_clips_beyond_its_scratch():
     status = _noalloc(eng, d, out, eval_grid=4096)
     assert status == 1
     assert b"fixed maximum of 32 MiB" in L.lib().huv_last_error()
+
+
+def test_noalloc_rejects_tensor_core_forms():
+    import torch
+    eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(), grid=HB.GridConfig(256, 1.0),
+                              max_kernels=8)
+    d = torch.zeros((1, 256, 256), dtype=torch.uint8, device="cuda")
+    out = torch.empty((1, 256, 256), dtype=torch.float32, device="cuda")
+    for form in ("tc", "tc_rows", "hybrid"):
+        assert _noalloc(eng, d, out, form=form) != 0
+        assert b"FP32 FFT form only" in L.lib().huv_last_error()
