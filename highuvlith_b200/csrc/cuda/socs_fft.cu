@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
 // is Hermitian in my, so Re and Im of the transform are the two real
 // columns.  grid: (L / (S or 2 S), clips); out: [clip][L][L].
 template <int LG, int S, int MODE>
-__global__ void __launch_bounds__(fr_threads(LG, S))
+__global__ void __launch_bounds__(fr_threads(LG, S), MODE == 0 ? 3 : 2)
     socs_cols_xt(const float2* __restrict__ Tt, int K, int hb, float keep, float flare,
                  const float* __restrict__ mean, float* __restrict__ out, const float2* __restrict__ tw) {
   constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
   }
   // MODE 0: kernel k's band columns (one contiguous block of S B values)
   // arrive by cp.async in P[k & 1] while kernel k - 1 is transformed.
-  float2* P2 = b1 + fr_buf(L, S);  // second band buffer (MODE 0)
+  float2* P2 = b0 + (NP - 1) * fr_buf(L, S);  // second band buffer (MODE 0), after the FFT buffers used
   auto prefetch = [&](int k) {
     const float2* src = Tt + ((static_cast<size_t>(clip) * K + k) * L + x0) * B;
     float2* dst = (k & 1) ? P2 : P;
@@ -631,10 +631,9 @@ cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, floa
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st) {
   if (!xt_ok(lgm, hb)) return socs_cols(T, K, hb, lgm, clips, keep, flare, mean, out, mode, tw, st);
   const int B = 2 * hb + 1, S = xt_S(lgm), L = 1 << lgm;
-  // the column pass always places its second band buffer after two FFT
-  // buffers (mode 0 double-buffers the band columns)
+  // band columns (mode 0: double-buffered) and the FFT buffers the passes use
   const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) * (mode == 0 ? 2 : 1) +
-                    2 * static_cast<size_t>(fr_buf(L, S)) * sizeof(float2);
+                    (fr_passes(lgm) - 1) * static_cast<size_t>(fr_buf(L, S)) * sizeof(float2);
   const dim3 g(L / (mode == 0 ? S : 2 * S), clips);
 #define HUV_COLS_XT(LG, SS)                                                                                   \
   if (mode == 0)                                                                                            \
