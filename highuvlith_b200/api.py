@@ -265,6 +265,11 @@ class SimulationEngine:
         device.  ``pixel_transfer=True`` gives ``compute(mask)`` of the
         pixel-aligned mask the raster depicts (Mask::spectrum, mask.rs:616-657);
         ``False`` gives ``compute_from_transmittance`` (aerial.rs:1789-1798).
+        ``form``: "fft" (FP32 register-radix FFTs throughout), "tc" (split-BF16x3
+        tcgen05 y-contraction and band interpolation), "tc_rows" (row
+        transforms on tcgen05 too), "hybrid" (FP32 FFT field pass, tcgen05
+        band interpolation) or "auto" (hybrid where the tensor-core form
+        applies, else fft).
         Returns a float32 (B, N, N) tensor (``out`` if given)."""
         import torch
         n = self.grid.size
