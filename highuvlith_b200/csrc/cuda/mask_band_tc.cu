@@ -47,10 +47,11 @@ __host__ __device__ constexpr size_t mb_smem_bytes(int N) {
   return 1024 + kMbStages * static_cast<size_t>(mb_stage_bytes(N)) + 256;
 }
 
-// grid: (rows / 128); rows = clips * L, X: [rows][2 hb + 1].
+// grid: (rows / 128); rows = clips * L.  X: [rows][2 hb + 1], or with
+// `transposed` [clip][2 hb + 1][L] (each order's column contiguous in y).
 __global__ void __launch_bounds__(192, 1)
     band_rows_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmD, int kboxes,
-                 int N, int hb, uint32_t tmem_cols, float2* __restrict__ X, int* err) {
+                 int N, int hb, uint32_t tmem_cols, int L, int transposed, float2* __restrict__ X, int* err) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
@@ -169,13 +170,26 @@ __global__ void __launch_bounds__(192, 1)
       }
       __syncwarp();
       const int B = 2 * hb + 1;
-      float2* out = X + static_cast<size_t>(row0 + quad * 32) * B;
-      for (int w = lane; w < 32 * B; w += 32) {
-        const int r = w / B, mi = w - r * B;
-        const int m = mi - hb, am = m < 0 ? -m : m;
-        const float c = stage[r * ld + 1 + am];
-        const float s = am ? stage[r * ld + hb + 1 + am] : 0.f;
-        out[w] = make_float2(c, m >= 0 ? -s : s);
+      if (transposed) {
+        // one order per store: 32 consecutive y of one column (256 bytes)
+        const int grow = row0 + quad * 32;
+        const int clip = grow / L, y0 = grow - clip * L;
+        float2* out = X + static_cast<size_t>(clip) * B * L + y0 + lane;
+        for (int mi = 0; mi < B; ++mi) {
+          const int m = mi - hb, am = m < 0 ? -m : m;
+          const float c = stage[lane * ld + 1 + am];
+          const float s = am ? stage[lane * ld + hb + 1 + am] : 0.f;
+          out[static_cast<size_t>(mi) * L] = make_float2(c, m >= 0 ? -s : s);
+        }
+      } else {
+        float2* out = X + static_cast<size_t>(row0 + quad * 32) * B;
+        for (int w = lane; w < 32 * B; w += 32) {
+          const int r = w / B, mi = w - r * B;
+          const int m = mi - hb, am = m < 0 ? -m : m;
+          const float c = stage[r * ld + 1 + am];
+          const float s = am ? stage[r * ld + hb + 1 + am] : 0.f;
+          out[w] = make_float2(c, m >= 0 ? -s : s);
+        }
       }
     }
   }
@@ -257,12 +271,13 @@ std::vector<uint8_t> mask_rows_tc_digits(int n, int hb) {
   return tab;
 }
 
-// X[clip][y][m + hb] for u8 rasters [clips][n][n] on the tensor cores.
-// `digits` is mask_rows_tc_digits(n, hb) on the device.  Returns
-// cudaErrorNotSupported when the shape or the input's alignment rules the
-// path out (the caller then takes the FFT path).
+// X[clip][y][m + hb] (or, with `transposed`, X[clip][m + hb][y]) for u8
+// rasters [clips][n][n] on the tensor cores.  `digits` is
+// mask_rows_tc_digits(n, hb) on the device.  Returns cudaErrorNotSupported
+// when the shape or the input's alignment rules the path out (the caller
+// then takes the FFT path).
 cudaError_t mask_rows_tc(const void* in, int n, int hb, int clips, float2* X, const uint8_t* digits, int* err,
-                         cudaStream_t st) {
+                         cudaStream_t st, bool transposed) {
   if (!digits || !mask_rows_tc_supported(n, hb) || (reinterpret_cast<uintptr_t>(in) & 15u) != 0)
     return cudaErrorNotSupported;
   const int N = mask_rows_tc_cols(hb);
@@ -283,7 +298,7 @@ cudaError_t mask_rows_tc(const void* in, int n, int hb, int clips, float2* X, co
   const uint32_t cols = 3 * N <= 256 ? 256u : 512u;
   size_t smem = mb_smem_bytes(N);
   if (cols == 512u && smem < (120u << 10)) smem = 120u << 10;
-  band_rows_i8<<<clips * n / 128, 192, smem, st>>>(ma, md, n / 128, N, hb, cols, X, err);
+  band_rows_i8<<<clips * n / 128, 192, smem, st>>>(ma, md, n / 128, N, hb, cols, n, transposed ? 1 : 0, X, err);
   return cudaGetLastError();
 }
 

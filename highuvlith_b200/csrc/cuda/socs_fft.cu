@@ -441,11 +441,11 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
 }
 
 // band_cols_fwd with register-radix passes: forward FFT along y of S band
-// columns of X[clip][y][B] per block, the first pass reading X directly.
-// grid: (ceil(B / S), clips).
+// columns of X[clip][y][B] (or of X[clip][B][y] with `transposed`) per block,
+// the first pass reading X directly.  grid: (ceil(B / S), clips).
 template <int LG, int S>
 __global__ void __launch_bounds__(fr_threads(LG, S))
-    band_cols_reg(const float2* __restrict__ X, int hb, const float* __restrict__ ptx,
+    band_cols_reg(const float2* __restrict__ X, bool transposed, int hb, const float* __restrict__ ptx,
                   const float* __restrict__ W, float2* __restrict__ Mband, float* __restrict__ parts,
                   const float2* __restrict__ tw) {
   constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
@@ -463,9 +463,11 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
     const int s = t % S, j = t / S;
     const bool live = c0 + s < B;
     float2 v[16];
+    const size_t col_base = transposed ? static_cast<size_t>(c0 + s) * L : static_cast<size_t>(c0 + s);
+    const size_t row_step = transposed ? 1 : static_cast<size_t>(B);
 #pragma unroll
     for (int r = 0; r < 16; ++r)
-      v[r] = live ? Xc[static_cast<size_t>(j + r * (L / 16)) * B + c0 + s] : make_float2(0.f, 0.f);
+      v[r] = live ? Xc[col_base + static_cast<size_t>(j + r * (L / 16)) * row_step] : make_float2(0.f, 0.f);
     fr_first_pass_vals<LG, S, -1>(t, v, b0);
   }
   __syncthreads();
@@ -521,7 +523,7 @@ using namespace huv_dev;
 static int pick_threads(int work) { return work >= 256 ? 256 : 128; }
 
 cudaError_t mask_rows_tc(const void* in, int n, int hb, int clips, float2* X, const uint8_t* digits, int* err,
-                         cudaStream_t st);
+                         cudaStream_t st, bool transposed);
 bool xt_ok(int lg, int hb);
 cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
                       float2* T, const float2* tw, cudaStream_t st);
@@ -547,8 +549,13 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   // with more, shorter rows per block the radix-4 kernel's coalesced loads
   // win).
   cudaError_t rows_tc = cudaErrorNotSupported;
+  // the register-radix columns read a transposed row band ([clip][m][y]) when
+  // the tensor-core rows produce it
+  const bool cols_reg = xt_ok(lg, hb);
+  bool x_transposed = false;
   if (kind == 0 && row_digits) {
-    rows_tc = mask_rows_tc(in, n, hb, clips, X, row_digits, err, st);
+    rows_tc = mask_rows_tc(in, n, hb, clips, X, row_digits, err, st, cols_reg);
+    x_transposed = rows_tc == cudaSuccess && cols_reg;
     if (rows_tc != cudaSuccess && rows_tc != cudaErrorNotSupported) return rows_tc;
   }
   if (kind == 1 && lg == 10 && xt_ok(lg, hb)) {
@@ -573,7 +580,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   const int B = 2 * hb + 1;
   float* parts = (W && mean) ? mean + clips : nullptr;
   int nblk;
-  if (xt_ok(lg, hb)) {
+  if (cols_reg) {
     // register-radix columns: S <= 4 ... 32 columns per block, at most
     // ceil(B / 4) parts per clip as the callers size them
     const int S = xt_S(lg);
@@ -581,10 +588,10 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     const dim3 g(nblk, clips);
     const size_t sm = xt_buf_bytes(lg);
     switch (lg) {
-      case 7: band_cols_reg<7, 32><<<g, 256, sm, st>>>(X, hb, ptx, W, Mband, parts, tw); break;
-      case 8: band_cols_reg<8, 16><<<g, 256, sm, st>>>(X, hb, ptx, W, Mband, parts, tw); break;
-      case 9: band_cols_reg<9, 8><<<g, 256, sm, st>>>(X, hb, ptx, W, Mband, parts, tw); break;
-      default: band_cols_reg<10, 4><<<g, 256, sm, st>>>(X, hb, ptx, W, Mband, parts, tw); break;
+      case 7: band_cols_reg<7, 32><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 8: band_cols_reg<8, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 9: band_cols_reg<9, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      default: band_cols_reg<10, 4><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
     }
   } else {
     const int cpb = fit_units(4, 2 * (sizeof(float2) << lg));
