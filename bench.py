@@ -249,10 +249,26 @@ def ilt_leg(eng, stream, masks=64, iterations=3):
     eng.profile(False)
     launches, dev_total = prof["regions"]["ilt_cost_grad"]
     g_ms = dev_total / launches
+    ilt.optimize(eng, theta.clone(), tg, ilt.IltSettings(cost="resist", threshold=0.25, steepness=50.0,
+                                                         max_iterations=1))  # warm-up: optimizer kernels
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     res = ilt.optimize(eng, theta, tg, st)
     opt_s = time.perf_counter() - t0
-    return {"workload": f"{masks} contact-array targets 1024^2, K=31, resist 0.25/50, FP32",
+    # the full C4 run: every mask optimised concurrently for 50 iterations
+    st50 = ilt.IltSettings(cost="resist", threshold=0.25, steepness=50.0, max_iterations=50)
+    th50 = (tg - 0.5).contiguous()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res50 = ilt.optimize(eng, th50, tg, st50)
+    torch.cuda.synchronize()
+    c4_s = time.perf_counter() - t0
+    c4 = {"iterations": 50, "wall_s": c4_s, "masks": masks,
+          "mask_iterations_per_s": masks * float(np.mean(res50["iterations"])) / c4_s,
+          "mean_iterations_run": float(np.mean(res50["iterations"])),
+          "mean_cost_start": float(np.mean(res50["cost_history"][:, 0])),
+          "mean_cost_end": float(np.mean(res50["final_cost"]))}
+    return {"workload": f"{masks} contact-array targets 1024^2, K=31, resist 0.25/50, FP32", "c4_full_run": c4,
             "gradient_evals_per_s": masks / (g_ms / 1e3), "ms_per_batched_gradient": g_ms,
             "timing": "device: CUDA events around each batched evaluation on its stream, mean of 5",
             "wall_ms_per_call": wall_ms, "wall_gradient_evals_per_s": masks / (wall_ms / 1e3),
