@@ -236,4 +236,42 @@ __host__ __device__ __forceinline__ void fr_last_pass(int u, const float2* src, 
   fr_dft<R, DIR>(v);
 }
 
+// The last pass's twiddles of thread t (for each of its 16 / R butterflies,
+// w^{r j} for r = 1 .. R - 1, direction applied): they depend only on t, so
+// kernels that run the same transform shape many times load them once.
+template <int LG, int S, int DIR>
+__host__ __device__ __forceinline__ void fr_last_twiddles(
+    int t, const float2* tw,
+    float2 (&w)[16 / fr_radix(LG, fr_passes(LG) - 1)][fr_radix(LG, fr_passes(LG) - 1) - 1]) {
+  constexpr int P = fr_passes(LG) - 1;
+  constexpr int R = fr_radix(LG, P), T = fr_threads(LG, S);
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    const int j = (t + b * T) / S;
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      float2 x = tw[r * j];
+      if (DIR > 0) x.y = -x.y;
+      w[b][r - 1] = x;
+    }
+  }
+}
+
+// fr_last_pass with the twiddles of butterfly b preloaded (fr_last_twiddles).
+template <int LG, int S, int DIR>
+__host__ __device__ __forceinline__ void fr_last_pass_pre(int u, const float2* src,
+                                                          const float2 (&w)[fr_radix(LG, fr_passes(LG) - 1) - 1],
+                                                          int& s, int& j,
+                                                          float2 (&v)[fr_radix(LG, fr_passes(LG) - 1)]) {
+  constexpr int L = 1 << LG;
+  constexpr int R = fr_radix(LG, fr_passes(LG) - 1);
+  s = u % S;
+  j = u / S;
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = src[fr_idx<S>(j + r * (L / R), s)];
+#pragma unroll
+  for (int r = 1; r < R; ++r) v[r] = fr_mul(v[r], w[r - 1]);
+  fr_dft<R, DIR>(v);
+}
+
 }  // namespace huv_dev

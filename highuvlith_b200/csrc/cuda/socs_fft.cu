@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
 // is Hermitian in my, so Re and Im of the transform are the two real
 // columns.  grid: (L / (S or 2 S), clips); out: [clip][L][L].
 template <int LG, int S, int MODE>
-__global__ void __launch_bounds__(fr_threads(LG, S), MODE == 0 ? 3 : 2)
+__global__ void __launch_bounds__(fr_threads(LG, S), 2)
     socs_cols_xt(const float2* __restrict__ Tt, int K, int hb, float keep, float flare,
                  const float* __restrict__ mean, float* __restrict__ out, const float2* __restrict__ tw) {
   constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
@@ -333,6 +333,8 @@ __global__ void __launch_bounds__(fr_threads(LG, S), MODE == 0 ? 3 : 2)
     fr_cp_commit();
   };
   if (MODE == 0) prefetch(0);
+  float2 lw[16 / R][R - 1];  // last-pass twiddles, the same for every kernel
+  fr_last_twiddles<LG, S, +1>(t, tw, lw);
   for (int k = 0; k < K; ++k) {
     const float2* Pk = P;
     if (MODE == 0) {
@@ -365,7 +367,7 @@ __global__ void __launch_bounds__(fr_threads(LG, S), MODE == 0 ? 3 : 2)
     for (int b = 0; b < 16 / R; ++b) {
       int s, j;
       float2 v[R];
-      fr_last_pass<LG, S, +1>(t + b * T, cur, tw, s, j, v);
+      fr_last_pass_pre<LG, S, +1>(t + b * T, cur, lw[b], s, j, v);
 #pragma unroll
       for (int p = 0; p < R; ++p) {
         if (MODE == 0)
