@@ -369,26 +369,27 @@ __global__ void ilt_finish(const float* __restrict__ theta, const float* __restr
   if (threadIdx.x == 0) parts[static_cast<size_t>(mask) * gridDim.x + blockIdx.x] = c;
 }
 
-// The same as ilt_finish for grids that are multiples of 32: a block takes a
-// 32 x 32 tile, computes m = sigmoid(beta theta) once for the tile and its
+// The same as ilt_finish for grids that are multiples of TS: a block takes a
+// TS x TS tile, computes m = sigmoid(beta theta) once for the tile and its
 // 1-pixel periodic halo in shared memory (instead of up to nine sigmoids per
 // pixel), and writes its share of the regulariser cost to parts[mask][tile].
-// grid: ((n / 32)^2, masks), block 256.
+// grid: ((n / TS)^2, masks), block 256.
+template <int TS>
 __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict__ theta,
                                                          const float* __restrict__ dcdm, int n, float beta,
                                                          float tv_w, float tv_eps, float bin_w,
                                                          float* __restrict__ grad, double* __restrict__ parts) {
-  __shared__ float sm[34][35];
+  __shared__ float sm[TS + 2][TS + 3];
   __shared__ double red[32];
   const int mask = blockIdx.y;
   const size_t npix = static_cast<size_t>(n) * n;
-  const int tiles_x = n >> 5;
+  const int tiles_x = n / TS;
   const int ti = blockIdx.x / tiles_x, tj = blockIdx.x - ti * tiles_x;
   const float* th = theta + mask * npix;
   const float inv_n = 1.f / static_cast<float>(npix);
-  for (int e = threadIdx.x; e < 34 * 34; e += blockDim.x) {
-    const int r = e / 34, c = e - r * 34;
-    int i = ti * 32 - 1 + r, j = tj * 32 - 1 + c;
+  for (int e = threadIdx.x; e < (TS + 2) * (TS + 2); e += blockDim.x) {
+    const int r = e / (TS + 2), c = e - r * (TS + 2);
+    int i = ti * TS - 1 + r, j = tj * TS - 1 + c;
     i = i < 0 ? i + n : (i >= n ? i - n : i);
     j = j < 0 ? j + n : (j >= n ? j - n : j);
     sm[r][c] = 1.f / (1.f + __expf(-beta * th[static_cast<size_t>(i) * n + j]));
@@ -397,9 +398,9 @@ __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict_
   // per-thread partials of the 4 pixels in FP32, the block sum in FP64
   float tv_part = 0.f, bin_part = 0.f;
   const float eps2 = tv_eps * tv_eps;
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < TS * TS / 256; ++q) {
     const int pidx = threadIdx.x + 256 * q;
-    const int r = (pidx >> 5) + 1, c = (pidx & 31) + 1;
+    const int r = pidx / TS + 1, c = pidx % TS + 1;
     const float m = sm[r][c];
     float g = 0.f;
     if (tv_w > 0.f) {
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict_
       g += bin_w * 4.f * (1.f - 2.f * m) * inv_n;
     }
     if (grad) {
-      const size_t gp = mask * npix + static_cast<size_t>(ti * 32 + r - 1) * n + tj * 32 + c - 1;
+      const size_t gp = mask * npix + static_cast<size_t>(ti * TS + r - 1) * n + tj * TS + c - 1;
       grad[gp] = ((dcdm ? dcdm[gp] : 0.f) + g) * beta * m * (1.f - m);
     }
   }
@@ -652,8 +653,11 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   const size_t s_q = grad ? a256(sizeof(float2) * B * B) : 0;
   const size_t s_t2 = grad ? a256(sizeof(float2) * static_cast<size_t>(B) * n) : 0;
   const size_t s_parts = a256(sizeof(double) * kRedBlocks * 2);
-  const bool tiled = n % 32 == 0;
-  const int reg_parts = tiled ? (n / 32) * (n / 32) : kRedBlocks;
+  // 64 x 64 regulariser tiles where the grid allows (fewer, longer blocks),
+  // else 32 x 32, else the untiled kernel
+  const int tile = n % 64 == 0 ? 64 : (n % 32 == 0 ? 32 : 0);
+  const bool tiled = tile > 0;
+  const int reg_parts = tiled ? (n / tile) * (n / tile) : kRedBlocks;
   const size_t s_preg = a256(sizeof(double) * std::max(reg_parts, 2 * kRedBlocks));
   const size_t per = s_t + s_x + s_m + s_mean + s_T + s_im + s_c + s_x2 + s_img + s_V + s_q + s_t2 + 2 * s_parts +
                      s_preg + a256(sizeof(double) * 4);
@@ -758,8 +762,13 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
       dcdm = tbuf;  // the transmittance is no longer needed
       check_cuda(socs_cols_x(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, twn, st), "ilt grad cols");
     }
-    if (tiled)
-      ilt_finish_tiled<<<dim3(reg_parts, nc), 256, 0, st>>>(
+    if (tile == 64)
+      ilt_finish_tiled<64><<<dim3(reg_parts, nc), 256, 0, st>>>(
+          th, dcdm, n, static_cast<float>(p.beta), static_cast<float>(p.tv_weight),
+          static_cast<float>(p.tv_epsilon), static_cast<float>(p.binarization_weight),
+          grad ? grad + npix * c0 : nullptr, preg);
+    else if (tiled)
+      ilt_finish_tiled<32><<<dim3(reg_parts, nc), 256, 0, st>>>(
           th, dcdm, n, static_cast<float>(p.beta), static_cast<float>(p.tv_weight),
           static_cast<float>(p.tv_epsilon), static_cast<float>(p.binarization_weight),
           grad ? grad + npix * c0 : nullptr, preg);
@@ -842,7 +851,7 @@ std::vector<double> Engine::surrogate_error(Surrogate* sur, const huv_ilt_params
   DeviceSet& ds = device_set(p.defocus_nm);
   int M = choose_eval_grid(ds, 0);
   if (tc_supported(ds, std::max(M, 128)) && n >= 128)
-    run_tc_form(bt, ds, std::max(M, 128), b, st);
+    run_tc_form(bt, ds, std::max(M, 128), b, st, 0, nullptr, kTcCoreFftField);  // the hybrid form
   else
     run_fft_form(bt, ds, M, b, st);
   // per mask: max |a - b| and max |b|
@@ -871,25 +880,24 @@ namespace huv {
 
 namespace {
 
-struct DevVec {
-  void* p = nullptr;
-  size_t bytes = 0;
-  void ensure(size_t b) {
-    if (b <= bytes) return;
-    cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-    check_cuda(cudaMalloc(&p, b), "cudaMalloc(ilt state)");
-    bytes = b;
-  }
-  ~DevVec() { cudaFree(p); }
-  template <typename T>
-  T* as() const {
-    return static_cast<T*>(p);
-  }
-};
-
 }  // namespace
+
+void IltOptState::DevVec::ensure(size_t b) {
+  if (b <= bytes) return;
+  cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+  check_cuda(cudaMalloc(&p, b), "cudaMalloc(ilt state)");
+  bytes = b;
+}
+
+void IltOptState::release() {
+  for (DevVec* v : {&grad, &dir, &gnew, &trial, &tgt, &gold, &cost_d, &parts, &dots, &alpha, &gamma, &idx}) {
+    cudaFree(v->p);
+    v->p = nullptr;
+    v->bytes = 0;
+  }
+}
 
 void Engine::ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int masks, float* theta, const float* target,
                           double* final_cost, int* iterations, double* history, cudaStream_t st, Surrogate* sur,
@@ -897,7 +905,20 @@ void Engine::ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int mas
   using namespace huv_dev;
   const size_t npix = static_cast<size_t>(n) * n;
   const size_t blk = sizeof(float) * npix;
-  DevVec grad, dir, gnew, trial, tgt, gold, cost_d, parts, dots, alpha, gamma, idx;
+  // optimizer state kept by the engine across calls (grown, never shrunk)
+  IltOptState& S = ilt_state;
+  auto& grad = S.grad;
+  auto& dir = S.dir;
+  auto& gnew = S.gnew;
+  auto& trial = S.trial;
+  auto& tgt = S.tgt;
+  auto& gold = S.gold;
+  auto& cost_d = S.cost_d;
+  auto& parts = S.parts;
+  auto& dots = S.dots;
+  auto& alpha = S.alpha;
+  auto& gamma = S.gamma;
+  auto& idx = S.idx;
   grad.ensure(blk * masks);
   dir.ensure(blk * masks);
   gnew.ensure(blk * masks);
@@ -914,10 +935,10 @@ void Engine::ilt_optimize(const huv_ilt_params& p, const huv_ilt_opt& o, int mas
   const double lr = o.learning_rate, tol = o.convergence_tol;
   const int threads = 256;
 
-  auto upload = [&](DevVec& v, const void* h, size_t b) {
+  auto upload = [&](IltOptState::DevVec& v, const void* h, size_t b) {
     check_cuda(cudaMemcpyAsync(v.p, h, b, cudaMemcpyHostToDevice, st), "upload ilt scalars");
   };
-  auto fetch = [&](const DevVec& v, void* h, size_t b) {
+  auto fetch = [&](const IltOptState::DevVec& v, void* h, size_t b) {
     check_cuda(cudaMemcpyAsync(h, v.p, b, cudaMemcpyDeviceToHost, st), "fetch ilt scalars");
     check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize(ilt)");
   };

@@ -130,6 +130,7 @@ Engine::~Engine() {
     prof.release();
     cudaFree(dev_err);
     cudaFree(ilt_cost_dev);
+    ilt_state.release();
     cudaFree(ws);
     cudaFree(io_in);
     cudaFree(io_out);

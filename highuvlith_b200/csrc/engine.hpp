@@ -29,6 +29,23 @@ void check_cuda(cudaError_t e, const char* what);
 // (HUV_FORM_HYBRID).
 constexpr int kTcCoreFftRows = 0, kTcCoreGemmRows = 1, kTcCoreFftField = 2;
 
+// Device state of the ILT optimizer (gradients, directions, trial masks,
+// reductions), kept by the engine so that repeated optimizer calls do not
+// allocate; every buffer only grows.
+struct IltOptState {
+  struct DevVec {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t b);
+    template <typename T>
+    T* as() const {
+      return static_cast<T*>(p);
+    }
+  };
+  DevVec grad, dir, gnew, trial, tgt, gold, cost_d, parts, dots, alpha, gamma, idx;
+  void release();
+};
+
 struct TcState {
   int lgm = 0;          // evaluation grid the state was built for (log2)
   void* gy = nullptr;   // A_E planes [2][2M][kpE] bf16
@@ -166,6 +183,7 @@ struct Engine {
   double* ilt_cost_buffer(int n);
   double* ilt_cost_dev = nullptr;
   int ilt_cost_cap = 0;
+  IltOptState ilt_state;
   int choose_eval_grid(const DeviceSet& ds, int requested) const;
   bool tc_supported(const DeviceSet& ds, int M) const;
   // K_use / W_use: kernel count and flare weights to use (0 / nullptr = the whole set).
