@@ -1,10 +1,13 @@
 // Register-radix Stockham FFT over S interleaved sequences (FP32 complex).
 //
-// Each pass of radix R (16, 8, 4) loads R points of one butterfly into
-// registers, applies the Stockham twiddles w^{r k}, does the R-point DFT in
-// registers (16 = 4 x 4 and 8 = 4 x 2 with the internal twiddles W16^e) and
-// stores R points; a length L = 2^LG takes 2 or 3 passes instead of log4(L)
-// shared-memory round trips.  Data sit in shared memory sequence-minor:
+// Each pass of radix R (16, 12, 10, 8, 4) loads R points of one butterfly
+// into registers, applies the Stockham twiddles w^{r k}, does the R-point DFT
+// in registers (16 = 4 x 4, 8 = 4 x 2, 12 = 3 x 4, 10 = 5 x 2 with their
+// internal twiddles as constants) and stores R points; a length L of
+// 128, 160, 192, 256 takes 2 passes, 512 and 1024 take 3, instead of
+// log4(L) shared-memory round trips.  Lengths 160 = 16 x 10 and
+// 192 = 16 x 12 serve evaluation grids just above 4h that a power of two
+// would overshoot.  Data sit in shared memory sequence-minor:
 // element i of sequence s at ((i + pad(i)) * S + s), pad(i) = i / 16 when
 // S < 16, so that the lanes of a half-warp (consecutive s, then consecutive
 // butterflies) touch distinct banks in every pass, including the strided
@@ -62,6 +65,72 @@ __host__ __device__ __forceinline__ void fr_dft4(float2& a0, float2& a1, float2&
   a3 = fr_sub(d02, d13);
 }
 
+// exp(DIR * 2 pi i e / N) for N = 10, 12 (e in [0, N)), from the exact
+// values of cos and sin at multiples of pi / 5 and pi / 6.
+template <int N, int DIR>
+__host__ __device__ __forceinline__ float2 fr_w(int e) {
+  float c, s;
+  if constexpr (N == 10) {
+    // cos / sin of e pi / 5, e = 0 .. 9
+    constexpr float cs[10] = {1.0f, 0.80901699437494742f, 0.30901699437494742f, -0.30901699437494742f,
+                              -0.80901699437494742f, -1.0f, -0.80901699437494742f, -0.30901699437494742f,
+                              0.30901699437494742f, 0.80901699437494742f};
+    constexpr float sn[10] = {0.0f, 0.58778525229247313f, 0.95105651629515357f, 0.95105651629515357f,
+                              0.58778525229247313f, 0.0f, -0.58778525229247313f, -0.95105651629515357f,
+                              -0.95105651629515357f, -0.58778525229247313f};
+    c = cs[e % 10];
+    s = sn[e % 10];
+  } else {
+    // cos / sin of e pi / 6, e = 0 .. 11
+    constexpr float cs[12] = {1.0f, 0.86602540378443865f, 0.5f, 0.0f, -0.5f, -0.86602540378443865f,
+                              -1.0f, -0.86602540378443865f, -0.5f, 0.0f, 0.5f, 0.86602540378443865f};
+    constexpr float sn[12] = {0.0f, 0.5f, 0.86602540378443865f, 1.0f, 0.86602540378443865f, 0.5f,
+                              0.0f, -0.5f, -0.86602540378443865f, -1.0f, -0.86602540378443865f, -0.5f};
+    c = cs[e % 12];
+    s = sn[e % 12];
+  }
+  return make_float2(c, DIR > 0 ? s : -s);
+}
+
+// multiply by DIR i: (x + i y) -> DIR (-y + i x)
+template <int DIR>
+__host__ __device__ __forceinline__ float2 fr_idir(float2 a) {
+  return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// 3-point DFT in place: X1,2 = v0 - (v1 + v2) / 2 +- DIR i sqrt(3)/2 (v1 - v2).
+template <int DIR>
+__host__ __device__ __forceinline__ void fr_dft3(float2 (&v)[3]) {
+  constexpr float h = 0.86602540378443865f;
+  const float2 t = fr_add(v[1], v[2]);
+  const float2 d = fr_sub(v[1], v[2]);
+  const float2 a = make_float2(v[0].x - 0.5f * t.x, v[0].y - 0.5f * t.y);
+  const float2 b = fr_idir<DIR>(make_float2(h * d.x, h * d.y));
+  v[0] = fr_add(v[0], t);
+  v[1] = fr_add(a, b);
+  v[2] = fr_sub(a, b);
+}
+
+// 5-point DFT in place (c1, s1 = cos, sin 2 pi / 5; c2, s2 = cos, sin 4 pi / 5):
+// X1,4 = v0 + c1 (v1 + v4) + c2 (v2 + v3) +- DIR i (s1 (v1 - v4) + s2 (v2 - v3)),
+// X2,3 = v0 + c2 (v1 + v4) + c1 (v2 + v3) +- DIR i (s2 (v1 - v4) - s1 (v2 - v3)).
+template <int DIR>
+__host__ __device__ __forceinline__ void fr_dft5(float2 (&v)[5]) {
+  constexpr float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+  constexpr float s1 = 0.95105651629515357f, s2 = 0.58778525229247313f;
+  const float2 t1 = fr_add(v[1], v[4]), t2 = fr_add(v[2], v[3]);
+  const float2 d1 = fr_sub(v[1], v[4]), d2 = fr_sub(v[2], v[3]);
+  const float2 a1 = make_float2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+  const float2 a2 = make_float2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+  const float2 b1 = fr_idir<DIR>(make_float2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y));
+  const float2 b2 = fr_idir<DIR>(make_float2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y));
+  v[0] = fr_add(v[0], fr_add(t1, t2));
+  v[1] = fr_add(a1, b1);
+  v[4] = fr_sub(a1, b1);
+  v[2] = fr_add(a2, b2);
+  v[3] = fr_sub(a2, b2);
+}
+
 // R-point DFT of v in place, natural order in and out.
 template <int R, int DIR>
 __host__ __device__ __forceinline__ void fr_dft(float2 (&v)[R]) {
@@ -84,6 +153,43 @@ __host__ __device__ __forceinline__ void fr_dft(float2 (&v)[R]) {
     for (int p = 0; p < 4; ++p) {
       v[p] = fr_add(u[0][p], u[1][p]);
       v[p + 4] = fr_sub(u[0][p], u[1][p]);
+    }
+  } else if constexpr (R == 10) {
+    // n = q + 2 m, k = p + 5 q': X = sum_q W2^{q q'} W10^{q p} [sum_m v W5^{m p}]
+    float2 u[2][5];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) u[q][m] = v[q + 2 * m];
+      fr_dft5<DIR>(u[q]);
+    }
+#pragma unroll
+    for (int p = 1; p < 5; ++p) u[1][p] = fr_mul(u[1][p], fr_w<10, DIR>(p));
+#pragma unroll
+    for (int p = 0; p < 5; ++p) {
+      v[p] = fr_add(u[0][p], u[1][p]);
+      v[p + 5] = fr_sub(u[0][p], u[1][p]);
+    }
+  } else if constexpr (R == 12) {
+    // n = q + 4 m, k = p + 3 q': X = sum_q W4^{q q'} W12^{q p} [sum_m v W3^{m p}]
+    float2 u[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+      for (int m = 0; m < 3; ++m) u[q][m] = v[q + 4 * m];
+      fr_dft3<DIR>(u[q]);
+    }
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+#pragma unroll
+      for (int p = 1; p < 3; ++p) u[q][p] = fr_mul(u[q][p], fr_w<12, DIR>(q * p));
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      fr_dft4<DIR>(u[0][p], u[1][p], u[2][p], u[3][p]);
+      v[p] = u[0][p];
+      v[p + 3] = u[1][p];
+      v[p + 6] = u[2][p];
+      v[p + 9] = u[3][p];
     }
   } else if constexpr (R == 16) {
     // n = q + 4 m, k = p + 4 q': X = sum_q W4^{q q'} W16^{q p} [sum_m v W4^{m p}]
@@ -111,14 +217,21 @@ __host__ __device__ __forceinline__ void fr_dft(float2 (&v)[R]) {
   }
 }
 
-// Radix plan: LG 7 = 16 x 8, 8 = 16 x 16, 9 = 16 x 8 x 4, 10 = 16 x 16 x 4.
-__host__ __device__ constexpr int fr_passes(int LG) { return LG <= 8 ? 2 : 3; }
-__host__ __device__ constexpr int fr_radix(int LG, int pass) {
-  return pass == 0 ? 16 : (LG == 7 ? 8 : (LG == 8 ? 16 : (LG == 9 ? (pass == 1 ? 8 : 4) : (pass == 1 ? 16 : 4))));
+// Radix plan by length: 128 = 16 x 8, 160 = 16 x 10, 192 = 16 x 12,
+// 256 = 16 x 16, 512 = 16 x 8 x 4, 1024 = 16 x 16 x 4.
+__host__ __device__ constexpr int fr_passes(int L) { return L <= 256 ? 2 : 3; }
+__host__ __device__ constexpr int fr_radix(int L, int pass) {
+  return pass == 0 ? 16
+                   : (L == 128 ? 8
+                               : (L == 160 ? 10
+                                           : (L == 192 ? 12
+                                                       : (L == 256 ? 16
+                                                                   : (L == 512 ? (pass == 1 ? 8 : 4)
+                                                                               : (pass == 1 ? 16 : 4))))));
 }
 // Stockham sub-transform size before pass `pass`.
-__host__ __device__ constexpr int fr_ns(int LG, int pass) {
-  return pass == 0 ? 1 : fr_ns(LG, pass - 1) * fr_radix(LG, pass - 1);
+__host__ __device__ constexpr int fr_ns(int L, int pass) {
+  return pass == 0 ? 1 : fr_ns(L, pass - 1) * fr_radix(L, pass - 1);
 }
 
 // Shared-memory index of element i of sequence s.
@@ -129,8 +242,14 @@ __host__ __device__ __forceinline__ int fr_idx(int i, int s) {
 // Buffer length (float2) for S sequences of length L.
 __host__ __device__ constexpr int fr_buf(int L, int S) { return (S < 16 ? L + L / 16 : L) * S; }
 
-// Threads of one block: one radix-16 butterfly per thread per pass.
-__host__ __device__ constexpr int fr_threads(int LG, int S) { return S * (1 << LG) / 16; }
+// Threads of one block (256 for every plan), butterflies of pass `pass`
+// over S sequences, and butterflies per thread (rounded up; the last round
+// is guarded where the count is not a multiple of 256).
+__host__ __device__ constexpr int fr_threads(int L, int S) { return (void)L, (void)S, 256; }
+__host__ __device__ constexpr int fr_nb(int L, int S, int pass) { return S * L / fr_radix(L, pass); }
+__host__ __device__ constexpr int fr_per(int L, int S, int pass) {
+  return (fr_nb(L, S, pass) + fr_threads(L, S) - 1) / fr_threads(L, S);
+}
 
 // Asynchronous 8-byte global -> shared copies (cp.async, L1-allocating) for
 // prefetching the next kernel's band columns while the current one is
@@ -146,23 +265,23 @@ __device__ __forceinline__ void fr_cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Sequences per block of the register-radix kernels for L = 2^lg (256
+// Sequences per block of the register-radix kernels for length L (256
 // threads each), 0 where no instance exists; shared-memory bytes of the
 // ping-pong buffers of one block and the kernels' shared-memory ceiling.
-__host__ __device__ constexpr int xt_S(int lg) {
-  return lg == 7 ? 32 : lg == 8 ? 16 : lg == 9 ? 8 : lg == 10 ? 4 : 0;
+__host__ __device__ constexpr int xt_S(int L) {
+  return L == 128 ? 32 : (L == 160 || L == 192 || L == 256) ? 16 : L == 512 ? 8 : L == 1024 ? 4 : 0;
 }
-__host__ __device__ constexpr size_t xt_buf_bytes(int lg) {
-  return (fr_passes(lg) - 1) * static_cast<size_t>(fr_buf(1 << lg, xt_S(lg))) * sizeof(float2);
+__host__ __device__ constexpr size_t xt_buf_bytes(int L) {
+  return xt_S(L) ? (fr_passes(L) - 1) * static_cast<size_t>(fr_buf(L, xt_S(L))) * sizeof(float2) : 0;
 }
 constexpr int kXtSmemMax = 110 * 1024;
 
 // First pass (radix 16, no twiddles) for thread t, reading a zero-padded
 // band: position i of sequence s holds P[s][mx] for the order mx - hb = i
 // (i <= hb) or i - L (i >= L - hb), and zero elsewhere.  Requires 2 hb < L.
-template <int LG, int S, int DIR>
+template <int L, int S, int DIR>
 __host__ __device__ __forceinline__ void fr_first_pass_band(int t, const float2* P, int B, int hb, float2* dst) {
-  constexpr int L = 1 << LG;
+  if (t >= fr_nb(L, S, 0)) return;
   const int s = t % S, j = t / S;
   float2 v[16];
 #pragma unroll
@@ -178,8 +297,9 @@ __host__ __device__ __forceinline__ void fr_first_pass_band(int t, const float2*
 
 // First pass (radix 16, no twiddles) for thread t given its 16 inputs
 // v[r] = element j + r L / 16 of sequence s (s = t % S, j = t / S).
-template <int LG, int S, int DIR>
+template <int L, int S, int DIR>
 __host__ __device__ __forceinline__ void fr_first_pass_vals(int t, float2 (&v)[16], float2* dst) {
+  if (t >= fr_nb(L, S, 0)) return;
   const int s = t % S, j = t / S;
   fr_dft<16, DIR>(v);
 #pragma unroll
@@ -187,14 +307,14 @@ __host__ __device__ __forceinline__ void fr_first_pass_vals(int t, float2 (&v)[1
 }
 
 // Middle pass `pass` (not the first, not the last) for thread t: src -> dst.
-template <int LG, int S, int DIR, int PASS>
+template <int L, int S, int DIR, int PASS>
 __host__ __device__ __forceinline__ void fr_mid_pass(int t, const float2* src, float2* dst, const float2* tw) {
-  constexpr int L = 1 << LG;
-  constexpr int R = fr_radix(LG, PASS), Ns = fr_ns(LG, PASS), T = fr_threads(LG, S);
+  constexpr int R = fr_radix(L, PASS), Ns = fr_ns(L, PASS), T = fr_threads(L, S);
   constexpr int stride = L / (Ns * R);
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
+  for (int b = 0; b < fr_per(L, S, PASS); ++b) {
     const int u = t + b * T;
+    if (u >= fr_nb(L, S, PASS)) break;
     const int s = u % S, j = u / S;
     const int k = j & (Ns - 1);
     float2 v[R];
@@ -215,12 +335,11 @@ __host__ __device__ __forceinline__ void fr_mid_pass(int t, const float2* src, f
 
 // Last pass for butterfly u: loads, twiddles and transforms; returns the
 // sequence s and j; v[p] is output element x = j + p * (L / R).
-template <int LG, int S, int DIR>
+template <int L, int S, int DIR>
 __host__ __device__ __forceinline__ void fr_last_pass(int u, const float2* src, const float2* tw, int& s, int& j,
-                                                      float2 (&v)[fr_radix(LG, fr_passes(LG) - 1)]) {
-  constexpr int L = 1 << LG;
-  constexpr int P = fr_passes(LG) - 1;
-  constexpr int R = fr_radix(LG, P), Ns = fr_ns(LG, P);
+                                                      float2 (&v)[fr_radix(L, fr_passes(L) - 1)]) {
+  constexpr int P = fr_passes(L) - 1;
+  constexpr int R = fr_radix(L, P), Ns = fr_ns(L, P);
   constexpr int stride = L / (Ns * R);  // 1
   s = u % S;
   j = u / S;
@@ -239,15 +358,15 @@ __host__ __device__ __forceinline__ void fr_last_pass(int u, const float2* src, 
 // The last pass's twiddles of thread t (for each of its 16 / R butterflies,
 // w^{r j} for r = 1 .. R - 1, direction applied): they depend only on t, so
 // kernels that run the same transform shape many times load them once.
-template <int LG, int S, int DIR>
+template <int L, int S, int DIR>
 __host__ __device__ __forceinline__ void fr_last_twiddles(
     int t, const float2* tw,
-    float2 (&w)[16 / fr_radix(LG, fr_passes(LG) - 1)][fr_radix(LG, fr_passes(LG) - 1) - 1]) {
-  constexpr int P = fr_passes(LG) - 1;
-  constexpr int R = fr_radix(LG, P), T = fr_threads(LG, S);
+    float2 (&w)[fr_per(L, S, fr_passes(L) - 1)][fr_radix(L, fr_passes(L) - 1) - 1]) {
+  constexpr int P = fr_passes(L) - 1;
+  constexpr int R = fr_radix(L, P), T = fr_threads(L, S);
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
-    const int j = (t + b * T) / S;
+  for (int b = 0; b < fr_per(L, S, P); ++b) {
+    const int j = ((t + b * T) / S) % (L / R);  // guarded butterflies: any valid index
 #pragma unroll
     for (int r = 1; r < R; ++r) {
       float2 x = tw[r * j];
@@ -258,13 +377,12 @@ __host__ __device__ __forceinline__ void fr_last_twiddles(
 }
 
 // fr_last_pass with the twiddles of butterfly b preloaded (fr_last_twiddles).
-template <int LG, int S, int DIR>
+template <int L, int S, int DIR>
 __host__ __device__ __forceinline__ void fr_last_pass_pre(int u, const float2* src,
-                                                          const float2 (&w)[fr_radix(LG, fr_passes(LG) - 1) - 1],
+                                                          const float2 (&w)[fr_radix(L, fr_passes(L) - 1) - 1],
                                                           int& s, int& j,
-                                                          float2 (&v)[fr_radix(LG, fr_passes(LG) - 1)]) {
-  constexpr int L = 1 << LG;
-  constexpr int R = fr_radix(LG, fr_passes(LG) - 1);
+                                                          float2 (&v)[fr_radix(L, fr_passes(L) - 1)]) {
+  constexpr int R = fr_radix(L, fr_passes(L) - 1);
   s = u % S;
   j = u / S;
 #pragma unroll

@@ -177,13 +177,13 @@ __global__ void ilt_cols_adj(const float2* __restrict__ T, const float* __restri
 // FFT_y, band rows [-hb, hb] kept: V[mask][k][my'][x] (the layout of
 // ilt_rows_adj).  grid: (L / S, masks); shared: P (S B), two FFT buffers,
 // a second band buffer P2 (S B).
-template <int LG, int S>
-__global__ void __launch_bounds__(fr_threads(LG, S))
+template <int L, int S>
+__global__ void __launch_bounds__(fr_threads(L, S))
     ilt_cols_adj_xt(const float2* __restrict__ Tt, const float* __restrict__ G, int K, int hb, float keep,
                     const double* __restrict__ sums, float flare_over_n, float2* __restrict__ V,
                     const float2* __restrict__ tw) {
-  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
-  constexpr int R = fr_radix(LG, NP - 1);
+  constexpr int T = fr_threads(L, S), NP = fr_passes(L);
+  constexpr int R = fr_radix(L, NP - 1);
   extern __shared__ float2 smem[];
   const int B = 2 * hb + 1;
   const int mask = blockIdx.y;
@@ -224,17 +224,17 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
       fr_cp_wait<0>();
     }
     __syncthreads();
-    fr_first_pass_band<LG, S, +1>(t, (k & 1) ? P2 : P, B, hb, b0);
+    fr_first_pass_band<L, S, +1>(t, (k & 1) ? P2 : P, B, hb, b0);
     __syncthreads();
     if constexpr (NP == 3) {
-      fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
+      fr_mid_pass<L, S, +1, 1>(t, b0, b1, tw);
       __syncthreads();
     }
 #pragma unroll
     for (int b = 0; b < 16 / R; ++b) {
       int s, j;
       float2 v[R];
-      fr_last_pass<LG, S, +1>(t + b * T, inv, tw, s, j, v);
+      fr_last_pass<L, S, +1>(t + b * T, inv, tw, s, j, v);
 #pragma unroll
       for (int p = 0; p < R; ++p) {
         const float w = g[b * R + p];
@@ -247,12 +247,12 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
       float2 v[16];
 #pragma unroll
       for (int r = 0; r < 16; ++r) v[r] = oth[fr_idx<S>(j + r * (L / 16), s)];
-      fr_first_pass_vals<LG, S, -1>(t, v, inv);
+      fr_first_pass_vals<L, S, -1>(t, v, inv);
     }
     __syncthreads();
     const float2* cur = inv;
     if constexpr (NP == 3) {
-      fr_mid_pass<LG, S, -1, 1>(t, inv, oth, tw);
+      fr_mid_pass<L, S, -1, 1>(t, inv, oth, tw);
       __syncthreads();
       cur = oth;
     }
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
     for (int b = 0; b < 16 / R; ++b) {
       int s, j;
       float2 v[R];
-      fr_last_pass<LG, S, -1>(t + b * T, cur, tw, s, j, v);
+      fr_last_pass<L, S, -1>(t + b * T, cur, tw, s, j, v);
 #pragma unroll
       for (int p = 0; p < R; ++p) {
         const int idx = j + p * (L / R);
@@ -562,12 +562,12 @@ cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int
                       float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
                       const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
-cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int L, int clips,
                         float2* T, const float2* tw, cudaStream_t st);
-cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 
-bool xt_ok(int lg, int hb);
+bool xt_ok(int L, int hb);
 
 cudaError_t ilt_set_smem() {
   const int big = 200 * 1024;
@@ -575,21 +575,22 @@ cudaError_t ilt_set_smem() {
   if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
   if ((e = cudaFuncSetAttribute(huv_dev::ilt_rows_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
   const int xt = huv_dev::kXtSmemMax;
-  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<7, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<128, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
     return e;
-  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<256, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
     return e;
-  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<9, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<512, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
     return e;
-  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<10, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<1024, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
     return e;
   return cudaSuccess;
 }
 
-// Shared memory of ilt_cols_adj_xt: two band-column buffers and two FFT buffers.
-size_t ilt_adj_xt_smem(int lg, int hb) {
-  const int S = huv_dev::xt_S(lg);
-  return (2 * static_cast<size_t>(S) * (2 * hb + 1) + 2 * static_cast<size_t>(huv_dev::fr_buf(1 << lg, S))) *
+// Shared memory of ilt_cols_adj_xt on L points: two band-column buffers and
+// two FFT buffers.
+size_t ilt_adj_xt_smem(int L, int hb) {
+  const int S = huv_dev::xt_S(L);
+  return (2 * static_cast<size_t>(S) * (2 * hb + 1) + 2 * static_cast<size_t>(huv_dev::fr_buf(L, S))) *
          sizeof(float2);
 }
 }  // namespace huv_launch
@@ -699,10 +700,11 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     // fields of every kernel on the evaluation grid, the image on it, then on N x N
     // x-major row transforms (register-radix kernels) when the adjoint's
     // register-radix column pass fits too, else the [k][my][x] layout
-    const bool xt = xt_ok(lgm, hb) && ilt_adj_xt_smem(lgm, hb) <= static_cast<size_t>(kXtSmemMax);
+    // (the ILT's grids are powers of two; ilt_cols_adj_xt has no 160 / 192 instance)
+    const bool xt = xt_ok(M, hb) && ilt_adj_xt_smem(M, hb) <= static_cast<size_t>(kXtSmemMax);
     if (xt) {
-      check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "ilt socs_rows");
-      check_cuda(socs_cols_x(T, K, hb, lgm, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
+      check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "ilt socs_rows");
+      check_cuda(socs_cols_x(T, K, hb, M, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
     } else {
       check_cuda(socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "ilt socs_rows");
       check_cuda(socs_cols(T, K, hb, lgm, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
@@ -712,8 +714,8 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
                               nullptr),
                  "ilt band(I)");
       const float scale = 1.0f / static_cast<float>(mpix);
-      check_cuda(socs_rows_x(nullptr, scale, C, 1, h2, lgn, nc, X2, twn, st), "ilt interp rows");
-      check_cuda(socs_cols_x(X2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, img, 1, twn, st), "ilt interp cols");
+      check_cuda(socs_rows_x(nullptr, scale, C, 1, h2, n, nc, X2, twn, st), "ilt interp rows");
+      check_cuda(socs_cols_x(X2, 1, h2, n, nc, 1.f, 0.f, nullptr, img, 1, twn, st), "ilt interp cols");
     }
     ilt_data<<<dim3(kRedBlocks, nc), 256, 0, st>>>(img, tg, npix, p.cost_kind, static_cast<float>(p.threshold),
                                                    static_cast<float>(p.steepness), static_cast<float>(p.dose),
@@ -728,21 +730,21 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
         check_cuda(band_forward(img, HUV_INPUT_RASTER_F32, n, lgn, h2, nc, X, C, nullptr, nullptr, nullptr, twn, st, nullptr,
                                 nullptr),
                    "ilt band(G)");
-        check_cuda(socs_rows_x(nullptr, 1.0f / static_cast<float>(npix), C, 1, h2, lgm, nc, X2, twm, st),
+        check_cuda(socs_rows_x(nullptr, 1.0f / static_cast<float>(npix), C, 1, h2, M, nc, X2, twm, st),
                    "ilt G rows");
-        check_cuda(socs_cols_x(X2, 1, h2, lgm, nc, 1.f, 0.f, nullptr, IM, 1, twm, st), "ilt G cols");
+        check_cuda(socs_cols_x(X2, 1, h2, M, nc, 1.f, 0.f, nullptr, IM, 1, twm, st), "ilt G cols");
         Gm = IM;
         grid_scale = static_cast<float>(static_cast<double>(npix) / static_cast<double>(mpix));
       }
       if (xt) {
-        const dim3 ga(M / xt_S(lgm), nc);
-        const size_t sm = ilt_adj_xt_smem(lgm, hb);
+        const dim3 ga(M / xt_S(M), nc);
+        const size_t sm = ilt_adj_xt_smem(M, hb);
         const float fo = flare / static_cast<float>(npix);
-        switch (lgm) {
-          case 7: ilt_cols_adj_xt<7, 32><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
-          case 8: ilt_cols_adj_xt<8, 16><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
-          case 9: ilt_cols_adj_xt<9, 8><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
-          default: ilt_cols_adj_xt<10, 4><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+        switch (M) {
+          case 128: ilt_cols_adj_xt<128, 32><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+          case 256: ilt_cols_adj_xt<256, 16><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+          case 512: ilt_cols_adj_xt<512, 8><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+          default: ilt_cols_adj_xt<1024, 4><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
         }
       } else {
         const int Wc = fit_units(8, 2 * (sizeof(float2) << lgm) + (sizeof(float) << lgm));
@@ -758,9 +760,9 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
       // Re IFFT(Q) = IFFT(Hermitian part of Q): a real synthesis, two
       // columns per transform on the register-radix path
       hermitian_part<<<(nc * ((B * B + 1) / 2) + 255) / 256, 256, 0, st>>>(Q, B, nc);
-      check_cuda(socs_rows_x(nullptr, scale, Q, 1, hb, lgn, nc, T2, twn, st), "ilt grad rows");
+      check_cuda(socs_rows_x(nullptr, scale, Q, 1, hb, n, nc, T2, twn, st), "ilt grad rows");
       dcdm = tbuf;  // the transmittance is no longer needed
-      check_cuda(socs_cols_x(T2, 1, hb, lgn, nc, 1.f, 0.f, nullptr, dcdm, 1, twn, st), "ilt grad cols");
+      check_cuda(socs_cols_x(T2, 1, hb, n, nc, 1.f, 0.f, nullptr, dcdm, 1, twn, st), "ilt grad cols");
     }
     if (tile == 64)
       ilt_finish_tiled<64><<<dim3(reg_parts, nc), 256, 0, st>>>(

@@ -242,12 +242,12 @@ __global__ void socs_cols_inv(const float2* __restrict__ T, int K, int hb, int l
 
 // Inverse transform along x of every (kernel, band row) product; S sequences
 // per block.  grid: (ceil(K * B / S), clips).
-template <int LG, int S>
-__global__ void __launch_bounds__(fr_threads(LG, S))
+template <int L, int S>
+__global__ void __launch_bounds__(fr_threads(L, S))
     socs_rows_xt(const float2* __restrict__ kband, float scale, const float2* __restrict__ Mband, int K, int hb,
                  float2* __restrict__ Tt, const float2* __restrict__ tw) {
-  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
-  constexpr int R = fr_radix(LG, NP - 1);
+  constexpr int T = fr_threads(L, S), NP = fr_passes(L);
+  constexpr int R = fr_radix(L, NP - 1);
   extern __shared__ float2 smem[];
   const int B = 2 * hb + 1;
   const int clip = blockIdx.y;
@@ -273,19 +273,20 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
     }
   }
   __syncthreads();
-  fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
+  fr_first_pass_band<L, S, +1>(t, P, B, hb, b0);
   __syncthreads();
   const float2* src = b0;
   if constexpr (NP == 3) {
-    fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
+    fr_mid_pass<L, S, +1, 1>(t, b0, b1, tw);
     __syncthreads();
     src = b1;
   }
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
+  for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
+    if (t + b * T >= fr_nb(L, S, NP - 1)) break;
     int s, j;
     float2 v[R];
-    fr_last_pass<LG, S, +1>(t + b * T, src, tw, s, j, v);
+    fr_last_pass<L, S, +1>(t + b * T, src, tw, s, j, v);
     if (s >= nseq) continue;
     const int seq = seq0 + s;
     const int k = seq / B, my = seq - k * B;
@@ -301,12 +302,12 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
 // columns per sequence, z = T(., x0 + 2s) + i T(., x0 + 2s + 1); each column
 // is Hermitian in my, so Re and Im of the transform are the two real
 // columns.  grid: (L / (S or 2 S), clips); out: [clip][L][L].
-template <int LG, int S, int MODE>
-__global__ void __launch_bounds__(fr_threads(LG, S), 2)
+template <int L, int S, int MODE>
+__global__ void __launch_bounds__(fr_threads(L, S), 2)
     socs_cols_xt(const float2* __restrict__ Tt, int K, int hb, float keep, float flare,
                  const float* __restrict__ mean, float* __restrict__ out, const float2* __restrict__ tw) {
-  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
-  constexpr int R = fr_radix(LG, NP - 1);
+  constexpr int T = fr_threads(L, S), NP = fr_passes(L);
+  constexpr int R = fr_radix(L, NP - 1);
   constexpr int XS = MODE == 1 ? 2 * S : S;
   extern __shared__ float2 smem[];
   const int B = 2 * hb + 1;
@@ -316,10 +317,11 @@ __global__ void __launch_bounds__(fr_threads(LG, S), 2)
   float2* P = smem;  // [S][B]
   float2* b0 = smem + S * B;
   float2* b1 = b0 + fr_buf(L, S);
-  float acc[16];
-  float2 res[16];
+  constexpr int NO = fr_per(L, S, NP - 1) * R;  // outputs per thread
+  float acc[NO];
+  float2 res[NO];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) {
+  for (int i = 0; i < NO; ++i) {
     acc[i] = 0.f;
     res[i] = make_float2(0.f, 0.f);
   }
@@ -333,8 +335,8 @@ __global__ void __launch_bounds__(fr_threads(LG, S), 2)
     fr_cp_commit();
   };
   if (MODE == 0) prefetch(0);
-  float2 lw[16 / R][R - 1];  // last-pass twiddles, the same for every kernel
-  fr_last_twiddles<LG, S, +1>(t, tw, lw);
+  float2 lw[fr_per(L, S, NP - 1)][R - 1];  // last-pass twiddles, the same for every kernel
+  fr_last_twiddles<L, S, +1>(t, tw, lw);
   for (int k = 0; k < K; ++k) {
     const float2* Pk = P;
     if (MODE == 0) {
@@ -355,19 +357,20 @@ __global__ void __launch_bounds__(fr_threads(LG, S), 2)
       }
     }
     __syncthreads();
-    fr_first_pass_band<LG, S, +1>(t, Pk, B, hb, b0);
+    fr_first_pass_band<L, S, +1>(t, Pk, B, hb, b0);
     __syncthreads();
     const float2* cur = b0;
     if constexpr (NP == 3) {
-      fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
+      fr_mid_pass<L, S, +1, 1>(t, b0, b1, tw);
       __syncthreads();
       cur = b1;
     }
 #pragma unroll
-    for (int b = 0; b < 16 / R; ++b) {
+    for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
+      if (t + b * T >= fr_nb(L, S, NP - 1)) break;
       int s, j;
       float2 v[R];
-      fr_last_pass_pre<LG, S, +1>(t + b * T, cur, lw[b], s, j, v);
+      fr_last_pass_pre<L, S, +1>(t + b * T, cur, lw[b], s, j, v);
 #pragma unroll
       for (int p = 0; p < R; ++p) {
         if (MODE == 0)
@@ -381,8 +384,9 @@ __global__ void __launch_bounds__(fr_threads(LG, S), 2)
   const float add = (MODE == 0 && mean) ? flare * mean[clip] : 0.f;
   float* oc = out + static_cast<size_t>(clip) * L * L;
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
+  for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
     const int u = t + b * T;
+    if (u >= fr_nb(L, S, NP - 1)) break;
     const int s = u % S, j = u / S;
 #pragma unroll
     for (int p = 0; p < R; ++p) {
@@ -400,40 +404,40 @@ __global__ void __launch_bounds__(fr_threads(LG, S), 2)
 // last pass leaves the spectra in natural order in shared memory, and the
 // two real rows' bands are split from Z(m) and conj Z(-m).
 // grid: (clips * L / (2 S)); X: [clip][y][B].
-template <int LG, int S>
-__global__ void __launch_bounds__(fr_threads(LG, S))
+template <int L, int S>
+__global__ void __launch_bounds__(fr_threads(L, S))
     band_rows_reg(const float* __restrict__ in, int hb, float2* __restrict__ X, const float2* __restrict__ tw) {
-  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
+  constexpr int T = fr_threads(L, S), NP = fr_passes(L);
   extern __shared__ float2 smem[];
   const int B = 2 * hb + 1;
   const size_t row0 = static_cast<size_t>(blockIdx.x) * 2 * S;
   const int t = threadIdx.x;
   float2* b0 = smem;
   float2* b1 = b0 + fr_buf(L, S);
-  {
+  if (t < fr_nb(L, S, 0)) {
     const int s = t % S, j = t / S;
     const float* ra = in + (row0 + 2 * s) * L + j;
     float2 v[16];
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = make_float2(ra[r * (L / 16)], ra[L + r * (L / 16)]);
-    fr_first_pass_vals<LG, S, -1>(t, v, b0);
+    fr_first_pass_vals<L, S, -1>(t, v, b0);
   }
   __syncthreads();
   float2* cur = b0;
   if constexpr (NP == 3) {
-    fr_mid_pass<LG, S, -1, 1>(t, b0, b1, tw);
+    fr_mid_pass<L, S, -1, 1>(t, b0, b1, tw);
     __syncthreads();
-    fr_mid_pass<LG, S, -1, 2>(t, b1, b0, tw);
+    fr_mid_pass<L, S, -1, 2>(t, b1, b0, tw);
   } else {
-    fr_mid_pass<LG, S, -1, 1>(t, b0, b1, tw);
+    fr_mid_pass<L, S, -1, 1>(t, b0, b1, tw);
     cur = b1;
   }
   __syncthreads();
   for (int e = t; e < S * B; e += T) {
     const int s = e / B, mi = e - s * B;
-    const int idx = (mi - hb) & (L - 1);
+    const int idx = mi - hb < 0 ? mi - hb + L : mi - hb;
     const float2 z = cur[fr_idx<S>(idx, s)];
-    const float2 zc = cconj(cur[fr_idx<S>((L - idx) & (L - 1), s)]);
+    const float2 zc = cconj(cur[fr_idx<S>(idx == 0 ? 0 : L - idx, s)]);
     const float2 xa = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y + zc.y));
     const float2 d = csub(z, zc);
     const float2 xb = make_float2(0.5f * d.y, -0.5f * d.x);
@@ -445,13 +449,13 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
 // band_cols_fwd with register-radix passes: forward FFT along y of S band
 // columns of X[clip][y][B] (or of X[clip][B][y] with `transposed`) per block,
 // the first pass reading X directly.  grid: (ceil(B / S), clips).
-template <int LG, int S>
-__global__ void __launch_bounds__(fr_threads(LG, S))
+template <int L, int S>
+__global__ void __launch_bounds__(fr_threads(L, S))
     band_cols_reg(const float2* __restrict__ X, bool transposed, int hb, const float* __restrict__ ptx,
                   const float* __restrict__ W, float2* __restrict__ Mband, float* __restrict__ parts,
                   const float2* __restrict__ tw) {
-  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
-  constexpr int R = fr_radix(LG, NP - 1);
+  constexpr int T = fr_threads(L, S), NP = fr_passes(L);
+  constexpr int R = fr_radix(L, NP - 1);
   extern __shared__ float2 smem[];
   __shared__ float red[T / 32];
   const int B = 2 * hb + 1;
@@ -461,7 +465,7 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
   float2* b0 = smem;
   float2* b1 = b0 + fr_buf(L, S);
   const float2* Xc = X + static_cast<size_t>(clip) * L * B;
-  {
+  if (t < fr_nb(L, S, 0)) {
     const int s = t % S, j = t / S;
     const bool live = c0 + s < B;
     float2 v[16];
@@ -470,22 +474,23 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
 #pragma unroll
     for (int r = 0; r < 16; ++r)
       v[r] = live ? Xc[col_base + static_cast<size_t>(j + r * (L / 16)) * row_step] : make_float2(0.f, 0.f);
-    fr_first_pass_vals<LG, S, -1>(t, v, b0);
+    fr_first_pass_vals<L, S, -1>(t, v, b0);
   }
   __syncthreads();
   const float2* cur = b0;
   if constexpr (NP == 3) {
-    fr_mid_pass<LG, S, -1, 1>(t, b0, b1, tw);
+    fr_mid_pass<L, S, -1, 1>(t, b0, b1, tw);
     __syncthreads();
     cur = b1;
   }
   float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
   float part = 0.f;
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
+  for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
+    if (t + b * T >= fr_nb(L, S, NP - 1)) break;
     int s, j;
     float2 v[R];
-    fr_last_pass<LG, S, -1>(t + b * T, cur, tw, s, j, v);
+    fr_last_pass<L, S, -1>(t + b * T, cur, tw, s, j, v);
     const int mx = c0 + s;
     if (mx >= B) continue;
 #pragma unroll
@@ -540,7 +545,10 @@ cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float 
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X,
                          float2* Mband, const float* ptx, const float* W, float* mean,
                          const float2* tw, cudaStream_t st, const uint8_t* row_digits, int* err) {
-  const int S = fit_units(2, 2 * (sizeof(float2) << lg));
+  // n need not be a power of two when the register-radix kernels serve it
+  // (160 = 16 x 10, 192 = 16 x 12); the radix-4 kernels use lg = log2 n.
+  const bool pow2 = (n & (n - 1)) == 0;
+  const int S = pow2 ? fit_units(2, 2 * (sizeof(float2) << lg)) : 1;
   const int rows_per_block = (kind == 2) ? S : 2 * S;
   const size_t sm1 = 2 * (static_cast<size_t>(S) << lg) * sizeof(float2);
   dim3 g1(n / rows_per_block, clips);
@@ -553,21 +561,27 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   cudaError_t rows_tc = cudaErrorNotSupported;
   // the register-radix columns read a transposed row band ([clip][m][y]) when
   // the tensor-core rows produce it
-  const bool cols_reg = xt_ok(lg, hb);
+  const bool cols_reg = xt_ok(n, hb);
   bool x_transposed = false;
   if (kind == 0 && row_digits) {
     rows_tc = mask_rows_tc(in, n, hb, clips, X, row_digits, err, st, cols_reg);
     x_transposed = rows_tc == cudaSuccess && cols_reg;
     if (rows_tc != cudaSuccess && rows_tc != cudaErrorNotSupported) return rows_tc;
   }
-  if (kind == 1 && lg == 10 && xt_ok(lg, hb)) {
-    const int Sr = xt_S(lg);
+  if (kind == 1 && (n == 1024 || n == 160 || n == 192) && xt_ok(n, hb)) {
+    const int Sr = xt_S(n);
     const dim3 gr(static_cast<unsigned>(static_cast<size_t>(clips) * n / (2 * Sr)));
     const size_t smr = 2 * static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
     const float* fin = static_cast<const float*>(in);
-    band_rows_reg<10, 4><<<gr, 256, smr, st>>>(fin, hb, X, tw);
+    if (n == 1024)
+      band_rows_reg<1024, 4><<<gr, 256, smr, st>>>(fin, hb, X, tw);
+    else if (n == 160)
+      band_rows_reg<160, 16><<<gr, 256, smr, st>>>(fin, hb, X, tw);
+    else
+      band_rows_reg<192, 16><<<gr, 256, smr, st>>>(fin, hb, X, tw);
     rows_tc = cudaSuccess;
   }
+  if (!pow2 && rows_tc != cudaSuccess) return cudaErrorInvalidValue;  // no radix-4 kernel for this length
   // Only device rasters come here (rectangle clips take the analytic path).
   switch (kind) {
     case 0:
@@ -585,17 +599,20 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   if (cols_reg) {
     // register-radix columns: S <= 4 ... 32 columns per block, at most
     // ceil(B / 4) parts per clip as the callers size them
-    const int S = xt_S(lg);
+    const int S = xt_S(n);
     nblk = (B + S - 1) / S;
     const dim3 g(nblk, clips);
-    const size_t sm = xt_buf_bytes(lg);
-    switch (lg) {
-      case 7: band_cols_reg<7, 32><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 8: band_cols_reg<8, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 9: band_cols_reg<9, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      default: band_cols_reg<10, 4><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+    const size_t sm = xt_buf_bytes(n);
+    switch (n) {
+      case 128: band_cols_reg<128, 32><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 160: band_cols_reg<160, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 192: band_cols_reg<192, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 256: band_cols_reg<256, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 512: band_cols_reg<512, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      default: band_cols_reg<1024, 4><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
     }
   } else {
+    if (!pow2) return cudaErrorInvalidValue;
     const int cpb = fit_units(4, 2 * (sizeof(float2) << lg));
     nblk = (B + cpb - 1) / cpb;
     const size_t sm2 = 2 * (static_cast<size_t>(cpb) << lg) * sizeof(float2);
@@ -605,30 +622,44 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   return cudaGetLastError();
 }
 
-// Whether the register-radix kernels (x-major band layout) apply to L = 2^lg
-// and band half-width hb: every one of them within the shared-memory budget.
-bool xt_ok(int lg, int hb) {
-  const int S = xt_S(lg);
-  if (S == 0 || 2 * hb >= (1 << lg)) return false;
+// Whether the register-radix kernels (x-major band layout) apply to length
+// L (128, 160, 192, 256, 512, 1024) and band half-width hb: every one of
+// them within the shared-memory budget.
+bool xt_ok(int L, int hb) {
+  const int S = xt_S(L);
+  if (S == 0 || 2 * hb >= L) return false;
   // the largest user: the column pass with two band buffers and two FFT buffers
   const size_t cols = 2 * static_cast<size_t>(S) * (2 * hb + 1) * sizeof(float2) +
-                      2 * static_cast<size_t>(fr_buf(1 << lg, S)) * sizeof(float2);
+                      2 * static_cast<size_t>(fr_buf(L, S)) * sizeof(float2);
   return cols <= static_cast<size_t>(kXtSmemMax);
 }
 
-// Rows of every (kernel, band row) product into T, x-major when xt_ok (the
-// layout socs_cols_x reads), else the [k][my][x] layout of socs_rows.
-cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+static int ilog2_exact(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return (1 << l) == v ? l : -1;
+}
+
+// Rows of every (kernel, band row) product into T on a grid of L points,
+// x-major when xt_ok (the layout socs_cols_x reads), else (L a power of two)
+// the [k][my][x] layout of socs_rows.
+cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int L, int clips,
                         float2* T, const float2* tw, cudaStream_t st) {
-  if (!xt_ok(lgm, hb)) return socs_rows(kband, scale, Mband, K, hb, lgm, clips, T, tw, st);
-  const int B = 2 * hb + 1, S = xt_S(lgm);
+  if (!xt_ok(L, hb)) {
+    const int lg = ilog2_exact(L);
+    if (lg < 0) return cudaErrorInvalidValue;
+    return socs_rows(kband, scale, Mband, K, hb, lg, clips, T, tw, st);
+  }
+  const int B = 2 * hb + 1, S = xt_S(L);
   const dim3 g((K * B + S - 1) / S, clips);
-  const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) + xt_buf_bytes(lgm);
-  switch (lgm) {
-    case 7: socs_rows_xt<7, 32><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
-    case 8: socs_rows_xt<8, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
-    case 9: socs_rows_xt<9, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
-    default: socs_rows_xt<10, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+  const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) + xt_buf_bytes(L);
+  switch (L) {
+    case 128: socs_rows_xt<128, 32><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 160: socs_rows_xt<160, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 192: socs_rows_xt<192, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 256: socs_rows_xt<256, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 512: socs_rows_xt<512, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    default: socs_rows_xt<1024, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
   }
   return cudaGetLastError();
 }
@@ -636,24 +667,30 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
 // Column pass over socs_rows_x's T (same lgm and hb).  mode 0: sum of |E_k|^2;
 // mode 1: synthesis of a real image from a Hermitian band (K = 1), two
 // columns per transform when xt_ok.
-cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st) {
-  if (!xt_ok(lgm, hb)) return socs_cols(T, K, hb, lgm, clips, keep, flare, mean, out, mode, tw, st);
-  const int B = 2 * hb + 1, S = xt_S(lgm), L = 1 << lgm;
+  if (!xt_ok(L, hb)) {
+    const int lg = ilog2_exact(L);
+    if (lg < 0) return cudaErrorInvalidValue;
+    return socs_cols(T, K, hb, lg, clips, keep, flare, mean, out, mode, tw, st);
+  }
+  const int B = 2 * hb + 1, S = xt_S(L);
   // band columns (mode 0: double-buffered) and the FFT buffers the passes use
   const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) * (mode == 0 ? 2 : 1) +
-                    (fr_passes(lgm) - 1) * static_cast<size_t>(fr_buf(L, S)) * sizeof(float2);
+                    (fr_passes(L) - 1) * static_cast<size_t>(fr_buf(L, S)) * sizeof(float2);
   const dim3 g(L / (mode == 0 ? S : 2 * S), clips);
-#define HUV_COLS_XT(LG, SS)                                                                                   \
+#define HUV_COLS_XT(LL, SS)                                                                                   \
   if (mode == 0)                                                                                            \
-    socs_cols_xt<LG, SS, 0><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw);                      \
+    socs_cols_xt<LL, SS, 0><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw);                      \
   else                                                                                                      \
-    socs_cols_xt<LG, SS, 1><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw);
-  switch (lgm) {
-    case 7: HUV_COLS_XT(7, 32) break;
-    case 8: HUV_COLS_XT(8, 16) break;
-    case 9: HUV_COLS_XT(9, 8) break;
-    default: HUV_COLS_XT(10, 4) break;
+    socs_cols_xt<LL, SS, 1><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw);
+  switch (L) {
+    case 128: HUV_COLS_XT(128, 32) break;
+    case 160: HUV_COLS_XT(160, 16) break;
+    case 192: HUV_COLS_XT(192, 16) break;
+    case 256: HUV_COLS_XT(256, 16) break;
+    case 512: HUV_COLS_XT(512, 8) break;
+    default: HUV_COLS_XT(1024, 4) break;
   }
 #undef HUV_COLS_XT
   return cudaGetLastError();
@@ -696,15 +733,14 @@ cudaError_t set_smem_limits() {
   const int xt = kXtSmemMax;
 #define HUV_XT_ATTR(K)                                                                    \
   if ((e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, xt))) return e;
-  HUV_XT_ATTR((socs_rows_xt<7, 32>)) HUV_XT_ATTR((socs_rows_xt<8, 16>))
-  HUV_XT_ATTR((socs_rows_xt<9, 8>)) HUV_XT_ATTR((socs_rows_xt<10, 4>))
-  HUV_XT_ATTR((socs_cols_xt<7, 32, 0>)) HUV_XT_ATTR((socs_cols_xt<8, 16, 0>))
-  HUV_XT_ATTR((socs_cols_xt<9, 8, 0>)) HUV_XT_ATTR((socs_cols_xt<10, 4, 0>))
-  HUV_XT_ATTR((socs_cols_xt<7, 32, 1>)) HUV_XT_ATTR((socs_cols_xt<8, 16, 1>))
-  HUV_XT_ATTR((socs_cols_xt<9, 8, 1>)) HUV_XT_ATTR((socs_cols_xt<10, 4, 1>))
-  HUV_XT_ATTR((band_cols_reg<7, 32>)) HUV_XT_ATTR((band_cols_reg<8, 16>))
-  HUV_XT_ATTR((band_cols_reg<9, 8>)) HUV_XT_ATTR((band_cols_reg<10, 4>))
-  HUV_XT_ATTR((band_rows_reg<10, 4>))
+#define HUV_XT_ALL(LL, SS)                                                                                \
+  HUV_XT_ATTR((socs_rows_xt<LL, SS>)) HUV_XT_ATTR((socs_cols_xt<LL, SS, 0>))                           \
+  HUV_XT_ATTR((socs_cols_xt<LL, SS, 1>)) HUV_XT_ATTR((band_cols_reg<LL, SS>))
+  HUV_XT_ALL(128, 32) HUV_XT_ALL(160, 16) HUV_XT_ALL(192, 16) HUV_XT_ALL(256, 16) HUV_XT_ALL(512, 8)
+  HUV_XT_ALL(1024, 4)
+  HUV_XT_ATTR((band_rows_reg<1024, 4>)) HUV_XT_ATTR((band_rows_reg<160, 16>))
+  HUV_XT_ATTR((band_rows_reg<192, 16>))
+#undef HUV_XT_ALL
 #undef HUV_XT_ATTR
   return cudaSuccess;
 }

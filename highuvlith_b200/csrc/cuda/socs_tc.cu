@@ -410,14 +410,14 @@ __global__ void socs_rows_tc(const float2* __restrict__ kband, float scale, cons
 // reads them as the zero-padded band, and the last pass writes the split
 // operand straight from registers (consecutive lanes = consecutive band rows
 // of one x, so each store covers contiguous words).
-// grid: (ceil(K * nrows / S), problems); block fr_threads(LG, S).
-template <int LG, int S>
-__global__ void __launch_bounds__(fr_threads(LG, S))
+// grid: (ceil(K * nrows / S), problems); block fr_threads(L, S).
+template <int L, int S>
+__global__ void __launch_bounds__(fr_threads(L, S))
     socs_rows_reg(const float2* __restrict__ kband, float scale, const float2* __restrict__ Mband, int K, int hb,
                   int row_off, int nrows, int kp, int zero_to, __nv_bfloat16* __restrict__ Bop,
                   const float2* __restrict__ tw) {
-  constexpr int L = 1 << LG, T = fr_threads(LG, S), NP = fr_passes(LG);
-  constexpr int R = fr_radix(LG, NP - 1);
+  constexpr int T = fr_threads(L, S), NP = fr_passes(L);
+  constexpr int R = fr_radix(L, NP - 1);
   extern __shared__ float2 smem[];
   const int B = 2 * hb + 1;
   const int prob = blockIdx.y;
@@ -443,20 +443,21 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
     }
   }
   __syncthreads();
-  fr_first_pass_band<LG, S, +1>(t, P, B, hb, b0);
+  fr_first_pass_band<L, S, +1>(t, P, B, hb, b0);
   __syncthreads();
   const float2* src = b0;
   if constexpr (NP == 3) {
-    fr_mid_pass<LG, S, +1, 1>(t, b0, b1, tw);
+    fr_mid_pass<L, S, +1, 1>(t, b0, b1, tw);
     __syncthreads();
     src = b1;
   }
   const size_t plane = static_cast<size_t>(L) * kp;
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
+  for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
+    if (t + b * T >= fr_nb(L, S, NP - 1)) break;
     int s, j;
     float2 v[R];
-    fr_last_pass<LG, S, +1>(t + b * T, src, tw, s, j, v);
+    fr_last_pass<L, S, +1>(t + b * T, src, tw, s, j, v);
     if (s >= nseq) continue;
     const int seq = seq0 + s;
     const int k = seq / nrows, myr = seq - k * nrows;
@@ -485,10 +486,10 @@ __global__ void __launch_bounds__(fr_threads(LG, S))
 }
 
 // Sequences per block of socs_rows_reg for L = 2^lg (0: no instance).
-constexpr int rows_reg_S(int lg) { return lg == 7 ? 32 : lg == 8 ? 16 : lg == 9 ? 8 : lg == 10 ? 4 : 0; }
-constexpr size_t rows_reg_smem(int lg, int B) {
-  return (static_cast<size_t>(rows_reg_S(lg)) * B +
-          (fr_passes(lg) - 1) * static_cast<size_t>(fr_buf(1 << lg, rows_reg_S(lg)))) *
+constexpr int rows_reg_S(int L) { return xt_S(L); }
+constexpr size_t rows_reg_smem(int L, int B) {
+  return (static_cast<size_t>(rows_reg_S(L)) * B +
+          (fr_passes(L) - 1) * static_cast<size_t>(fr_buf(L, rows_reg_S(L)))) *
          sizeof(float2);
 }
 
@@ -528,9 +529,10 @@ using namespace huv_dev;
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
                          const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
                          const uint8_t* row_digits, int* err);
-cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+bool xt_ok(int L, int hb);
+cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int L, int clips,
                         float2* T, const float2* tw, cudaStream_t st);
-cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 
 namespace {
@@ -609,21 +611,24 @@ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 // L = 128 .. 1024 (band within 110 KiB of shared memory), else the
 // shared-memory radix-4 kernel.
 void launch_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int row_off, int nrows,
-                 int lg, int kp, int zero_to, __nv_bfloat16* Bop, const float2* tw, int problems, cudaStream_t st) {
+                 int L, int kp, int zero_to, __nv_bfloat16* Bop, const float2* tw, int problems, cudaStream_t st) {
   const int B = 2 * hb + 1;
-  const int S = rows_reg_S(lg);
-  if (S > 0 && 2 * hb < (1 << lg) && rows_reg_smem(lg, B) <= 110 * 1024) {
+  const int S = rows_reg_S(L);
+  if (S > 0 && 2 * hb < L && rows_reg_smem(L, B) <= 110 * 1024) {
     const dim3 g((K * nrows + S - 1) / S, problems);
-    const size_t sm = rows_reg_smem(lg, B);
-    const int th = fr_threads(lg, S);
-    switch (lg) {
-      case 7: socs_rows_reg<7, 32><<<g, th, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
-      case 8: socs_rows_reg<8, 16><<<g, th, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
-      case 9: socs_rows_reg<9, 8><<<g, th, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
-      default: socs_rows_reg<10, 4><<<g, th, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+    const size_t sm = rows_reg_smem(L, B);
+    switch (L) {
+      case 128: socs_rows_reg<128, 32><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      case 160: socs_rows_reg<160, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      case 192: socs_rows_reg<192, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      case 256: socs_rows_reg<256, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      case 512: socs_rows_reg<512, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      default: socs_rows_reg<1024, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
     }
     return;
   }
+  int lg = 0;
+  while ((1 << lg) < L) ++lg;
   const int S8 = fit_units(8, 2 * (sizeof(float2) << lg));
   const dim3 g((K * nrows + S8 - 1) / S8, problems);
   const size_t sm = 2 * (static_cast<size_t>(S8) << lg) * sizeof(float2);
@@ -652,14 +657,12 @@ cudaError_t tc_set_smem() {
     return e;
   if ((e = cudaFuncSetAttribute(socs_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   const int reg_bytes = 110 * 1024;
-  if ((e = cudaFuncSetAttribute(socs_rows_reg<7, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes)))
+#define HUV_ROWS_ATTR(LL, SS)                                                                                \
+  if ((e = cudaFuncSetAttribute(socs_rows_reg<LL, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes))) \
     return e;
-  if ((e = cudaFuncSetAttribute(socs_rows_reg<8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes)))
-    return e;
-  if ((e = cudaFuncSetAttribute(socs_rows_reg<9, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes)))
-    return e;
-  if ((e = cudaFuncSetAttribute(socs_rows_reg<10, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, reg_bytes)))
-    return e;
+  HUV_ROWS_ATTR(128, 32) HUV_ROWS_ATTR(160, 16) HUV_ROWS_ATTR(192, 16) HUV_ROWS_ATTR(256, 16)
+  HUV_ROWS_ATTR(512, 8) HUV_ROWS_ATTR(1024, 4)
+#undef HUV_ROWS_ATTR
   return cudaSuccess;
 }
 
@@ -688,6 +691,13 @@ inline int ilog2i(int v) {
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 }  // namespace
 
+bool Engine::hybrid_supported(const DeviceSet& ds, int M) const {
+  const int kpI = ((2 * (2 * ds.hb + 1)) + 63) / 64 * 64;
+  const bool pow2 = (M & (M - 1)) == 0;
+  return n >= 128 && n % 128 == 0 && M <= n && kpI <= 192 && huv_launch::encode_fn() != nullptr &&
+         (pow2 || (huv_launch::xt_ok(M, ds.hb) && huv_launch::xt_ok(M, 2 * ds.hb)));
+}
+
 bool Engine::tc_supported(const DeviceSet& ds, int M) const {
   const int kpE = ((2 * ds.B) + 63) / 64 * 64;
   const int kpI = ((2 * (2 * ds.hb + 1)) + 63) / 64 * 64;
@@ -704,7 +714,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     check_cuda(tc_set_smem(), "cudaFuncSetAttribute(tc)");
     smem_set = true;
   }
-  const int lgn = ilog2i(n), lgm = ilog2i(M);
+  const int lgn = ilog2i(n), lgm = ilog2i(M);  // lgm: log2 of M rounded up (M need not be a power of two)
   const int B = ds.B, K = K_use > 0 ? K_use : ds.K, hb = ds.hb;
   const float* Wf = W_use ? W_use : ds.W;
   const int h2 = 2 * hb, B2 = 2 * h2 + 1;
@@ -715,8 +725,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   // 2 B columns: their tensor maps end at column 2 B, so TMA fills the rest
   // of the last 64-wide box with zeros instead of reading padding.
   const int kbE = kstE * 16, kbI = kstI * 16;
-  TcState& tc = ds.tc[lgm];
-  if (!tc.gy) {
+  TcState& tc = ds.tc[M];
+  if (!fft_field && !tc.gy) {
     // A_E: rows (y, re/im) over the M grid, K = (my, re/im).
     std::vector<double> ae(static_cast<size_t>(2 * M) * kcE);
     for (int y = 0; y < M; ++y)
@@ -730,6 +740,13 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
         im[2 * mi] = s;
         im[2 * mi + 1] = c;
       }
+    const auto pe = split_planes(ae, 2 * M, kcE, kpE);
+    check_cuda(cudaMalloc(&tc.gy, pe.size() * 2), "cudaMalloc(A_E)");
+    check_cuda(cudaMemcpy(tc.gy, pe.data(), pe.size() * 2, cudaMemcpyHostToDevice), "upload A_E");
+    if (!make_map(&tc.map_ae, tc.gy, 2ull * 2 * M, kpE, 128))
+      throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the DFT operands");
+  }
+  if (!tc.gx) {
     // A_I: rows y over the N grid, K = (qy >= 0, re/im), Hermitian weights.
     std::vector<double> ai(static_cast<size_t>(n) * kcI);
     for (int y = 0; y < n; ++y)
@@ -739,13 +756,10 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
         ai[static_cast<size_t>(y) * kcI + 2 * q] = w * std::cos(th);
         ai[static_cast<size_t>(y) * kcI + 2 * q + 1] = -w * std::sin(th);
       }
-    const auto pe = split_planes(ae, 2 * M, kcE, kpE);
     const auto pi = split_planes(ai, n, kcI, kpI);
-    check_cuda(cudaMalloc(&tc.gy, pe.size() * 2), "cudaMalloc(A_E)");
     check_cuda(cudaMalloc(&tc.gx, pi.size() * 2), "cudaMalloc(A_I)");
-    check_cuda(cudaMemcpy(tc.gy, pe.data(), pe.size() * 2, cudaMemcpyHostToDevice), "upload A_E");
     check_cuda(cudaMemcpy(tc.gx, pi.data(), pi.size() * 2, cudaMemcpyHostToDevice), "upload A_I");
-    if (!make_map(&tc.map_ae, tc.gy, 2ull * 2 * M, kpE, 128) || !make_map(&tc.map_ai, tc.gx, 2ull * n, kpI, 128))
+    if (!make_map(&tc.map_ai, tc.gx, 2ull * n, kpI, 128))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the DFT operands");
     tc.lgm = lgm;
   }
@@ -756,7 +770,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const size_t per_m = align256(sizeof(float2) * B * B);
   const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kbE * 2);
   const int rbn = B <= kRowBN ? kRowBN : kRowBNWide;  // rows of P (band rows my, padded)
-  if (B > kRowBNWide) throw Error(HUV_ERR_UNSUPPORTED, "TC form: band wider than 96 orders");
+  if (gemm_rows && B > kRowBNWide) throw Error(HUV_ERR_UNSUPPORTED, "TC form: band wider than 96 orders");
   const size_t per_p = gemm_rows ? align256(static_cast<size_t>(K) * 2 * rbn * kpE * 2) : 0;
   const size_t per_i = align256(sizeof(float) * M * M);
   const size_t per_x2 = align256(sizeof(float2) * M * B2);
@@ -783,8 +797,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   float2* C = reinterpret_cast<float2*>(take(per_c));
   __nv_bfloat16* BI = reinterpret_cast<__nv_bfloat16*>(take(per_bi));
   float* mean = reinterpret_cast<float*>(take(per_mean));
-  const float2* twn = twiddle(lgn);
-  const float2* twm = twiddle(lgm);
+  const float2* twn = twiddle_n(n);
+  const float2* twm = twiddle_n(M);
   const size_t smem_tc = tc_smem_bytes(3);
   for (int c0 = 0; c0 < b.n_clips; c0 += chunk) {
     const int nc = std::min(chunk, b.n_clips - c0);
@@ -809,17 +823,17 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       // sum lambda |E|^2 in registers, normalisation and flare -> IM
       float2* T = reinterpret_cast<float2*>(BE);
       prof.begin("socs_rows_inv", st);
-      check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");
+      check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "socs_rows");
       prof.end(st);
       prof.begin("socs_cols_inv", st);
-      check_cuda(socs_cols_x(T, K, hb, lgm, nc, ds.keep, ds.flare, mean, IM, 0, twm, st), "socs_cols");
+      check_cuda(socs_cols_x(T, K, hb, M, nc, ds.keep, ds.flare, mean, IM, 0, twm, st), "socs_cols");
       prof.end(st);
     }
     if (!fft_field) prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
     if (fft_field) {
     } else if (!gemm_rows) {
       // Row transforms as FP32 register-radix FFTs, emitting the split operand.
-      launch_rows(ds.kband, 0.f, Mb, K, hb, 0, B, lgm, kbE, 0, BE, twm, nc, st);
+      launch_rows(ds.kband, 0.f, Mb, K, hb, 0, B, M, kbE, 0, BE, twm, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc");
     } else {
       // Row transforms of every kernel's band product on tensor cores: the
@@ -881,7 +895,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     {
       prof.begin("socs_rows_tc<interp>", st);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
-      launch_rows(nullptr, scale, C, 1, h2, h2, nrI, lgn, kbI, 0, BI, twn, nc, st);
+      launch_rows(nullptr, scale, C, 1, h2, h2, nrI, n, kbI, 0, BI, twn, nc, st);
       check_cuda(cudaGetLastError(), "socs_rows_tc(interp)");
       prof.end(st);
     }

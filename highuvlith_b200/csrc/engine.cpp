@@ -32,9 +32,10 @@ cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int
                       float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
                       const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
-cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
+bool xt_ok(int L, int hb);
+cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int L, int clips,
                         float2* T, const float2* tw, cudaStream_t st);
-cudaError_t socs_cols_x(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 cudaError_t set_smem_limits();
 void tc_release(huv::TcState& tc);
@@ -259,10 +260,11 @@ void Engine::ensure_device() {
   device_ready = true;
 }
 
-const float2* Engine::twiddle(int lg) {
-  auto it = twiddles.find(lg);
+const float2* Engine::twiddle(int lg) { return twiddle_n(1 << lg); }
+
+const float2* Engine::twiddle_n(int L) {
+  auto it = twiddles.find(L);
   if (it != twiddles.end()) return it->second;
-  const int L = 1 << lg;
   std::vector<float2> h(L);
   for (int t = 0; t < L; ++t) {
     const double a = -2.0 * 3.14159265358979323846 * t / L;
@@ -271,7 +273,7 @@ const float2* Engine::twiddle(int lg) {
   float2* d = nullptr;
   check_cuda(cudaMalloc(&d, sizeof(float2) * L), "cudaMalloc(twiddle)");
   check_cuda(cudaMemcpy(d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice), "cudaMemcpy(twiddle)");
-  twiddles[lg] = d;
+  twiddles[L] = d;
   return d;
 }
 
@@ -409,24 +411,33 @@ void* Engine::workspace(size_t bytes) {
   return ws;
 }
 
-int Engine::choose_eval_grid(const DeviceSet& ds, int requested) const {
+int Engine::choose_eval_grid(const DeviceSet& ds, int requested, bool mixed) const {
   const int min_m = 4 * ds.hb + 1;
+  const bool mixed_ok = [&](int m) {
+    return (m == 160 || m == 192) && m <= n && huv_launch::xt_ok(m, ds.hb) && huv_launch::xt_ok(m, 2 * ds.hb);
+  }(requested);
   if (requested > 0) {
-    if ((requested & (requested - 1)) != 0 || requested > n || requested < min_m)
-      throw Error(HUV_ERR_INVALID_PARAMETER,
-                  "eval_grid: must be a power of two with 4h < M <= N (h = " + std::to_string(ds.hb) + ")");
+    if (((requested & (requested - 1)) != 0 && !(mixed && mixed_ok)) || requested > n || requested < min_m)
+      throw Error(HUV_ERR_INVALID_PARAMETER, "eval_grid: must be a power of two (or 160 / 192 for the FFT and "
+                                             "hybrid forms) with 4h < M <= N (h = " + std::to_string(ds.hb) + ")");
     return requested;
   }
   int m = 8;
   while (m < min_m) m <<= 1;
-  return std::min(m, n);
+  m = std::min(m, n);
+  if (mixed) {
+    // a register-radix length between 4h and the next power of two
+    for (int c : {160, 192})
+      if (c >= min_m && c < m && c < n && huv_launch::xt_ok(c, ds.hb) && huv_launch::xt_ok(c, 2 * ds.hb)) return c;
+  }
+  return m;
 }
 
 static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use,
                           const float* W_use) {
-  const int lgn = ilog2(n), lgm = ilog2(M);
+  const int lgn = ilog2(n), lgm = ilog2(M);  // lgm: rounded up where M is 160 or 192
   const int B = ds.B, K = K_use > 0 ? K_use : ds.K, hb = ds.hb;
   const float* Wf = W_use ? W_use : ds.W;
   const bool coarse = M < n;
@@ -456,8 +467,8 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
   float2* C = reinterpret_cast<float2*>(base + (per_x + per_m + per_t + per_i + per_x2) * chunk);
   float2* T2 = reinterpret_cast<float2*>(base + (per_x + per_m + per_t + per_i + per_x2 + per_c) * chunk);
   float* mean = reinterpret_cast<float*>(base + (per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2) * chunk);
-  const float2* twn = twiddle(lgn);
-  const float2* twm = twiddle(lgm);
+  const float2* twn = twiddle_n(n);
+  const float2* twm = twiddle_n(M);
   for (int c0 = 0; c0 < b.n_clips; c0 += chunk) {
     const int nc = std::min(chunk, b.n_clips - c0);
     const void* in = static_cast<const char*>(b.input) + in_elem * static_cast<size_t>(n) * n * c0;
@@ -473,10 +484,10 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
     prof.end(st);
     prof.launches += 2;
     prof.begin("socs_rows_inv", st);
-    check_cuda(huv_launch::socs_rows_x(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "socs_rows");
+    check_cuda(huv_launch::socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "socs_rows");
     prof.end(st);
     prof.begin("socs_cols_inv", st);
-    check_cuda(huv_launch::socs_cols_x(T, K, hb, lgm, nc, ds.keep, ds.flare, mean, coarse ? IM : o, 0, twm, st),
+    check_cuda(huv_launch::socs_cols_x(T, K, hb, M, nc, ds.keep, ds.flare, mean, coarse ? IM : o, 0, twm, st),
                "socs_cols");
     prof.end(st);
     prof.launches += 2;
@@ -488,8 +499,8 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
       prof.end(st);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
       prof.begin("interp_rows_cols", st);
-      check_cuda(huv_launch::socs_rows_x(nullptr, scale, C, 1, h2, lgn, nc, T2, twn, st), "socs_rows(interp)");
-      check_cuda(huv_launch::socs_cols_x(T2, 1, h2, lgn, nc, 1.f, 0.f, nullptr, o, 1, twn, st), "socs_cols(interp)");
+      check_cuda(huv_launch::socs_rows_x(nullptr, scale, C, 1, h2, n, nc, T2, twn, st), "socs_rows(interp)");
+      check_cuda(huv_launch::socs_cols_x(T2, 1, h2, n, nc, 1.f, 0.f, nullptr, o, 1, twn, st), "socs_cols(interp)");
       prof.end(st);
       prof.launches += 4;
     }
@@ -506,16 +517,21 @@ void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
   ensure_device();
   if (b.input_kind == HUV_INPUT_RECTS) upload_rects(b);
   DeviceSet& ds = device_set(b.defocus_nm == 0.0 ? 0.0 : b.defocus_nm);
-  const int M = choose_eval_grid(ds, b.eval_grid);
-  // The tensor-core form tiles the evaluation grid by 128; an automatically
-  // chosen grid below that is raised to 128 (still exact: any M > 4h is).
-  const int Mtc = (b.eval_grid == 0 && M < 128 && n >= 128) ? 128 : M;
   int form = b.form;
-  if (form == HUV_FORM_AUTO) form = tc_supported(ds, Mtc) ? HUV_FORM_HYBRID : HUV_FORM_FFT;
-  if (form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS || form == HUV_FORM_HYBRID) {
+  // FFT and hybrid forms evaluate on the smallest supported grid above 4h
+  // (160 or 192 where that beats the next power of two); the tcgen05
+  // y-contraction tiles the grid by 128, so its automatic grid is a power of
+  // two raised to 128 (still exact: any M > 4h is).
+  const int Mp2 = choose_eval_grid(ds, form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS ? b.eval_grid : 0);
+  const int Mtc = (b.eval_grid == 0 && Mp2 < 128 && n >= 128) ? 128 : Mp2;
+  const int M = (form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS) ? Mp2 : choose_eval_grid(ds, b.eval_grid, true);
+  if (form == HUV_FORM_AUTO) form = hybrid_supported(ds, M) ? HUV_FORM_HYBRID : HUV_FORM_FFT;
+  if (form == HUV_FORM_HYBRID) {
+    if (!hybrid_supported(ds, M)) throw Error(HUV_ERR_UNSUPPORTED, "hybrid form: unsupported band/grid for this build");
+    run_tc_form(b, ds, M, out, st, 0, nullptr, kTcCoreFftField);
+  } else if (form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS) {
     if (!tc_supported(ds, Mtc)) throw Error(HUV_ERR_UNSUPPORTED, "TC form: unsupported band/grid for this build");
-    run_tc_form(b, ds, Mtc, out, st, 0, nullptr,
-                form == HUV_FORM_TC_ROWS ? kTcCoreGemmRows : (form == HUV_FORM_HYBRID ? kTcCoreFftField : kTcCoreFftRows));
+    run_tc_form(b, ds, Mtc, out, st, 0, nullptr, form == HUV_FORM_TC_ROWS ? kTcCoreGemmRows : kTcCoreFftRows);
   } else if (form == HUV_FORM_FFT) {
     run_fft_form(b, ds, M, out, st);
   } else {

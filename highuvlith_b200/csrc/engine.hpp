@@ -47,7 +47,7 @@ struct IltOptState {
 };
 
 struct TcState {
-  int lgm = 0;          // evaluation grid the state was built for (log2)
+  int lgm = 0;          // evaluation grid the state was built for (log2, rounded up)
   void* gy = nullptr;   // A_E planes [2][2M][kpE] bf16
   void* gx = nullptr;   // A_I planes [2][N][kpI] bf16
   CUtensorMap map_ae, map_ai;
@@ -172,6 +172,8 @@ struct Engine {
   // device helpers
   void ensure_device();
   const float2* twiddle(int lg);
+  // Twiddle table exp(-2 pi i t / L), t < L, for any supported length L.
+  const float2* twiddle_n(int L);
   // Digit planes of the tensor-core row band of u8 rasters for band
   // half-width hb (NULL when that path does not apply to this grid, or when
   // HUV_MASK_ROWS=fft in the environment selects the FFT rows).
@@ -184,7 +186,11 @@ struct Engine {
   double* ilt_cost_dev = nullptr;
   int ilt_cost_cap = 0;
   IltOptState ilt_state;
-  int choose_eval_grid(const DeviceSet& ds, int requested) const;
+  // Evaluation grid M > 4h.  `mixed`: also the register-radix lengths 160
+  // and 192 (the FFT and hybrid forms), else powers of two only.
+  int choose_eval_grid(const DeviceSet& ds, int requested, bool mixed = false) const;
+  // Whether the hybrid form (FFT field pass on M, tcgen05 interpolation) serves M.
+  bool hybrid_supported(const DeviceSet& ds, int M) const;
   bool tc_supported(const DeviceSet& ds, int M) const;
   // K_use / W_use: kernel count and flare weights to use (0 / nullptr = the whole set).
   void run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use = 0,

@@ -122,13 +122,15 @@ std::vector<Choice> candidates(Engine* e, DeviceSet& ds) {
   while (m < 4 * ds.hb + 1) m <<= 1;
   m = std::min(m, n);
   const int mtc = std::max(m, 128);
-  if (mtc <= n && e->tc_supported(ds, mtc)) {
-    out.push_back(Choice{HUV_FORM_TC, mtc, 0});
-    out.push_back(Choice{HUV_FORM_HYBRID, mtc, 0});
-  }
+  // the FFT and hybrid forms may evaluate on a register-radix grid (160, 192)
+  // between 4h and the next power of two
+  const int mx = e->choose_eval_grid(ds, 0, true);
+  if (mtc <= n && e->tc_supported(ds, mtc)) out.push_back(Choice{HUV_FORM_TC, mtc, 0});
+  if (e->hybrid_supported(ds, mx)) out.push_back(Choice{HUV_FORM_HYBRID, mx, 0});
+  if (mx != m) out.push_back(Choice{HUV_FORM_FFT, mx, 0});
   out.push_back(Choice{HUV_FORM_FFT, m, 0});
   if (2 * m <= n && m < n) out.push_back(Choice{HUV_FORM_FFT, 2 * m, 0});
-  if (m < n && out.size() < 4) out.push_back(Choice{HUV_FORM_FFT, n, 0});
+  if (m < n && out.size() < 5) out.push_back(Choice{HUV_FORM_FFT, n, 0});
   return out;
 }
 
