@@ -423,18 +423,36 @@ def run_ours(args):
 
     # roofline of the dominant kernel
     hbm, tc_burst, tc_sus, peak_kind = peaks()
+    K, S = diag["num_kernels"], diag["num_frequencies"]
     # DRAM bytes (read + write) per clip of each timed region, from ncu
     # captures of this workload at 32 clips (cold cache, serialised;
     # profiles/socs_tc_and_fft_c2_traffic_32clips.md), scaled to a launch by
-    # its clips
+    # its clips.  FFT and hybrid forms on the 160-point grid, the TC form's
+    # y-contraction on 256.
     traffic_per_clip = {"tc_dft_gemm<sumsq>": (166.38e6 + 6.65e6) / 32,
                         "socs_rows_tc": (19.29e6 + 110.03e6) / 32,
-                        "tc_dft_gemm<interp>": (22.77e6 + 71.55e6) / 32,
-                        "mask_band": (33.82e6 + 19.74e6 + 0.01e6) / 32,
-                        "socs_cols_inv": (152.44e6 + 0.22e6) / 32,
-                        "socs_rows_inv": (2.91e6 + 90.31e6) / 32,
-                        "interp_rows_cols": (5.93e6 + 0.21e6 + 39.12e6 + 77.20e6) / 32}
-    K, S = diag["num_kernels"], diag["num_frequencies"]
+                        "tc_dft_gemm<interp>": (22.75e6 + 70.90e6) / 32,
+                        "mask_band": (33.82e6 + 19.75e6 + 0.01e6) / 32,
+                        "socs_cols_inv": (95.29e6 + 0.13e6) / 32,
+                        "socs_rows_inv": (2.87e6 + 33.84e6) / 32,
+                        "interp_band": (3.29e6 + 6.12e6) / 32,
+                        "interp_rows_cols": (5.73e6 + 39.09e6 + 77.49e6) / 32}
+    # each region's own algorithmic bytes per clip (operands in and out once)
+    hb_ = diag["band_half_width"]
+    Bb = 2 * hb_ + 1
+    m_p2 = 8
+    while m_p2 < 4 * hb_ + 1:
+        m_p2 *= 2
+    m_mix = next((c for c in (160, 192) if 4 * hb_ + 1 <= c < m_p2), m_p2)
+    m_tc = max(m_p2, 128)
+    m_f = m_tc if args.form in ("tc", "tc_rows") else m_mix
+    kb = 16 * ((2 * Bb + 15) // 16)
+    own_bytes = {"socs_cols_inv": 8 * K * Bb * m_f + 4 * m_f * m_f,
+                 "socs_rows_inv": 8 * K * Bb * m_f + 8 * Bb * Bb,
+                 "tc_dft_gemm<sumsq>": 4 * K * m_f * kb + 4 * m_f * m_f,
+                 "socs_rows_tc": 4 * K * m_f * kb + 8 * Bb * Bb,
+                 "tc_dft_gemm<interp>": 4 * N_GRID * N_GRID + 4 * N_GRID * kb,
+                 "mask_band": N_GRID * N_GRID + 16 * N_GRID * Bb + 8 * Bb * Bb}
     bytes_per_image = 4 * N_GRID ** 2 + 4 * N_GRID ** 2 + 8 * K * S
     launches = max(prof["launches"], 1)
     per_launch_s = prof["ms"] / launches / 1e3
@@ -453,6 +471,11 @@ def run_ours(args):
                         "region's mean launch time (CUDA events on the launching stream)",
                 "regions": {k: {"launches": v[0], "ms": v[1], "share": v[1] / total_ms if total_ms > 0 else None}
                             for k, v in prof["regions"].items()}}
+    if prof["kernel"] in own_bytes and per_launch_s > 0:
+        kb_s = own_bytes[prof["kernel"]] * images_per_launch / per_launch_s / 1e9
+        roofline["kernel_own"] = {"algorithmic_bytes_per_clip": own_bytes[prof["kernel"]], "achieved": kb_s,
+                                  "unit": "GB/s", "frac": kb_s / hbm, "eval_grid": m_f,
+                                  "note": "the dominant region's own operands (in and out once) / its mean launch time"}
     gi = prof["regions"].get("tc_dft_gemm<interp>")
     if gi and gi[1] > 0:
         # the band interpolation on tensor cores: a real N x N x 2(2h2+1)
