@@ -197,11 +197,12 @@ __global__ void __launch_bounds__(fr_threads(L, S))
   float2* oth = NP == 3 ? b0 : b1;
   const float add = sums ? flare_over_n * static_cast<float>(sums[mask * 2 + 1]) : 0.f;
   const float* Gm = G + static_cast<size_t>(mask) * L * L;
-  float g[16];
+  constexpr int NB = fr_per(L, S, NP - 1);  // last-pass butterflies per thread
+  float g[NB * R];
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
+  for (int b = 0; b < NB; ++b) {
     const int u = t + b * T;
-    const int s = u % S, j = u / S;
+    const int s = u % S, j = (u / S) % (L / R);  // guarded butterflies read a valid row
 #pragma unroll
     for (int p = 0; p < R; ++p)
       g[b * R + p] = keep * Gm[static_cast<size_t>(j + p * (L / R)) * L + x0 + s] + add;
@@ -231,7 +232,8 @@ __global__ void __launch_bounds__(fr_threads(L, S))
       __syncthreads();
     }
 #pragma unroll
-    for (int b = 0; b < 16 / R; ++b) {
+    for (int b = 0; b < NB; ++b) {
+      if (t + b * T >= fr_nb(L, S, NP - 1)) break;
       int s, j;
       float2 v[R];
       fr_last_pass<L, S, +1>(t + b * T, inv, tw, s, j, v);
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(fr_threads(L, S))
       }
     }
     __syncthreads();
-    {
+    if (t < fr_nb(L, S, 0)) {
       const int s = t % S, j = t / S;
       float2 v[16];
 #pragma unroll
@@ -258,7 +260,8 @@ __global__ void __launch_bounds__(fr_threads(L, S))
     }
     float2* Vk = V + (static_cast<size_t>(mask) * K + k) * B * L + x0;
 #pragma unroll
-    for (int b = 0; b < 16 / R; ++b) {
+    for (int b = 0; b < NB; ++b) {
+      if (t + b * T >= fr_nb(L, S, NP - 1)) break;
       int s, j;
       float2 v[R];
       fr_last_pass<L, S, -1>(t + b * T, cur, tw, s, j, v);
@@ -285,6 +288,105 @@ __global__ void hermitian_part(float2* __restrict__ Q, int B, int masks) {
     const float2 h = make_float2(0.5f * (a.x + c.x), 0.5f * (a.y - c.y));
     q[i] = h;
     q[j] = make_float2(h.x, -h.y);
+  }
+}
+
+// ilt_rows_adj with register-radix passes: CTA per (mask, band row my'),
+// kernels taken S at a time as the S sequences of one transform (rows of V
+// read straight from global memory in the first pass), forward FFT_x, and
+// for each kept order conj(kappa_k) . value summed over the lanes that hold
+// the same order (warp shuffles), then over the batches in registers.
+// grid: (B, masks); shared: two FFT buffers.
+template <int L, int S>
+__global__ void __launch_bounds__(fr_threads(L, S))
+    ilt_rows_adj_xt(const float2* __restrict__ V, const float2* __restrict__ kband, int K, int hb,
+                    float2* __restrict__ Q, const float2* __restrict__ tw) {
+  constexpr int T = fr_threads(L, S), NP = fr_passes(L);
+  constexpr int R = fr_radix(L, NP - 1);
+  constexpr int NB = fr_per(L, S, NP - 1);
+  constexpr int G = S < 32 ? S : 32;  // lanes of one order within a warp
+  static_assert(32 % S == 0 || S % 32 == 0, "the lanes of one order must form a shuffle group");
+  static_assert(fr_nb(L, S, NP - 1) % T == 0, "last-pass butterflies must fill every thread (warp-uniform)");
+  extern __shared__ float2 smem[];
+  const int B = 2 * hb + 1;
+  const int mask = blockIdx.y, my = blockIdx.x;
+  const int t = threadIdx.x;
+  float2* b0 = smem;
+  float2* b1 = b0 + fr_buf(L, S);
+  float2 acc[NB * R];
+#pragma unroll
+  for (int i = 0; i < NB * R; ++i) acc[i] = make_float2(0.f, 0.f);
+  for (int k0 = 0; k0 < K; k0 += S) {
+    if (t < fr_nb(L, S, 0)) {
+      const int s = t % S, j = t / S;
+      const bool live = k0 + s < K;
+      const float2* row = V + ((static_cast<size_t>(mask) * K + (live ? k0 + s : 0)) * B + my) * L + j;
+      float2 v[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = live ? row[r * (L / 16)] : make_float2(0.f, 0.f);
+      fr_first_pass_vals<L, S, -1>(t, v, b0);
+    }
+    __syncthreads();
+    const float2* cur = b0;
+    if constexpr (NP == 3) {
+      fr_mid_pass<L, S, -1, 1>(t, b0, b1, tw);
+      __syncthreads();
+      cur = b1;
+    }
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      int s, j;
+      float2 v[R];
+      fr_last_pass<L, S, -1>(t + b * T, cur, tw, s, j, v);
+      const int k = k0 + s;
+#pragma unroll
+      for (int p = 0; p < R; ++p) {
+        const int idx = j + p * (L / R);
+        const int mi = idx <= hb ? idx + hb : (idx >= L - hb ? idx - L + hb : -1);
+        float2 w = make_float2(0.f, 0.f);
+        if (mi >= 0 && k < K) {
+          const float2 u = kband[(static_cast<size_t>(k) * B + my) * B + mi];
+          w = make_float2(u.x * v[p].x + u.y * v[p].y, u.x * v[p].y - u.y * v[p].x);  // conj(u) v
+        }
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) {
+          w.x += __shfl_xor_sync(0xffffffffu, w.x, o);
+          w.y += __shfl_xor_sync(0xffffffffu, w.y, o);
+        }
+        acc[b * R + p].x += w.x;
+        acc[b * R + p].y += w.y;
+      }
+    }
+    __syncthreads();
+  }
+  // with S > 32 an order's S lanes span S / 32 warps: they are summed in
+  // shared memory (b0 is free after the final barrier)
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const int u = t + b * T;
+    const int s = u % S, j = u / S;
+    if (s % G != 0) continue;
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      const int idx = j + p * (L / R);
+      const int mi = idx <= hb ? idx + hb : (idx >= L - hb ? idx - L + hb : -1);
+      if (mi < 0) continue;
+      if (S <= 32) {
+        Q[(static_cast<size_t>(mask) * B + my) * B + mi] = acc[b * R + p];
+      } else {
+        b0[(s / G) * L + idx] = acc[b * R + p];
+      }
+    }
+  }
+  if constexpr (S > 32) {
+    __syncthreads();
+    for (int idx = t; idx < L; idx += T) {
+      const int mi = idx <= hb ? idx + hb : (idx >= L - hb ? idx - L + hb : -1);
+      if (mi < 0) continue;
+      float2 a = make_float2(0.f, 0.f);
+      for (int g = 0; g < S / G; ++g) a = fr_add(a, b0[g * L + idx]);
+      Q[(static_cast<size_t>(mask) * B + my) * B + mi] = a;
+    }
   }
 }
 
@@ -583,6 +685,16 @@ cudaError_t ilt_set_smem() {
     return e;
   if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<1024, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
     return e;
+#define HUV_ILT_XT(LL, SS)                                                                                   \
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_rows_adj_xt<LL, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt))) \
+    return e;
+  HUV_ILT_XT(128, 32) HUV_ILT_XT(160, 16) HUV_ILT_XT(192, 16) HUV_ILT_XT(256, 16) HUV_ILT_XT(512, 8)
+  HUV_ILT_XT(1024, 4)
+#undef HUV_ILT_XT
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<160, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+    return e;
+  if ((e = cudaFuncSetAttribute(huv_dev::ilt_cols_adj_xt<192, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, xt)))
+    return e;
   return cudaSuccess;
 }
 
@@ -633,12 +745,15 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   const int K = ds.K, hb = ds.hb, B = ds.B;
   const int h2 = 2 * hb, B2 = 2 * h2 + 1;
   const int lgn = ilog2i(n);
-  const int M = choose_eval_grid(ds, 0);
-  const int lgm = ilog2i(M);
+  // the smallest supported grid above 4h: 160 or 192 where the register-radix
+  // forward and adjoint kernels serve it, else a power of two
+  int M = choose_eval_grid(ds, 0, true);
+  if ((M & (M - 1)) != 0 && ilt_adj_xt_smem(M, hb) > static_cast<size_t>(kXtSmemMax)) M = choose_eval_grid(ds, 0);
+  const int lgm = ilog2i(M);  // rounded up where M is 160 or 192 (radix-4 paths are not used then)
   const bool coarse = M < n;
   const size_t npix = static_cast<size_t>(n) * n, mpix = static_cast<size_t>(M) * M;
-  const float2* twn = twiddle(lgn);
-  const float2* twm = twiddle(lgm);
+  const float2* twn = twiddle_n(n);
+  const float2* twm = twiddle_n(M);
   const float flare = ds.flare, keep = ds.keep;
   // Per-mask workspace.
   const size_t s_t = a256(sizeof(float) * npix);           // transmittance, then dC/dm
@@ -740,22 +855,30 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
         const dim3 ga(M / xt_S(M), nc);
         const size_t sm = ilt_adj_xt_smem(M, hb);
         const float fo = flare / static_cast<float>(npix);
+        const dim3 gr(B, nc);
+        const size_t smr = 2 * static_cast<size_t>(fr_buf(M, xt_S(M))) * sizeof(float2);
+#define HUV_ILT_ADJ(LL, SS)                                                                 \
+  ilt_cols_adj_xt<LL, SS><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm);    \
+  ilt_rows_adj_xt<LL, SS><<<gr, 256, smr, st>>>(V, ds.kband, K, hb, Q, twm);
         switch (M) {
-          case 128: ilt_cols_adj_xt<128, 32><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
-          case 256: ilt_cols_adj_xt<256, 16><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
-          case 512: ilt_cols_adj_xt<512, 8><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
-          default: ilt_cols_adj_xt<1024, 4><<<ga, 256, sm, st>>>(T, Gm, K, hb, keep, sums, fo, V, twm); break;
+          case 128: HUV_ILT_ADJ(128, 32) break;
+          case 160: HUV_ILT_ADJ(160, 16) break;
+          case 192: HUV_ILT_ADJ(192, 16) break;
+          case 256: HUV_ILT_ADJ(256, 16) break;
+          case 512: HUV_ILT_ADJ(512, 8) break;
+          default: HUV_ILT_ADJ(1024, 4) break;
         }
+#undef HUV_ILT_ADJ
       } else {
         const int Wc = fit_units(8, 2 * (sizeof(float2) << lgm) + (sizeof(float) << lgm));
         const size_t sm = 2 * (static_cast<size_t>(Wc) << lgm) * sizeof(float2) +
                           (static_cast<size_t>(Wc) << lgm) * sizeof(float);
         ilt_cols_adj<<<dim3(M / Wc, nc), 256, sm, st>>>(T, Gm, K, hb, lgm, Wc, keep, sums,
                                                         flare / static_cast<float>(npix), V, twm);
+        const int S = fit_units(4, 2 * (sizeof(float2) << lgm));
+        const size_t sm2 = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
+        ilt_rows_adj<<<dim3(B, nc), 256, sm2, st>>>(V, ds.kband, K, hb, lgm, S, Q, twm);
       }
-      const int S = fit_units(4, 2 * (sizeof(float2) << lgm));
-      const size_t sm2 = 2 * (static_cast<size_t>(S) << lgm) * sizeof(float2);
-      ilt_rows_adj<<<dim3(B, nc), 256, sm2, st>>>(V, ds.kband, K, hb, lgm, S, Q, twm);
       const float scale = static_cast<float>(2.0 * (1.0 - p.absorber) * p.weight) * grid_scale;
       // Re IFFT(Q) = IFFT(Hermitian part of Q): a real synthesis, two
       // columns per transform on the register-radix path
