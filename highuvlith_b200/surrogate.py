@@ -147,7 +147,7 @@ def train_timed(fno: FnoSurrogate, pairs: PairSource, pairs_total: int, batch: i
     torch.cuda.synchronize()
     el = time.perf_counter() - t0
     return losses, {"steps": steps, "pairs": steps * batch, "elapsed_s": el, "pairs_per_s": steps * batch / el,
-                    "host_wait_s": t_gen}
+                    "pair_s": t_gen}
 
 
 def relative_image_error(fno: FnoSurrogate, engine: SimulationEngine, masks) -> np.ndarray:

@@ -123,6 +123,26 @@ def test_u8_levels_tensor_rows_match_fft_rows_and_oracle(form, monkeypatch):
                 assert rel_err(a[c], ref) < tol, (n, c, rel_err(a[c], ref))
 
 
+@pytest.mark.parametrize("form", ["fft", "hybrid"])
+@pytest.mark.parametrize("eval_grid", [160, 192])
+def test_mixed_radix_eval_grids_match_oracle(form, eval_grid):
+    """Evaluation on the mixed-radix 160 (16 x 10) and 192 (16 x 12) point
+    grids, requested explicitly, against the FP64 oracle on the full grid."""
+    torch = _torch()
+    case = SMALL[3]  # EUV quasar on 256^2
+    _, src, opt, grid, kmax, fill, oopt = case
+    eng = HB.SimulationEngine(src, opt, grid=grid, max_kernels=kmax)
+    oeng = _oracle_engine(fill, oopt, grid, src.wavelength_nm, kmax)
+    n = grid.size
+    _, rasters = gen_batch(3, n, base_seed=17, wmin=6, wmax=32, dmin=0.2, dmax=0.6)
+    d = torch.from_numpy(rasters).cuda()
+    out = eng.compute_batch(d, form=form, eval_grid=eval_grid).cpu().numpy()
+    tol = 1e-5 if form == "fft" else 1e-4
+    for c in range(3):
+        ref = oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[c]))
+        assert rel_err(out[c], ref) < tol, (c, rel_err(out[c], ref))
+
+
 def test_clear_and_dark_masks():
     """Clear mask images to 1 (flare keeps it 1); an opaque mask to 0."""
     torch = _torch()
