@@ -392,4 +392,11 @@ __host__ __device__ __forceinline__ void fr_last_pass_pre(int u, const float2* s
   fr_dft<R, DIR>(v);
 }
 
+// Scale of the coarse intensity while it is carried in FP16 split planes by
+// the separable band interpolation: planes hold I / s with s = 16 mean(I),
+// so their scale does not depend on the normalisation, and a non-negative
+// band-limited image on M^2 points (max <= M^2 mean) stays below M^2 / 16
+// (2304 at M = 192), far inside FP16's range.
+__device__ __forceinline__ float interp_scale(float mean) { return 16.f * fmaxf(mean, 1e-20f); }
+
 }  // namespace huv_dev

@@ -16,6 +16,7 @@
 // sqrt(lambda_k / divisor) / N^2, so |E|^2 sums directly to the normalised
 // image.  The flare mean is computed exactly from the band by Parseval:
 // mean(I0) = sum_f W(f) |M(f)|^2 with W = sum_k lambda_k |u_k|^2 / N^4.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -301,11 +302,15 @@ __global__ void __launch_bounds__(fr_threads(L, S))
 // registers across k.  MODE 1 (band synthesis of a real image, K = 1): two
 // columns per sequence, z = T(., x0 + 2s) + i T(., x0 + 2s + 1); each column
 // is Hermitian in my, so Re and Im of the transform are the two real
-// columns.  grid: (L / (S or 2 S), clips); out: [clip][L][L].
+// columns.  grid: (L / (S or 2 S), clips); out: [clip][L][L].  MODE 0 with
+// `split` set writes v = I / interp_scale(mean) as two FP16 planes instead
+// (hi, and lo = the rounding remainder), [clip][plane][L][L]: the B operand
+// of the separable band interpolation on tensor cores.
 template <int L, int S, int MODE>
 __global__ void __launch_bounds__(fr_threads(L, S), 2)
     socs_cols_xt(const float2* __restrict__ Tt, int K, int hb, float keep, float flare,
-                 const float* __restrict__ mean, float* __restrict__ out, const float2* __restrict__ tw) {
+                 const float* __restrict__ mean, float* __restrict__ out, const float2* __restrict__ tw,
+                 __half* __restrict__ split) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
   constexpr int R = fr_radix(L, NP - 1);
   constexpr int XS = MODE == 1 ? 2 * S : S;
@@ -382,6 +387,7 @@ __global__ void __launch_bounds__(fr_threads(L, S), 2)
     __syncthreads();
   }
   const float add = (MODE == 0 && mean) ? flare * mean[clip] : 0.f;
+  const float inv = (MODE == 0 && split) ? 1.f / interp_scale(mean ? mean[clip] : 0.f) : 1.f;
   float* oc = out + static_cast<size_t>(clip) * L * L;
 #pragma unroll
   for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
@@ -391,7 +397,13 @@ __global__ void __launch_bounds__(fr_threads(L, S), 2)
 #pragma unroll
     for (int p = 0; p < R; ++p) {
       const size_t y = static_cast<size_t>(j + p * (L / R));
-      if (MODE == 0)
+      if (MODE == 0 && split) {
+        const float v = (keep * acc[b * R + p] + add) * inv;
+        const __half hi = __float2half_rn(v);
+        __half* sc = split + static_cast<size_t>(clip) * 2 * L * L + y * L + x0 + s;
+        sc[0] = hi;
+        sc[static_cast<size_t>(L) * L] = __float2half_rn(v - __half2float(hi));
+      } else if (MODE == 0)
         oc[y * L + x0 + s] = keep * acc[b * R + p] + add;
       else
         *reinterpret_cast<float2*>(oc + y * L + x0 + 2 * s) = res[b * R + p];
@@ -664,16 +676,9 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
   return cudaGetLastError();
 }
 
-// Column pass over socs_rows_x's T (same lgm and hb).  mode 0: sum of |E_k|^2;
-// mode 1: synthesis of a real image from a Hermitian band (K = 1), two
-// columns per transform when xt_ok.
-cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
-                        const float* mean, float* out, int mode, const float2* tw, cudaStream_t st) {
-  if (!xt_ok(L, hb)) {
-    const int lg = ilog2_exact(L);
-    if (lg < 0) return cudaErrorInvalidValue;
-    return socs_cols(T, K, hb, lg, clips, keep, flare, mean, out, mode, tw, st);
-  }
+namespace {
+cudaError_t cols_xt(const float2* T, int K, int hb, int L, int clips, float keep, float flare, const float* mean,
+                    float* out, int mode, const float2* tw, cudaStream_t st, __half* split) {
   const int B = 2 * hb + 1, S = xt_S(L);
   // band columns (mode 0: double-buffered) and the FFT buffers the passes use
   const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) * (mode == 0 ? 2 : 1) +
@@ -681,9 +686,9 @@ cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float 
   const dim3 g(L / (mode == 0 ? S : 2 * S), clips);
 #define HUV_COLS_XT(LL, SS)                                                                                   \
   if (mode == 0)                                                                                            \
-    socs_cols_xt<LL, SS, 0><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw);                      \
+    socs_cols_xt<LL, SS, 0><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw, split);               \
   else                                                                                                      \
-    socs_cols_xt<LL, SS, 1><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw);
+    socs_cols_xt<LL, SS, 1><<<g, 256, sm, st>>>(T, K, hb, keep, flare, mean, out, tw, nullptr);
   switch (L) {
     case 128: HUV_COLS_XT(128, 32) break;
     case 160: HUV_COLS_XT(160, 16) break;
@@ -694,6 +699,29 @@ cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float 
   }
 #undef HUV_COLS_XT
   return cudaGetLastError();
+}
+}  // namespace
+
+// Column pass over socs_rows_x's T (same lgm and hb).  mode 0: sum of |E_k|^2;
+// mode 1: synthesis of a real image from a Hermitian band (K = 1), two
+// columns per transform when xt_ok.
+cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
+                        const float* mean, float* out, int mode, const float2* tw, cudaStream_t st) {
+  if (!xt_ok(L, hb)) {
+    const int lg = ilog2_exact(L);
+    if (lg < 0) return cudaErrorInvalidValue;
+    return socs_cols(T, K, hb, lg, clips, keep, flare, mean, out, mode, tw, st);
+  }
+  return cols_xt(T, K, hb, L, clips, keep, flare, mean, out, mode, tw, st, nullptr);
+}
+
+// socs_cols_x mode 0 writing (keep * sum |E_k|^2 + flare * mean) / s, s =
+// interp_scale(mean), as split FP16 planes [clip][2][L][L] (half elements at
+// `split`).  Needs xt_ok(L, hb) and the per-clip mean.
+cudaError_t socs_cols_split(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
+                            const float* mean, void* split, const float2* tw, cudaStream_t st) {
+  if (!xt_ok(L, hb) || !mean) return cudaErrorInvalidValue;
+  return cols_xt(T, K, hb, L, clips, keep, flare, mean, nullptr, 0, tw, st, static_cast<__half*>(split));
 }
 
 cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,

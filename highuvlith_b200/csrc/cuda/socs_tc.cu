@@ -22,6 +22,7 @@
 // in-flight work with bounded waits, frees tensor memory and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 #include <stdint.h>
@@ -74,6 +75,10 @@ struct TcGemmParams {
   int bop_cols;         // band rows my written (2 bop_cols <= bop_ld)
   // MODE 1: 1 = store the output tiles with TMA (tmO) through shared memory
   int out_tma;
+  // MODE 3: problems in all; CTA z takes problems z G .. z G + G - 1
+  int nprob;
+  // A and B are FP16 planes (else BF16); MODE 3 always
+  int f16;
 };
 
 __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
@@ -101,7 +106,12 @@ __host__ __device__ constexpr size_t tc_smem_bytes(int kboxes, int bn = kTcBN, b
 // next GEMM's operand: bop[g][plane][x][2 my + re/im]; grid as MODE 1.
 // MODE 1 with p.out_tma: each epilogue warp stages 32 x 32 tiles in shared
 // memory (128B swizzle, double-buffered) and stores them with TMA through
-// tmO, a [problems * a_rows][out_ld] f32 map with 32 x 32 boxes.
+// tmO, a [problems * a_rows][out_ld] f32 map with 32 x 32 boxes; MODE 1 with
+// p.mean multiplies the tile by interp_scale(mean[problem]).  MODE 3: step g
+// is problem z G + g (the A tile stays resident across problems); the
+// accumulator tile (rows of A, columns n_tile BN + j) is split into FP16
+// hi/lo and stored row by row as bop[problem][plane][row][col] (half
+// elements); grid: (column tiles, a_rows / 128, ceil(nprob / G)).
 template <int MODE, int BN = kTcBN>
 __global__ void __launch_bounds__(192, 1)
     tc_dft_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -126,6 +136,8 @@ __global__ void __launch_bounds__(192, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n_tile = blockIdx.x, m_tile = blockIdx.y, prob = blockIdx.z;
+  // steps of this CTA (MODE 3: the last group of problems may be short)
+  const int G = MODE == 3 ? min(p.G, p.nprob - prob * p.G) : p.G;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kTcStages; ++s) {
@@ -164,7 +176,7 @@ __global__ void __launch_bounds__(192, 1)
         for (int kb = 0; kb < p.kboxes; ++kb)
           tma_load_2d(sA + (part * p.kboxes + kb) * kABox, &tmA, kb * 64, part * p.a_rows + m_tile * 128, a_full);
       int it = 0;
-      for (int g = 0; g < p.G && !*abort_flag; ++g) {
+      for (int g = 0; g < G && !*abort_flag; ++g) {
         for (int kb = 0; kb < p.kboxes; ++kb, ++it) {
           const int s = it % kTcStages;
           const uint32_t ph = (it / kTcStages) & 1;
@@ -185,12 +197,12 @@ __global__ void __launch_bounds__(192, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = idesc_bf16(128, BN);
+      const uint32_t idesc = (MODE == 3 || p.f16) ? idesc_f16(128, BN) : idesc_bf16(128, BN);
       bool ok = mbar_wait(a_full, 0, kWaitLimitNs);
       if (!ok) fail(2);
       tc_fence_after();
       int it = 0;
-      for (int g = 0; g < p.G && ok && !*abort_flag; ++g) {
+      for (int g = 0; g < G && ok && !*abort_flag; ++g) {
         const int buf = g & 1;
         if (!mbar_wait(&tempty[buf], ((g >> 1) & 1) ^ 1, kWaitLimitNs)) {
           fail(3);
@@ -243,7 +255,8 @@ __global__ void __launch_bounds__(192, 1)
     const int odd = lane & 1;
     bool ok = true;
     int nst = 0;  // MODE 1 TMA-store tiles issued by this warp
-    for (int g = 0; g < p.G; ++g) {
+    const float osc = (MODE == 1 && p.mean) ? interp_scale(p.mean[prob]) : 1.f;
+    for (int g = 0; g < G; ++g) {
       const int buf = g & 1;
       // Warp-uniform outcome: tcgen05.ld below is .sync.aligned.
       const bool got = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (g >> 1) & 1, kWaitLimitNs));
@@ -287,10 +300,41 @@ __global__ void __launch_bounds__(192, 1)
         }
         __syncwarp();
       }
+      if (MODE == 3) {
+        // one accumulator row per lane: row X of problem prob G + g
+        const long long X = m_tile * 128 + row;
+        __half* hi = reinterpret_cast<__half*>(p.bop) + (static_cast<long long>(prob) * p.G + g) * p.bop_prob +
+                     X * p.bop_ld + n_tile * BN;
+        __half* lo = hi + p.bop_plane;
 #pragma unroll
-      for (int c0 = 0; c0 < (MODE == 2 ? 0 : BN); c0 += 32) {
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+          float v[16];
+          tmem_ld16(taddr + c0, v);
+          uint32_t hw[8], lw[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const __half2 h2 = __floats2half2_rn(v[2 * i], v[2 * i + 1]);
+            const float2 hf = __half22float2(h2);
+            const __half2 l2 = __floats2half2_rn(v[2 * i] - hf.x, v[2 * i + 1] - hf.y);
+            hw[i] = *reinterpret_cast<const uint32_t*>(&h2);
+            lw[i] = *reinterpret_cast<const uint32_t*>(&l2);
+          }
+          uint4* hq = reinterpret_cast<uint4*>(hi + c0);
+          uint4* lq = reinterpret_cast<uint4*>(lo + c0);
+          hq[0] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+          hq[1] = make_uint4(hw[4], hw[5], hw[6], hw[7]);
+          lq[0] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+          lq[1] = make_uint4(lw[4], lw[5], lw[6], lw[7]);
+        }
+      }
+#pragma unroll
+      for (int c0 = 0; c0 < (MODE >= 2 ? 0 : BN); c0 += 32) {
         float v[32];
         tmem_ld32(taddr + c0, v);
+        if (MODE == 1 && p.mean) {
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v[i] *= osc;
+        }
         if (MODE == 0) {
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
@@ -534,6 +578,8 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
                         float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
+cudaError_t socs_cols_split(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
+                            const float* mean, void* split, const float2* tw, cudaStream_t st);
 
 namespace {
 
@@ -552,15 +598,17 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // 2-D bf16 tensor map over a K-major [rows][kp] array, box 64 x box_rows, 128B swizzle.
 // With cols > 0 the map ends at column cols (< kp): TMA fills the columns
 // beyond it with zeros instead of reading them.
-bool make_map(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_rows, int cols = 0) {
+bool make_map(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_rows, int cols = 0,
+              bool f16 = false) {
   auto fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols > 0 ? cols : kp), rows};
   cuuint64_t strides[1] = {static_cast<cuuint64_t>(kp) * 2};
   cuuint32_t box[2] = {64, static_cast<cuuint32_t>(box_rows)};
   cuuint32_t estr[2] = {1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  return fn(map, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr),
+            dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -589,6 +637,21 @@ float host_bf16_to_f(uint16_t h) {
   float f;
   std::memcpy(&f, &u, 4);
   return f;
+}
+
+// FP16 split planes [2][rows][kp] (hi, lo = the FP32 remainder rounded to FP16)
+// of a real matrix given row-major values [rows][kc].
+std::vector<uint16_t> split_planes_f16(const std::vector<double>& v, int rows, int kc, int kp) {
+  std::vector<uint16_t> out(2 * static_cast<size_t>(rows) * kp, 0);
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < kc; ++c) {
+      const float f = static_cast<float>(v[static_cast<size_t>(r) * kc + c]);
+      const __half hi = __float2half_rn(f);
+      const __half lo = __float2half_rn(f - __half2float(hi));
+      out[static_cast<size_t>(r) * kp + c] = static_cast<__half_raw>(hi).x;
+      out[(static_cast<size_t>(rows) + r) * kp + c] = static_cast<__half_raw>(lo).x;
+    }
+  return out;
 }
 
 // Split planes [2][rows][kp] of a real matrix given row-major values [rows][kc].
@@ -655,6 +718,15 @@ cudaError_t tc_set_smem() {
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<2, kRowBNWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, kRowBNWide, true)))))
     return e;
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, 64)))))
+    return e;
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 80>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, 80)))))
+    return e;
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 96>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, 96)))))
+    return e;
   if ((e = cudaFuncSetAttribute(socs_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   const int reg_bytes = 110 * 1024;
 #define HUV_ROWS_ATTR(LL, SS)                                                                                \
@@ -669,6 +741,7 @@ cudaError_t tc_set_smem() {
 void tc_release(huv::TcState& tc) {
   cudaFree(tc.gy);
   cudaFree(tc.gx);
+  cudaFree(tc.gp);
   tc = huv::TcState();
 }
 
@@ -725,7 +798,36 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   // 2 B columns: their tensor maps end at column 2 B, so TMA fills the rest
   // of the last 64-wide box with zeros instead of reading padding.
   const int kbE = kstE * 16, kbI = kstI * 16;
+  // Separable interpolation (evaluation grids up to 192 points, FP32 field
+  // pass): the coarse intensity is band-limited to |f| <= h2 < M / 2, so
+  // I_N = P I_M P^T exactly, with the real N x M matrix
+  //     P(Y, m) = (1/M) sum_{|f| <= h2} exp(2 pi i f (Y/N - m/M))
+  // (a Dirichlet kernel).  Z^T = P I_M^T is one small tcgen05 GEMM (MODE 3,
+  // split operand out) and I_N = P Z the store-mode GEMM (MODE 1), in place
+  // of the band transform of I_M and the N-point row transforms.  Operands
+  // are FP16 hi/lo planes (22 significant bits against BF16's 16) with I_M
+  // carried as I_M / interp_scale(mean); the final GEMM multiplies it back.
+  const bool sep = fft_field && M <= 192 && M % 16 == 0 && xt_ok(M, hb);
   TcState& tc = ds.tc[M];
+  if (sep && !tc.gp) {
+    constexpr int kpP = 192;
+    std::vector<double> pm(static_cast<size_t>(n) * M);
+    const double nm = static_cast<double>(n) * M;
+    for (int y = 0; y < n; ++y)
+      for (int m = 0; m < M; ++m) {
+        // t = Y/N - m/M = q / (N M); sum_{|f|<=H} e^{2 pi i f t} = sin((2H+1) pi t) / sin(pi t)
+        const long long q = static_cast<long long>(y) * M - static_cast<long long>(m) * n;
+        const double v = q == 0 ? static_cast<double>(2 * h2 + 1)
+                                : std::sin((2 * h2 + 1) * kPi * static_cast<double>(q) / nm) /
+                                      std::sin(kPi * static_cast<double>(q) / nm);
+        pm[static_cast<size_t>(y) * M + m] = v / M;
+      }
+    const auto pp = split_planes_f16(pm, n, M, kpP);
+    check_cuda(cudaMalloc(&tc.gp, pp.size() * 2), "cudaMalloc(P)");
+    check_cuda(cudaMemcpy(tc.gp, pp.data(), pp.size() * 2, cudaMemcpyHostToDevice), "upload P");
+    if (!make_map(&tc.map_pi, tc.gp, 2ull * n, kpP, 128, 0, true))
+      throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the interpolation operand");
+  }
   if (!fft_field && !tc.gy) {
     // A_E: rows (y, re/im) over the M grid, K = (my, re/im).
     std::vector<double> ae(static_cast<size_t>(2 * M) * kcE);
@@ -775,7 +877,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const size_t per_i = align256(sizeof(float) * M * M);
   const size_t per_x2 = align256(sizeof(float2) * M * B2);
   const size_t per_c = align256(sizeof(float2) * B2 * B2);
-  const size_t per_bi = align256(static_cast<size_t>(2) * n * kbI * 2);
+  const size_t per_bi = align256(static_cast<size_t>(2) * n * std::max(kbI, M) * 2);
   const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
   const size_t per_clip = per_x + per_m + per_be + per_p + per_i + per_x2 + per_c + per_bi + per_mean;
   const size_t budget = size_t(1) << 30;
@@ -826,7 +928,10 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "socs_rows");
       prof.end(st);
       prof.begin("socs_cols_inv", st);
-      check_cuda(socs_cols_x(T, K, hb, M, nc, ds.keep, ds.flare, mean, IM, 0, twm, st), "socs_cols");
+      if (sep)  // I_M / s as FP16 split planes [clip][2][M][M] (the bytes of the f32 IM)
+        check_cuda(socs_cols_split(T, K, hb, M, nc, ds.keep, ds.flare, mean, IM, twm, st), "socs_cols");
+      else
+        check_cuda(socs_cols_x(T, K, hb, M, nc, ds.keep, ds.flare, mean, IM, 0, twm, st), "socs_cols");
       prof.end(st);
     }
     if (!fft_field) prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
@@ -887,12 +992,49 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       prof.end(st);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<0>");
     }
-    prof.begin("interp_band", st);
-    check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st, nullptr,
-                            nullptr),
-               "band_forward(interp)");
-    prof.end(st);
-    {
+    CUtensorMap mbZ;
+    if (sep) {
+      // Z^T[clip][plane][Y][y] = sum_x P(Y, x) I_M(y, x) / s, FP16 split planes:
+      // A = P (rows Y), B = I_M / s (rows y, K = x), s = interp_scale(mean);
+      // G clips per CTA share the A tile.
+      constexpr int G1 = 4;
+      const int bn1 = M / 2;
+      CUtensorMap mbS;
+      if (!make_map(&mbS, IM, static_cast<uint64_t>(nc) * 2 * M, M, bn1, M, true) ||
+          !make_map(&mbZ, BI, static_cast<uint64_t>(nc) * 2 * n, M, kTcBN, M, true))
+        throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the interpolation operands");
+      TcGemmParams p{};
+      p.kboxes = (M + 63) / 64;
+      p.ksteps = M / 16;
+      p.G = G1;
+      p.nprob = nc;
+      p.a_rows = n;
+      p.b_prob = G1 * 2 * M;
+      p.b_step = 2 * M;
+      p.b_plane = M;
+      p.err = dev_err;
+      p.bop = BI;
+      p.bop_prob = 2ll * n * M;
+      p.bop_plane = static_cast<long long>(n) * M;
+      p.bop_ld = M;
+      const dim3 g(2, n / 128, (nc + G1 - 1) / G1);
+      prof.begin("tc_dft_gemm<interp_x>", st);
+      if (bn1 == 64)
+        tc_dft_gemm<3, 64><<<g, 192, tc_smem_bytes(3, 64), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+      else if (bn1 == 80)
+        tc_dft_gemm<3, 80><<<g, 192, tc_smem_bytes(3, 80), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+      else if (bn1 == 96)
+        tc_dft_gemm<3, 96><<<g, 192, tc_smem_bytes(3, 96), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+      else
+        throw Error(HUV_ERR_UNSUPPORTED, "separable interpolation: evaluation grid must be 128, 160 or 192");
+      prof.end(st);
+      check_cuda(cudaGetLastError(), "tc_dft_gemm<3>");
+    } else {
+      prof.begin("interp_band", st);
+      check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st,
+                              nullptr, nullptr),
+                 "band_forward(interp)");
+      prof.end(st);
       prof.begin("socs_rows_tc<interp>", st);
       const float scale = 1.0f / (static_cast<float>(M) * static_cast<float>(M));
       launch_rows(nullptr, scale, C, 1, h2, h2, nrI, n, kbI, 0, BI, twn, nc, st);
@@ -901,8 +1043,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     }
     {
       TcGemmParams p{};
-      p.kboxes = kpI / 64;
-      p.ksteps = kstI;
+      p.kboxes = sep ? (M + 63) / 64 : kpI / 64;
+      p.ksteps = sep ? M / 16 : kstI;
       p.G = n / kTcBN;
       p.a_rows = n;
       p.b_prob = 2 * n;
@@ -912,7 +1054,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.out_plane = static_cast<long long>(n) * n;
       p.keep = 1.f;
       p.flare = 0.f;
-      p.mean = nullptr;
+      p.mean = sep ? mean : nullptr;  // separable: undo the planes' scale
+      p.f16 = sep ? 1 : 0;
       p.out = o;
       p.err = dev_err;
       CUtensorMap mo;
@@ -920,11 +1063,15 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       if (!p.out_tma) mo = tc.map_ai;  // unused
       dim3 g(1, n / 128, nc);
       prof.begin("tc_dft_gemm<interp>", st);
-      tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_ai, mbI, mo, p);
+      if (sep)
+        tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_pi, mbZ, mo, p);
+      else
+        tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_ai, mbI, mo, p);
       prof.end(st);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
     }
-    prof.launches += gemm_rows ? 8 : 7;
+    // mask band (rows, columns, mean), 2 field launches (3 with the row GEMM), 2 (separable) or 4 interpolation launches
+    prof.launches += sep ? 7 : (gemm_rows ? 10 : 9);
   }
 }
 

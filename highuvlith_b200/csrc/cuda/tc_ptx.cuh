@@ -196,6 +196,11 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
          (static_cast<uint32_t>(M >> 4) << 24);
 }
 
+// Instruction descriptor, kind::f16: D f32, A/B both f16, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
+  return (1u << 4) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+}
+
 // Instruction descriptor, kind::i8: D s32, A and B both unsigned 8-bit, both
 // K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_u8(int M, int N) {

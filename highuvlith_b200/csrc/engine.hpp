@@ -50,7 +50,8 @@ struct TcState {
   int lgm = 0;          // evaluation grid the state was built for (log2, rounded up)
   void* gy = nullptr;   // A_E planes [2][2M][kpE] bf16
   void* gx = nullptr;   // A_I planes [2][N][kpI] bf16
-  CUtensorMap map_ae, map_ai;
+  void* gp = nullptr;   // separable interpolation matrix planes [2][N][192] fp16 (M <= 192)
+  CUtensorMap map_ae, map_ai, map_pi;
 };
 
 // One kernel set on the device: band kernels K x B x B (complex FP32,
