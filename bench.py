@@ -447,11 +447,17 @@ def run_ours(args):
     m_tc = max(m_p2, 128)
     m_f = m_tc if args.form in ("tc", "tc_rows") else m_mix
     kb = 16 * ((2 * Bb + 15) // 16)
+    # hybrid form on an evaluation grid of at most 192 points: separable
+    # interpolation I_N = P I_M P^T (two GEMMs with K = M), else the band
+    # transform of I_M and a GEMM over the Hermitian half band (K = 2 (2h + 1))
+    sep = args.form in ("auto", "hybrid") and m_f <= 192
+    k_int = m_f if sep else 2 * (2 * hb_ + 1)
     own_bytes = {"socs_cols_inv": 8 * K * Bb * m_f + 4 * m_f * m_f,
                  "socs_rows_inv": 8 * K * Bb * m_f + 8 * Bb * Bb,
                  "tc_dft_gemm<sumsq>": 4 * K * m_f * kb + 4 * m_f * m_f,
                  "socs_rows_tc": 4 * K * m_f * kb + 8 * Bb * Bb,
-                 "tc_dft_gemm<interp>": 4 * N_GRID * N_GRID + 4 * N_GRID * kb,
+                 "tc_dft_gemm<interp>": 4 * N_GRID * N_GRID + 4 * N_GRID * (k_int if sep else kb),
+                 "tc_dft_gemm<interp_x>": 4 * m_f * m_f + 4 * N_GRID * m_f,
                  "mask_band": N_GRID * N_GRID + 16 * N_GRID * Bb + 8 * Bb * Bb}
     bytes_per_image = 4 * N_GRID ** 2 + 4 * N_GRID ** 2 + 8 * K * S
     launches = max(prof["launches"], 1)
@@ -478,14 +484,13 @@ def run_ours(args):
                                   "note": "the dominant region's own operands (in and out once) / its mean launch time"}
     gi = prof["regions"].get("tc_dft_gemm<interp>")
     if gi and gi[1] > 0:
-        # the band interpolation on tensor cores: a real N x N x 2(2h2+1)
-        # GEMM per image (2 N^2 (2 (4h + 1)) FLOP, split products counted once)
-        kc = 2 * (4 * diag["band_half_width"] + 1)
-        flop_i = 2.0 * N_GRID * N_GRID * kc * N_CLIPS * args.steps
+        # the band interpolation's N x N output GEMM: 2 N^2 k_int FLOP per
+        # image (split products counted once)
+        flop_i = 2.0 * N_GRID * N_GRID * k_int * N_CLIPS * args.steps
         roofline["tensor_interp"] = {"kernel": "tc_dft_gemm<interp>", "achieved": flop_i / (gi[1] / 1e3) / 1e12,
                                      "peak": tc_burst, "unit": "TFLOP/s",
                                      "frac": flop_i / (gi[1] / 1e3) / 1e12 / tc_burst if tc_burst else None,
-                                     "issued_products_per_algorithmic": 3}
+                                     "gemm_k": k_int, "issued_products_per_algorithmic": 3}
     g = prof["regions"].get("tc_dft_gemm<sumsq>")
     if g and g[1] > 0:
         # the |E|^2 contraction on tensor cores: 8 B M^2 K FLOP per image (complex MAC = 8,
