@@ -425,9 +425,8 @@ def run_ours(args):
     hbm, tc_burst, tc_sus, peak_kind = peaks()
     K, S = diag["num_kernels"], diag["num_frequencies"]
     # DRAM bytes (read + write) per clip of each timed region, from ncu
-    # captures of this workload at 32 clips (cold cache, serialised;
-    # profiles/socs_tc_and_fft_c2_traffic_32clips.md), scaled to a launch by
-    # its clips.  FFT and hybrid forms on the 160-point grid, the TC form's
+    # captures of this workload at 32 clips (cold cache, serialised), scaled
+    # to a launch by its clips.  FFT and hybrid forms on the 160-point grid, the TC form's
     # y-contraction on 256.
     traffic_per_clip = {"tc_dft_gemm<sumsq>": (166.38e6 + 6.65e6) / 32,
                         "socs_rows_tc": (19.29e6 + 110.03e6) / 32,
@@ -436,7 +435,8 @@ def run_ours(args):
                         "socs_cols_inv": (95.29e6 + 0.13e6) / 32,
                         "socs_rows_inv": (2.87e6 + 33.84e6) / 32,
                         "interp_band": (3.29e6 + 6.12e6) / 32,
-                        "interp_rows_cols": (5.73e6 + 39.09e6 + 77.49e6) / 32}
+                        "interp_rows_cols": (5.73e6 + 39.09e6 + 77.49e6) / 32,
+                        "tc_dft_gemm<interp_x>": (4.09e6 + 0.01e6) / 32}
     # each region's own algorithmic bytes per clip (operands in and out once)
     hb_ = diag["band_half_width"]
     Bb = 2 * hb_ + 1
@@ -452,6 +452,8 @@ def run_ours(args):
     # transform of I_M and a GEMM over the Hermitian half band (K = 2 (2h + 1))
     sep = args.form in ("auto", "hybrid") and m_f <= 192
     k_int = m_f if sep else 2 * (2 * hb_ + 1)
+    if sep:  # the separable form's output GEMM (ncu --set full, 32 clips)
+        traffic_per_clip["tc_dft_gemm<interp>"] = (22.46e6 + 77.88e6) / 32
     own_bytes = {"socs_cols_inv": 8 * K * Bb * m_f + 4 * m_f * m_f,
                  "socs_rows_inv": 8 * K * Bb * m_f + 8 * Bb * Bb,
                  "tc_dft_gemm<sumsq>": 4 * K * m_f * kb + 4 * m_f * m_f,
