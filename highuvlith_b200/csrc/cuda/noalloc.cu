@@ -86,6 +86,8 @@ extern "C" huv_status huv_image_batch_noalloc(void* engine, const huv_batch* bat
     }
     if (!b.input || !out) throw huv::Error(HUV_ERR_INVALID_PARAMETER, "input/out: null pointer");
     if (b.input_kind < 0 || b.input_kind > 2) throw huv::Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
+    if ((reinterpret_cast<uintptr_t>(out) & 15u) != 0 || (reinterpret_cast<uintptr_t>(b.input) & 15u) != 0)
+      throw huv::Error(HUV_ERR_INVALID_PARAMETER, "input/out: device buffers must be 16-byte aligned");
     if (b.form != HUV_FORM_AUTO && b.form != HUV_FORM_FFT)
       throw huv::Error(HUV_ERR_UNSUPPORTED, "the allocation-free path runs the FP32 FFT form only");
     if (!std::isfinite(b.defocus_nm)) throw huv::Error(HUV_ERR_INVALID_PARAMETER, "defocus_nm: must be finite");
@@ -171,7 +173,7 @@ extern "C" huv_status huv_image_batch_noalloc(void* engine, const huv_batch* bat
                        "allocation-free path: one clip needs " + std::to_string((off + per_clip) >> 20) +
                            " MiB of scratch, above its fixed maximum of " +
                            std::to_string(kNoAllocScratchBytes >> 20) + " MiB; use huv_image_batch");
-    const int chunk = std::min<int>(b.n_clips, static_cast<int>((kNoAllocScratchBytes - off) / per_clip));
+    const int chunk = huv::balanced_chunk(static_cast<int>((kNoAllocScratchBytes - off) / per_clip), b.n_clips);
     char* cb = base + off;
     float2* X = reinterpret_cast<float2*>(cb);
     float2* Mb = reinterpret_cast<float2*>(cb + per_x * chunk);

@@ -875,14 +875,13 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   if (gemm_rows && B > kRowBNWide) throw Error(HUV_ERR_UNSUPPORTED, "TC form: band wider than 96 orders");
   const size_t per_p = gemm_rows ? align256(static_cast<size_t>(K) * 2 * rbn * kpE * 2) : 0;
   const size_t per_i = align256(sizeof(float) * M * M);
-  const size_t per_x2 = align256(sizeof(float2) * M * B2);
-  const size_t per_c = align256(sizeof(float2) * B2 * B2);
+  const size_t per_x2 = sep ? 0 : align256(sizeof(float2) * M * B2);  // band of I_M (band-transform path)
+  const size_t per_c = sep ? 0 : align256(sizeof(float2) * B2 * B2);
   const size_t per_bi = align256(static_cast<size_t>(2) * n * std::max(kbI, M) * 2);
   const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
   const size_t per_clip = per_x + per_m + per_be + per_p + per_i + per_x2 + per_c + per_bi + per_mean;
   const size_t budget = size_t(1) << 30;
-  int chunk = static_cast<int>(std::max<size_t>(1, budget / per_clip));
-  chunk = std::min(chunk, b.n_clips);
+  const int chunk = balanced_chunk(static_cast<int>(std::max<size_t>(1, budget / per_clip)), b.n_clips);
   char* base = static_cast<char*>(workspace(per_clip * chunk + 4096));
   size_t off = 0;
   auto take = [&](size_t per) {

@@ -456,8 +456,7 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
   const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
   const size_t per_clip = per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2 + per_mean;
   const size_t budget = size_t(1) << 30;
-  int chunk = static_cast<int>(std::max<size_t>(1, budget / per_clip));
-  chunk = std::min(chunk, b.n_clips);
+  const int chunk = balanced_chunk(static_cast<int>(std::max<size_t>(1, budget / per_clip)), b.n_clips);
   char* base = static_cast<char*>(workspace(per_clip * chunk + 4096));
   float2* X = reinterpret_cast<float2*>(base);
   float2* Mb = reinterpret_cast<float2*>(base + per_x * chunk);
@@ -514,6 +513,10 @@ void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
   if (!b.input || !out) throw Error(HUV_ERR_INVALID_PARAMETER, "input/out: null pointer");
   if (b.input_kind < 0 || b.input_kind > 3) throw Error(HUV_ERR_INVALID_PARAMETER, "input_kind: unknown");
   if (!std::isfinite(b.defocus_nm)) throw Error(HUV_ERR_INVALID_PARAMETER, "defocus_nm: must be finite");
+  // device rasters are read with TMA and vector loads, images written with vector stores
+  if ((reinterpret_cast<uintptr_t>(out) & 15u) != 0 ||
+      (b.input_kind != HUV_INPUT_RECTS && (reinterpret_cast<uintptr_t>(b.input) & 15u) != 0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "input/out: device buffers must be 16-byte aligned");
   ensure_device();
   if (b.input_kind == HUV_INPUT_RECTS) upload_rects(b);
   DeviceSet& ds = device_set(b.defocus_nm == 0.0 ? 0.0 : b.defocus_nm);

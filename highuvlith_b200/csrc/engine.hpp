@@ -15,6 +15,16 @@
 
 namespace huv {
 
+// Clips per chunk when a batch of n must be cut into chunks of at most
+// max_chunk: the fewest chunks, sized evenly (216 + 40 becomes 128 + 128),
+// so that the last chunk does not run the kernels on a partial wave.
+inline int balanced_chunk(int max_chunk, int n) {
+  if (n <= 0) return 1;
+  max_chunk = max_chunk < 1 ? 1 : max_chunk;
+  const int chunks = (n + max_chunk - 1) / max_chunk;
+  return (n + chunks - 1) / chunks;
+}
+
 void set_last_error(const std::string& m);
 const char* last_error();
 void check_cuda(cudaError_t e, const char* what);

@@ -197,7 +197,8 @@ huv_status huv_engine_kernels(void* engine, double defocus_nm, double* eigenvalu
 /* Batched aerial images on the device: out is n_clips*N*N floats (device),
  * [clip][y][x], pixel centres x_j = -L/2 + (j + 1/2) p.  Equivalent per clip to
  * compute(mask, z) (pixel_transfer = 1) or compute_from_transmittance(t, z)
- * (pixel_transfer = 0), normalisation and flare included (aerial.rs:1775-1816). */
+ * (pixel_transfer = 0), normalisation and flare included (aerial.rs:1775-1816).
+ * Device rasters and out must be 16-byte aligned (HUV_ERR_INVALID_PARAMETER). */
 huv_status huv_image_batch(void* engine, const huv_batch* batch, float* out, void* stream);
 
 /* Same call with HOST input and output buffers: copies in, images, copies out

@@ -115,6 +115,24 @@ def test_invalid_inputs_return_status():
     assert lib.huv_engine_destroy(None) is None
 
 
+def test_misaligned_device_buffers_are_rejected_before_any_launch():
+    """The device entry points read rasters with TMA / vector loads and write
+    images with vector stores, so input and out must be 16-byte aligned; a
+    misaligned pointer is refused on the host (no CUDA call is made)."""
+    eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(),
+                              grid=HB.GridConfig(64, 1.0), max_kernels=4)
+    lib = _lib.lib()
+    buf = np.zeros(64 * 64 * 2 + 16, np.float32)
+    base = (buf.ctypes.data + 15) & ~15
+    b = _lib.Batch(1, 0, base, 1, 0.0, 0, 0)
+    for fn in (lib.huv_image_batch, lib.huv_image_batch_noalloc):
+        assert fn(eng.handle, ctypes.byref(b), ctypes.c_void_p(base + 4), None) == 1
+        assert b"16-byte aligned" in lib.huv_last_error()
+    b.input = base + 1
+    assert lib.huv_image_batch(eng.handle, ctypes.byref(b), ctypes.c_void_p(base), None) == 1
+    assert b"16-byte aligned" in lib.huv_last_error()
+
+
 def test_c2_kernel_set_shape():
     """C2: EUV NA 0.33, sigma 0.5, 1024 x 1 nm -> r = 37.55, h = 37, S = 4429, K = 32."""
     eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(),
