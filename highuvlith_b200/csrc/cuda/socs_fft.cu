@@ -500,11 +500,22 @@ __global__ void __launch_bounds__(fr_threads(L, S))
 #pragma unroll
   for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
     if (t + b * T >= fr_nb(L, S, NP - 1)) break;
+    // butterfly (s, j) produces orders j + p L / R: skip it unless one of
+    // them lies in the band (75 of 256 last-pass butterflies at L = 1024, h = 37)
+    {
+      const int u = t + b * T, su = u % S, ju = u / S;
+      bool need = false;
+#pragma unroll
+      for (int p = 0; p < R; ++p) {
+        const int idx = ju + p * (L / R);
+        need = need || idx <= hb || idx >= L - hb;
+      }
+      if (!need || c0 + su >= B) continue;
+    }
     int s, j;
     float2 v[R];
     fr_last_pass<L, S, -1>(t + b * T, cur, tw, s, j, v);
     const int mx = c0 + s;
-    if (mx >= B) continue;
 #pragma unroll
     for (int p = 0; p < R; ++p) {
       const int idx = j + p * (L / R);

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(192, 1)
     tc_dft_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmO, TcGemmParams p) {
   constexpr uint32_t kBBox = b_box_bytes(BN);
-  constexpr uint32_t kTmemCols = 2 * BN <= 128 ? 128 : 256;
+  constexpr uint32_t kTmemCols = 2 * BN <= 128 ? 128 : (2 * BN <= 256 ? 256 : 512);
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
@@ -718,11 +718,11 @@ cudaError_t tc_set_smem() {
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<2, kRowBNWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, kRowBNWide, true)))))
     return e;
-  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(tc_smem_bytes(3, 64)))))
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, 128)))))
     return e;
-  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 80>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(tc_smem_bytes(3, 80)))))
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 160>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, 160)))))
     return e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 96>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, 96)))))
@@ -995,9 +995,28 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     if (sep) {
       // Z^T[clip][plane][Y][y] = sum_x P(Y, x) I_M(y, x) / s, FP16 split planes:
       // A = P (rows Y), B = I_M / s (rows y, K = x), s = interp_scale(mean);
-      // G clips per CTA share the A tile.
-      constexpr int G1 = 4;
-      const int bn1 = M / 2;
+      // G1 clips per CTA share the A tile.  The MMA covers all M columns at
+      // once where the B ring fits (M = 128, 160: N = M, 4 + 5 KB of operands
+      // per 80 tensor cycles at M = 160), else two halves (M = 192).
+      const int bn1 = M <= 160 ? M : M / 2;
+      const int ntile1 = M / bn1, mtiles = n / 128;
+      // Clips per CTA: the fewest (up to 8) whose grid fits one wave of one
+      // CTA per SM, else 8.  Each CTA's run is latency-bound (per step: one
+      // clip's B ring through 3 stages), so longer runs over a resident A
+      // tile beat more CTAs: at 128 clips 1 / 2 / 4 / 8 clips per CTA time
+      // 1.24 / 1.12 / 1.03 / 0.99 ms per 20 launches.
+      static int sms = 0;
+      if (!sms) {
+        int dev = 0;
+        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+      }
+      int G1 = 8;
+      for (int gc = 1; gc < 8; ++gc)
+        if (static_cast<long long>(ntile1) * mtiles * ((nc + gc - 1) / gc) <= sms) {
+          G1 = gc;
+          break;
+        }
       CUtensorMap mbS;
       if (!make_map(&mbS, IM, static_cast<uint64_t>(nc) * 2 * M, M, bn1, M, true) ||
           !make_map(&mbZ, BI, static_cast<uint64_t>(nc) * 2 * n, M, kTcBN, M, true))
@@ -1016,12 +1035,12 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.bop_prob = 2ll * n * M;
       p.bop_plane = static_cast<long long>(n) * M;
       p.bop_ld = M;
-      const dim3 g(2, n / 128, (nc + G1 - 1) / G1);
+      const dim3 g(ntile1, mtiles, (nc + G1 - 1) / G1);
       prof.begin("tc_dft_gemm<interp_x>", st);
-      if (bn1 == 64)
-        tc_dft_gemm<3, 64><<<g, 192, tc_smem_bytes(3, 64), st>>>(tc.map_pi, mbS, tc.map_pi, p);
-      else if (bn1 == 80)
-        tc_dft_gemm<3, 80><<<g, 192, tc_smem_bytes(3, 80), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+      if (bn1 == 128)
+        tc_dft_gemm<3, 128><<<g, 192, tc_smem_bytes(3, 128), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+      else if (bn1 == 160)
+        tc_dft_gemm<3, 160><<<g, 192, tc_smem_bytes(3, 160), st>>>(tc.map_pi, mbS, tc.map_pi, p);
       else if (bn1 == 96)
         tc_dft_gemm<3, 96><<<g, 192, tc_smem_bytes(3, 96), st>>>(tc.map_pi, mbS, tc.map_pi, p);
       else
