@@ -816,8 +816,8 @@ struct Fno {
     check_cuda(cudaMalloc(&twy, ty.size() * 8), "cudaMalloc(twy)");
     check_cuda(cudaMemcpy(twx, tx.data(), tx.size() * 8, cudaMemcpyHostToDevice), "upload twx");
     check_cuda(cudaMemcpy(twy, ty.data(), ty.size() * 8, cudaMemcpyHostToDevice), "upload twy");
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<uint64_t> attr{0};
+    huv::once_per_device(attr, [] {
       const int big = 200 * 1024;
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_dft_x<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_dft_x<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
@@ -826,8 +826,7 @@ struct Fno {
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_layer_out, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
       check_cuda(cudaFuncSetAttribute(huv_dev::fno_spec_to_dv, cudaFuncAttributeMaxDynamicSharedMemorySize, big), "attr");
-      attr = true;
-    }
+    });
     tc = S >= 128 && S % 128 == 0 && C == 64 && P == 128 && m <= 16;
     if (tc) {
       check_cuda(huv_launch::fno_tc_set_smem(), "cudaFuncSetAttribute(fno tc)");

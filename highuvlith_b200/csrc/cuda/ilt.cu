@@ -736,11 +736,8 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
                       double* cost_dev, cudaStream_t st) {
   using namespace huv_dev;
   using namespace huv_launch;
-  static bool smem_set = false;
-  if (!smem_set) {
-    check_cuda(ilt_set_smem(), "cudaFuncSetAttribute(ilt)");
-    smem_set = true;
-  }
+  static std::atomic<uint64_t> smem_set{0};
+  once_per_device(smem_set, [] { check_cuda(ilt_set_smem(), "cudaFuncSetAttribute(ilt)"); });
   DeviceSet& ds = device_set(p.defocus_nm == 0.0 ? 0.0 : p.defocus_nm);
   const int K = ds.K, hb = ds.hb, B = ds.B;
   const int h2 = 2 * hb, B2 = 2 * h2 + 1;

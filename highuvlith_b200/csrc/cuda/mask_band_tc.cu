@@ -30,6 +30,7 @@
 #include <cudaTypedefs.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cmath>
 #include <vector>
 
@@ -281,12 +282,16 @@ cudaError_t mask_rows_tc(const void* in, int n, int hb, int clips, float2* X, co
   if (!digits || !mask_rows_tc_supported(n, hb) || (reinterpret_cast<uintptr_t>(in) & 15u) != 0)
     return cudaErrorNotSupported;
   const int N = mask_rows_tc_cols(hb);
-  static bool attr_set = false;
-  if (!attr_set) {
+  // the attribute is per device: bit d set once device d has it
+  static std::atomic<uint64_t> attr_set{0};
+  int dev = 0;
+  if (cudaError_t e = cudaGetDevice(&dev)) return e;
+  const uint64_t bit = dev >= 0 && dev < 64 ? (uint64_t(1) << dev) : 0;
+  if (!bit || !(attr_set.load(std::memory_order_acquire) & bit)) {
     cudaError_t e = cudaFuncSetAttribute(band_rows_i8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(mb_smem_bytes(160) + (40 << 10)));
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    if (bit) attr_set.fetch_or(bit, std::memory_order_acq_rel);
   }
   CUtensorMap ma, md;
   if (!make_u8_map(&ma, in, static_cast<uint64_t>(clips) * n, n, 128) ||

@@ -782,11 +782,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
                          const float* W_use, int core) {
   const bool gemm_rows = core == kTcCoreGemmRows, fft_field = core == kTcCoreFftField;
   using namespace huv_launch;
-  static bool smem_set = false;
-  if (!smem_set) {
-    check_cuda(tc_set_smem(), "cudaFuncSetAttribute(tc)");
-    smem_set = true;
-  }
+  static std::atomic<uint64_t> smem_set{0};
+  once_per_device(smem_set, [] { check_cuda(tc_set_smem(), "cudaFuncSetAttribute(tc)"); });
   const int lgn = ilog2i(n), lgm = ilog2i(M);  // lgm: log2 of M rounded up (M need not be a power of two)
   const int B = ds.B, K = K_use > 0 ? K_use : ds.K, hb = ds.hb;
   const float* Wf = W_use ? W_use : ds.W;
@@ -1005,12 +1002,9 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       // clip's B ring through 3 stages), so longer runs over a resident A
       // tile beat more CTAs: at 128 clips 1 / 2 / 4 / 8 clips per CTA time
       // 1.24 / 1.12 / 1.03 / 0.99 ms per 20 launches.
-      static int sms = 0;
-      if (!sms) {
-        int dev = 0;
-        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-      }
+      int sms = 0, dev = 0;
+      check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+      check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
       int G1 = 8;
       for (int gc = 1; gc < 8; ++gc)
         if (static_cast<long long>(ntile1) * mtiles * ((nc + gc - 1) / gc) <= sms) {

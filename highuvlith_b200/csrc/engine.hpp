@@ -4,6 +4,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -28,6 +29,19 @@ inline int balanced_chunk(int max_chunk, int n) {
 void set_last_error(const std::string& m);
 const char* last_error();
 void check_cuda(cudaError_t e, const char* what);
+
+// Runs fn once per CUDA device for settings that CUDA keeps per device
+// (function attributes): bit d of `done` is set after device d ran it.  Two
+// threads may both run fn for one device; the calls it makes are idempotent.
+template <class F>
+void once_per_device(std::atomic<uint64_t>& done, F&& fn) {
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  const uint64_t bit = dev >= 0 && dev < 64 ? (uint64_t(1) << dev) : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+  fn();
+  if (bit) done.fetch_or(bit, std::memory_order_acq_rel);
+}
 
 // Device-side state of the tensor-core form for one kernel set: the split
 // BF16 DFT operands (A_E over the evaluation grid, A_I for the interpolation
