@@ -143,6 +143,36 @@ def test_mixed_radix_eval_grids_match_oracle(form, eval_grid):
         assert rel_err(out[c], ref) < tol, (c, rel_err(out[c], ref))
 
 
+@pytest.mark.parametrize("normalization", ["clear_field", "absolute"])
+def test_hybrid_fp16_planes_on_extreme_clips(normalization):
+    """The separable interpolation carries I / (16 mean) in FP16 planes: a
+    lone contact in a dark field (peak far above the mean), an opaque clip
+    (mean 0: the image must stay exactly 0), a clear clip and a random clip,
+    under both normalisations, against the FP32 FFT form and the oracle."""
+    torch = _torch()
+    _, src, opt, grid, kmax, fill, oopt = SMALL[3]  # EUV quasar on 256^2
+    eng = HB.SimulationEngine(src, opt, grid=grid, max_kernels=kmax, normalization=normalization)
+    n = grid.size
+    clips = np.zeros((4, n, n), np.uint8)
+    clips[0, n // 2 - 4:n // 2 + 4, n // 2 - 4:n // 2 + 4] = 1  # one 8 x 8 contact
+    clips[2] = 1
+    _, rnd = gen_batch(1, n, base_seed=29, wmin=6, wmax=32, dmin=0.2, dmax=0.6)
+    clips[3] = rnd[0]
+    d = torch.from_numpy(clips).cuda()
+    hyb = eng.compute_batch(d, form="hybrid", eval_grid=160).cpu().numpy()
+    fft = eng.compute_batch(d, form="fft", eval_grid=160).cpu().numpy()
+    assert np.all(np.isfinite(hyb))
+    assert np.max(np.abs(hyb[1])) == 0.0
+    for c in (0, 2, 3):
+        assert rel_err(hyb[c], fft[c]) < 2e-5, (c, rel_err(hyb[c], fft[c]))
+    assert np.max(hyb[0]) / max(float(np.mean(hyb[0])), 1e-30) > 50  # the dark-field case is one
+    if normalization == "clear_field":  # (a truncated kernel set images a clear clip slightly below 1)
+        oeng = _oracle_engine(fill, oopt, grid, src.wavelength_nm, kmax)
+        for c in (0, 2):
+            ref = oeng.compute_from_spectrum(H.spectrum_from_raster(clips[c]))
+            assert rel_err(hyb[c], ref) < 1e-4, (c, rel_err(hyb[c], ref))
+
+
 def test_clear_and_dark_masks():
     """Clear mask images to 1 (flare keeps it 1); an opaque mask to 0."""
     torch = _torch()
