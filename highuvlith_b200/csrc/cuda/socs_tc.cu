@@ -391,6 +391,204 @@ __global__ void __launch_bounds__(192, 1)
   if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
 }
 
+// Output GEMM of the band interpolation with 256-column tiles:
+// out(y, g * 256 + j) = osc * sum_k P(y, k) Z(g * 256 + j, k) over hi/lo
+// planes (hi.hi + hi.lo + lo.hi): FP16 with osc = interp_scale(mean) for the
+// separable form (p.f16, p.mean), BF16 with osc = 1 for the Hermitian
+// half-band operands.  P's 128-row
+// tile stays resident in shared memory (64-wide boxes, 128B swizzle); Z's
+// 256-row tiles stream through a 3-stage ring of 32-wide boxes (64B
+// swizzle, 32 KB per stage with both planes), so each MMA is 128 x 256 x 16
+// and reads 12 KB of operands per 128 tensor cycles.  Accumulators
+// double-buffered in all 512 TMEM columns.  Roles as tc_dft_gemm MODE 1
+// (warp 0 TMA, warp 1 MMA issue, warps 2-5 epilogue with TMA stores).
+// grid: (1, a_rows / 128, problems); p.G = out columns / 256.
+constexpr int kW256Stages = 3;
+constexpr uint32_t kW256BBox = 256 * 64;  // one plane: 256 rows x 32 fp16
+__host__ __device__ constexpr size_t w256_smem_bytes() {
+  return 1024 + 2 * 3 * static_cast<size_t>(kABox) + kW256Stages * 2 * static_cast<size_t>(kW256BBox) + kOutStage +
+         256;
+}
+
+__global__ void __launch_bounds__(192, 1)
+    tc_interp_w256(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const __grid_constant__ CUtensorMap tmO, TcGemmParams p) {
+  constexpr uint32_t kTmemCols = 512;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  uint8_t* sA = base;                                    // [plane][3 boxes] x 16 KB
+  uint8_t* sB = sA + 2 * 3 * kABox;                      // [stage][plane] x 16 KB
+  uint8_t* sO = sB + kW256Stages * 2 * kW256BBox;        // epilogue staging
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sO + kOutStage);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + kW256Stages;
+  uint64_t* a_full = bars + 2 * kW256Stages;
+  uint64_t* tfull = bars + 2 * kW256Stages + 1;
+  uint64_t* tempty = bars + 2 * kW256Stages + 3;
+  uint64_t* done = bars + 2 * kW256Stages + 5;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kW256Stages + 6);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m_tile = blockIdx.y, prob = blockIdx.z;
+  const int kbb = (p.ksteps + 1) / 2;  // 32-wide B boxes per step
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kW256Stages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(a_full, 1);
+    mbar_init(&tfull[0], 1);
+    mbar_init(&tfull[1], 1);
+    mbar_init(&tempty[0], 4);
+    mbar_init(&tempty[1], 4);
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, kTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  auto fail = [&](int code) {
+    *abort_flag = 1;
+    if (p.err) atomicExch(p.err, code);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      prefetch_tmap(&tmA);
+      prefetch_tmap(&tmB);
+      mbar_arrive_expect_tx(a_full, 2u * p.kboxes * kABox);
+      for (int part = 0; part < 2; ++part)
+        for (int kb = 0; kb < p.kboxes; ++kb)
+          tma_load_2d(sA + (part * 3 + kb) * kABox, &tmA, kb * 64, part * p.a_rows + m_tile * 128, a_full);
+      int it = 0;
+      for (int g = 0; g < p.G && !*abort_flag; ++g) {
+        for (int kb = 0; kb < kbb; ++kb, ++it) {
+          const int s = it % kW256Stages;
+          const uint32_t ph = (it / kW256Stages) & 1;
+          if (!mbar_wait(&empty[s], ph ^ 1, kWaitLimitNs)) {
+            fail(21);
+            break;
+          }
+          mbar_arrive_expect_tx(&full[s], 2u * kW256BBox);
+          const int row = prob * p.b_prob + g * 256;
+          tma_load_2d(sB + (s * 2 + 0) * kW256BBox, &tmB, kb * 32, row, &full[s]);
+          tma_load_2d(sB + (s * 2 + 1) * kW256BBox, &tmB, kb * 32, row + p.b_plane, &full[s]);
+        }
+      }
+      // Drain: every load issued must have landed before the CTA may exit.
+      mbar_wait(a_full, 0, kWaitLimitNs);
+      for (int q = (it > kW256Stages ? it - kW256Stages : 0); q < it; ++q)
+        mbar_wait(&full[q % kW256Stages], (q / kW256Stages) & 1, kWaitLimitNs);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = p.f16 ? idesc_f16(128, 256) : idesc_bf16(128, 256);
+      bool ok = mbar_wait(a_full, 0, kWaitLimitNs);
+      if (!ok) fail(22);
+      tc_fence_after();
+      int it = 0;
+      for (int g = 0; g < p.G && ok && !*abort_flag; ++g) {
+        const int buf = g & 1;
+        if (!mbar_wait(&tempty[buf], ((g >> 1) & 1) ^ 1, kWaitLimitNs)) {
+          fail(23);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + buf * 256;
+        for (int kb = 0; kb < kbb; ++kb, ++it) {
+          const int s = it % kW256Stages;
+          if (!mbar_wait(&full[s], (it / kW256Stages) & 1, kWaitLimitNs)) {
+            fail(24);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t b_hi = smem_desc_sw64(smem_u32(sB + (s * 2 + 0) * kW256BBox));
+          const uint64_t b_lo = smem_desc_sw64(smem_u32(sB + (s * 2 + 1) * kW256BBox));
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) {
+            const int kstep = kb * 2 + ks;
+            if (kstep < p.ksteps) {
+              // A: 64-wide box kstep / 4, 32 bytes per 16-wide K step inside it
+              const uint64_t a_hi =
+                  smem_desc_sw128(smem_u32(sA + (0 * 3 + kstep / 4) * kABox)) + static_cast<uint64_t>(2 * (kstep % 4));
+              const uint64_t a_lo =
+                  smem_desc_sw128(smem_u32(sA + (1 * 3 + kstep / 4) * kABox)) + static_cast<uint64_t>(2 * (kstep % 4));
+              const uint64_t adv = static_cast<uint64_t>(2 * ks);
+              tc_mma_bf16(d, a_hi, b_hi + adv, idesc, kstep > 0 ? 1u : 0u);
+              tc_mma_bf16(d, a_hi, b_lo + adv, idesc, 1u);
+              tc_mma_bf16(d, a_lo, b_hi + adv, idesc, 1u);
+            }
+          }
+          tc_commit(&empty[s]);
+        }
+        if (!ok) break;
+        tc_commit(&tfull[buf]);
+      }
+      // All MMAs issued by this thread have completed once `done` flips.
+      tc_commit(done);
+      mbar_wait(done, 0, kWaitLimitNs);
+    }
+  } else {
+    // Epilogue warps 2..5: TMEM lane quadrant = warp % 4.
+    const int quad = warp & 3;
+    const float osc = p.mean ? interp_scale(p.mean[prob]) : 1.f;
+    int nst = 0;  // TMA-store tiles issued by this warp
+    for (int g = 0; g < p.G; ++g) {
+      const int buf = g & 1;
+      // Warp-uniform outcome: tcgen05.ld below is .sync.aligned.
+      const bool got = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (g >> 1) & 1, kWaitLimitNs));
+      if (!got) {
+        if (lane == 0) fail(25);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + buf * 256;
+#pragma unroll 1
+      for (int c0 = 0; c0 < 256; c0 += 32) {
+        float v[32];
+        tmem_ld32(taddr + c0, v);
+        // buffer `sb` was last read by the store issued two tiles ago
+        const int sbuf = nst & 1;
+        if (lane == 0 && nst >= 2) bulk_wait_read<1>();
+        __syncwarp();
+        uint8_t* sb = sO + (quad * 2 + sbuf) * kOutTile;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          *reinterpret_cast<float4*>(sb + lane * 128 + ((q ^ (lane & 7)) << 4)) =
+              make_float4(osc * v[4 * q], osc * v[4 * q + 1], osc * v[4 * q + 2], osc * v[4 * q + 3]);
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          tma_store_2d(&tmO, sb, g * 256 + c0, prob * p.a_rows + m_tile * 128 + quad * 32);
+          bulk_commit();
+        }
+        ++nst;
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[buf]);
+    }
+    // Every TMA store must have finished before the CTA's shared memory goes.
+    if (lane == 0 && nst > 0) bulk_wait<0>();
+    __syncwarp();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
+}
+
 // Row transform along x of the band products, written as the tensor-core
 // B operand: Bop[problem][k][plane][x][kk], kk = 2 * (row - row_off) + re/im,
 // planes hi / lo, K-major with row stride kp.  Rows [row_off, row_off + nrows)
@@ -612,6 +810,20 @@ bool make_map(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2-D fp16 / bf16 tensor map (box 32 x box_rows, 64B swizzle) over
+// [rows][cols], row stride kp elements: 256-row B tiles of tc_interp_w256.
+bool make_map_sw64(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_rows, int cols, bool f16) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), rows};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(kp) * 2};
+  cuuint32_t box[2] = {32, static_cast<cuuint32_t>(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(map, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // 2-D f32 tensor map over [rows][cols] (row stride cols floats), 32 x 32
 // boxes with 128B swizzle: the TMA-store target of the interpolation GEMM.
 bool make_out_map(CUtensorMap* map, void* ptr, uint64_t rows, uint64_t cols) {
@@ -717,6 +929,9 @@ cudaError_t tc_set_smem() {
     return e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<2, kRowBNWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, kRowBNWide, true)))))
+    return e;
+  if ((e = cudaFuncSetAttribute(tc_interp_w256, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(w256_smem_bytes()))))
     return e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, 128)))))
@@ -1074,8 +1289,15 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.out_tma = make_out_map(&mo, o, static_cast<uint64_t>(nc) * n, n) ? 1 : 0;
       if (!p.out_tma) mo = tc.map_ai;  // unused
       dim3 g(1, n / 128, nc);
+      CUtensorMap mbZ64;
+      const bool w256 = p.out_tma && n % 256 == 0 &&
+                        make_map_sw64(&mbZ64, BI, static_cast<uint64_t>(nc) * 2 * n, sep ? M : kbI, 256,
+                                      sep ? M : kcI, sep);
       prof.begin("tc_dft_gemm<interp>", st);
-      if (sep)
+      if (w256) {  // 128 x 256 tiles, the B operand through 32-wide boxes
+        p.G = n / 256;
+        tc_interp_w256<<<g, 192, w256_smem_bytes(), st>>>(sep ? tc.map_pi : tc.map_ai, mbZ64, mo, p);
+      } else if (sep)
         tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_pi, mbZ, mo, p);
       else
         tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_ai, mbI, mo, p);

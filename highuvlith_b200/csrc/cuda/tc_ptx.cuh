@@ -190,6 +190,18 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
   return d;
 }
 
+// Shared-memory matrix descriptor: K-major, 64-byte swizzle, rows of 64 B,
+// 8-row groups 512 B apart (the layout TMA writes with SWIZZLE_64B).
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFF) >> 4);       // start address
+  d |= static_cast<uint64_t>(1) << 16;                        // leading byte offset (unused for swizzled K-major)
+  d |= static_cast<uint64_t>(512 >> 4) << 32;                 // stride byte offset: 8 rows x 64 B
+  d |= static_cast<uint64_t>(1) << 46;                        // descriptor version (sm_100)
+  d |= static_cast<uint64_t>(4) << 61;                        // layout: SWIZZLE_64B
+  return d;
+}
+
 // Instruction descriptor, kind::f16: D f32, A/B bf16, both K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
