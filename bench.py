@@ -453,7 +453,7 @@ def run_ours(args):
     sep = args.form in ("auto", "hybrid") and m_f <= 192
     k_int = m_f if sep else 2 * (2 * hb_ + 1)
     if sep:  # the separable form's output GEMM (ncu --set full, 32 clips)
-        traffic_per_clip["tc_dft_gemm<interp>"] = (22.96e6 + 76.30e6) / 32
+        traffic_per_clip["tc_dft_gemm<interp>"] = (22.98e6 + 75.12e6) / 32
     own_bytes = {"socs_cols_inv": 8 * K * Bb * m_f + 4 * m_f * m_f,
                  "socs_rows_inv": 8 * K * Bb * m_f + 8 * Bb * Bb,
                  "tc_dft_gemm<sumsq>": 4 * K * m_f * kb + 4 * m_f * m_f,
