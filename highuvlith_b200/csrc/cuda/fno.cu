@@ -1052,9 +1052,9 @@ huv_status huv_fno_create(int32_t grid, int32_t width, int32_t modes, int32_t la
   return fno_guard([&] {
     if (!fno_out) throw Error(HUV_ERR_INVALID_PARAMETER, "fno_out: null");
     if (width != 64 || proj != 128)
-      throw Error(HUV_ERR_UNSUPPORTED, "fno: this build's kernels are specialised to width 64, projection 128");
+      throw Error(HUV_ERR_UNSUPPORTED, "fno: the FNO kernels are specialised to width 64, projection 128");
     if (modes > 16)
-      throw Error(HUV_ERR_UNSUPPORTED, "fno: this build's DFT tiles hold at most 16 retained modes per axis");
+      throw Error(HUV_ERR_UNSUPPORTED, "fno: the DFT tiles hold at most 16 retained modes per axis");
     if (grid < 8 || (grid & (grid - 1)) || modes < 1 || 2 * modes > grid || layers < 1)
       throw Error(HUV_ERR_INVALID_PARAMETER, "fno: grid power of two >= 8, 1 <= modes <= grid/2, layers >= 1");
     *fno_out = new Fno(grid, width, modes, layers, proj, seed, device);

@@ -530,10 +530,10 @@ void Engine::image_batch(const huv_batch& b, float* out, cudaStream_t st) {
   const int M = (form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS) ? Mp2 : choose_eval_grid(ds, b.eval_grid, true);
   if (form == HUV_FORM_AUTO) form = hybrid_supported(ds, M) ? HUV_FORM_HYBRID : HUV_FORM_FFT;
   if (form == HUV_FORM_HYBRID) {
-    if (!hybrid_supported(ds, M)) throw Error(HUV_ERR_UNSUPPORTED, "hybrid form: unsupported band/grid for this build");
+    if (!hybrid_supported(ds, M)) throw Error(HUV_ERR_UNSUPPORTED, "hybrid form: band or grid outside what its kernels support");
     run_tc_form(b, ds, M, out, st, 0, nullptr, kTcCoreFftField);
   } else if (form == HUV_FORM_TC || form == HUV_FORM_TC_ROWS) {
-    if (!tc_supported(ds, Mtc)) throw Error(HUV_ERR_UNSUPPORTED, "TC form: unsupported band/grid for this build");
+    if (!tc_supported(ds, Mtc)) throw Error(HUV_ERR_UNSUPPORTED, "TC form: band or grid outside what its kernels support");
     run_tc_form(b, ds, Mtc, out, st, 0, nullptr, form == HUV_FORM_TC_ROWS ? kTcCoreGemmRows : kTcCoreFftRows);
   } else if (form == HUV_FORM_FFT) {
     run_fft_form(b, ds, M, out, st);

@@ -5,7 +5,7 @@
 //
 // Follows KernelBuilder::build (crates/highuvlith-core/src/aerial.rs:1041-1317)
 // and select_kernel_count (aerial.rs:992-1029).  The reference switches to a
-// randomized eigensolver for large problems; this build always solves
+// randomized eigensolver for large problems; the host builder always solves
 // densely (exact), which the reference's own tests bound to 1e-5 in the image.
 #include <algorithm>
 #include <atomic>

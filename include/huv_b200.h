@@ -40,7 +40,7 @@ typedef enum {
   HUV_ERR_CUDA = 8,                    /* a CUDA runtime call failed */
   HUV_ERR_OUT_OF_MEMORY = 9,           /* device or host allocation failed */
   HUV_ERR_DEVICE_TIMEOUT = 10,         /* a bounded device-side wait gave up */
-  HUV_ERR_UNSUPPORTED = 11             /* valid request this build does not serve */
+  HUV_ERR_UNSUPPORTED = 11             /* valid request the library does not serve */
 } huv_status;
 
 /* Pupil fills (crates/highuvlith-core/src/source.rs:163-186, 1178-1248) plus the
