@@ -455,7 +455,9 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
   const size_t per_t2 = coarse ? align256(sizeof(float2) * static_cast<size_t>(B2) * n) : 0;
   const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
   const size_t per_clip = per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2 + per_mean;
-  const size_t budget = size_t(1) << 30;
+  // 2 GiB of workspace per chunk: a C2 step (256 clips) runs as one chunk, so the
+  // column pass (2 blocks per SM, 10 blocks per clip) fills whole waves
+  const size_t budget = size_t(2) << 30;
   const int chunk = balanced_chunk(static_cast<int>(std::max<size_t>(1, budget / per_clip)), b.n_clips);
   char* base = static_cast<char*>(workspace(per_clip * chunk + 4096));
   float2* X = reinterpret_cast<float2*>(base);
