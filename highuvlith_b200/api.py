@@ -267,10 +267,12 @@ class SimulationEngine:
         ``False`` gives ``compute_from_transmittance`` (aerial.rs:1789-1798).
         ``form``: "fft" (FP32 register-radix FFTs throughout), "tc" (split-BF16x3
         tcgen05 y-contraction and band interpolation), "tc_rows" (row
-        transforms on tcgen05 too), "hybrid" (FP32 FFT field pass, tcgen05
-        band interpolation) or "auto" (hybrid where the tensor-core form
-        applies, else fft).
-        Returns a float32 (B, N, N) tensor (``out`` if given)."""
+        transforms on tcgen05 too), "hybrid" (FP32 FFT field pass on the
+        coarse grid, then the exact band interpolation I_N = P I_M P^T as two
+        split-FP16x3 tcgen05 GEMMs) or "auto" (hybrid where its kernels
+        apply, else fft).
+        Returns a float32 (B, N, N) tensor; ``out``, if given, must be a
+        contiguous float32 (B, N, N) tensor on the rasters' device."""
         import torch
         n = self.grid.size
         if rasters.dim() == 2:
@@ -282,6 +284,10 @@ class SimulationEngine:
         rasters = rasters.contiguous()
         if out is None:
             out = torch.empty((rasters.shape[0], n, n), dtype=torch.float32, device=rasters.device)
+        elif (out.dtype != torch.float32 or out.device != rasters.device or not out.is_contiguous()
+              or tuple(out.shape) != (rasters.shape[0], n, n)):
+            raise ValueError(f"out must be a contiguous float32 ({rasters.shape[0]}, {n}, {n}) tensor on "
+                             f"{rasters.device}")
         b = L.Batch(rasters.shape[0], self._kind(rasters), rasters.data_ptr(), int(pixel_transfer),
                     float(focus_nm), L.FORM[form], int(eval_grid))
         st = (stream or torch.cuda.current_stream(rasters.device)).cuda_stream
@@ -292,7 +298,8 @@ class SimulationEngine:
                            form: str = "auto", eval_grid: int = 0, out: Optional[np.ndarray] = None,
                            stream=None) -> np.ndarray:
         """Same as ``compute_batch`` from host memory to host memory (copies
-        included; pinned buffers make them faster)."""
+        included; pinned buffers make them faster).  ``out``, if given, must
+        be a writeable C-contiguous float32 (B, N, N) array."""
         n = self.grid.size
         r = np.ascontiguousarray(rasters)
         if r.ndim == 2:
@@ -305,6 +312,9 @@ class SimulationEngine:
             raise ValueError(f"rasters must be (B, {n}, {n})")
         if out is None:
             out = np.empty((r.shape[0], n, n), dtype=np.float32)
+        elif (not isinstance(out, np.ndarray) or out.dtype != np.float32 or out.shape != (r.shape[0], n, n)
+              or not out.flags.c_contiguous or not out.flags.writeable):
+            raise ValueError(f"out must be a writeable C-contiguous float32 ({r.shape[0]}, {n}, {n}) array")
         b = L.Batch(r.shape[0], kind, r.ctypes.data, int(pixel_transfer), float(focus_nm), L.FORM[form],
                     int(eval_grid))
         st = 0

@@ -133,6 +133,22 @@ def test_misaligned_device_buffers_are_rejected_before_any_launch():
     assert b"16-byte aligned" in lib.huv_last_error()
 
 
+def test_host_output_buffer_is_validated_before_the_call():
+    """compute_batch_host writes through the output's raw pointer, so a
+    wrong dtype, shape or layout is refused in Python first."""
+    eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(),
+                              grid=HB.GridConfig(64, 1.0), max_kernels=4)
+    masks = np.zeros((2, 64, 64), np.uint8)
+    bad = [np.empty((2, 64, 64), np.float64), np.empty((1, 64, 64), np.float32),
+           np.empty((2, 64, 128), np.float32)[:, :, ::2]]
+    ro = np.empty((2, 64, 64), np.float32)
+    ro.flags.writeable = False
+    bad.append(ro)
+    for out in bad:
+        with pytest.raises(ValueError):
+            eng.compute_batch_host(masks, out=out)
+
+
 def test_c2_kernel_set_shape():
     """C2: EUV NA 0.33, sigma 0.5, 1024 x 1 nm -> r = 37.55, h = 37, S = 4429, K = 32."""
     eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(),
