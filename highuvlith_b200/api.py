@@ -359,6 +359,9 @@ class SimulationEngine:
         view = self._rect_clips(clips, feature, background)
         if out is None:
             out = torch.empty((len(clips), n, n), dtype=torch.float32, device=f"cuda:{self.device}")
+        elif (out.dtype != torch.float32 or not out.is_cuda or not out.is_contiguous()
+              or tuple(out.shape) != (len(clips), n, n)):
+            raise ValueError(f"out must be a contiguous float32 ({len(clips)}, {n}, {n}) CUDA tensor")
         b = L.Batch(len(clips), L.INPUT_RECTS, C.addressof(view), 0, float(focus_nm), L.FORM[form], int(eval_grid))
         st = (stream or torch.cuda.current_stream(out.device)).cuda_stream
         L.check(L.lib().huv_image_batch(self._h, C.byref(b), out.data_ptr(), st))
@@ -400,6 +403,10 @@ class SimulationEngine:
         z = np.ascontiguousarray(np.asarray(focus_nm, dtype=np.float64).reshape(-1))
         if out is None:
             out = torch.empty((len(z), rasters.shape[0], n, n), dtype=torch.float32, device=rasters.device)
+        elif (out.dtype != torch.float32 or out.device != rasters.device or not out.is_contiguous()
+              or tuple(out.shape) != (len(z), rasters.shape[0], n, n)):
+            raise ValueError(f"out must be a contiguous float32 ({len(z)}, {rasters.shape[0]}, {n}, {n}) tensor "
+                             f"on {rasters.device}")
         b = L.Batch(rasters.shape[0], self._kind(rasters), rasters.data_ptr(), int(pixel_transfer), 0.0,
                     L.FORM[form], int(eval_grid))
         st = (stream or torch.cuda.current_stream(rasters.device)).cuda_stream

@@ -55,33 +55,51 @@ class FnoSurrogate:
     def load(self, path: str) -> None:
         self.set_params(np.load(path)["params"])
 
+    def _maps(self, t, name: str):
+        """A (B, grid, grid) float32 contiguous CUDA copy (or the tensor itself)."""
+        g = self.grid
+        if t.dim() != 3 or tuple(t.shape[1:]) != (g, g) or not t.is_cuda:
+            raise ValueError(f"{name} must be a (B, {g}, {g}) CUDA tensor")
+        return t.float().contiguous()
+
     def forward(self, masks, out=None, stream=None):
         import torch
-        masks = masks.contiguous().float()
+        masks = self._maps(masks, "masks")
         if out is None:
             out = torch.empty_like(masks)
+        elif (out.dtype != torch.float32 or out.device != masks.device or not out.is_contiguous()
+              or tuple(out.shape) != tuple(masks.shape)):
+            raise ValueError(f"out must be a contiguous float32 {tuple(masks.shape)} tensor on {masks.device}")
         st = (stream or torch.cuda.current_stream()).cuda_stream
         L.check(L.lib().huv_fno_forward(self._h, masks.shape[0], masks.data_ptr(), out.data_ptr(), st))
         return out
 
     def backward(self, masks, targets=None, dout=None, want_param_grad=True, want_input_grad=False, stream=None):
         import torch
-        masks = masks.contiguous().float()
+        masks = self._maps(masks, "masks")
+        targets = self._maps(targets, "targets") if targets is not None else None
+        dout = self._maps(dout, "dout") if dout is not None else None
+        for name, t in (("targets", targets), ("dout", dout)):
+            if t is not None and tuple(t.shape) != tuple(masks.shape):
+                raise ValueError(f"{name} must have the masks' shape {tuple(masks.shape)}")
         pg = torch.empty(self.num_params(), dtype=torch.float32, device=masks.device) if want_param_grad else None
         dm = torch.empty_like(masks) if want_input_grad else None
         loss = C.c_float(0.0)
         st = (stream or torch.cuda.current_stream()).cuda_stream
         L.check(L.lib().huv_fno_backward(self._h, masks.shape[0], masks.data_ptr(),
-                                         targets.contiguous().data_ptr() if targets is not None else None,
-                                         dout.contiguous().data_ptr() if dout is not None else None,
+                                         targets.data_ptr() if targets is not None else None,
+                                         dout.data_ptr() if dout is not None else None,
                                          pg.data_ptr() if pg is not None else None,
                                          dm.data_ptr() if dm is not None else None, C.byref(loss), st))
         return loss.value, pg, dm
 
     def train_step(self, masks, targets, lr: float = 1e-3, weight_decay: float = 0.0, stream=None) -> float:
         import torch
+        masks, targets = self._maps(masks, "masks"), self._maps(targets, "targets")
+        if tuple(targets.shape) != tuple(masks.shape):
+            raise ValueError(f"targets must have the masks' shape {tuple(masks.shape)}")
         loss = C.c_float(0.0)
         st = (stream or torch.cuda.current_stream()).cuda_stream
-        L.check(L.lib().huv_fno_train_step(self._h, masks.shape[0], masks.contiguous().data_ptr(),
-                                           targets.contiguous().data_ptr(), lr, weight_decay, C.byref(loss), st))
+        L.check(L.lib().huv_fno_train_step(self._h, masks.shape[0], masks.data_ptr(),
+                                           targets.data_ptr(), lr, weight_decay, C.byref(loss), st))
         return loss.value

@@ -43,12 +43,30 @@ def initial_theta_from_target(target):
     return target - 0.5
 
 
-def cost_and_gradient(engine, theta, target, settings: IltSettings, want_gradient: bool = True, stream=None):
-    """theta, target: float32 torch tensors (B, N, N) on the engine's device.
-    Returns (costs numpy (B,), gradient tensor or None)."""
+def _masks_on_device(engine, theta, target, in_place: bool):
+    """theta (B, N, N) float32 CUDA tensor (kept as given when it is updated
+    in place, else converted), target converted to match it."""
     import torch
-    theta = theta.contiguous()
-    target = target.contiguous()
+    n = engine.grid.size
+    if theta.dim() != 3 or tuple(theta.shape[1:]) != (n, n) or not theta.is_cuda:
+        raise ValueError(f"theta must be a (B, {n}, {n}) CUDA tensor")
+    if in_place:
+        if theta.dtype != torch.float32 or not theta.is_contiguous():
+            raise ValueError("theta is updated in place: it must be a contiguous float32 tensor")
+    else:
+        theta = theta.to(dtype=torch.float32).contiguous()
+    target = torch.as_tensor(target).to(device=theta.device, dtype=torch.float32).contiguous()
+    if tuple(target.shape) != tuple(theta.shape):
+        raise ValueError(f"target must have theta's shape {tuple(theta.shape)}, got {tuple(target.shape)}")
+    return theta, target
+
+
+def cost_and_gradient(engine, theta, target, settings: IltSettings, want_gradient: bool = True, stream=None):
+    """theta, target: torch tensors (B, N, N) on the engine's device (float32
+    is used; other dtypes are converted).  Returns (costs numpy (B,),
+    gradient tensor or None)."""
+    import torch
+    theta, target = _masks_on_device(engine, theta, target, in_place=False)
     b = theta.shape[0]
     cost = np.zeros(b)
     grad = torch.empty_like(theta) if want_gradient else None
@@ -60,9 +78,11 @@ def cost_and_gradient(engine, theta, target, settings: IltSettings, want_gradien
 
 
 def optimize(engine, theta, target, settings: IltSettings, stream=None):
-    """Run the ILT stage loop on every mask; theta is updated in place.
+    """Run the ILT stage loop on every mask; theta (a contiguous float32
+    (B, N, N) CUDA tensor) is updated in place.
     Returns dict(final_cost, iterations, cost_history)."""
     import torch
+    theta, target = _masks_on_device(engine, theta, target, in_place=True)
     b = theta.shape[0]
     fc = np.zeros(b)
     its = np.zeros(b, dtype=np.int32)
@@ -70,6 +90,6 @@ def optimize(engine, theta, target, settings: IltSettings, stream=None):
     opt = L.IltOpt(settings.max_iterations, settings.learning_rate, settings.convergence_tol)
     st = (stream or torch.cuda.current_stream(theta.device)).cuda_stream
     L.check(L.lib().huv_ilt_optimize(engine.handle, C.byref(settings._params()), C.byref(opt), b,
-                                     theta.data_ptr(), target.contiguous().data_ptr(), fc.ctypes.data,
+                                     theta.data_ptr(), target.data_ptr(), fc.ctypes.data,
                                      its.ctypes.data, hist.ctypes.data, st))
     return {"final_cost": fc, "iterations": its, "cost_history": hist}

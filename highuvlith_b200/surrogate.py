@@ -176,6 +176,8 @@ def optimize_with_surrogate(engine: SimulationEngine, fno: FnoSurrogate, theta, 
     ``final_cost`` is the exact SOCS cost; ``cost_history`` holds the costs
     the optimizer saw (surrogate ones until a takeover)."""
     import torch
+    from .ilt import _masks_on_device
+    theta, target = _masks_on_device(engine, theta, target, in_place=True)
     b = theta.shape[0]
     fc = np.zeros(b)
     its = np.zeros(b, dtype=np.int32)
@@ -186,7 +188,7 @@ def optimize_with_surrogate(engine: SimulationEngine, fno: FnoSurrogate, theta, 
     sur.error_bound = error_bound
     st = (stream or torch.cuda.current_stream(theta.device)).cuda_stream
     L.check(L.lib().huv_ilt_optimize_surrogate(engine.handle, fno.handle, C.byref(settings._params()), C.byref(opt),
-                                               b, theta.data_ptr(), target.contiguous().data_ptr(), C.byref(sur),
+                                               b, theta.data_ptr(), target.data_ptr(), C.byref(sur),
                                                fc.ctypes.data, its.ctypes.data, hist.ctypes.data, st))
     return SurrogateReport(fc, its, hist, sur.surrogate_iterations, sur.exact_iterations, sur.takeover_iteration,
                            [sur.judge_errors[i] for i in range(min(sur.n_judges, 64))])

@@ -149,6 +149,21 @@ def test_host_output_buffer_is_validated_before_the_call():
             eng.compute_batch_host(masks, out=out)
 
 
+def test_ilt_inputs_are_validated_before_the_call():
+    """The ILT wrappers pass raw device pointers: a theta of the wrong grid,
+    a host tensor, or a target of another shape is refused in Python."""
+    import torch
+    from highuvlith_b200 import ilt
+    eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(),
+                              grid=HB.GridConfig(64, 1.0), max_kernels=4)
+    st = ilt.IltSettings(max_iterations=1)
+    for theta in (torch.zeros((1, 32, 32)), torch.zeros((1, 64, 64)), torch.zeros((64, 64))):
+        with pytest.raises(ValueError):
+            ilt.cost_and_gradient(eng, theta, theta, st)
+        with pytest.raises(ValueError):
+            ilt.optimize(eng, theta, theta, st)
+
+
 def test_c2_kernel_set_shape():
     """C2: EUV NA 0.33, sigma 0.5, 1024 x 1 nm -> r = 37.55, h = 37, S = 4429, K = 32."""
     eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(),
