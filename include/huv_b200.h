@@ -143,11 +143,12 @@ typedef struct {
 
 /* Which device form evaluates the SOCS sum. */
 typedef enum {
-  HUV_FORM_AUTO = 0, /* autotuned choice */
+  HUV_FORM_AUTO = 0, /* hybrid where its kernels apply, else FFT (huv_plan_* times the forms per group) */
   HUV_FORM_FFT = 1,  /* plain FP32 FFT form */
   HUV_FORM_TC = 2,   /* split-BF16x3 tcgen05 DFT-GEMM form (row transforms as FP32 FFTs) */
   HUV_FORM_TC_ROWS = 3, /* the same with the row transforms as tcgen05 DFT-GEMMs too */
-  HUV_FORM_HYBRID = 4   /* FP32 FFT field pass on the evaluation grid + tcgen05 band interpolation */
+  HUV_FORM_HYBRID = 4   /* FP32 FFT field pass on the evaluation grid + tcgen05 band interpolation
+                           (separable, split-FP16x3, on evaluation grids of at most 192 points) */
 } huv_form;
 
 typedef struct {
