@@ -166,34 +166,51 @@ def cpu_model() -> str:
 
 
 def run_reference(args):
-    """Reference arm: the reference's CPU algorithm (C restatement of the
-    Rust path; the Rust crate cannot be built here) on the host cores."""
+    """Reference arm: the reference's CPU algorithm (FP64 restatements of the
+    Rust path; the Rust crate cannot be built here) on every host core.  Two
+    series are warmed up on the same sample, the C port (radix-2 FFT) and
+    pocketfft (scipy.fft); the faster one is timed."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from highuvlith_b200.clips import gen_batch
+    from oracle import socs_scipy
     threads = os.cpu_count() or 1
     _, ks = oracle_kernel_set()
     per_step = max(4, min(threads, 64))
     _, rasters = gen_batch(per_step, N_GRID, base_seed=2026)
-    for _ in range(args.warmup):
-        cpu_sample(ks, rasters, threads)
+    prep = socs_scipy.Prepared(ks)
+    series = {"c_port_radix2": lambda: cpu_sample(ks, rasters, threads),
+              "scipy_pocketfft": lambda: _timed(lambda: socs_scipy.images(prep, rasters, threads=threads,
+                                                                          want_output=False))}
+    warm = {}
+    for name, fn in series.items():
+        for _ in range(max(1, args.warmup // 2)):
+            warm[name] = per_step / fn()
+    best = max(warm, key=warm.get)
     t = 0.0
     for _ in range(args.steps):
-        t += cpu_sample(ks, rasters, threads)
+        t += series[best]()
     v = per_step * args.steps / t
-    sample = f"{per_step} clips of the workload per step ({cpu_model()})"
+    sample = f"{per_step} clips of the workload per step, series {best} ({cpu_model()})"
     line = {
         "metric": METRIC, "value": v, "unit": "images/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "clips_per_step": per_step},
         "cpu_baseline": {"value": v, "unit": "images/s", "cores": threads, "kind": "port", "sample": sample,
-                         "note": "C restatement of the reference's Rust CPU path (reference binary unavailable)"},
+                         "series_warmup_images_per_s": warm,
+                         "note": "FP64 restatement of the reference's Rust CPU path (reference binary unavailable)"},
         "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+def _timed(fn):
+    t0 = time.perf_counter()
+    fn()
+    return time.perf_counter() - t0
 
 
 def accuracy(img: np.ndarray, raster: np.ndarray):
@@ -386,6 +403,80 @@ def uneven_leg(stream, n_clips=2048, steps=3):
             "setup_s": {"engines": t_engines, "clip_generation": t_gen, "plan_autotune_capture": t_plan}}
 
 
+def cpu_baseline_leg(gen_batch):
+    """CPU baseline on the host cores, a bounded sample of the workload: the
+    C port (radix-2 FFT) and the pocketfft series (scipy.fft), both FP64 on
+    every host thread; ``value`` is the faster of the two."""
+    from oracle import socs_scipy
+    threads = os.cpu_count() or 1
+    _, ks = oracle_kernel_set()
+    sample_n = max(4, min(threads, 32))
+    _, srast = gen_batch(sample_n, N_GRID, base_seed=2026)
+    t = cpu_sample(ks, srast, threads)
+    while t < 8.0 and sample_n < 512:
+        sample_n *= 2
+        _, srast = gen_batch(sample_n, N_GRID, base_seed=2026)
+        t = cpu_sample(ks, srast, threads)
+    c_rate = sample_n / t
+    prep = socs_scipy.Prepared(ks)
+    sp_n = max(threads, 8)
+    _, sp_rast = gen_batch(sp_n, N_GRID, base_seed=2026)
+    t0 = time.perf_counter()
+    socs_scipy.images(prep, sp_rast, threads=threads, want_output=False)
+    sp_rate = sp_n / (time.perf_counter() - t0)
+    return {"value": max(c_rate, sp_rate), "unit": "images/s", "cores": threads, "kind": "port",
+            "sample": f"{sample_n} clips (C port) and {sp_n} clips (pocketfft) of the workload, FP64, {cpu_model()}",
+            "series": {"c_port_radix2": c_rate, "scipy_pocketfft": sp_rate}}
+
+
+def forms_leg(step, stream, diag, K, tc_sus):
+    """Every device form on the same batch (two timed steps each), with the
+    whole-path work per image: the reference's FFT FLOPs
+    (5 N^2 log2 N^2 + K (5 B N log2 N + 5 N^2 log2 N)) for the FFT forms, and
+    the split-BF16 DFT-GEMM FLOPs of the coarse-grid formulation (band forward
+    4 B N^2 + 8 B^2 N, inverse K 8 (B^2 M + B M^2), interpolation
+    8 (M^2 N + M N^2), split products counted once) for the TC forms."""
+    import torch
+    forms = {}
+    for name, form, eg in (("fft_full_grid", "fft", N_GRID), ("fft_coarse_grid", "fft", 0), ("tc", "tc", 0),
+                           ("tc_gemm_rows", "tc_rows", 0), ("hybrid", "hybrid", 0)):
+        try:
+            step(form, eg)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(2):
+                step(form, eg)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            fms = e0.elapsed_time(e1) / 2
+            forms[name] = {"ms_per_step": fms, "images_per_s": N_CLIPS / (fms / 1e3)}
+        except Exception as exc:  # report, do not hide
+            forms[name] = {"unavailable": str(exc)[:200]}
+    Bw = 2 * diag["band_half_width"] + 1
+    M_eval = 256
+    lgN = math.log2(N_GRID)
+    f_fft = 5 * N_GRID ** 2 * 2 * lgN + K * (5 * Bw * N_GRID * lgN + 5 * N_GRID ** 2 * lgN)
+    f_tc = (4 * Bw * N_GRID ** 2 + 8 * Bw * Bw * N_GRID + K * 8 * (Bw * Bw * M_eval + Bw * M_eval ** 2)
+            + 8 * (M_eval ** 2 * N_GRID + M_eval * N_GRID ** 2))
+    for name, f, peak in (("fft_full_grid", f_fft, None), ("fft_coarse_grid", f_fft, None),
+                          ("tc", f_tc, tc_sus), ("tc_gemm_rows", f_tc, tc_sus)):
+        r = forms.get(name, {})
+        if "images_per_s" in r:
+            r["algorithmic_gflop_per_image"] = f / 1e9
+            r["algorithmic_tflops"] = f * r["images_per_s"] / 1e12
+            if peak:
+                r["frac_of_bf16_sustained"] = r["algorithmic_tflops"] / peak
+    rate = {k: v["images_per_s"] for k, v in forms.items() if isinstance(v, dict) and "images_per_s" in v}
+    if "fft_coarse_grid" in rate:
+        for k in ("tc", "tc_gemm_rows", "hybrid"):
+            if k in rate:
+                forms[f"{k}_over_fft_coarse_grid"] = rate[k] / rate["fft_coarse_grid"]
+    if "tc" in rate and "fft_full_grid" in rate:
+        forms["tc_over_fft_full_grid"] = rate["tc"] / rate["fft_full_grid"]
+    return forms
+
+
 def run_ours(args):
     import torch
     from highuvlith_b200.clips import gen_batch
@@ -465,25 +556,33 @@ def run_ours(args):
     launches = max(prof["launches"], 1)
     per_launch_s = prof["ms"] / launches / 1e3
     images_per_launch = N_CLIPS * args.steps / launches
-    achieved = bytes_per_image * images_per_launch / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
     total_ms = ms * args.steps
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": (traffic_per_clip[prof["kernel"]] * images_per_launch
-                            if prof["kernel"] in traffic_per_clip else None),
+    # whole path: 4 N^2 bytes in (u8 raster counted as the FP32 transmittance
+    # the reference reads) + 4 N^2 out + 8 K S of band kernels per image, over
+    # the step time
+    whole = bytes_per_image * value / 1e9
+    roofline = {"bound": "hbm", "peak": hbm, "unit": "GB/s", "kernel": prof["kernel"],
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                "whole_path": {"algorithmic_bytes_per_image": bytes_per_image, "achieved": whole,
+                               "frac": whole / hbm, "note": "(4 N^2 in + 4 N^2 out + 8 K S) per image x images/s"},
+                "kernel_share_of_step": prof["ms"] / total_ms if ms > 0 else None,
                 "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum per clip "
                                 "at 32 clips, x clips per launch)",
-                "kernel": prof["kernel"], "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
-                "algorithmic_bytes_per_image": bytes_per_image,
-                "kernel_share_of_step": prof["ms"] / total_ms if ms > 0 else None,
-                "note": "achieved = SURVEY 8(d) algorithmic bytes per image x images per launch / the dominant "
-                        "region's mean launch time (CUDA events on the launching stream)",
                 "regions": {k: {"launches": v[0], "ms": v[1], "share": v[1] / total_ms if total_ms > 0 else None}
                             for k, v in prof["regions"].items()}}
     if prof["kernel"] in own_bytes and per_launch_s > 0:
+        # the dominant region's own operands, each read or written once, over
+        # its mean launch time (CUDA events on the launching stream)
         kb_s = own_bytes[prof["kernel"]] * images_per_launch / per_launch_s / 1e9
-        roofline["kernel_own"] = {"algorithmic_bytes_per_clip": own_bytes[prof["kernel"]], "achieved": kb_s,
-                                  "unit": "GB/s", "frac": kb_s / hbm, "eval_grid": m_f,
-                                  "note": "the dominant region's own operands (in and out once) / its mean launch time"}
+        roofline.update({"achieved": kb_s, "frac": kb_s / hbm,
+                         "algorithmic_bytes_per_clip": own_bytes[prof["kernel"]], "clips_per_launch": images_per_launch,
+                         "eval_grid": m_f,
+                         "note": "achieved = the dominant region's own algorithmic bytes per clip x clips per launch "
+                                 "/ its mean launch time"})
+    else:
+        roofline.update({"achieved": whole, "frac": whole / hbm, "note": "achieved = whole-path bytes / step time"})
+    roofline["traffic"] = (traffic_per_clip[prof["kernel"]] * images_per_launch
+                           if prof["kernel"] in traffic_per_clip else None)
     gi = prof["regions"].get("tc_dft_gemm<interp>")
     if gi and gi[1] > 0:
         # the band interpolation's N x N output GEMM: 2 N^2 k_int FLOP per
@@ -523,68 +622,26 @@ def run_ours(args):
            "d2h_bytes_per_step": int(h_out.numel() * 4), "call": "huv_image_batch_host (pinned host buffers)"}
 
     extra = {}
+
+    def leg(name, fn):
+        """Run one extra leg; a failure is recorded in the line, never fatal."""
+        try:
+            extra[name] = fn()
+        except Exception as exc:  # report, do not hide
+            extra[name] = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+
     if rank == 0 and world == 1 and not args.quick:
-        # other device forms on the same batch (fewer steps), for the TC-vs-plain factor
-        forms = {}
-        for name, form, eg in (("fft_full_grid", "fft", N_GRID), ("fft_coarse_grid", "fft", 0), ("tc", "tc", 0),
-                               ("tc_gemm_rows", "tc_rows", 0), ("hybrid", "hybrid", 0)):
-            try:
-                step(form, eg)
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                for _ in range(2):
-                    step(form, eg)
-                e1.record(stream)
-                torch.cuda.synchronize()
-                fms = e0.elapsed_time(e1) / 2
-                forms[name] = {"ms_per_step": fms, "images_per_s": N_CLIPS / (fms / 1e3)}
-            except Exception as exc:  # report, do not hide
-                forms[name] = {"unavailable": str(exc)[:200]}
-        # SURVEY 8(d) whole-path work per image: the reference's FFT FLOPs
-        # (5 N^2 log2 N^2 + K (5 B N log2 N + 5 N^2 log2 N)) for the FFT forms,
-        # the split-BF16 DFT-GEMM FLOPs of the coarse-grid formulation (band
-        # forward 4 B N^2 + 8 B^2 N, inverse K 8 (B^2 M + B M^2), interpolation
-        # 8 (M^2 N + M N^2), split products counted once) for the TC form
-        Bw = 2 * diag["band_half_width"] + 1
-        M_eval = 256
-        lgN = math.log2(N_GRID)
-        f_fft = 5 * N_GRID ** 2 * 2 * lgN + K * (5 * Bw * N_GRID * lgN + 5 * N_GRID ** 2 * lgN)
-        f_tc = (4 * Bw * N_GRID ** 2 + 8 * Bw * Bw * N_GRID + K * 8 * (Bw * Bw * M_eval + Bw * M_eval ** 2)
-                + 8 * (M_eval ** 2 * N_GRID + M_eval * N_GRID ** 2))
-        for name, f, peak in (("fft_full_grid", f_fft, None), ("fft_coarse_grid", f_fft, None),
-                              ("tc", f_tc, tc_sus), ("tc_gemm_rows", f_tc, tc_sus)):
-            r = forms.get(name, {})
-            if "images_per_s" in r:
-                r["algorithmic_gflop_per_image"] = f / 1e9
-                r["algorithmic_tflops"] = f * r["images_per_s"] / 1e12
-                if peak:
-                    r["frac_of_bf16_sustained"] = r["algorithmic_tflops"] / peak
-        if "images_per_s" in forms.get("tc", {}) and "images_per_s" in forms.get("fft_coarse_grid", {}):
-            forms["tc_over_fft_coarse_grid"] = forms["tc"]["images_per_s"] / forms["fft_coarse_grid"]["images_per_s"]
-            forms["tc_over_fft_full_grid"] = forms["tc"]["images_per_s"] / forms["fft_full_grid"]["images_per_s"]
-        if "images_per_s" in forms.get("hybrid", {}) and "images_per_s" in forms.get("fft_coarse_grid", {}):
-            forms["hybrid_over_fft_coarse_grid"] = (forms["hybrid"]["images_per_s"]
-                                                    / forms["fft_coarse_grid"]["images_per_s"])
-        extra["forms"] = forms
-        extra["ilt"] = ilt_leg(eng, stream)
-        extra["uneven_batch"] = uneven_leg(stream, n_clips=args.uneven_clips)
-        extra["focus_sweep"] = focus_sweep_leg()
-        step(args.form, args.eval_grid)
-        torch.cuda.synchronize()
-        extra["accuracy"] = accuracy(d_out[0].cpu().numpy(), rasters[0])
-        # CPU baseline: the oracle's C port on host cores, bounded sample
-        threads = os.cpu_count() or 1
-        _, ks = oracle_kernel_set()
-        sample_n = max(4, min(threads, 32))
-        _, srast = gen_batch(sample_n, N_GRID, base_seed=2026)
-        t = cpu_sample(ks, srast, threads)
-        while t < 8.0 and sample_n < 512:
-            sample_n *= 2
-            _, srast = gen_batch(sample_n, N_GRID, base_seed=2026)
-            t = cpu_sample(ks, srast, threads)
-        extra["cpu_baseline"] = {"value": sample_n / t, "unit": "images/s", "cores": threads, "kind": "port",
-                                 "sample": f"{sample_n} clips of the workload, FP64, {cpu_model()}"}
+        def acc_leg():
+            step(args.form, args.eval_grid)
+            torch.cuda.synchronize()
+            return accuracy(d_out[0].cpu().numpy(), rasters[0])
+
+        leg("accuracy", acc_leg)
+        leg("cpu_baseline", lambda: cpu_baseline_leg(gen_batch))
+        leg("forms", lambda: forms_leg(step, stream, diag, K, tc_sus))
+        leg("ilt", lambda: ilt_leg(eng, stream))
+        leg("focus_sweep", focus_sweep_leg)
+        leg("uneven_batch", lambda: uneven_leg(stream, n_clips=args.uneven_clips))
 
     if rank == 0:
         line = {

@@ -774,7 +774,7 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   const size_t s_preg = a256(sizeof(double) * std::max(reg_parts, 2 * kRedBlocks));
   const size_t per = s_t + s_x + s_m + s_mean + s_T + s_im + s_c + s_x2 + s_img + s_V + s_q + s_t2 + 2 * s_parts +
                      s_preg + a256(sizeof(double) * 4);
-  const size_t budget = size_t(2) << 30;
+  const size_t budget = chunk_budget();
   const int chunk = balanced_chunk(static_cast<int>(std::max<size_t>(1, budget / per)), masks);
   char* base = static_cast<char*>(workspace(per * chunk + 4096));
   size_t off = 0;

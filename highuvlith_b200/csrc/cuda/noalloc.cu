@@ -96,8 +96,23 @@ extern "C" huv_status huv_image_batch_noalloc(void* engine, const huv_batch* bat
     huv::check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
     char* base = static_cast<char*>(scratch_for_device(e->device));
 
-    // Host-side band kernels (pre-scaled like the engine's device set).
-    std::shared_ptr<huv::KernelSet> ks = e->kernel_set(b.defocus_nm == 0.0 ? 0.0 : b.defocus_nm);
+    // Host-side band kernels (pre-scaled like the engine's device set).  The
+    // engine's plane cache is only read: a plane it does not hold is built
+    // here on the host (FP64, as the engine's host build does) and dropped
+    // after the call, never cached, so no device set is built or evicted.
+    // An engine whose kernels are built on the GPU would need device memory
+    // for that build, so it must hold the plane already.
+    const double z = b.defocus_nm == 0.0 ? 0.0 : b.defocus_nm;
+    std::shared_ptr<huv::KernelSet> ks = e->held_set(z);
+    if (!ks) {
+      if (e->settings.kernel_build != HUV_BUILD_HOST)
+        throw huv::Error(HUV_ERR_UNSUPPORTED,
+                         "allocation-free path: focus plane not cached, and this engine builds kernels on the GPU; "
+                         "image the plane once with huv_image_batch (or huv_image_focus_sweep) first");
+      ks = std::make_shared<huv::KernelSet>(huv::build_kernels(e->points, e->optics, e->n, e->pixel_nm, e->lambda,
+                                                               e->settings.max_kernels,
+                                                               e->settings.kernel_energy_fraction, z));
+    }
     const int n = e->n;
     const int h = ks->band_half_width(), B = 2 * h + 1, K = ks->num_kernels();
     const int S = static_cast<int>(ks->support.size());

@@ -1092,9 +1092,9 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   const size_t per_bi = align256(static_cast<size_t>(2) * n * std::max(kbI, M) * 2);
   const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
   const size_t per_clip = per_x + per_m + per_be + per_p + per_i + per_x2 + per_c + per_bi + per_mean;
-  // 2 GiB of workspace per chunk: a C2 step (256 clips) runs as one chunk, so the
-  // column pass (2 blocks per SM, 10 blocks per clip) fills whole waves
-  const size_t budget = size_t(2) << 30;
+  // a C2 step (256 clips) runs as one chunk of the engine's own workspace, so
+  // the column pass (2 blocks per SM, 10 blocks per clip) fills whole waves
+  const size_t budget = chunk_budget();
   const int chunk = balanced_chunk(static_cast<int>(std::max<size_t>(1, budget / per_clip)), b.n_clips);
   char* base = static_cast<char*>(workspace(per_clip * chunk + 4096));
   size_t off = 0;

@@ -168,6 +168,13 @@ std::shared_ptr<KernelSet> Engine::kernel_set(double z) {
   return ks;
 }
 
+std::shared_ptr<KernelSet> Engine::held_set(double z) {
+  if (z == 0.0) return focus;
+  for (auto& e : cache)
+    if (e.z == z) return e.ks;
+  return nullptr;
+}
+
 void Engine::cache_insert(double z, std::shared_ptr<KernelSet> ks) {
   if (settings.kernel_cache_capacity <= 0) {
     scratch_set = ks;
@@ -340,6 +347,7 @@ DeviceSet& Engine::device_set(double z) {
   }
   DeviceSet d;
   d.source = ks.get();
+  d.hold = ks;
   d.hb = h;
   d.B = B;
   d.K = K;
@@ -455,9 +463,9 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
   const size_t per_t2 = coarse ? align256(sizeof(float2) * static_cast<size_t>(B2) * n) : 0;
   const size_t per_mean = align256(sizeof(float) * (1 + (B + 3) / 4));
   const size_t per_clip = per_x + per_m + per_t + per_i + per_x2 + per_c + per_t2 + per_mean;
-  // 2 GiB of workspace per chunk: a C2 step (256 clips) runs as one chunk, so the
-  // column pass (2 blocks per SM, 10 blocks per clip) fills whole waves
-  const size_t budget = size_t(2) << 30;
+  // a C2 step (256 clips) runs as one chunk of the engine's own workspace, so
+  // the column pass (2 blocks per SM, 10 blocks per clip) fills whole waves
+  const size_t budget = chunk_budget();
   const int chunk = balanced_chunk(static_cast<int>(std::max<size_t>(1, budget / per_clip)), b.n_clips);
   char* base = static_cast<char*>(workspace(per_clip * chunk + 4096));
   float2* X = reinterpret_cast<float2*>(base);

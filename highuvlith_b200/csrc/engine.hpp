@@ -83,6 +83,9 @@ struct TcState {
 // (B x B) and the pixel-transfer factors (B).
 struct DeviceSet {
   const KernelSet* source = nullptr;
+  // Keeps `source` alive while this copy refers to it, so a later set can
+  // never be allocated at the same address and mistaken for it.
+  std::shared_ptr<KernelSet> hold;
   int hb = 0, B = 0, K = 0;
   float keep = 1.f, flare = 0.f;
   float2* kband = nullptr;
@@ -179,6 +182,9 @@ struct Engine {
   ~Engine();
 
   std::shared_ptr<KernelSet> kernel_set(double z);
+  // The kernel set of plane z if the engine holds it already (the in-focus
+  // set or a cached plane), else null; builds, evicts and allocates nothing.
+  std::shared_ptr<KernelSet> held_set(double z);
   void cache_insert(double z, std::shared_ptr<KernelSet> ks);
   // The kernel set of focus plane z, built where settings.kernel_build says.
   KernelSet build_set(double z);
@@ -205,6 +211,14 @@ struct Engine {
   const uint8_t* row_digit_table(int hb);
   DeviceSet& device_set(double z);
   void* workspace(size_t bytes);
+  // Bytes a batch chunk may take of the workspace: 2 GiB of the engine's
+  // own (a C2 step of 256 clips is one chunk), or what a captured plan's
+  // workspace holds beyond the 4 KiB alignment slack every chunk adds.
+  size_t chunk_budget() const {
+    constexpr size_t kOwn = size_t(2) << 30, kSlack = 8192;
+    if (!ws_override) return kOwn;
+    return ws_override_bytes > kSlack ? ws_override_bytes - kSlack : 1;
+  }
   // Device buffer of at least n doubles for per-mask ILT costs, kept (and
   // grown) for the engine's lifetime.
   double* ilt_cost_buffer(int n);

@@ -260,8 +260,11 @@ huv_status huv_plan_create(const huv_clip* clips, int32_t n_clips, int32_t pixel
     }
     rep << "]";
     plan->report = rep.str();
-    // One shared workspace for all groups (groups run one after another).
-    const size_t wsb = (size_t(1) << 30) + 8192;
+    // One shared workspace for all groups (groups run one after another):
+    // as large as an engine's own chunk budget plus the per-chunk slack, so
+    // each group's chunks are those of its standalone runs (every chunking
+    // in the engine sizes itself by Engine::chunk_budget()).
+    const size_t wsb = (size_t(2) << 30) + 8192;
     huv::check_cuda(cudaMalloc(&plan->ws, wsb), "cudaMalloc(plan workspace)");
     plan->ws_bytes = wsb;
     auto with_ws = [&](auto&& body) {

@@ -337,7 +337,11 @@ huv_status huv_fno_train_step(void* fno, int32_t batch, const float* masks, cons
  * HUV_ERR_INVALID_PARAMETER.  The first call on a device performs the
  * set-up (takes the array's device address); make it before any stream
  * capture.  All calls share the array: calls that overlap on the GPU race.
- * form must be HUV_FORM_AUTO or HUV_FORM_FFT. */
+ * form must be HUV_FORM_AUTO or HUV_FORM_FFT.  The engine's focus-plane
+ * cache is only read: a plane it does not hold is built on the host for
+ * this call and not cached, and on an engine whose kernels are built on the
+ * GPU (kernel_build DEVICE or DEVICE_RULE) an uncached plane is rejected
+ * with HUV_ERR_UNSUPPORTED (image it once with huv_image_batch first). */
 huv_status huv_image_batch_noalloc(void* engine, const huv_batch* batch, float* out, void* stream);
 
 /* Synchronise `stream` and report device-side failures of earlier calls on

@@ -185,3 +185,22 @@ def test_union_spectrum_of_overlapping_pixel_aligned_rects_equals_raster_spectru
     c = H.rects_union_spectrum(rects, g, feature=0.0, background=1.0)
     d = H.spectrum_from_raster(1.0 - ras)
     assert np.max(np.abs(c - d)) < 1e-12 * np.max(np.abs(d))
+
+
+def test_cpu_ports_match_the_numpy_oracle():
+    """The two timed CPU restatements (the C port with its radix-2 FFT and
+    the pocketfft series) image like oracle.hopkins, flare included."""
+    from highuvlith_b200.clips import gen_batch
+    from oracle import cpu, socs_scipy
+    for fill, optics, lam, kmax in ((H.fill_conventional(0.5), H.euv_nxe_033(), 13.5, 16),
+                                    (H.fill_dipole(0.8, 0.1, 0.0), H.ProjectionOptics(1.35, immersion_index=1.437),
+                                     193.368, 12)):
+        eng = H.Engine(fill, optics, H.Grid(128, 1.0), lam, max_kernels=kmax)
+        ks = eng.kernel_set(0.0)
+        _, r = gen_batch(2, 128, base_seed=31, wmin=4, wmax=24)
+        a = cpu.images(ks, r, optics.flare)
+        b = socs_scipy.images(socs_scipy.Prepared(ks, flare=optics.flare), r)
+        for c in range(2):
+            ref = eng.compute_from_spectrum(H.spectrum_from_raster(r[c]))
+            assert np.max(np.abs(a[c] - ref)) / ref.max() < 1e-6
+            assert np.max(np.abs(b[c] - ref)) / ref.max() < 1e-6

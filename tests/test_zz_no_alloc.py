@@ -21,9 +21,9 @@ from highuvlith_b200.clips import gen_batch
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(eng, rasters, out, eval_grid=0, form="fft"):
+def _noalloc(eng, rasters, out, eval_grid=0, form="fft", z=0.0):
     import torch
-    b = L.Batch(rasters.shape[0], L.INPUT_U8, rasters.data_ptr(), 1, 0.0, L.FORM[form], eval_grid)
+    b = L.Batch(rasters.shape[0], L.INPUT_U8, rasters.data_ptr(), 1, float(z), L.FORM[form], eval_grid)
     st = torch.cuda.current_stream().cuda_stream
     return L.lib().huv_image_batch_noalloc(eng.handle, C.byref(b), out.data_ptr(), st)
 
@@ -41,6 +41,48 @@ def test_noalloc_matches_allocating_entry_point_twice():
         torch.cuda.synchronize()
         err = torch.max(torch.abs(out - ref)).item() / torch.max(ref).item()
         assert err < 1e-5, err
+
+
+def test_noalloc_defocus_planes_allocate_nothing_and_match_oracle():
+    """A defocused plane on a host-build engine (built on the host for the
+    call, never cached) and a cached plane on a device-build engine with a
+    one-plane cache: the device's free memory is unchanged across each call
+    after the first, the images match huv_image_batch and the FP64 oracle,
+    and an uncached plane on the device-build engine is rejected without
+    building anything."""
+    import torch
+    from oracle import hopkins as H
+    n, z = 128, 35.0
+    _, rasters = gen_batch(2, n, base_seed=77, wmin=4, wmax=24)
+    d = torch.from_numpy(rasters).cuda()
+    oeng = H.Engine(H.fill_conventional(0.5), H.euv_nxe_033(), H.Grid(n, 1.0), 13.5, max_kernels=16)
+    ref = np.stack([oeng.compute_from_spectrum(H.spectrum_from_raster(r), z) for r in rasters])
+    for build, capacity in (("host", 32), ("device", 1)):
+        eng = HB.SimulationEngine(HB.SourceConfig.euv(0.5), HB.OpticsConfig.euv_nxe_033(), grid=HB.GridConfig(n, 1.0),
+                                  max_kernels=16, kernel_build=build, kernel_cache_capacity=capacity)
+        out = torch.full((2, n, n), float("nan"), device="cuda")
+        if build == "device":
+            # the plane must be held by the engine: an uncached one is refused
+            free0 = torch.cuda.mem_get_info()[0]
+            assert _noalloc(eng, d, out, z=z) == 11  # HUV_ERR_UNSUPPORTED
+            assert b"not cached" in L.lib().huv_last_error()
+            torch.cuda.synchronize()
+            assert torch.cuda.mem_get_info()[0] == free0
+            eng.compute_batch(d, focus_nm=z, form="fft")  # caches the plane (allocates, as it may)
+        L.check(_noalloc(eng, d, out, z=z))  # first call: set-up of the array's address
+        torch.cuda.synchronize()
+        want = eng.compute_batch(d, focus_nm=z, form="fft").cpu().numpy()
+        for _ in range(2):
+            out.fill_(float("nan"))
+            torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
+            L.check(_noalloc(eng, d, out, z=z))
+            torch.cuda.synchronize()
+            assert torch.cuda.mem_get_info()[0] == free0, build
+            got = out.cpu().numpy()
+            assert np.max(np.abs(got - want)) / np.max(want) < 1e-5, build
+            for c in range(2):
+                assert np.max(np.abs(got[c] - ref[c])) / np.max(ref[c]) < 1e-5, (build, c)
 
 
 def test_noalloc_rejects_clips_beyond_its_scratch():
