@@ -60,6 +60,14 @@ class Diagnostics(C.Structure):
                 ("num_source_points", C.c_int32)]
 
 
+class KernelSetDesc(C.Structure):
+    """huv_kernel_set."""
+    _fields_ = [("grid_size", C.c_int32), ("pixel_nm", C.c_double), ("n_kernels", C.c_int32),
+                ("eigenvalues", C.c_void_p), ("kernels", C.c_void_p), ("defocus_nm", C.c_double),
+                ("wavelength_nm", C.c_double), ("captured_energy_fraction", C.c_double),
+                ("flare_fraction", C.c_double)]
+
+
 class Clip(C.Structure):
     _fields_ = [("engine", C.c_void_p), ("max_kernels", C.c_int32), ("input_kind", C.c_int32),
                 ("input", C.c_void_p), ("out", C.c_void_p)]
@@ -106,6 +114,7 @@ SIGNATURES = {
     "huv_engine_create": (C.c_int, [C.POINTER(Source), C.POINTER(Optics), C.POINTER(Grid),
                                     C.POINTER(Settings), C.c_int32, C.POINTER(C.c_void_p)]),
     "huv_engine_destroy": (None, [C.c_void_p]),
+    "huv_kernelset_create": (C.c_int, [C.POINTER(KernelSetDesc), C.c_int32, C.POINTER(C.c_void_p)]),
     "huv_engine_source_points": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     "huv_engine_diagnostics": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Diagnostics)]),
     "huv_engine_clear_field": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_double)]),
@@ -116,6 +125,7 @@ SIGNATURES = {
     "huv_rasterize_rects": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                       C.c_void_p, C.c_void_p]),
     "huv_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "huv_debug_probe_wait": (C.c_int, [C.c_int64]),
     "huv_fno_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
                                  C.POINTER(C.c_void_p)]),
     "huv_fno_destroy": (None, [C.c_void_p]),

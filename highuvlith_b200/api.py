@@ -128,6 +128,105 @@ class MaskConfig:
         return out
 
 
+class AerialImageResult:
+    """One aerial image and its measurements, the reference's Python result
+    (crates/highuvlith-py/src/py_results.rs:15-238): ``intensity`` (ny, nx)
+    indexed [y, x] (FP32, read-only), the field extent, and CD / NILS /
+    contrast of the y = 0 cross-section (metrics.rs).  Also usable as an
+    array (``np.asarray(result)``)."""
+
+    __slots__ = ("_i", "x_min_nm", "x_max_nm", "y_min_nm", "y_max_nm")
+
+    def __init__(self, intensity: np.ndarray, field_nm: float):
+        i = np.asarray(intensity)
+        i.flags.writeable = False
+        self._i = i
+        self.x_min_nm, self.x_max_nm = -field_nm / 2.0, field_nm / 2.0
+        self.y_min_nm, self.y_max_nm = -field_nm / 2.0, field_nm / 2.0
+
+    @property
+    def intensity(self) -> np.ndarray:
+        return self._i
+
+    def __array__(self, dtype=None, copy=None):
+        return self._i if dtype is None else self._i.astype(dtype)
+
+    @property
+    def shape(self):
+        return self._i.shape
+
+    @property
+    def pixel_nm(self) -> float:
+        return (self.x_max_nm - self.x_min_nm) / self._i.shape[1]
+
+    @property
+    def x_nm(self) -> np.ndarray:
+        return self.x_min_nm + (np.arange(self._i.shape[1]) + 0.5) * self.pixel_nm
+
+    @property
+    def y_nm(self) -> np.ndarray:
+        py = (self.y_max_nm - self.y_min_nm) / self._i.shape[0]
+        return self.y_min_nm + (np.arange(self._i.shape[0]) + 0.5) * py
+
+    @property
+    def extent_nm(self):
+        return (self.x_min_nm, self.x_max_nm, self.y_min_nm, self.y_max_nm)
+
+    def cross_section(self, y_nm: float = 0.0):
+        """(x_nm, intensity) of the row nearest y_nm."""
+        ny = self._i.shape[0]
+        py = (self.y_max_nm - self.y_min_nm) / ny
+        row = int(min(max(round((y_nm - self.y_min_nm) / py - 0.5), 0), ny - 1))
+        return self.x_nm, np.array(self._i[row], dtype=np.float64)
+
+    def _profile(self):
+        from . import metrics
+        return metrics, self.x_nm, metrics.centre_profile(self._i)
+
+    def image_contrast(self) -> float:
+        from . import metrics
+        return metrics.image_contrast(self._i)
+
+    def cd(self, threshold: float = 0.3, tone: str = "dark") -> Optional[float]:
+        m, x, p = self._profile()
+        return m.printed_cd(p, x, threshold, _tone(tone))
+
+    def nils_periodic(self, threshold: float = 0.3, tone: str = "dark",
+                      width_nm: Optional[float] = None) -> Optional[float]:
+        m, x, p = self._profile()
+        return m.nils(p, x, threshold, _tone(tone), width_nm)
+
+    def nils(self, threshold: float = 0.3) -> Optional[float]:
+        """Legacy open-profile NILS (metrics.rs:603-617)."""
+        m, x, p = self._profile()
+        return m.nils_open(p, x, threshold)
+
+    def image_log_slope(self, threshold: float = 0.3, tone: str = "dark") -> Optional[float]:
+        m, x, p = self._profile()
+        return m.image_log_slope(p, x, threshold, _tone(tone))
+
+    def features(self, threshold: float = 0.3, tone: str = "dark"):
+        m, x, p = self._profile()
+        return m.features(p, x, threshold, _tone(tone))
+
+    def __eq__(self, other) -> bool:
+        if not isinstance(other, AerialImageResult):
+            return NotImplemented
+        return (np.allclose(self.extent_nm, other.extent_nm, rtol=0, atol=1e-9) and self.shape == other.shape
+                and bool(np.all(np.abs(self._i.astype(np.float64) - other._i) < 1e-12)))
+
+    def __repr__(self) -> str:
+        return (f"AerialImageResult({self._i.shape[0]}x{self._i.shape[1]}, x=[{self.x_min_nm:.1f}, "
+                f"{self.x_max_nm:.1f}]nm, y=[{self.y_min_nm:.1f}, {self.y_max_nm:.1f}]nm)")
+
+
+def _tone(tone: str) -> str:
+    t = tone.lower()
+    if t not in ("dark", "bright"):
+        raise ValueError(f"tone must be 'dark' or 'bright', got {tone!r}")
+    return t
+
+
 _NORMALIZATION = {"clear_field": 0, "absolute": 1}
 # Where the FP64 kernel set is built: host C++ (dense), the GPU (dense), or the
 # GPU with the reference's solver rule (randomized subspace iteration for
@@ -170,6 +269,32 @@ class SimulationEngine:
         self._h = h
         self._destroy = L.lib().huv_engine_destroy
 
+    @classmethod
+    def from_kernel_set(cls, eigenvalues, kernels, flare_fraction: float = 0.0, defocus_nm: float = 0.0,
+                        pixel_nm: float = 1.0, wavelength_nm: float = 0.0, captured_energy_fraction: float = 1.0,
+                        device: int = 0) -> "SimulationEngine":
+        """An engine over a caller-built kernel set for one focus plane, in
+        the layout ``kernels(z)`` returns (the reference's KernelSet,
+        aerial.rs:216-228, 1912-1942): ``eigenvalues`` (K,) non-increasing
+        with the normalisation folded in, ``kernels`` complex (K, n, n) in
+        FFT layout.  Images at that plane only (huv_kernelset_create)."""
+        ev = np.ascontiguousarray(np.asarray(eigenvalues, dtype=np.float64).reshape(-1))
+        ker = np.ascontiguousarray(np.asarray(kernels, dtype=np.complex128))
+        if ker.ndim != 3 or ker.shape[1] != ker.shape[2] or ker.shape[0] != ev.size:
+            raise ValueError("kernels must be complex (K, n, n) with K = len(eigenvalues)")
+        ks = L.KernelSetDesc(ker.shape[1], float(pixel_nm), ev.size, ev.ctypes.data, ker.ctypes.data,
+                             float(defocus_nm), float(wavelength_nm), float(captured_energy_fraction),
+                             float(flare_fraction))
+        h = C.c_void_p()
+        L.check(L.lib().huv_kernelset_create(C.byref(ks), device, C.byref(h)))
+        self = cls.__new__(cls)
+        self.source = self.optics = self.mask = None
+        self.grid = GridConfig(ker.shape[1], float(pixel_nm))
+        self.device = device
+        self._h = h
+        self._destroy = L.lib().huv_engine_destroy
+        return self
+
     def __del__(self):
         # The destroy function is bound at construction: at interpreter exit
         # module globals may already be gone.
@@ -196,7 +321,7 @@ class SimulationEngine:
         return {
             "num_kernels": d.num_kernels, "captured_energy_fraction": d.captured_energy_fraction,
             "num_frequencies": d.num_frequencies, "num_columns": d.num_columns,
-            "method": ["dense_tcc", "dense_gram", "randomized"][d.method],
+            "method": ["dense_tcc", "dense_gram", "randomized", "supplied"][d.method],
             "support_exceeds_nyquist": bool(d.support_exceeds_nyquist),
             "clear_field_intensity": d.clear_field_intensity, "normalized": bool(d.normalized),
             "band_half_width": d.band_half_width, "num_source_points": d.num_source_points,
@@ -323,13 +448,14 @@ class SimulationEngine:
         L.check(L.lib().huv_image_batch_host(self._h, C.byref(b), out.ctypes.data, st))
         return out
 
-    def compute_aerial_image(self, focus_nm: float = 0.0, mask: Optional[MaskConfig] = None) -> np.ndarray:
+    def compute_aerial_image(self, focus_nm: float = 0.0, mask: Optional[MaskConfig] = None) -> AerialImageResult:
         """Image of ``mask`` (or the engine's own mask) at ``focus_nm``
-        (py_simulation.rs:169-179)."""
+        (py_simulation.rs:169-179), as an AerialImageResult."""
         m = mask or self.mask
         if m is None:
             raise ValueError("no mask given")
-        return self.compute_batch_host(m.rasterize(self.grid), focus_nm, pixel_transfer=True)[0]
+        img = self.compute_batch_host(m.rasterize(self.grid), focus_nm, pixel_transfer=True)[0]
+        return AerialImageResult(img, self.grid.field_nm)
 
     @staticmethod
     def _rect_clips(clips, feature, background):
@@ -378,7 +504,8 @@ class SimulationEngine:
         L.check(L.lib().huv_image_batch_host(self._h, C.byref(b), out.ctypes.data, None))
         return out
 
-    def compute_through_focus(self, focus_nm: Sequence[float], mask: Optional[MaskConfig] = None) -> List[np.ndarray]:
+    def compute_through_focus(self, focus_nm: Sequence[float],
+                              mask: Optional[MaskConfig] = None) -> List[AerialImageResult]:
         """Images of ``mask`` at several focus planes (py_simulation.rs:319-330,
         aerial.rs:1820-1825): kernels of uncached planes built concurrently,
         every plane imaged on the device (huv_image_focus_sweep)."""
@@ -387,7 +514,8 @@ class SimulationEngine:
         if m is None:
             raise ValueError("no mask given")
         r = torch.from_numpy(np.ascontiguousarray(m.rasterize(self.grid))[None]).to(f"cuda:{self.device}")
-        return [img[0] for img in self.compute_batch_through_focus(r, focus_nm).cpu().numpy()]
+        return [AerialImageResult(img[0], self.grid.field_nm)
+                for img in self.compute_batch_through_focus(r, focus_nm).cpu().numpy()]
 
     def compute_batch_through_focus(self, rasters, focus_nm: Sequence[float], pixel_transfer: bool = True,
                                     form: str = "auto", eval_grid: int = 0, out=None, stream=None):
@@ -413,12 +541,15 @@ class SimulationEngine:
         L.check(L.lib().huv_image_focus_sweep(self._h, C.byref(b), z.ctypes.data, len(z), out.data_ptr(), st))
         return out
 
-    def compute_from_transmittance(self, transmittance, focus_nm: float = 0.0) -> np.ndarray:
+    def compute_from_transmittance(self, transmittance, focus_nm: float = 0.0) -> AerialImageResult:
         """Image of a complex transmittance map (n, n) [y, x]
         (py_simulation.rs:375-393); the spectrum is the plain FFT."""
         t = np.asarray(transmittance)
+        n = self.grid.size
+        if t.shape != (n, n):
+            raise ValueError(f"transmittance must be ({n}, {n}) to match the grid, got {t.shape}")
         t = t.astype(np.complex64) if np.iscomplexobj(t) else t.astype(np.float32)
-        return self.compute_batch_host(t, focus_nm, pixel_transfer=False)[0]
+        return AerialImageResult(self.compute_batch_host(t, focus_nm, pixel_transfer=False)[0], self.grid.field_nm)
 
 
 def rasterize_rects(n: int, clips: Sequence[Sequence[Tuple[int, int, int, int]]], dark_field: bool = True,

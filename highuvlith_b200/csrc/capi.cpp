@@ -80,6 +80,14 @@ huv_status huv_engine_create(const huv_source* source, const huv_optics* optics,
   });
 }
 
+huv_status huv_kernelset_create(const huv_kernel_set* set, int32_t device, void** engine_out) {
+  return guarded([&] {
+    if (!set || !engine_out) throw Error(HUV_ERR_INVALID_PARAMETER, "huv_kernelset_create: null argument");
+    *engine_out = nullptr;
+    *engine_out = new Engine(*set, device);
+  });
+}
+
 void huv_engine_destroy(void* engine) { delete static_cast<Engine*>(engine); }
 
 huv_status huv_engine_source_points(void* engine, double* xyw, int32_t capacity, int32_t* count) {

@@ -759,6 +759,8 @@ cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float 
   return cudaGetLastError();
 }
 
+cudaError_t field_fused_set_smem();
+
 cudaError_t set_smem_limits() {
   const int big = 200 * 1024;
   cudaError_t e;
@@ -781,7 +783,7 @@ cudaError_t set_smem_limits() {
   HUV_XT_ATTR((band_rows_reg<192, 16>))
 #undef HUV_XT_ALL
 #undef HUV_XT_ATTR
-  return cudaSuccess;
+  return field_fused_set_smem();
 }
 
 }  // namespace huv_launch

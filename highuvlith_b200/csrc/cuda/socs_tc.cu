@@ -27,6 +27,7 @@
 #include <cudaTypedefs.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -79,6 +80,10 @@ struct TcGemmParams {
   int nprob;
   // A and B are FP16 planes (else BF16); MODE 3 always
   int f16;
+  // > 0: before its first MMA the MMA-issuing thread waits this long on a
+  // barrier nothing arrives at, so the wait runs out and the kernel takes
+  // its give-up path (a test of the bounded waits; 0 in normal use)
+  unsigned long long probe_wait_ns;
 };
 
 __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(192, 1)
         for (int kb = 0; kb < p.kboxes; ++kb, ++it) {
           const int s = it % kTcStages;
           const uint32_t ph = (it / kTcStages) & 1;
-          if (!mbar_wait(&empty[s], ph ^ 1, kWaitLimitNs)) {
+          if (!mbar_wait_or_abort(&empty[s], ph ^ 1, kWaitLimitNs, abort_flag)) {
             fail(1);
             break;
           }
@@ -200,11 +205,15 @@ __global__ void __launch_bounds__(192, 1)
       const uint32_t idesc = (MODE == 3 || p.f16) ? idesc_f16(128, BN) : idesc_bf16(128, BN);
       bool ok = mbar_wait(a_full, 0, kWaitLimitNs);
       if (!ok) fail(2);
+      if (ok && p.probe_wait_ns && !mbar_wait(done, 0, p.probe_wait_ns)) {  // nothing arrives at `done` yet
+        fail(6);
+        ok = false;
+      }
       tc_fence_after();
       int it = 0;
       for (int g = 0; g < G && ok && !*abort_flag; ++g) {
         const int buf = g & 1;
-        if (!mbar_wait(&tempty[buf], ((g >> 1) & 1) ^ 1, kWaitLimitNs)) {
+        if (!mbar_wait_or_abort(&tempty[buf], ((g >> 1) & 1) ^ 1, kWaitLimitNs, abort_flag)) {
           fail(3);
           break;
         }
@@ -259,7 +268,7 @@ __global__ void __launch_bounds__(192, 1)
     for (int g = 0; g < G; ++g) {
       const int buf = g & 1;
       // Warp-uniform outcome: tcgen05.ld below is .sync.aligned.
-      const bool got = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (g >> 1) & 1, kWaitLimitNs));
+      const bool got = __all_sync(0xffffffffu, mbar_wait_or_abort(&tfull[buf], (g >> 1) & 1, kWaitLimitNs, abort_flag));
       if (!got) {
         if (lane == 0) fail(5);
         ok = false;
@@ -475,7 +484,7 @@ __global__ void __launch_bounds__(192, 1)
         for (int kb = 0; kb < kbb; ++kb, ++it) {
           const int s = it % kW256Stages;
           const uint32_t ph = (it / kW256Stages) & 1;
-          if (!mbar_wait(&empty[s], ph ^ 1, kWaitLimitNs)) {
+          if (!mbar_wait_or_abort(&empty[s], ph ^ 1, kWaitLimitNs, abort_flag)) {
             fail(21);
             break;
           }
@@ -495,11 +504,15 @@ __global__ void __launch_bounds__(192, 1)
       const uint32_t idesc = p.f16 ? idesc_f16(128, 256) : idesc_bf16(128, 256);
       bool ok = mbar_wait(a_full, 0, kWaitLimitNs);
       if (!ok) fail(22);
+      if (ok && p.probe_wait_ns && !mbar_wait(done, 0, p.probe_wait_ns)) {  // nothing arrives at `done` yet
+        fail(26);
+        ok = false;
+      }
       tc_fence_after();
       int it = 0;
       for (int g = 0; g < p.G && ok && !*abort_flag; ++g) {
         const int buf = g & 1;
-        if (!mbar_wait(&tempty[buf], ((g >> 1) & 1) ^ 1, kWaitLimitNs)) {
+        if (!mbar_wait_or_abort(&tempty[buf], ((g >> 1) & 1) ^ 1, kWaitLimitNs, abort_flag)) {
           fail(23);
           break;
         }
@@ -547,7 +560,7 @@ __global__ void __launch_bounds__(192, 1)
     for (int g = 0; g < p.G; ++g) {
       const int buf = g & 1;
       // Warp-uniform outcome: tcgen05.ld below is .sync.aligned.
-      const bool got = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (g >> 1) & 1, kWaitLimitNs));
+      const bool got = __all_sync(0xffffffffu, mbar_wait_or_abort(&tfull[buf], (g >> 1) & 1, kWaitLimitNs, abort_flag));
       if (!got) {
         if (lane == 0) fail(25);
         break;
@@ -768,6 +781,15 @@ __global__ void band_products(const float2* __restrict__ kband, const float2* __
 namespace huv_launch {
 
 using namespace huv_dev;
+
+// Length of the probe wait the tensor-core kernels take before their first
+// MMA (0 = none); set by huv_debug_probe_wait for tests of the give-up path.
+std::atomic<unsigned long long> g_probe_wait_ns{0};
+size_t field_fused_part_bytes(int L, int K);
+cudaError_t socs_field_fused(const float2* kband, const float2* Mband, int K, int hb, int L, int clips, float keep,
+                             float flare, const float* mean, float* out, void* split, float* part, const float2* tw,
+                             cudaStream_t st);
+unsigned long long probe_wait_ns() { return g_probe_wait_ns.load(std::memory_order_relaxed); }
 cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
                          const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
                          const uint8_t* row_digits, int* err);
@@ -1082,7 +1104,9 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
                              : (b.input_kind == HUV_INPUT_RASTER_F32 ? 4 : (b.input_kind == HUV_INPUT_RECTS ? 0 : 8));
   const size_t per_x = align256(sizeof(float2) * n * B);
   const size_t per_m = align256(sizeof(float2) * B * B);
-  const size_t per_be = align256(static_cast<size_t>(K) * 2 * M * kbE * 2);
+  const bool fused = fft_field && field_fused(ds, M);
+  const size_t per_be = align256(std::max(static_cast<size_t>(K) * 2 * M * kbE * 2,
+                                          fused ? field_fused_part_bytes(M, K) : size_t(0)));
   const int rbn = B <= kRowBN ? kRowBN : kRowBNWide;  // rows of P (band rows my, padded)
   if (gemm_rows && B > kRowBNWide) throw Error(HUV_ERR_UNSUPPORTED, "TC form: band wider than 96 orders");
   const size_t per_p = gemm_rows ? align256(static_cast<size_t>(K) * 2 * rbn * kpE * 2) : 0;
@@ -1137,15 +1161,25 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       // buffer (K B M complex fits in its K 2 M kbE bf16), columns with
       // sum lambda |E|^2 in registers, normalisation and flare -> IM
       float2* T = reinterpret_cast<float2*>(BE);
-      prof.begin("socs_rows_inv", st);
-      check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "socs_rows");
-      prof.end(st);
-      prof.begin("socs_cols_inv", st);
-      if (sep)  // I_M / s as FP16 split planes [clip][2][M][M] (the bytes of the f32 IM)
-        check_cuda(socs_cols_split(T, K, hb, M, nc, ds.keep, ds.flare, mean, IM, twm, st), "socs_cols");
-      else
-        check_cuda(socs_cols_x(T, K, hb, M, nc, ds.keep, ds.flare, mean, IM, 0, twm, st), "socs_cols");
-      prof.end(st);
+      if (fused) {
+        // one kernel per kernel group: rows and columns in shared memory; the
+        // groups' partial sums (if any) in the operand buffer
+        prof.begin("socs_field_fused", st);
+        check_cuda(socs_field_fused(ds.kband, Mb, K, hb, M, nc, ds.keep, ds.flare, mean, sep ? nullptr : IM,
+                                    sep ? static_cast<void*>(IM) : nullptr, reinterpret_cast<float*>(BE), twm, st),
+                   "socs_field_fused");
+        prof.end(st);
+      } else {
+        prof.begin("socs_rows_inv", st);
+        check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "socs_rows");
+        prof.end(st);
+        prof.begin("socs_cols_inv", st);
+        if (sep)  // I_M / s as FP16 split planes [clip][2][M][M] (the bytes of the f32 IM)
+          check_cuda(socs_cols_split(T, K, hb, M, nc, ds.keep, ds.flare, mean, IM, twm, st), "socs_cols");
+        else
+          check_cuda(socs_cols_x(T, K, hb, M, nc, ds.keep, ds.flare, mean, IM, 0, twm, st), "socs_cols");
+        prof.end(st);
+      }
     }
     if (!fft_field) prof.begin(gemm_rows ? "tc_dft_gemm<rows>" : "socs_rows_tc", st);
     if (fft_field) {
@@ -1168,6 +1202,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.b_step = 2 * rbn;
       p.b_plane = rbn;
       p.err = dev_err;
+      p.probe_wait_ns = huv_launch::probe_wait_ns();
       p.bop = BE;
       p.bop_g = 2ll * M * kbE;
       p.bop_prob = static_cast<long long>(K) * 2 * M * kbE;
@@ -1199,6 +1234,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.mean = mean;
       p.out = IM;
       p.err = dev_err;
+      p.probe_wait_ns = huv_launch::probe_wait_ns();
       dim3 g(M / kTcBN, 2 * M / 128, nc);
       prof.begin("tc_dft_gemm<sumsq>", st);
       tc_dft_gemm<0><<<g, 192, smem_tc, st>>>(tc.map_ae, mbE, tc.map_ae, p);
@@ -1242,6 +1278,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.b_step = 2 * M;
       p.b_plane = M;
       p.err = dev_err;
+      p.probe_wait_ns = huv_launch::probe_wait_ns();
       p.bop = BI;
       p.bop_prob = 2ll * n * M;
       p.bop_plane = static_cast<long long>(n) * M;
@@ -1287,6 +1324,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.f16 = sep ? 1 : 0;
       p.out = o;
       p.err = dev_err;
+      p.probe_wait_ns = huv_launch::probe_wait_ns();
       CUtensorMap mo;
       p.out_tma = make_out_map(&mo, o, static_cast<uint64_t>(nc) * n, n) ? 1 : 0;
       if (!p.out_tma) mo = tc.map_ai;  // unused
@@ -1307,8 +1345,14 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
     }
     // mask band (rows, columns, mean), 2 field launches (3 with the row GEMM), 2 (separable) or 4 interpolation launches
-    prof.launches += sep ? 7 : (gemm_rows ? 10 : 9);
+    // (the fused field pass is one launch, two when kernel groups are reduced)
+    prof.launches += (sep ? 7 : (gemm_rows ? 10 : 9)) - (fused && field_fused_part_bytes(M, K) == 0 ? 1 : 0);
   }
 }
 
 }  // namespace huv
+
+extern "C" huv_status huv_debug_probe_wait(int64_t ns) {
+  huv_launch::g_probe_wait_ns.store(ns > 0 ? static_cast<unsigned long long>(ns) : 0ull);
+  return HUV_OK;
+}

@@ -59,6 +59,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64
   return true;
 }
 
+// mbar_wait that also gives up as soon as another role of the CTA has set
+// `abort` (after a failed wait of its own): a wait on work that an aborted
+// role will never deliver ends at once instead of at its limit.  Not for the
+// drain waits on copies already in flight, which must complete.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, uint64_t limit_ns,
+                                                   const volatile int* abort) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort || globaltimer_ns() - t0 > limit_ns) return false;
+  }
+  return true;
+}
+
 // 2-D TMA tile load global -> shared, completion counted on `bar` (bytes).
 __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* map, int c0, int c1,
                                             uint64_t* bar) {

@@ -38,6 +38,11 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
 cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
 cudaError_t set_smem_limits();
+bool field_fused_ok(int L, int hb);
+size_t field_fused_part_bytes(int L, int K);
+cudaError_t socs_field_fused(const float2* kband, const float2* Mband, int K, int hb, int L, int clips, float keep,
+                             float flare, const float* mean, float* out, void* split, float* part, const float2* tw,
+                             cudaStream_t st);
 void tc_release(huv::TcState& tc);
 void tc_release_all(std::map<int, huv::TcState>& m);
 bool mask_rows_tc_supported(int n, int hb);
@@ -114,6 +119,78 @@ Engine::Engine(const huv_source& s, const huv_optics& o, const huv_grid& g, cons
   focus = std::make_shared<KernelSet>(build_set(0.0));
 }
 
+Engine::Engine(const huv_kernel_set& set, int dev) : device(dev) {
+  const int n_ = set.grid_size, K = set.n_kernels;
+  if (n_ < 8 || n_ > 8192 || (n_ & (n_ - 1)) != 0)
+    throw Error(HUV_ERR_GRID_NOT_POWER_OF_TWO, "kernel set: grid_size must be a power of two in [8, 8192]");
+  if (K < 1) throw Error(HUV_ERR_INVALID_PARAMETER, "kernel set: n_kernels must be at least 1");
+  if (!set.eigenvalues || !set.kernels) throw Error(HUV_ERR_INVALID_PARAMETER, "kernel set: null array");
+  if (!(std::isfinite(set.defocus_nm))) throw Error(HUV_ERR_INVALID_PARAMETER, "kernel set: defocus_nm must be finite");
+  if (!(set.flare_fraction >= 0.0 && set.flare_fraction < 1.0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "kernel set: flare_fraction must be in [0, 1)");
+  if (!(set.captured_energy_fraction > 0.0 && set.captured_energy_fraction <= 1.0))
+    throw Error(HUV_ERR_INVALID_PARAMETER, "kernel set: captured_energy_fraction must be in (0, 1]");
+  for (int k = 0; k < K; ++k) {
+    const double v = set.eigenvalues[k];
+    if (!(std::isfinite(v) && v >= 0.0) || (k > 0 && v > set.eigenvalues[k - 1]))
+      throw Error(HUV_ERR_INVALID_PARAMETER, "kernel set: eigenvalues must be finite, >= 0 and non-increasing");
+  }
+  n = n_;
+  pixel_nm = std::isfinite(set.pixel_nm) && set.pixel_nm > 0 ? set.pixel_nm : 1.0;
+  lambda = set.wavelength_nm;
+  optics.flare = set.flare_fraction;
+  fixed_set = true;
+  fixed_z = set.defocus_nm;
+  // images stay as the eigenvalues give them: the normalisation is folded in
+  settings = huv_settings{K, 1.0, 0, 1, 0, HUV_BUILD_HOST};
+  // sparse form: the union of the kernels' non-zero frequencies
+  const size_t nn = static_cast<size_t>(n) * n;
+  std::vector<char> used(nn, 0);
+  for (int k = 0; k < K; ++k)
+    for (size_t i = 0; i < nn; ++i) {
+      const double re = set.kernels[2 * (k * nn + i)], im = set.kernels[2 * (k * nn + i) + 1];
+      if (!(std::isfinite(re) && std::isfinite(im)))
+        throw Error(HUV_ERR_INVALID_PARAMETER, "kernel set: kernels must be finite");
+      if (re != 0.0 || im != 0.0) used[i] = 1;
+    }
+  auto ks = std::make_shared<KernelSet>();
+  ks->n = n;
+  for (size_t i = 0; i < nn; ++i)
+    if (used[i]) ks->support.push_back(static_cast<int64_t>(i));
+  if (ks->support.empty()) throw Error(HUV_ERR_NO_DIFFRACTION_ORDERS, "kernel set: every kernel is zero");
+  const size_t S = ks->support.size();
+  ks->values.resize(static_cast<size_t>(K) * S);
+  for (int k = 0; k < K; ++k)
+    for (size_t t = 0; t < S; ++t) {
+      const size_t o = 2 * (k * nn + static_cast<size_t>(ks->support[t]));
+      ks->values[k * S + t] = cd(set.kernels[o], set.kernels[o + 1]);
+    }
+  ks->eigenvalues.assign(set.eigenvalues, set.eigenvalues + K);
+  ks->all_values = ks->eigenvalues;
+  double sum = 0.0, clear = 0.0;
+  for (int k = 0; k < K; ++k) {
+    sum += ks->eigenvalues[k];
+    // the field of a clear mask is the kernel's DC value (spectrum N^2 at DC, 1/N^2 inverse)
+    if (ks->support[0] == 0) clear += ks->eigenvalues[k] * std::norm(ks->values[k * S]);
+  }
+  ks->trace = sum / set.captured_energy_fraction;
+  ks->clear_field = clear;
+  ks->pupil_peak = clear;
+  ks->method = 3;  // supplied by the caller
+  ks->num_columns = 0;
+  ks->defocus_nm = set.defocus_nm;
+  ks->wavelength_nm = set.wavelength_nm;
+  ks->exceeds_nyquist = 2 * ks->band_half_width() >= n;
+  focus = ks;
+}
+
+double Engine::plane_key(double z) const {
+  if (!fixed_set) return z == 0.0 ? 0.0 : z;
+  if (z == 0.0 || z == fixed_z) return 0.0;
+  throw Error(HUV_ERR_UNSUPPORTED, "engine over a supplied kernel set: only its own focus plane (" +
+                                       std::to_string(fixed_z) + " nm) can be imaged");
+}
+
 Engine::~Engine() {
   if (device_ready) {
     cudaSetDevice(device);
@@ -149,6 +226,7 @@ Engine::~Engine() {
 }
 
 KernelSet Engine::build_set(double z) {
+  if (fixed_set) throw Error(HUV_ERR_UNSUPPORTED, "engine over a supplied kernel set: no other focus plane");
   if (settings.kernel_build == HUV_BUILD_HOST)
     return build_kernels(points, optics, n, pixel_nm, lambda, settings.max_kernels, settings.kernel_energy_fraction, z);
   return build_kernels_device(points, optics, n, pixel_nm, lambda, settings.max_kernels,
@@ -157,6 +235,7 @@ KernelSet Engine::build_set(double z) {
 }
 
 std::shared_ptr<KernelSet> Engine::kernel_set(double z) {
+  z = plane_key(z);
   if (z == 0.0) return focus;
   for (auto& e : cache)
     if (e.z == z) {
@@ -169,6 +248,7 @@ std::shared_ptr<KernelSet> Engine::kernel_set(double z) {
 }
 
 std::shared_ptr<KernelSet> Engine::held_set(double z) {
+  z = plane_key(z);
   if (z == 0.0) return focus;
   for (auto& e : cache)
     if (e.z == z) return e.ks;
@@ -204,7 +284,7 @@ void Engine::prebuild_planes(const double* z, int planes) {
   {
     std::lock_guard<std::mutex> lock(mu);
     for (int p = 0; p < planes; ++p) {
-      const double zz = z[p];
+      const double zz = plane_key(z[p]);
       if (zz == 0.0 || std::find(todo.begin(), todo.end(), zz) != todo.end()) continue;
       bool have = false;
       for (const auto& e : cache) have = have || e.z == zz;
@@ -299,6 +379,7 @@ const uint8_t* Engine::row_digit_table(int hb) {
 }
 
 DeviceSet& Engine::device_set(double z) {
+  z = plane_key(z);
   std::shared_ptr<KernelSet> ks = kernel_set(z);
   DeviceSet* slot = nullptr;
   if (z == 0.0) {
@@ -443,6 +524,14 @@ int Engine::choose_eval_grid(const DeviceSet& ds, int requested, bool mixed) con
 
 static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
+bool Engine::field_fused(const DeviceSet& ds, int M) const {
+  static const bool two_kernel = [] {
+    const char* env = std::getenv("HUV_FIELD_PASS");
+    return env && std::string(env) == "two_kernel";
+  }();
+  return !two_kernel && huv_launch::field_fused_ok(M, ds.hb);
+}
+
 void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use,
                           const float* W_use) {
   const int lgn = ilog2(n), lgm = ilog2(M);  // lgm: rounded up where M is 160 or 192
@@ -456,7 +545,9 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
   // Per-clip workspace.
   const size_t per_x = align256(sizeof(float2) * n * B);
   const size_t per_m = align256(sizeof(float2) * B * B);
-  const size_t per_t = align256(sizeof(float2) * static_cast<size_t>(K) * B * M);
+  const bool fused = field_fused(ds, M);
+  const size_t per_t = align256(std::max(sizeof(float2) * static_cast<size_t>(K) * B * M,
+                                         fused ? huv_launch::field_fused_part_bytes(M, K) : size_t(0)));
   const size_t per_i = coarse ? align256(sizeof(float) * M * M) : 0;
   const size_t per_x2 = coarse ? align256(sizeof(float2) * M * B2) : 0;
   const size_t per_c = coarse ? align256(sizeof(float2) * B2 * B2) : 0;
@@ -492,14 +583,24 @@ void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float*
                  "band_forward");
     prof.end(st);
     prof.launches += 2;
-    prof.begin("socs_rows_inv", st);
-    check_cuda(huv_launch::socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "socs_rows");
-    prof.end(st);
-    prof.begin("socs_cols_inv", st);
-    check_cuda(huv_launch::socs_cols_x(T, K, hb, M, nc, ds.keep, ds.flare, mean, coarse ? IM : o, 0, twm, st),
-               "socs_cols");
-    prof.end(st);
-    prof.launches += 2;
+    if (fused) {
+      // the partial sums of the kernel groups reuse T's bytes (K B M complex per clip)
+      prof.begin("socs_field_fused", st);
+      check_cuda(huv_launch::socs_field_fused(ds.kband, Mb, K, hb, M, nc, ds.keep, ds.flare, mean, coarse ? IM : o,
+                                              nullptr, reinterpret_cast<float*>(T), twm, st),
+                 "socs_field_fused");
+      prof.end(st);
+      prof.launches += huv_launch::field_fused_part_bytes(M, K) ? 2 : 1;
+    } else {
+      prof.begin("socs_rows_inv", st);
+      check_cuda(huv_launch::socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "socs_rows");
+      prof.end(st);
+      prof.begin("socs_cols_inv", st);
+      check_cuda(huv_launch::socs_cols_x(T, K, hb, M, nc, ds.keep, ds.flare, mean, coarse ? IM : o, 0, twm, st),
+                 "socs_cols");
+      prof.end(st);
+      prof.launches += 2;
+    }
     if (coarse) {
       prof.begin("interp_band", st);
       check_cuda(huv_launch::band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr,

@@ -179,6 +179,9 @@ struct CacheEntry {
 
 struct Engine {
   Engine(const huv_source& s, const huv_optics& o, const huv_grid& g, const huv_settings& st, int device);
+  // An engine over a caller-supplied kernel set for one focus plane
+  // (huv_kernelset_create): no source or optics, no other planes.
+  Engine(const huv_kernel_set& set, int device);
   ~Engine();
 
   std::shared_ptr<KernelSet> kernel_set(double z);
@@ -228,6 +231,11 @@ struct Engine {
   // Evaluation grid M > 4h.  `mixed`: also the register-radix lengths 160
   // and 192 (the FFT and hybrid forms), else powers of two only.
   int choose_eval_grid(const DeviceSet& ds, int requested, bool mixed = false) const;
+  // Whether the field pass on an M grid runs as the fused kernel (row and
+  // column transforms of each kernel in one CTA, no HBM round trip): M = 128
+  // or 160 and the band fits its shared memory; HUV_FIELD_PASS=two_kernel in
+  // the environment selects the row kernel + column kernel pair instead.
+  bool field_fused(const DeviceSet& ds, int M) const;
   // Whether the hybrid form (FFT field pass on M, tcgen05 interpolation) serves M.
   bool hybrid_supported(const DeviceSet& ds, int M) const;
   bool tc_supported(const DeviceSet& ds, int M) const;
@@ -258,6 +266,12 @@ struct Engine {
 
   huv_settings settings;
   int device;
+  // Engines over a caller-supplied set hold that one plane, at fixed_z.
+  bool fixed_set = false;
+  double fixed_z = 0.0;
+  // The key a focus plane is held under: the fixed set's own plane is the
+  // engine's plane 0; any other plane of a fixed set is refused.
+  double plane_key(double z) const;
   Fill fill;
   Optics optics;
   int n = 0;

@@ -40,19 +40,28 @@ def image_contrast(image: np.ndarray) -> float:
     return (mx - mn) / (mx + mn) if mx + mn > 0.0 else 0.0
 
 
-def crossings(profile: np.ndarray, x: np.ndarray, threshold: float) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
-    """Threshold crossings of a periodic uniform profile: (position, slope,
-    rising), in increasing position within the period."""
+def crossings(profile: np.ndarray, x: np.ndarray, threshold: float,
+              periodic: bool = True) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Threshold crossings of a uniform profile: (position, slope, rising),
+    in increasing position.  ``periodic``: the profile wraps (the segment
+    from the last sample to the first counts, slopes wrap); else it is open
+    (metrics.rs:135-183 node slopes: three-point next to the ends,
+    one-sided at them)."""
     y = np.asarray(profile, dtype=np.float64)
     n = y.size
     if n < 5:
         raise ValueError("profile needs at least 5 samples")
     h = float(x[1] - x[0])
     m = (-np.roll(y, -2) + 8.0 * np.roll(y, -1) - 8.0 * np.roll(y, 1) + np.roll(y, 2)) / (12.0 * h)
+    if not periodic:
+        m[[1, n - 2]] = [(y[2] - y[0]) / (2.0 * h), (y[n - 1] - y[n - 3]) / (2.0 * h)]
+        m[0], m[n - 1] = (y[1] - y[0]) / h, (y[n - 1] - y[n - 2]) / h
     y0, y1 = y, np.roll(y, -1)
     m0, m1 = m, np.roll(m, -1)
     a0, a1 = y0 >= threshold, y1 >= threshold
     k = np.nonzero(a0 != a1)[0]
+    if not periodic:
+        k = k[k < n - 1]
     if k.size == 0:
         empty = np.zeros(0)
         return empty, empty, np.zeros(0, dtype=bool)
@@ -135,3 +144,46 @@ def nils(profile, x, threshold: float, tone: str = "dark", width_nm: Optional[fl
         return None
     ils = 0.5 * (abs(f[3]) + abs(f[4])) / threshold
     return float((width_nm if width_nm is not None else f[1]) * ils)
+
+
+def features(profile, x, threshold: float, tone: str = "dark"):
+    """Every ``tone`` feature of a periodic profile as (left, right, width,
+    centre) in nm (metrics.rs:388-421); a feature crossing the field edge has
+    ``right`` beyond the field."""
+    feats, _, _ = _features(profile, x, threshold, tone)
+    return [(float(f[0]), float(f[0] + f[1]), float(f[1]), float(f[2])) for f in feats]
+
+
+def image_log_slope(profile, x, threshold: float, tone: str = "dark") -> Optional[float]:
+    """|d ln I / dx| at the edges of the feature nearest the centre, the two
+    edge slopes averaged (metrics.rs:436-449)."""
+    if not (threshold > 0.0):
+        return None
+    f = _nearest(*_features(profile, x, threshold, tone))
+    return None if f is None else float(0.5 * (abs(f[3]) + abs(f[4])) / threshold)
+
+
+def measure_cd_open(profile, x, threshold: float) -> Optional[float]:
+    """Width between the consecutive crossings of an open profile whose
+    midpoint is nearest the profile centre, whatever its tone
+    (metrics.rs:560-580)."""
+    pos, _, _ = crossings(profile, x, threshold, periodic=False)
+    if pos.size < 2:
+        return None
+    centre = 0.5 * (float(x[0]) + float(x[-1]))
+    i = int(np.argmin(np.abs(0.5 * (pos[:-1] + pos[1:]) - centre)))
+    return float(abs(pos[i + 1] - pos[i]))
+
+
+def nils_open(profile, x, threshold: float) -> Optional[float]:
+    """Legacy NILS of an open profile: the slope at the crossing nearest the
+    centre times measure_cd_open, over the threshold (metrics.rs:603-617)."""
+    if abs(threshold) < 1e-15:
+        return None
+    pos, slope, _ = crossings(profile, x, threshold, periodic=False)
+    if pos.size == 0:
+        return None
+    centre = 0.5 * (float(x[0]) + float(x[-1]))
+    edge = int(np.argmin(np.abs(pos - centre)))
+    cd = measure_cd_open(profile, x, threshold)
+    return None if cd is None else float(cd * abs(slope[edge]) / abs(threshold))

@@ -180,6 +180,37 @@ huv_status huv_engine_create(const huv_source* source, const huv_optics* optics,
                              int32_t device, void** engine_out);
 void huv_engine_destroy(void* engine);
 
+/* A caller-built SOCS kernel set for one focus plane, in the layout of the
+ * reference's KernelSet (aerial.rs:216-228) as AerialImageEngine::kernels
+ * returns it (aerial.rs:1912-1942): for the set's grid the image before
+ * flare is sum_k eigenvalues[k] |IFFT(kernels[k] . spectrum)|^2, with the
+ * normalisation already folded into the eigenvalues. */
+typedef struct {
+  int32_t grid_size;               /* n: each kernel is n x n (power of two, 8 .. 8192) */
+  double pixel_nm;                 /* grid pixel (reported only) */
+  int32_t n_kernels;               /* K >= 1 */
+  const double* eigenvalues;       /* K, non-increasing, >= 0 (KernelSet::eigenvalues) */
+  const double* kernels;           /* K * n * n complex, (re, im) interleaved, k-major, FFT layout
+                                      [ky][kx]; zero outside the frequency support (KernelSet::kernels) */
+  double defocus_nm;               /* focus plane the set was built for (KernelSet::defocus_nm) */
+  double wavelength_nm;            /* KernelSet::wavelength_nm (reported only) */
+  double captured_energy_fraction; /* KernelSet::captured_energy_fraction, in (0, 1] */
+  double flare_fraction;           /* uniform flare after the SOCS sum, in [0, 1)
+                                      (the optics' flare, aerial.rs:1741-1748) */
+} huv_kernel_set;
+
+/* An engine over a caller-supplied kernel set (replaces the kernel upload
+ * a Rust caller of AerialImageEngine::kernels would need; the reference's
+ * engines always build their own kernels, aerial.rs:1521-1637).  The set is
+ * copied (its support and values, as the engine's own sets are held), so
+ * the caller's arrays may be freed on return.  The handle serves every
+ * imaging entry point (huv_image_batch, _host, _noalloc, plans, ILT) at the
+ * set's own focus plane: a batch names defocus_nm = 0 or the set's
+ * defocus_nm; any other plane is HUV_ERR_UNSUPPORTED (the engine has no
+ * source or optics to build it).  Destroy with huv_engine_destroy.  Needs no
+ * device until the first imaging call. */
+huv_status huv_kernelset_create(const huv_kernel_set* set, int32_t device, void** engine_out);
+
 /* Source points (AerialImageEngine::source_points): xyw is count*3 doubles. */
 huv_status huv_engine_source_points(void* engine, double* xyw, int32_t capacity, int32_t* count);
 
@@ -349,6 +380,15 @@ huv_status huv_image_batch_noalloc(void* engine, const huv_batch* batch, float* 
  * (the flag is cleared by the report).  The device calls above are
  * asynchronous and cannot report such failures themselves. */
 huv_status huv_device_status(void* engine, void* stream);
+
+/* Test hook for the give-up path of the bounded waits (no counterpart in
+ * the reference).  ns > 0: every tensor-core GEMM launched afterwards (the
+ * TC and hybrid forms) first waits ns nanoseconds on a barrier nothing
+ * arrives at; the wait runs out, the kernel records the failure, unwinds
+ * (in-flight copies drained, tensor memory freed) and the next
+ * huv_device_status reports HUV_ERR_DEVICE_TIMEOUT.  ns <= 0 turns it off
+ * (the default).  Process-wide; not for production use. */
+huv_status huv_debug_probe_wait(int64_t ns);
 
 /* Axis-aligned rectangles -> pixel-aligned binary rasters on the device
  * (mask.rs:1717-1741 for pixel-aligned Rect features on a dark- or bright-field

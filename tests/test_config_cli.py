@@ -120,3 +120,38 @@ def test_cli_simulate_json(tmp_path, capsys):
     assert cli.main(["simulate", "--config", str(p), "--dose", "33"]) == 0
     out2 = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert math.isclose(out2["threshold"], 0.3 * 30 / 33)
+
+
+def test_aerial_image_result_measures_like_the_oracle():
+    """AerialImageResult (py_results.rs:15-238) on a periodic two-tone
+    image: extent, axes, cross-section, CD, NILS, log-slope and features
+    against the oracle's restatement of metrics.rs."""
+    from highuvlith_b200.api import AerialImageResult
+    from oracle import metrics as OM
+    n, p = 256, 2.0
+    x = -n * p / 2 + (np.arange(n) + 0.5) * p
+    prof = 0.5 + 0.42 * np.cos(2 * np.pi * x / 128.0) + 0.05 * np.cos(2 * np.pi * 3 * x / 128.0)
+    img = np.tile(prof.astype(np.float32), (n, 1))
+    r = AerialImageResult(img, n * p)
+    assert r.shape == (n, n) and r.pixel_nm == p and r.extent_nm == (-256.0, 256.0, -256.0, 256.0)
+    np.testing.assert_allclose(r.x_nm, x)
+    np.testing.assert_allclose(r.y_nm, x)
+    assert not r.intensity.flags.writeable
+    xs, row = r.cross_section(0.0)
+    np.testing.assert_allclose(row, img[n // 2])
+    cp = OM.centre_profile(img.astype(np.float64))
+    for tone in ("dark", "bright"):
+        # FP32 intensity: agreement to 1e-5 nm / 1e-6 in NILS
+        assert abs(r.cd(0.3, tone) - OM.measure_cd_periodic(list(cp), list(x), 0.3, tone)) < 1e-5
+        assert abs(r.nils_periodic(0.3, tone) - OM.nils_periodic(list(cp), list(x), 0.3, tone)) < 1e-6
+        feats = OM.periodic_features(list(cp), list(x), 0.3, tone)
+        mine = r.features(0.3, tone)
+        assert len(mine) == len(feats)
+        for a, b in zip(sorted(mine), sorted(f[:4] for f in feats)):
+            np.testing.assert_allclose(a, b, atol=1e-5)
+        f = OM._nearest_centre(feats, x[0] - p / 2, n * p)
+        assert abs(r.image_log_slope(0.3, tone) - 0.5 * (abs(f[4]) + abs(f[5])) / 0.3) < 1e-6
+    assert abs(r.image_contrast() - OM.image_contrast(img.astype(np.float64))) < 1e-7
+    assert r.nils(0.3) is not None and r == AerialImageResult(img.copy(), n * p)
+    with pytest.raises(ValueError):
+        r.cd(0.3, "grey")

@@ -125,3 +125,38 @@ def test_device_optimizer_decreases_cost_monotonically():
     # the returned theta images to the recorded final cost
     c, _ = ilt.cost_and_gradient(eng, theta, torch.from_numpy(targets).cuda(), st, want_gradient=False)
     np.testing.assert_allclose(c, res["final_cost"], rtol=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scene,flare", [("euv", 0.0), ("arf", 0.02)])
+def test_device_stage_loop_follows_the_oracle_trajectory(scene, flare):
+    """run_stage (ilt.rs:755-866): the device's CG Polak-Ribiere+ / Armijo
+    loop and the oracle's FP64 restatement from the same theta_0, compared
+    iteration by iteration.  Tolerance: each recorded cost within 1e-3
+    relative of the oracle's (the device costs are FP32 sums; a 1e-5
+    difference in a trial cost may move an Armijo acceptance, which is why
+    the bound is not tighter), over at least 6 iterations."""
+    import torch
+    from highuvlith_b200 import ilt
+    n, iters = 128, 8
+    eng, ev, ker = _device_case(n, scene=scene)
+    target = OI.contact_array_target(n, 1.0 if scene == "euv" else 4.0, 20.0 if scene == "euv" else 80.0,
+                                     40.0 if scene == "euv" else 160.0, 40.0 if scene == "euv" else 160.0, 2, 2)
+    theta0 = (target - 0.5).astype(np.float32)
+    st = ilt.IltSettings(cost="resist", max_iterations=iters)
+    theta = torch.from_numpy(theta0[None].copy()).cuda()
+    res = ilt.optimize(eng, theta, torch.from_numpy(target[None].astype(np.float32)).cuda(), st)
+    dev = res["cost_history"][0]
+    dev = dev[~np.isnan(dev)]
+    cfg = OI.IltConfig(cost="resist", threshold=0.25, steepness=50.0, flare=flare, tv_weight=0.01, bin_weight=0.0)
+    prob = OI.IltProblem(ev, ker, target, cfg)
+    theta_ref, hist = OI.run_stage(prob, theta0.astype(np.float64), iters, st.learning_rate, st.convergence_tol)
+    k = min(len(dev), len(hist))
+    assert k >= 7, (len(dev), len(hist))
+    rel = np.abs(dev[:k] - np.asarray(hist[:k])) / np.abs(np.asarray(hist[:k]))
+    assert np.all(rel < 1e-3), rel
+    assert res["iterations"][0] == len(hist) - 1
+    # the final masks agree where the trajectories agree
+    m_dev = 1.0 / (1.0 + np.exp(-4.0 * theta.cpu().numpy()[0].astype(np.float64)))
+    m_ref = prob.mask(theta_ref)
+    assert np.max(np.abs(m_dev - m_ref)) < 2e-2
