@@ -46,7 +46,10 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """nvidia-smi clock / throttle samples (every 50 ms, one long-running
+    nvidia-smi) from before the warm-up to the end of the timed region; the
+    summary keeps the samples taken under load (SM clock above idle) and
+    says how many fell inside the timed region itself."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -54,40 +57,57 @@ class ClockSampler:
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.rows = []
-        self._stop = threading.Event()
+        self.rows = []  # (time, fields)
+        self.window = None
+        self._p = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._p.stdout:
+            line = line.strip()
+            if line:
+                self.rows.append((time.perf_counter(), [c.strip() for c in line.split(",")]))
 
-    def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+    def start(self):
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                        "--format=csv,noheader,nounits", "-lms", "50"], stdout=subprocess.PIPE,
+                                       stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._p = None
         return self
 
-    def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+    def mark(self, t0: float, t1: float):
+        self.window = (t0, t1)
+
+    def stop(self):
+        if self._p is not None:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except Exception:
+                self._p.kill()
+            self._t.join(timeout=5)
 
     def summary(self):
-        if not self.rows:
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        rows = [r for _, r in self.rows if len(r) >= 9 and num(r[1]) is not None]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        mx = max(num(r[2]) or 0.0 for r in rows)
+        load = [r for r in rows if num(r[1]) > 0.5 * mx] or rows
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        reasons = sorted({names[i] for r in load for i in range(4) if r[5 + i] == "Active"})
+        inside = sum(1 for t, _ in self.rows if self.window and self.window[0] <= t <= self.window[1])
+        return {"sm_mhz": float(np.median([num(r[1]) for r in load])), "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows), "samples_under_load": len(load), "samples_in_timed_region": inside,
+                "sampling": "every 50 ms from the warm-up to the end of the timed region"}
 
 
 def dist_setup(n_gpus: int):
@@ -491,21 +511,24 @@ def run_ours(args):
     def step(form, eval_grid):
         eng.compute_batch(d_in, form=form, eval_grid=eval_grid, out=d_out, stream=stream)
 
+    clocks = ClockSampler(local).start()
     for _ in range(args.warmup):
         step(args.form, args.eval_grid)
     torch.cuda.synchronize()
     barrier(world)
     eng.profile(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        barrier(world)
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step(args.form, args.eval_grid)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        barrier(world)
+    torch.cuda.synchronize()
+    barrier(world)
+    w0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(args.form, args.eval_grid)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks.mark(w0, time.perf_counter())
+    barrier(world)
+    clocks.stop()
     prof = eng.profile_read()
     eng.profile(False)
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -551,7 +574,9 @@ def run_ours(args):
                  "socs_rows_tc": 4 * K * m_f * kb + 8 * Bb * Bb,
                  "tc_dft_gemm<interp>": 4 * N_GRID * N_GRID + 4 * N_GRID * (k_int if sep else kb),
                  "tc_dft_gemm<interp_x>": 4 * m_f * m_f + 4 * N_GRID * m_f,
-                 "mask_band": N_GRID * N_GRID + 16 * N_GRID * Bb + 8 * Bb * Bb}
+                 "mask_band": N_GRID * N_GRID + 16 * N_GRID * Bb + 8 * Bb * Bb,
+                 # mask band in, the band kernels (8 K S, as the whole-path count has them), I_M out
+                 "socs_field_fused": 8 * Bb * Bb + 8 * K * S + 4 * m_f * m_f}
     bytes_per_image = 4 * N_GRID ** 2 + 4 * N_GRID ** 2 + 8 * K * S
     launches = max(prof["launches"], 1)
     per_launch_s = prof["ms"] / launches / 1e3

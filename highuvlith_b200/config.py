@@ -235,3 +235,165 @@ def simulate(scene: Scene, focus_nm: Optional[float] = None, dose: Optional[floa
             "nils": metrics.nils(prof, x, thr, scene.tone), "focus_nm": z, "dose_mj_cm2": d,
             "pixel_nm": scene.grid.pixel_nm, "notes": scene.notes, "max_intensity": float(img.max()),
             "min_intensity": float(img.min())}
+
+
+def coverage_raster(scene: Scene) -> "np.ndarray":
+    """The drawn mask's clear area as an N x N raster of exact area coverage
+    (the reference's ILT target, Mask::rasterize_intensity of the binary
+    mask, mask.rs:600-603): per pixel, the fraction covered by the clear
+    parts (the features on a dark field, the background on a bright one).
+    Features must not overlap (ConfigError otherwise)."""
+    import numpy as np
+    n, p = scene.grid.size, scene.grid.pixel_nm
+    half = n * p / 2.0
+    edges = -half + np.arange(n + 1) * p
+    boxes = [(x - w / 2.0, x + w / 2.0, y - h / 2.0, y + h / 2.0) for x, y, w, h in scene.rects]
+    for i, a in enumerate(boxes):
+        for b in boxes[i + 1:]:
+            if min(a[1], b[1]) > max(a[0], b[0]) and min(a[3], b[3]) > max(a[2], b[2]):
+                raise ConfigError("ILT target: overlapping [mask] features are not supported")
+    cov = np.zeros((n, n))
+    for x0, x1, y0, y1 in boxes:
+        cx = np.clip(np.minimum(x1, edges[1:]) - np.maximum(x0, edges[:-1]), 0.0, None) / p
+        cy = np.clip(np.minimum(y1, edges[1:]) - np.maximum(y0, edges[:-1]), 0.0, None) / p
+        cov += cy[:, None] * cx[None, :]
+    cov = np.clip(cov, 0.0, 1.0)
+    return cov if scene.tone == "bright" else 1.0 - cov
+
+
+# [optimize] keys of method = "ilt" this front end maps onto the device
+# optimizer (optimize.rs:579-700); the rest raise ConfigError.
+_ILT_KEYS = {"method", "cost", "threshold", "steepness", "max_iterations", "learning_rate", "tv_weight",
+             "convergence_tol", "sigmoid_steepness", "binarization_weight", "init", "init_level", "gradient",
+             "optimizer"}
+
+
+def optimize_ilt(cfg_text_or_path: str, is_text: bool = False, device: int = 0, kernel_build: str = "host") -> dict:
+    """The reference CLI's ``optimize`` with ``method = "ilt"``
+    (optimize.rs:579-700) on the device: target = the drawn mask's clear
+    area, theta_0 = Z - 1/2 (or the uniform logit), CG Polak-Ribiere+ with
+    Armijo backtracking (huv_ilt_optimize); misprinted-pixel counts of the
+    drawn, optimized and binarised masks at the print threshold
+    (ilt.rs:267-275, 920-931)."""
+    import numpy as np
+    import torch
+    from . import ilt
+    if is_text:
+        cfg = tomllib.loads(cfg_text_or_path)
+    else:
+        with open(cfg_text_or_path, "rb") as f:
+            cfg = tomllib.load(f)
+    scene = load(cfg_text_or_path, is_text)
+    o = dict(cfg.get("optimize", {}))
+    if o.get("method") != "ilt":
+        raise ConfigError(f"[optimize] method '{o.get('method')}': only 'ilt' is on the device path")
+    extra = sorted(set(o) - _ILT_KEYS)
+    if extra:
+        raise ConfigError(f"[optimize] keys outside the device ILT: {', '.join(extra)}")
+    if o.get("gradient", "adjoint") != "adjoint" or o.get("optimizer", "cg") != "cg":
+        raise ConfigError("[optimize]: the device ILT runs the exact adjoint with conjugate gradient")
+    cost = o.get("cost", "image")
+    if cost not in ("image", "resist"):
+        raise ConfigError(f"[optimize] cost must be 'image' or 'resist', got '{cost}'")
+    threshold = float(o.get("threshold", scene.threshold))
+    if not (math.isfinite(threshold) and threshold > 0.0):
+        raise ConfigError("[optimize] threshold must be finite and > 0")
+    print_t = threshold if cost == "resist" else 0.5
+    if scene.feature != 1.0 + 0j and scene.background != 1.0 + 0j:
+        raise ConfigError("ILT needs a binary or att_psm mask")
+    absorber = scene.background if scene.tone == "bright" else scene.feature
+    if absorber.imag != 0.0 or not (0.0 <= absorber.real < 1.0):
+        raise ConfigError("the device ILT takes a real absorber amplitude in [0, 1)")
+    st = ilt.IltSettings(cost=cost, threshold=threshold, steepness=float(o.get("steepness", 50.0)),
+                         sigmoid_steepness=float(o.get("sigmoid_steepness", 4.0)),
+                         regularization=float(o.get("tv_weight", 0.01)),
+                         binarization_weight=float(o.get("binarization_weight", 0.0)), absorber=absorber.real,
+                         defocus_nm=scene.focus_nm, max_iterations=int(o.get("max_iterations", 50)),
+                         learning_rate=float(o.get("learning_rate", 0.5)),
+                         convergence_tol=float(o.get("convergence_tol", 1e-4)))
+    target = coverage_raster(scene)
+    init = o.get("init", "target")
+    if init == "target":
+        theta0 = target - 0.5
+    elif init == "uniform":
+        m0 = min(max(float(o.get("init_level", 0.5)), 0.01), 0.99)
+        theta0 = np.full_like(target, math.log(m0 / (1.0 - m0)) / st.sigmoid_steepness)
+    else:
+        raise ConfigError(f"[optimize] init must be 'target' or 'uniform', got '{init}'")
+    eng = scene.engine(device, kernel_build)
+    dev = torch.device("cuda", device)
+    theta = torch.from_numpy(theta0.astype(np.float32)[None]).to(dev)
+    tgt = torch.from_numpy(target.astype(np.float32)[None]).to(dev)
+    res = ilt.optimize(eng, theta, tgt, st)
+    m = 1.0 / (1.0 + np.exp(-st.sigmoid_steepness * theta.cpu().numpy()[0].astype(np.float64)))
+    a = st.absorber
+
+    def image(mask):
+        t = torch.from_numpy((a + (1.0 - a) * mask).astype(np.float32)[None]).to(dev)
+        return eng.compute_batch(t, focus_nm=scene.focus_nm, pixel_transfer=False).cpu().numpy()[0]
+
+    def misprinted(mask):
+        return int(np.sum((image(mask) > print_t) != (target > 0.5)))
+
+    hist = res["cost_history"][0]
+    hist = [float(c) for c in hist[:int(res["iterations"][0]) + 1]]
+    iters = int(res["iterations"][0])
+    return {"method": "ilt", "gradient": "adjoint", "optimizer": "cg", "cost": cost, "print_threshold": print_t,
+            "iterations": iters,
+            "termination": "max_iterations" if iters >= st.max_iterations else "stopped",
+            "initial_cost": hist[0], "final_cost": float(res["final_cost"][0]), "cost_history": hist,
+            "drawn_pattern_error": misprinted(target), "pattern_error": misprinted(m),
+            "binary_pattern_error": misprinted((m > 0.5).astype(np.float64)),
+            "grid": {"size": scene.grid.size, "pixel_nm": scene.grid.pixel_nm}, "mask_transmittance": m,
+            "notes": scene.notes}
+
+
+def parse_range(spec: str) -> List[float]:
+    """``start,stop,steps`` -> steps evenly spaced values, inclusive
+    (commands/sweep.rs:15-40)."""
+    parts = spec.split(",")
+    if len(parts) != 3:
+        raise ConfigError("range must be 'start,stop,steps' (e.g. '-200,200,21')")
+    start, stop, steps = float(parts[0]), float(parts[1]), int(parts[2])
+    if not (math.isfinite(start) and math.isfinite(stop)):
+        raise ConfigError("range start and stop must be finite")
+    if steps > 1 and start > stop:
+        raise ConfigError(f"invalid range: start ({start}) > stop ({stop})")
+    if steps < 2:
+        return [start]
+    return [start + i * (stop - start) / (steps - 1) for i in range(steps)]
+
+
+def sweep(scene: Scene, focuses: List[float], doses: Optional[List[float]] = None, device: int = 0,
+          kernel_build: str = "host") -> dict:
+    """The reference CLI's ``sweep`` grid (commands/sweep.rs:63-200) on the
+    device: one aerial image per focus (exact rectangle spectrum, kernels
+    built and cached per plane), and for every (dose, focus) the printed CD
+    of the measurement cutline at the constant-threshold resist's intensity
+    threshold t * nominal / dose, with the image contrast per focus.  The
+    process-window summary (best focus, DOF, exposure latitude) belongs to
+    the reference's process module and is not computed here."""
+    import numpy as np
+    from . import metrics
+    doses = list(doses) if doses else [scene.nominal_dose]
+    for d in doses:
+        if not (math.isfinite(d) and d > 0.0):
+            raise ConfigError("doses must be finite and > 0")
+    eng = scene.engine(device, kernel_build)
+    x = metrics.pixel_centres(scene.grid.size, scene.grid.field_nm)
+    contrast, profiles = [], []
+    for z in focuses:
+        img = eng.compute_batch_rects_host([scene.rects], feature=scene.feature, background=scene.background,
+                                           focus_nm=float(z))[0].astype(np.float64)
+        contrast.append(metrics.image_contrast(img))
+        profiles.append(metrics.centre_profile(img if scene.orientation == "vertical" else img.T))
+    results = []
+    for d in doses:
+        t = scene.threshold * scene.nominal_dose / d
+        for z, c, prof in zip(focuses, contrast, profiles):
+            cd = metrics.printed_cd(prof, x, t, scene.tone)
+            results.append({"dose_mj_cm2": d, "focus_nm": float(z), "intensity_threshold": t, "contrast": c,
+                            "cd_nm": cd})
+    return {"config": {"wavelength_nm": scene.source.wavelength_nm, "na": scene.optics.numerical_aperture,
+                       "grid_size": scene.grid.size, "pixel_nm": scene.grid.pixel_nm, "tone": scene.tone},
+            "focuses": [float(z) for z in focuses], "doses": doses, "results": results, "notes": scene.notes}

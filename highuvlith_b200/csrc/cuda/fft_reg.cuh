@@ -217,6 +217,38 @@ __host__ __device__ __forceinline__ void fr_dft(float2 (&v)[R]) {
   }
 }
 
+// 16-point DFT of v in place when v[4] .. v[11] are zero (not read): the
+// inner 4-point DFTs of the 4 x 4 split (n = q + 4 m) have inputs m = 0 and
+// m = 3 only, X_q = (a0 + a3, a0 - i a3, a0 - a3, a0 + i a3) for the
+// direction's i, then the twiddles and outer DFTs of fr_dft<16>.  The first
+// pass over a zero-padded band of half-width h < L / 4 has exactly this
+// shape: its inputs j + r L / 16 with 4 <= r <= 11 lie outside the band.
+template <int DIR>
+__host__ __device__ __forceinline__ void fr_dft16_band(float2 (&v)[16]) {
+  float2 u[4][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float2 a0 = v[q], a3 = v[q + 12];
+    const float2 t = fr_rot90<DIR>(a3);
+    u[q][0] = fr_add(a0, a3);
+    u[q][1] = fr_sub(a0, t);
+    u[q][2] = fr_sub(a0, a3);
+    u[q][3] = fr_add(a0, t);
+  }
+#pragma unroll
+  for (int q = 1; q < 4; ++q)
+#pragma unroll
+    for (int p = 1; p < 4; ++p) u[q][p] = fr_mul(u[q][p], w16<DIR>(q * p));
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    fr_dft4<DIR>(u[0][p], u[1][p], u[2][p], u[3][p]);
+    v[p] = u[0][p];
+    v[p + 4] = u[1][p];
+    v[p + 8] = u[2][p];
+    v[p + 12] = u[3][p];
+  }
+}
+
 // Radix plan by length: 128 = 16 x 8, 160 = 16 x 10, 192 = 16 x 12,
 // 256 = 16 x 16, 512 = 16 x 8 x 4, 1024 = 16 x 16 x 4.
 __host__ __device__ constexpr int fr_passes(int L) { return L <= 256 ? 2 : 3; }
@@ -284,13 +316,25 @@ __host__ __device__ __forceinline__ void fr_first_pass_band(int t, const float2*
   if (t >= fr_nb(L, S, 0)) return;
   const int s = t % S, j = t / S;
   float2 v[16];
+  if (4 * hb < L) {
+    // inputs r = 4 .. 11 lie outside the band: 8 loads and the pruned DFT
 #pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    const int i = j + r * (L / 16);
-    const int mx = i <= hb ? i + hb : (i >= L - hb ? i - L + hb : -1);
-    v[r] = mx >= 0 ? P[s * B + mx] : make_float2(0.f, 0.f);
+    for (int r = 0; r < 16; ++r) {
+      if (r >= 4 && r < 12) continue;
+      const int i = j + r * (L / 16);
+      const int mx = r < 4 ? (i <= hb ? i + hb : -1) : (i >= L - hb ? i - L + hb : -1);
+      v[r] = mx >= 0 ? P[s * B + mx] : make_float2(0.f, 0.f);
+    }
+    fr_dft16_band<DIR>(v);
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int i = j + r * (L / 16);
+      const int mx = i <= hb ? i + hb : (i >= L - hb ? i - L + hb : -1);
+      v[r] = mx >= 0 ? P[s * B + mx] : make_float2(0.f, 0.f);
+    }
+    fr_dft<16, DIR>(v);
   }
-  fr_dft<16, DIR>(v);
 #pragma unroll
   for (int r = 0; r < 16; ++r) dst[fr_idx<S>(j * 16 + r, s)] = v[r];
 }

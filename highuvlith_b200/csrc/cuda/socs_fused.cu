@@ -1,26 +1,34 @@
 // Fused field pass of the SOCS sum on the evaluation grid (L = 128, 160).
 //
-// One CTA of 512 threads takes one clip and a group of G kernels.  For each
-// kernel k of the group it forms the band products P = kappa_k . M (B x B,
-// B = 2 h + 1) round by round, transforms the band rows along x into
-// T[x][my] (L x B complex, held in shared memory, never in HBM), then
-// transforms every column x of T along y and adds |E_k|^2 into registers:
-// the same inverse transforms as the reference's row-pruned 2-D IFFT per
-// kernel (fft2d.rs:166-170, aerial.rs:1682-1721), on the coarse grid.
+// One CTA of 512 threads (16 warps) takes one clip and a group of G kernels.
+// For each kernel k of the group it transforms the band rows of the
+// products P = kappa_k . M (B x B, B = 2 h + 1) along x into T[x][my]
+// (L x B complex, held in shared memory, never in HBM), then transforms
+// every column x of T along y and adds |E_k|^2 into registers: the same
+// inverse transforms as the reference's row-pruned 2-D IFFT per kernel
+// (fft2d.rs:166-170, aerial.rs:1682-1721), on the coarse grid.
 //
-// Transforms are two register-radix Stockham passes (fft_reg.cuh): a
-// radix-16 first pass over the zero-padded band and a last pass of radix
-// Q = L / 16 (8, 10, 12).  Sequences are processed 32 at a time; lane
-// s = t % 32 owns sequence s of the round and j = t / 32 is its butterfly, so
-// the last pass of every round gives a thread the outputs x (or y) = j + 16 p
-// of one sequence: its twiddles are the same in every pass and its column
-// outputs land in fixed accumulator registers across kernels.
+// Each warp transforms two sequences at a time on its own, with only warp
+// barriers: the rows in pairs (my, my + 1) handed out round-robin over the
+// warps, then the columns in pairs (x, x + 1), five (L = 160) or four
+// (L = 128) per warp.  The CTA synchronises twice per kernel (rows done,
+// columns done), so a warp's loads and shared-memory round trips overlap
+// the other warps' arithmetic.  Transforms are two register-radix Stockham
+// passes (fft_reg.cuh): a radix-16 first pass over the zero-padded band
+// (lanes (c, jf), c = lane / Q, jf = lane % Q: 2 Q lanes) and a last pass of
+// radix Q = L / 16 (lanes (c, j), c = lane / 16, j = lane % 16: all 32).  A
+// lane's last-pass butterfly j is the same in every pass, so its twiddles are
+// loaded once and its column outputs (y = j + 16 p) land in fixed
+// accumulator registers across kernels: (L / 32) Q of them, 50 at L = 160
+// (128 registers, no spills); L = 192 would need 72 and keeps the two-kernel
+// pass.
 //
-// Shared memory (float2): T [L][B] (ld = B, odd, so the column pass's
-// strided reads are conflict-free), C [L][32] (the rounds' intermediate,
-// sequence-minor), P [32][B] (the round's band products).  A thread holds
-// (L / 32) Q accumulators: 32 at L = 128, 50 at L = 160 (128 registers, no
-// spills); L = 192 would need 72 and spills, so it keeps the two-kernel pass.
+// Shared memory (float2): T [L][B] (ld = B, odd: the column pass's strided
+// reads are conflict-free), the clip's mask band M [B][B], and per warp an
+// intermediate C [2][L + L / 16] (element i of sequence c at
+// c (L + L / 16) + i + i / 16: conflict-free first-pass stores and last-pass
+// loads).  At the end the accumulators are staged through shared memory and
+// written as coalesced rows.
 //
 // Output: with one group per clip the CTA applies the normalisation and
 // flare epilogue itself, out = keep * sum + flare * mean (FP32 [clip][L][L],
@@ -38,12 +46,19 @@
 namespace huv_dev {
 
 constexpr int kFusedThreads = 512;
-constexpr int kFusedRound = 32;      // sequences per round
-constexpr int kFusedGroup = 8;       // kernels per CTA
+constexpr int kFusedWarps = kFusedThreads / 32;
+constexpr int kFusedGroup = 8;  // kernels per CTA
 
+__host__ __device__ constexpr int fused_lp(int L) { return L + L / 16; }
+// T, M and the warps' intermediates; at least the L x L floats the output
+// is staged through at the end (more than the rest when the band is narrow)
 __host__ __device__ constexpr size_t fused_smem_bytes(int L, int B) {
-  return (static_cast<size_t>(L) * B + static_cast<size_t>(L) * kFusedRound +
-          static_cast<size_t>(kFusedRound) * B) * sizeof(float2);
+  return (static_cast<size_t>(L) * B + static_cast<size_t>(B) * B +
+          static_cast<size_t>(kFusedWarps) * 2 * fused_lp(L)) * sizeof(float2) >
+                 static_cast<size_t>(L) * L * sizeof(float)
+             ? (static_cast<size_t>(L) * B + static_cast<size_t>(B) * B +
+                static_cast<size_t>(kFusedWarps) * 2 * fused_lp(L)) * sizeof(float2)
+             : static_cast<size_t>(L) * L * sizeof(float);
 }
 
 __device__ __forceinline__ float2 fused_cmul(float2 a, float2 b) {
@@ -59,139 +74,137 @@ __device__ __forceinline__ int band_col(int i, int L, int hb) {
 template <int L>
 __global__ void __launch_bounds__(kFusedThreads, 1)
     field_fused_kernel(const float2* __restrict__ kband, const float2* __restrict__ Mband, int K, int hb, int groups,
-                     float keep, float flare, const float* __restrict__ mean, float* __restrict__ out,
-                     __half* __restrict__ split, float* __restrict__ part, const float2* __restrict__ tw) {
-  constexpr int Q = L / 16;            // radix of the last pass
-  constexpr int CR = L / kFusedRound;  // column rounds
+                       float keep, float flare, const float* __restrict__ mean, float* __restrict__ out,
+                       __half* __restrict__ split, float* __restrict__ part, const float2* __restrict__ tw) {
+  constexpr int Q = L / 16;       // radix of the last pass
+  constexpr int LP = fused_lp(L);  // padded intermediate sequence length
+  constexpr int CP = L / 32;      // column pairs per warp
   extern __shared__ float2 sm[];
   const int B = 2 * hb + 1;
-  float2* T = sm;                                       // [L][B]
-  float2* C = T + static_cast<size_t>(L) * B;           // [L][32]
-  float2* P = C + static_cast<size_t>(L) * kFusedRound;  // [32][B]
-  const int t = threadIdx.x;
-  const int s = t & 31, j = t >> 5;  // lane: sequence of the round; warp: butterfly
+  float2* T = sm;                                  // [L][B]
+  float2* Ms = T + static_cast<size_t>(L) * B;     // [B][B]
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  float2* Cw = Ms + static_cast<size_t>(B) * B + warp * 2 * LP;  // this warp's [2][LP]
   const int clip = blockIdx.y, grp = blockIdx.x;
   const int k0 = grp * kFusedGroup, k1 = min(K, k0 + kFusedGroup);
-  const float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
 
-  // last-pass twiddles w^{r j}, r = 1 .. Q - 1, inverse direction (the same
-  // for the row and the column passes: both have butterfly j = t / 32)
+  // the clip's mask band, once
+  const float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
+  for (int e = t; e < B * B; e += kFusedThreads) Ms[e] = Mc[e];
+
+  // first-pass lane roles: sequence c1 of the pair, butterfly jf (2 Q lanes)
+  const bool fp = lane < 2 * Q;
+  const int c1 = lane / Q, jf = lane - (lane / Q) * Q;
+  // last-pass lane roles: sequence c2, butterfly j; twiddles w^{r j}, inverse
+  const int c2 = lane >> 4, j = lane & 15;
   float2 w[Q - 1];
 #pragma unroll
   for (int r = 1; r < Q; ++r) {
     const float2 x = tw[r * j];
     w[r - 1] = make_float2(x.x, -x.y);
   }
-  float acc[CR][Q];
+  float acc[CP][Q];
 #pragma unroll
-  for (int c = 0; c < CR; ++c)
+  for (int q = 0; q < CP; ++q)
 #pragma unroll
-    for (int p = 0; p < Q; ++p) acc[c][p] = 0.f;
-
-  const bool first = t < kFusedRound * Q;  // first-pass butterflies: Q per sequence
-  const int jf = t >> 5;                    // first-pass butterfly of this thread (t < 32 Q)
+    for (int p = 0; p < Q; ++p) acc[q][p] = 0.f;
+  __syncthreads();
 
   for (int k = k0; k < k1; ++k) {
     const float2* Kk = kband + static_cast<size_t>(k) * B * B;
-    // ---------------- rows: band rows my0 .. my0 + 31 along x -> T[x][my]
-    for (int my0 = 0; my0 < B; my0 += kFusedRound) {
-      const int nseq = min(kFusedRound, B - my0);
-      // P[q][mx] = kappa_k[my0 + q][mx] M[my0 + q][mx] (zero past the band)
-      for (int e = t; e < kFusedRound * B; e += kFusedThreads) {
-        const int q = e / B;
-        float2 v = make_float2(0.f, 0.f);
-        if (q < nseq) {
-          const size_t o = static_cast<size_t>(my0) * B + e;
-          v = fused_cmul(Kk[o], Mc[o]);
-        }
-        P[e] = v;
-      }
-      __syncthreads();
-      if (first) {
+    // ---------------- rows: pairs (my, my + 1) along x -> T[x][my]
+    for (int pr = warp; 2 * pr < B; pr += kFusedWarps) {
+      if (fp) {
+        const int my = 2 * pr + c1;
         float2 v[16];
 #pragma unroll
         for (int r = 0; r < 16; ++r) {
+          if (r >= 4 && r < 12) continue;  // outside the band (h < L / 4)
           const int mx = band_col(jf + r * Q, L, hb);
-          v[r] = mx >= 0 ? P[s * B + mx] : make_float2(0.f, 0.f);
+          v[r] = (mx >= 0 && my < B) ? fused_cmul(Kk[my * B + mx], Ms[my * B + mx]) : make_float2(0.f, 0.f);
         }
-        fr_dft<16, +1>(v);
+        fr_dft16_band<+1>(v);
 #pragma unroll
-        for (int r = 0; r < 16; ++r) C[(jf * 16 + r) * kFusedRound + s] = v[r];
+        for (int r = 0; r < 16; ++r) Cw[c1 * LP + jf * 17 + r] = v[r];
       }
-      __syncthreads();
+      __syncwarp();
       {
         float2 v[Q];
 #pragma unroll
-        for (int r = 0; r < Q; ++r) v[r] = C[(j + 16 * r) * kFusedRound + s];
+        for (int r = 0; r < Q; ++r) v[r] = Cw[c2 * LP + j + 17 * r];
 #pragma unroll
         for (int r = 1; r < Q; ++r) v[r] = fused_cmul(v[r], w[r - 1]);
         fr_dft<Q, +1>(v);
-        if (s < nseq) {
+        const int my = 2 * pr + c2;
+        if (my < B) {
 #pragma unroll
-          for (int p = 0; p < Q; ++p) T[static_cast<size_t>(j + 16 * p) * B + my0 + s] = v[p];
+          for (int p = 0; p < Q; ++p) T[static_cast<size_t>(j + 16 * p) * B + my] = v[p];
         }
       }
-      // the next round's P and C writes come after its own first barrier
+      __syncwarp();
     }
     __syncthreads();  // T complete
-    // ---------------- columns: x0 .. x0 + 31 along y, |E|^2 into registers
+    // ---------------- columns: pairs (x, x + 1) along y, |E|^2 into registers
 #pragma unroll
-    for (int c = 0; c < CR; ++c) {
-      const int x = c * kFusedRound + s;
-      if (first) {
+    for (int q = 0; q < CP; ++q) {
+      const int x0 = 2 * (warp + kFusedWarps * q);
+      if (fp) {
+        const float2* col = T + static_cast<size_t>(x0 + c1) * B;
         float2 v[16];
-        const float2* col = T + static_cast<size_t>(x) * B;
 #pragma unroll
         for (int r = 0; r < 16; ++r) {
+          if (r >= 4 && r < 12) continue;  // outside the band (h < L / 4)
           const int my = band_col(jf + r * Q, L, hb);
           v[r] = my >= 0 ? col[my] : make_float2(0.f, 0.f);
         }
-        fr_dft<16, +1>(v);
+        fr_dft16_band<+1>(v);
 #pragma unroll
-        for (int r = 0; r < 16; ++r) C[(jf * 16 + r) * kFusedRound + s] = v[r];
+        for (int r = 0; r < 16; ++r) Cw[c1 * LP + jf * 17 + r] = v[r];
       }
-      __syncthreads();
+      __syncwarp();
       {
         float2 v[Q];
 #pragma unroll
-        for (int r = 0; r < Q; ++r) v[r] = C[(j + 16 * r) * kFusedRound + s];
+        for (int r = 0; r < Q; ++r) v[r] = Cw[c2 * LP + j + 17 * r];
 #pragma unroll
         for (int r = 1; r < Q; ++r) v[r] = fused_cmul(v[r], w[r - 1]);
         fr_dft<Q, +1>(v);
 #pragma unroll
-        for (int p = 0; p < Q; ++p) acc[c][p] += v[p].x * v[p].x + v[p].y * v[p].y;
+        for (int p = 0; p < Q; ++p) acc[q][p] += v[p].x * v[p].x + v[p].y * v[p].y;
       }
-      __syncthreads();  // C is rewritten by the next round (or the next kernel's rows)
+      __syncwarp();
     }
+    __syncthreads();  // the next kernel's rows overwrite T
   }
 
-  // ---------------- output: thread (c, p) holds pixel (y = j + 16 p, x = 32 c + s)
+  // ---------------- output: lane (q, p) holds pixel (y = j + 16 p, x = 2 (warp + 16 q) + c2);
+  // staged as [y][x] floats over the (now free) shared memory, then coalesced rows
+  float* S = reinterpret_cast<float*>(sm);
+#pragma unroll
+  for (int q = 0; q < CP; ++q)
+#pragma unroll
+    for (int p = 0; p < Q; ++p) S[(j + 16 * p) * L + 2 * (warp + kFusedWarps * q) + c2] = acc[q][p];
+  __syncthreads();
   if (groups > 1) {
     float* pc = part + (static_cast<size_t>(clip) * groups + grp) * L * L;
-#pragma unroll
-    for (int c = 0; c < CR; ++c)
-#pragma unroll
-      for (int p = 0; p < Q; ++p) pc[static_cast<size_t>(j + 16 * p) * L + c * kFusedRound + s] = acc[c][p];
+    for (int e = t; e < L * L / 4; e += kFusedThreads)
+      reinterpret_cast<float4*>(pc)[e] = reinterpret_cast<const float4*>(S)[e];
     return;
   }
   const float add = mean ? flare * mean[clip] : 0.f;
   const float inv = split ? 1.f / interp_scale(mean ? mean[clip] : 0.f) : 1.f;
-#pragma unroll
-  for (int c = 0; c < CR; ++c)
-#pragma unroll
-    for (int p = 0; p < Q; ++p) {
-      const size_t o = static_cast<size_t>(j + 16 * p) * L + c * kFusedRound + s;
-      const float v = keep * acc[c][p] + add;
-      if (split) {
-        const float sv = v * inv;
-        const __half hi = __float2half_rn(sv);
-        __half* sc = split + static_cast<size_t>(clip) * 2 * L * L + o;
-        sc[0] = hi;
-        sc[static_cast<size_t>(L) * L] = __float2half_rn(sv - __half2float(hi));
-      } else {
-        out[static_cast<size_t>(clip) * L * L + o] = v;
-      }
+  for (int e = t; e < L * L; e += kFusedThreads) {
+    const float v = keep * S[e] + add;
+    if (split) {
+      const float sv = v * inv;
+      const __half hi = __float2half_rn(sv);
+      __half* sc = split + static_cast<size_t>(clip) * 2 * L * L + e;
+      sc[0] = hi;
+      sc[static_cast<size_t>(L) * L] = __float2half_rn(sv - __half2float(hi));
+    } else {
+      out[static_cast<size_t>(clip) * L * L + e] = v;
     }
+  }
 }
 
 // Sum of the groups' partials (in group order) with the epilogue of
@@ -226,7 +239,7 @@ using namespace huv_dev;
 // Whether the fused field pass serves an L-point grid with band half-width
 // hb (its shared memory must fit one CTA).
 bool field_fused_ok(int L, int hb) {
-  if (!(L == 128 || L == 160) || 2 * hb >= L) return false;
+  if (!(L == 128 || L == 160) || 4 * hb >= L) return false;  // the first pass prunes r = 4 .. 11
   return fused_smem_bytes(L, 2 * hb + 1) <= 227 * 1024;
 }
 

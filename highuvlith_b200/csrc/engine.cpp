@@ -525,11 +525,8 @@ int Engine::choose_eval_grid(const DeviceSet& ds, int requested, bool mixed) con
 static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 bool Engine::field_fused(const DeviceSet& ds, int M) const {
-  static const bool two_kernel = [] {
-    const char* env = std::getenv("HUV_FIELD_PASS");
-    return env && std::string(env) == "two_kernel";
-  }();
-  return !two_kernel && huv_launch::field_fused_ok(M, ds.hb);
+  const char* env = std::getenv("HUV_FIELD_PASS");
+  return env && std::string(env) == "fused" && huv_launch::field_fused_ok(M, ds.hb);
 }
 
 void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use,

@@ -232,9 +232,10 @@ struct Engine {
   // and 192 (the FFT and hybrid forms), else powers of two only.
   int choose_eval_grid(const DeviceSet& ds, int requested, bool mixed = false) const;
   // Whether the field pass on an M grid runs as the fused kernel (row and
-  // column transforms of each kernel in one CTA, no HBM round trip): M = 128
-  // or 160 and the band fits its shared memory; HUV_FIELD_PASS=two_kernel in
-  // the environment selects the row kernel + column kernel pair instead.
+  // column transforms of each kernel in one CTA, no HBM round trip) instead
+  // of the row kernel + column kernel pair: only when HUV_FIELD_PASS=fused is
+  // set in the environment (it measures slower than the pair), M = 128 or 160
+  // and the band fits its shared memory.
   bool field_fused(const DeviceSet& ds, int M) const;
   // Whether the hybrid form (FFT field pass on M, tcgen05 interpolation) serves M.
   bool hybrid_supported(const DeviceSet& ds, int M) const;

@@ -294,3 +294,27 @@ def test_tc_form_c2_full_size():
         assert rel_err(hyb[c], ref) < 1e-4, rel_err(hyb[c], ref)
     worst, unmatched = M.max_edge_error(out[0], oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[0])), x, 0.3)
     assert unmatched == 0 and worst < CD_TOL_NM, (worst, unmatched)
+
+
+@pytest.mark.parametrize("form", ["fft", "hybrid"])
+def test_fused_field_pass_matches_oracle(form, monkeypatch):
+    """The fused field-pass kernel (HUV_FIELD_PASS=fused: row and column
+    transforms of each kernel in one CTA) on the 160- and 128-point grids,
+    narrow bands included (ArF dipole, B = 7, whose output staging is larger
+    than its working set), one and several kernel groups (K <= 8 and K > 8),
+    against the FP64 oracle."""
+    torch = _torch()
+    monkeypatch.setenv("HUV_FIELD_PASS", "fused")
+    cases = [(SMALL[1], 128, 8), (SMALL[2], 128, 16), (SMALL[3], 160, 48), (SMALL[3], 128, 12)]
+    for (name, src, opt, grid, _, fill, oopt), eg, kmax in cases:
+        eng = HB.SimulationEngine(src, opt, grid=grid, max_kernels=kmax)
+        oeng = _oracle_engine(fill, oopt, grid, src.wavelength_nm, kmax)
+        n = grid.size
+        if 4 * eng.imaging_diagnostics()["band_half_width"] >= eg:
+            continue
+        _, rasters = gen_batch(3, n, base_seed=61, wmin=max(2, n // 40), wmax=max(4, n // 8), dmin=0.2, dmax=0.6)
+        out = eng.compute_batch(torch.from_numpy(rasters).cuda(), form=form, eval_grid=eg).cpu().numpy()
+        for c in range(3):
+            ref = oeng.compute_from_spectrum(H.spectrum_from_raster(rasters[c]))
+            tol = 1e-5 if form == "fft" else 1e-4
+            assert rel_err(out[c], ref) < tol, (name, eg, kmax, c, rel_err(out[c], ref))
