@@ -417,9 +417,13 @@ def uneven_leg(stream, n_clips=2048, steps=3):
     for g in groups:
         forms[g["form"]] = forms.get(g["form"], 0) + g["clips"]
     out_px = sum(k[1] * k[1] * counts[k] for k in keys)
+    tuned_ms = sum(g["clips"] * g["ms_per_clip"] for g in groups)
     return {"workload": f"{n_clips} uneven clips (N in 256..2048, K in 16..64, ArFi dipole + EUV quasar)",
             "clips_per_s": n_clips / (ms / 1e3), "ms_per_launch": ms, "graph_launches_per_step": 1,
             "groups": len(groups), "clips_by_form": forms, "output_gpix_per_s": out_px / (ms / 1e3) / 1e9,
+            "sum_of_tuned_group_ms": tuned_ms,
+            "group_detail": [{k: g[k] for k in ("n", "h", "K", "clips", "form", "eval_grid", "ms_per_clip")}
+                             for g in groups],
             "setup_s": {"engines": t_engines, "clip_generation": t_gen, "plan_autotune_capture": t_plan}}
 
 

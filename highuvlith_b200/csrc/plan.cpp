@@ -58,8 +58,16 @@ struct Plan {
   int pixel_transfer = 1;
   std::vector<huv_clip> clips;
   std::vector<Group> groups;
-  void* ws = nullptr;
+  // Branches of the captured graph: groups are spread over up to kBranches
+  // streams (largest estimated work first, each to the least loaded
+  // branch), each branch with its own workspace, so that groups too small
+  // to fill the GPU run beside each other.
+  static constexpr int kBranches = 4;
+  std::vector<void*> ws;
   size_t ws_bytes = 0;
+  std::vector<int> branch;  // per group
+  std::vector<cudaStream_t> bstream;
+  std::vector<cudaEvent_t> bevent;
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -73,7 +81,9 @@ struct Plan {
       cudaFree(g.stage_in);
       cudaFree(g.stage_out);
     }
-    cudaFree(ws);
+    for (void* w : ws) cudaFree(w);
+    for (cudaStream_t b : bstream) cudaStreamDestroy(b);
+    for (cudaEvent_t e : bevent) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -260,38 +270,67 @@ huv_status huv_plan_create(const huv_clip* clips, int32_t n_clips, int32_t pixel
     }
     rep << "]";
     plan->report = rep.str();
-    // One shared workspace for all groups (groups run one after another):
+    // Branch assignment: estimated work = clips x the tuned ms per clip
+    // (clips alone when not tuned), largest first, each to the branch with
+    // the least work so far.
+    const int nb = std::min<int>(Plan::kBranches, static_cast<int>(plan->groups.size()));
+    {
+      std::vector<int> order(plan->groups.size());
+      for (size_t i = 0; i < order.size(); ++i) order[i] = static_cast<int>(i);
+      auto work = [&](int i) {
+        const auto& g = plan->groups[i];
+        return static_cast<double>(g.clips.size()) * (g.choice.ms_per_clip > 0 ? g.choice.ms_per_clip : 1.0);
+      };
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+      std::vector<double> load(nb, 0.0);
+      plan->branch.assign(plan->groups.size(), 0);
+      for (int i : order) {
+        const int b = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+        plan->branch[i] = b;
+        load[b] += work(i);
+      }
+    }
+    // One workspace per branch (groups of a branch run one after another):
     // as large as an engine's own chunk budget plus the per-chunk slack, so
     // each group's chunks are those of its standalone runs (every chunking
     // in the engine sizes itself by Engine::chunk_budget()).
     const size_t wsb = (size_t(2) << 30) + 8192;
-    huv::check_cuda(cudaMalloc(&plan->ws, wsb), "cudaMalloc(plan workspace)");
+    plan->ws.assign(nb, nullptr);
+    for (int b = 0; b < nb; ++b) huv::check_cuda(cudaMalloc(&plan->ws[b], wsb), "cudaMalloc(plan workspace)");
     plan->ws_bytes = wsb;
-    auto with_ws = [&](auto&& body) {
-      for (auto& g : plan->groups) {
-        g.e->ws_override = plan->ws;
-        g.e->ws_override_bytes = plan->ws_bytes;
-      }
-      try {
-        body();
-      } catch (...) {
-        for (auto& g : plan->groups) g.e->ws_override = nullptr;
-        throw;
-      }
+    plan->bstream.assign(nb, nullptr);
+    plan->bevent.assign(nb + 1, nullptr);
+    for (int b = 0; b < nb; ++b)
+      huv::check_cuda(cudaStreamCreateWithFlags(&plan->bstream[b], cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : plan->bevent)
+      huv::check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    auto clear_ws = [&] {
       for (auto& g : plan->groups) g.e->ws_override = nullptr;
     };
-    // Full run (allocates every lazy operand), then capture.
-    with_ws([&] {
-      for (auto& g : plan->groups) {
-        std::lock_guard<std::mutex> lock(g.e->mu);
-        plan->run_group(g, g.choice, st);
-      }
+    auto run_on = [&](huv::Group& g, int b, cudaStream_t s) {
+      std::lock_guard<std::mutex> lock(g.e->mu);
+      g.e->ws_override = plan->ws[b];
+      g.e->ws_override_bytes = plan->ws_bytes;
+      plan->run_group(g, g.choice, s);
+    };
+    try {
+      // Full run, branch by branch on one stream (allocates every lazy operand).
+      for (size_t gi = 0; gi < plan->groups.size(); ++gi) run_on(plan->groups[gi], plan->branch[gi], st);
       huv::check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize(plan)");
+      // Capture: fork the branches off `st`, run each branch's groups on
+      // its stream, join them back.
       huv::check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
       try {
-        for (auto& g : plan->groups) {
-          std::lock_guard<std::mutex> lock(g.e->mu);
-          plan->run_group(g, g.choice, st);
+        huv::check_cuda(cudaEventRecord(plan->bevent[nb], st), "cudaEventRecord(fork)");
+        for (int b = 0; b < nb; ++b)
+          huv::check_cuda(cudaStreamWaitEvent(plan->bstream[b], plan->bevent[nb], 0), "cudaStreamWaitEvent(fork)");
+        for (size_t gi = 0; gi < plan->groups.size(); ++gi) {
+          const int b = plan->branch[gi];
+          run_on(plan->groups[gi], b, plan->bstream[b]);
+        }
+        for (int b = 0; b < nb; ++b) {
+          huv::check_cuda(cudaEventRecord(plan->bevent[b], plan->bstream[b]), "cudaEventRecord(join)");
+          huv::check_cuda(cudaStreamWaitEvent(st, plan->bevent[b], 0), "cudaStreamWaitEvent(join)");
         }
       } catch (...) {
         cudaGraph_t dead = nullptr;
@@ -301,7 +340,11 @@ huv_status huv_plan_create(const huv_clip* clips, int32_t n_clips, int32_t pixel
       }
       huv::check_cuda(cudaStreamEndCapture(st, &plan->graph), "cudaStreamEndCapture");
       huv::check_cuda(cudaGraphInstantiate(&plan->exec, plan->graph, 0), "cudaGraphInstantiate");
-    });
+    } catch (...) {
+      clear_ws();
+      throw;
+    }
+    clear_ws();
     *plan_out = plan;
     huv::set_last_error("");
     return HUV_OK;
