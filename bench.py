@@ -501,6 +501,83 @@ def forms_leg(step, stream, diag, K, tc_sus):
     return forms
 
 
+def surrogate_leg(train_pairs=1024):
+    """High-NA EUV (NA 0.55, obscuration 0.2, annular 0.3/0.8, K = 48, 512^2):
+    the FNO surrogate (4 layers, width 64, 16 x 16 modes) against the plain
+    FP32-FFT SOCS path and the default form, as image throughput (device
+    time, 16 transmittance maps) and as gradient throughput (the FNO's input
+    gradient against the exact ILT adjoint), then judged surrogate-assisted
+    ILT against exact ILT on 8 contact-array targets (20 iterations, judge
+    every 5th, bound 5 %) after a short training run on fresh SOCS pairs."""
+    import torch
+    from highuvlith_b200 import ilt
+    from highuvlith_b200.fno import FnoSurrogate
+    from highuvlith_b200.surrogate import PairSource, high_na_engine, optimize_with_surrogate, train_timed
+    from highuvlith_b200.targets import gen_contact_targets
+    eng = high_na_engine()
+    fno = FnoSurrogate(512, 16, 4, seed=3)
+    src = PairSource(eng, seed=11)
+    masks, _ = src.batch(16)
+
+    def dev_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {"workload": "High-NA EUV 512^2, K=48; FNO 4 x width 64, 16 x 16 modes; 16 maps per call"}
+    rate = {}
+    for name, fn in (("socs_fft", lambda: eng.compute_batch(masks, pixel_transfer=False, form="fft")),
+                     ("socs_auto", lambda: eng.compute_batch(masks, pixel_transfer=False)),
+                     ("fno_forward", lambda: fno.forward(masks))):
+        rate[name] = 16 / (dev_ms(fn) / 1e3)
+    tg_np, _ = gen_contact_targets(16, 512, 1.0, base_seed=5)
+    tg = torch.from_numpy(tg_np).cuda()
+    st = ilt.IltSettings(cost="resist", threshold=0.25, steepness=50.0, max_iterations=20)
+    th0 = ilt.initial_theta_from_target(tg).contiguous()
+    rate["exact_adjoint_gradient"] = 16 / (dev_ms(lambda: ilt.cost_and_gradient(eng, th0, tg, st)) / 1e3)
+    dout = torch.ones_like(masks)
+    rate["fno_input_gradient"] = 16 / (dev_ms(lambda: fno.backward(masks, dout=dout, want_param_grad=False,
+                                                                   want_input_grad=True)) / 1e3)
+    out["images_or_gradients_per_s"] = rate
+    out["fno_forward_over_socs_fft"] = rate["fno_forward"] / rate["socs_fft"]
+    out["fno_forward_over_socs_auto"] = rate["fno_forward"] / rate["socs_auto"]
+    out["fno_gradient_over_exact_adjoint"] = rate["fno_input_gradient"] / rate["exact_adjoint_gradient"]
+    _, tm = train_timed(fno, src, train_pairs, batch=16, log_every=0)
+    src.close()
+    out["training"] = {"pairs": tm["pairs"], "s": tm["elapsed_s"], "pairs_per_s": tm["pairs_per_s"]}
+    t8, th8 = tg[:8].contiguous(), th0[:8].contiguous()
+    ilt.optimize(eng, th8.clone(), t8, ilt.IltSettings(cost="resist", threshold=0.25, steepness=50.0,
+                                                       max_iterations=1))
+    optimize_with_surrogate(eng, fno, th8.clone(), t8, ilt.IltSettings(cost="resist", threshold=0.25,
+                                                                       steepness=50.0, max_iterations=1),
+                            judge_every=1, error_bound=0.05)
+    res = {}
+    th = th8.clone()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = ilt.optimize(eng, th, t8, st)
+    torch.cuda.synchronize()
+    res["exact"] = {"final_cost": float(np.mean(r["final_cost"])), "s": time.perf_counter() - t0}
+    th = th8.clone()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rep = optimize_with_surrogate(eng, fno, th, t8, st, judge_every=5, error_bound=0.05)
+    torch.cuda.synchronize()
+    res["surrogate_judged"] = {"final_cost": float(np.mean(rep.final_cost)), "s": time.perf_counter() - t0,
+                               "surrogate_iterations": rep.surrogate_iterations,
+                               "exact_iterations": rep.exact_iterations, "takeover_iteration": rep.takeover_iteration,
+                               "judge_errors": rep.judge_errors}
+    res["surrogate_over_exact_speed"] = res["exact"]["s"] / res["surrogate_judged"]["s"]
+    out["ilt_8_targets_20_iterations"] = res
+    return out
+
+
 def run_ours(args):
     import torch
     from highuvlith_b200.clips import gen_batch
@@ -612,6 +689,21 @@ def run_ours(args):
         roofline.update({"achieved": whole, "frac": whole / hbm, "note": "achieved = whole-path bytes / step time"})
     roofline["traffic"] = (traffic_per_clip[prof["kernel"]] * images_per_launch
                            if prof["kernel"] in traffic_per_clip else None)
+    # the FFT field-pass regions are bound by instruction issue, not HBM: their
+    # transform work as 5 L log2 L FLOP per L-point transform (rows: K B
+    # transforms, columns: K M transforms, on the M-point evaluation grid)
+    # against the nominal FP32 rate (148 SMs x 128 lanes x 2 x max SM clock)
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    fft_flop = {"socs_cols_inv": K * m_f * 5 * m_f * math.log2(m_f),
+                "socs_rows_inv": K * Bb * 5 * m_f * math.log2(m_f),
+                "socs_field_fused": K * (Bb + m_f) * 5 * m_f * math.log2(m_f)}
+    for region, fl in fft_flop.items():
+        reg = prof["regions"].get(region)
+        if reg and reg[1] > 0:
+            tf = fl * N_CLIPS * args.steps / (reg[1] / 1e3) / 1e12
+            roofline.setdefault("fft_regions", {})[region] = {
+                "transform_tflops": tf, "nominal_fp32_peak": fp32_peak, "frac_of_nominal_fp32": tf / fp32_peak,
+                "flop_per_clip": fl}
     gi = prof["regions"].get("tc_dft_gemm<interp>")
     if gi and gi[1] > 0:
         # the band interpolation's N x N output GEMM: 2 N^2 k_int FLOP per
@@ -671,6 +763,7 @@ def run_ours(args):
         leg("ilt", lambda: ilt_leg(eng, stream))
         leg("focus_sweep", focus_sweep_leg)
         leg("uneven_batch", lambda: uneven_leg(stream, n_clips=args.uneven_clips))
+        leg("surrogate", surrogate_leg)
 
     if rank == 0:
         line = {
@@ -707,7 +800,7 @@ def main():
     ap.add_argument("--uneven-clips", dest="uneven_clips", type=int, default=2048)
     ap.add_argument("--clips", type=int, default=N_CLIPS,
                     help="clips per GPU (default 256, the workload; smaller only for profiler captures)")
-    ap.add_argument("--leg", default=None, choices=["ilt", "uneven", "focus_sweep"],
+    ap.add_argument("--leg", default=None, choices=["ilt", "uneven", "focus_sweep", "surrogate"],
                     help="run one extra leg alone and print its JSON (for profiler captures)")
     args = ap.parse_args()
     N_CLIPS = args.clips
@@ -721,6 +814,8 @@ def main():
             out = ilt_leg(c2_engine(0), stream)
         elif args.leg == "uneven":
             out = uneven_leg(stream, n_clips=args.uneven_clips)
+        elif args.leg == "surrogate":
+            out = surrogate_leg()
         else:
             out = focus_sweep_leg()
         print(json.dumps({args.leg: out}))
