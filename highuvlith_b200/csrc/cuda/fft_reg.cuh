@@ -250,7 +250,7 @@ __host__ __device__ __forceinline__ void fr_dft16_band(float2 (&v)[16]) {
 }
 
 // Radix plan by length: 128 = 16 x 8, 160 = 16 x 10, 192 = 16 x 12,
-// 256 = 16 x 16, 512 = 16 x 8 x 4, 1024 = 16 x 16 x 4.
+// 256 = 16 x 16, 512 = 16 x 8 x 4, 1024 = 16 x 16 x 4, 2048 = 16 x 16 x 8.
 __host__ __device__ constexpr int fr_passes(int L) { return L <= 256 ? 2 : 3; }
 __host__ __device__ constexpr int fr_radix(int L, int pass) {
   return pass == 0 ? 16
@@ -259,7 +259,8 @@ __host__ __device__ constexpr int fr_radix(int L, int pass) {
                                            : (L == 192 ? 12
                                                        : (L == 256 ? 16
                                                                    : (L == 512 ? (pass == 1 ? 8 : 4)
-                                                                               : (pass == 1 ? 16 : 4))))));
+                                                                               : (L == 2048 ? (pass == 1 ? 16 : 8)
+                                                                                            : (pass == 1 ? 16 : 4)))))));
 }
 // Stockham sub-transform size before pass `pass`.
 __host__ __device__ constexpr int fr_ns(int L, int pass) {
@@ -301,7 +302,7 @@ __device__ __forceinline__ void fr_cp_wait() {
 // threads each), 0 where no instance exists; shared-memory bytes of the
 // ping-pong buffers of one block and the kernels' shared-memory ceiling.
 __host__ __device__ constexpr int xt_S(int L) {
-  return L == 128 ? 32 : (L == 160 || L == 192 || L == 256) ? 16 : L == 512 ? 8 : L == 1024 ? 4 : 0;
+  return L == 128 ? 32 : (L == 160 || L == 192 || L == 256) ? 16 : L == 512 ? 8 : L == 1024 ? 4 : L == 2048 ? 2 : 0;
 }
 __host__ __device__ constexpr size_t xt_buf_bytes(int L) {
   return xt_S(L) ? (fr_passes(L) - 1) * static_cast<size_t>(fr_buf(L, xt_S(L))) * sizeof(float2) : 0;

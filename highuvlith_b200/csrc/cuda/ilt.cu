@@ -812,7 +812,8 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     // x-major row transforms (register-radix kernels) when the adjoint's
     // register-radix column pass fits too, else the [k][my][x] layout
     // (the ILT's grids are powers of two; ilt_cols_adj_xt has no 160 / 192 instance)
-    const bool xt = xt_ok(M, hb) && ilt_adj_xt_smem(M, hb) <= static_cast<size_t>(kXtSmemMax);
+    // (the adjoint pair is instantiated up to 1024 points)
+    const bool xt = M <= 1024 && xt_ok(M, hb) && ilt_adj_xt_smem(M, hb) <= static_cast<size_t>(kXtSmemMax);
     if (xt) {
       check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "ilt socs_rows");
       check_cuda(socs_cols_x(T, K, hb, M, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");

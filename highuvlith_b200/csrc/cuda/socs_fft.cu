@@ -416,9 +416,9 @@ __global__ void __launch_bounds__(fr_threads(L, S), 2)
 // last pass leaves the spectra in natural order in shared memory, and the
 // two real rows' bands are split from Z(m) and conj Z(-m).
 // grid: (clips * L / (2 S)); X: [clip][y][B].
-template <int L, int S>
+template <int L, int S, typename In = float>
 __global__ void __launch_bounds__(fr_threads(L, S))
-    band_rows_reg(const float* __restrict__ in, int hb, float2* __restrict__ X, const float2* __restrict__ tw) {
+    band_rows_reg(const In* __restrict__ in, int hb, float2* __restrict__ X, const float2* __restrict__ tw) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
   extern __shared__ float2 smem[];
   const int B = 2 * hb + 1;
@@ -428,10 +428,11 @@ __global__ void __launch_bounds__(fr_threads(L, S))
   float2* b1 = b0 + fr_buf(L, S);
   if (t < fr_nb(L, S, 0)) {
     const int s = t % S, j = t / S;
-    const float* ra = in + (row0 + 2 * s) * L + j;
+    const In* ra = in + (row0 + 2 * s) * L + j;
     float2 v[16];
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = make_float2(ra[r * (L / 16)], ra[L + r * (L / 16)]);
+    for (int r = 0; r < 16; ++r)
+      v[r] = make_float2(static_cast<float>(ra[r * (L / 16)]), static_cast<float>(ra[L + r * (L / 16)]));
     fr_first_pass_vals<L, S, -1>(t, v, b0);
   }
   __syncthreads();
@@ -591,17 +592,28 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     x_transposed = rows_tc == cudaSuccess && cols_reg;
     if (rows_tc != cudaSuccess && rows_tc != cudaErrorNotSupported) return rows_tc;
   }
-  if (kind == 1 && (n == 1024 || n == 160 || n == 192) && xt_ok(n, hb)) {
+  if (kind == 1 && (n == 1024 || n == 160 || n == 192 || n == 2048) && xt_ok(n, hb)) {
     const int Sr = xt_S(n);
     const dim3 gr(static_cast<unsigned>(static_cast<size_t>(clips) * n / (2 * Sr)));
     const size_t smr = 2 * static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
     const float* fin = static_cast<const float*>(in);
     if (n == 1024)
       band_rows_reg<1024, 4><<<gr, 256, smr, st>>>(fin, hb, X, tw);
+    else if (n == 2048)
+      band_rows_reg<2048, 2><<<gr, 256, smr, st>>>(fin, hb, X, tw);
     else if (n == 160)
       band_rows_reg<160, 16><<<gr, 256, smr, st>>>(fin, hb, X, tw);
     else
       band_rows_reg<192, 16><<<gr, 256, smr, st>>>(fin, hb, X, tw);
+    rows_tc = cudaSuccess;
+  }
+  // u8 rows of 2048 points whose band is too wide for the tensor-core rows
+  // (3 digit-plane accumulators past 512 TMEM columns): register-radix rows
+  if (kind == 0 && rows_tc != cudaSuccess && n == 2048 && xt_ok(n, hb)) {
+    const int Sr = xt_S(n);
+    const dim3 gr(static_cast<unsigned>(static_cast<size_t>(clips) * n / (2 * Sr)));
+    const size_t smr = 2 * static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
+    band_rows_reg<2048, 2, uint8_t><<<gr, 256, smr, st>>>(static_cast<const uint8_t*>(in), hb, X, tw);
     rows_tc = cudaSuccess;
   }
   if (!pow2 && rows_tc != cudaSuccess) return cudaErrorInvalidValue;  // no radix-4 kernel for this length
@@ -632,6 +644,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
       case 192: band_cols_reg<192, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 256: band_cols_reg<256, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 512: band_cols_reg<512, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 2048: band_cols_reg<2048, 2><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       default: band_cols_reg<1024, 4><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
     }
   } else {
@@ -646,7 +659,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
 }
 
 // Whether the register-radix kernels (x-major band layout) apply to length
-// L (128, 160, 192, 256, 512, 1024) and band half-width hb: every one of
+// L (128, 160, 192, 256, 512, 1024, 2048) and band half-width hb: every one of
 // them within the shared-memory budget.
 bool xt_ok(int L, int hb) {
   const int S = xt_S(L);
@@ -682,6 +695,7 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
     case 192: socs_rows_xt<192, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 256: socs_rows_xt<256, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 512: socs_rows_xt<512, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 2048: socs_rows_xt<2048, 2><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     default: socs_rows_xt<1024, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
   }
   return cudaGetLastError();
@@ -706,6 +720,7 @@ cudaError_t cols_xt(const float2* T, int K, int hb, int L, int clips, float keep
     case 192: HUV_COLS_XT(192, 16) break;
     case 256: HUV_COLS_XT(256, 16) break;
     case 512: HUV_COLS_XT(512, 8) break;
+    case 2048: HUV_COLS_XT(2048, 2) break;
     default: HUV_COLS_XT(1024, 4) break;
   }
 #undef HUV_COLS_XT
@@ -778,9 +793,10 @@ cudaError_t set_smem_limits() {
   HUV_XT_ATTR((socs_rows_xt<LL, SS>)) HUV_XT_ATTR((socs_cols_xt<LL, SS, 0>))                           \
   HUV_XT_ATTR((socs_cols_xt<LL, SS, 1>)) HUV_XT_ATTR((band_cols_reg<LL, SS>))
   HUV_XT_ALL(128, 32) HUV_XT_ALL(160, 16) HUV_XT_ALL(192, 16) HUV_XT_ALL(256, 16) HUV_XT_ALL(512, 8)
-  HUV_XT_ALL(1024, 4)
+  HUV_XT_ALL(1024, 4) HUV_XT_ALL(2048, 2)
   HUV_XT_ATTR((band_rows_reg<1024, 4>)) HUV_XT_ATTR((band_rows_reg<160, 16>))
-  HUV_XT_ATTR((band_rows_reg<192, 16>))
+  HUV_XT_ATTR((band_rows_reg<192, 16>)) HUV_XT_ATTR((band_rows_reg<2048, 2>))
+  HUV_XT_ATTR((band_rows_reg<2048, 2, uint8_t>))
 #undef HUV_XT_ALL
 #undef HUV_XT_ATTR
   return field_fused_set_smem();

@@ -911,7 +911,7 @@ void launch_rows(const float2* kband, float scale, const float2* Mband, int K, i
                  int L, int kp, int zero_to, __nv_bfloat16* Bop, const float2* tw, int problems, cudaStream_t st) {
   const int B = 2 * hb + 1;
   const int S = rows_reg_S(L);
-  if (S > 0 && 2 * hb < L && rows_reg_smem(L, B) <= 110 * 1024) {
+  if (S > 0 && L <= 1024 && 2 * hb < L && rows_reg_smem(L, B) <= 110 * 1024) {  // instances up to 1024 points
     const dim3 g((K * nrows + S - 1) / S, problems);
     const size_t sm = rows_reg_smem(L, B);
     switch (L) {
