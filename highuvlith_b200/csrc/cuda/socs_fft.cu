@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(fr_threads(L, S), 2)
     const float2* Pk = P;
     if (MODE == 0) {
       if (k + 1 < K) {
-        prefetch(k + 1);  // its buffer was last read before the previous iteration's final barrier
+        prefetch(k + 1);  // its buffer was last read by kernel k - 1's first pass, before that barrier
         fr_cp_wait<1>();
       } else {
         fr_cp_wait<0>();
@@ -384,7 +384,11 @@ __global__ void __launch_bounds__(fr_threads(L, S), 2)
           res[b * R + p] = v[p];
       }
     }
-    __syncthreads();
+    // No barrier here: the next kernel's band buffer is written by cp.async
+    // (MODE 0) or plain stores (MODE 1) into a buffer whose readers (this
+    // first pass) passed the barrier above, and its first pass writes b0 only
+    // after the next loop-top barrier, which every thread reaches after its
+    // own last pass here.
   }
   const float add = (MODE == 0 && mean) ? flare * mean[clip] : 0.f;
   const float inv = (MODE == 0 && split) ? 1.f / interp_scale(mean ? mean[clip] : 0.f) : 1.f;
