@@ -863,7 +863,8 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
           case 192: HUV_ILT_ADJ(192, 16) break;
           case 256: HUV_ILT_ADJ(256, 16) break;
           case 512: HUV_ILT_ADJ(512, 8) break;
-          default: HUV_ILT_ADJ(1024, 4) break;
+          case 1024: HUV_ILT_ADJ(1024, 4) break;
+          default: throw Error(HUV_ERR_UNSUPPORTED, "ILT adjoint: no register-radix instance for this grid");
         }
 #undef HUV_ILT_ADJ
       } else {

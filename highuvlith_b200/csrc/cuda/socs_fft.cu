@@ -649,7 +649,8 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
       case 256: band_cols_reg<256, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 512: band_cols_reg<512, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 2048: band_cols_reg<2048, 2><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      default: band_cols_reg<1024, 4><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 1024: band_cols_reg<1024, 4><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      default: return cudaErrorInvalidValue;
     }
   } else {
     if (!pow2) return cudaErrorInvalidValue;
@@ -700,7 +701,8 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
     case 256: socs_rows_xt<256, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 512: socs_rows_xt<512, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 2048: socs_rows_xt<2048, 2><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
-    default: socs_rows_xt<1024, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 1024: socs_rows_xt<1024, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
@@ -725,7 +727,8 @@ cudaError_t cols_xt(const float2* T, int K, int hb, int L, int clips, float keep
     case 256: HUV_COLS_XT(256, 16) break;
     case 512: HUV_COLS_XT(512, 8) break;
     case 2048: HUV_COLS_XT(2048, 2) break;
-    default: HUV_COLS_XT(1024, 4) break;
+    case 1024: HUV_COLS_XT(1024, 4) break;
+    default: return cudaErrorInvalidValue;
   }
 #undef HUV_COLS_XT
   return cudaGetLastError();

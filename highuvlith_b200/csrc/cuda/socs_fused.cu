@@ -268,10 +268,12 @@ cudaError_t socs_field_fused(const float2* kband, const float2* Mband, int K, in
       field_fused_kernel<128><<<g, kFusedThreads, sm, st>>>(kband, Mband, K, hb, groups, keep, flare, mean, out, sp,
                                                            part, tw);
       break;
-    default:
+    case 160:
       field_fused_kernel<160><<<g, kFusedThreads, sm, st>>>(kband, Mband, K, hb, groups, keep, flare, mean, out, sp,
                                                              part, tw);
       break;
+    default:
+      return cudaErrorInvalidValue;
   }
   if (groups > 1) {
     const dim3 gr((L * L + 255) / 256, clips);

@@ -911,7 +911,8 @@ void launch_rows(const float2* kband, float scale, const float2* Mband, int K, i
                  int L, int kp, int zero_to, __nv_bfloat16* Bop, const float2* tw, int problems, cudaStream_t st) {
   const int B = 2 * hb + 1;
   const int S = rows_reg_S(L);
-  if (S > 0 && L <= 1024 && 2 * hb < L && rows_reg_smem(L, B) <= 110 * 1024) {  // instances up to 1024 points
+  const bool inst = L == 128 || L == 160 || L == 192 || L == 256 || L == 512 || L == 1024;  // the instances below
+  if (S > 0 && inst && 2 * hb < L && rows_reg_smem(L, B) <= 110 * 1024) {
     const dim3 g((K * nrows + S - 1) / S, problems);
     const size_t sm = rows_reg_smem(L, B);
     switch (L) {
@@ -920,7 +921,7 @@ void launch_rows(const float2* kband, float scale, const float2* Mband, int K, i
       case 192: socs_rows_reg<192, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
       case 256: socs_rows_reg<256, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
       case 512: socs_rows_reg<512, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
-      default: socs_rows_reg<1024, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;
+      default: socs_rows_reg<1024, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, row_off, nrows, kp, zero_to, Bop, tw); break;  // L == 1024
     }
     return;
   }
