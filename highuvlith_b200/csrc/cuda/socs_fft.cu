@@ -243,8 +243,11 @@ __global__ void socs_cols_inv(const float2* __restrict__ T, int K, int hb, int l
 
 // Inverse transform along x of every (kernel, band row) product; S sequences
 // per block.  grid: (ceil(K * B / S), clips).
+// Six blocks per SM (40 registers) on the coarse grids, where a block's
+// shared memory allows it (3.6 % faster at M = 160); the long transforms
+// are held to three (their buffers allow three blocks at most).
 template <int L, int S>
-__global__ void __launch_bounds__(fr_threads(L, S))
+__global__ void __launch_bounds__(fr_threads(L, S), (L <= 256 ? 6 : 3))
     socs_rows_xt(const float2* __restrict__ kband, float scale, const float2* __restrict__ Mband, int K, int hb,
                  float2* __restrict__ Tt, const float2* __restrict__ tw) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
