@@ -791,7 +791,9 @@ def main():
     global N_CLIPS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    # 200 steps: the timed region lasts long enough (about 0.25 s) for the
+    # clock sampler (every 50 ms) to see it
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="auto", choices=["auto", "fft", "tc", "tc_rows", "hybrid"])

@@ -413,11 +413,14 @@ __global__ void __launch_bounds__(192, 1)
 // (warp 0 TMA, warp 1 MMA issue, warps 2-5 epilogue with TMA stores).
 // grid: (1, a_rows / 128, problems); p.G = out columns / 256.
 constexpr int kW256Stages = 3;
+constexpr int kW256OutBufs = 2;           // 32 x 32 f32 staging tiles per epilogue warp
 constexpr uint32_t kW256BBox = 256 * 64;  // one plane: 256 rows x 32 fp16
+constexpr uint32_t kW256OutStage = 4 * kW256OutBufs * kOutTile;
 __host__ __device__ constexpr size_t w256_smem_bytes() {
-  return 1024 + 2 * 3 * static_cast<size_t>(kABox) + kW256Stages * 2 * static_cast<size_t>(kW256BBox) + kOutStage +
-         256;
+  return 1024 + 2 * 3 * static_cast<size_t>(kABox) + kW256Stages * 2 * static_cast<size_t>(kW256BBox) +
+         kW256OutStage + 256;
 }
+static_assert(w256_smem_bytes() <= 232448, "tc_interp_w256: more shared memory than one CTA may have");
 
 __global__ void __launch_bounds__(192, 1)
     tc_interp_w256(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -429,7 +432,7 @@ __global__ void __launch_bounds__(192, 1)
   uint8_t* sA = base;                                    // [plane][3 boxes] x 16 KB
   uint8_t* sB = sA + 2 * 3 * kABox;                      // [stage][plane] x 16 KB
   uint8_t* sO = sB + kW256Stages * 2 * kW256BBox;        // epilogue staging
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sO + kOutStage);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sO + kW256OutStage);
   uint64_t* full = bars;
   uint64_t* empty = bars + kW256Stages;
   uint64_t* a_full = bars + 2 * kW256Stages;
@@ -571,11 +574,11 @@ __global__ void __launch_bounds__(192, 1)
       for (int c0 = 0; c0 < 256; c0 += 32) {
         float v[32];
         tmem_ld32(taddr + c0, v);
-        // buffer `sb` was last read by the store issued two tiles ago
-        const int sbuf = nst & 1;
-        if (lane == 0 && nst >= 2) bulk_wait_read<1>();
+        // buffer `sb` was last read by the store issued kW256OutBufs tiles ago
+        const int sbuf = nst % kW256OutBufs;
+        if (lane == 0 && nst >= kW256OutBufs) bulk_wait_read<kW256OutBufs - 1>();
         __syncwarp();
-        uint8_t* sb = sO + (quad * 2 + sbuf) * kOutTile;
+        uint8_t* sb = sO + (quad * kW256OutBufs + sbuf) * kOutTile;
 #pragma unroll
         for (int q = 0; q < 8; ++q)
           *reinterpret_cast<float4*>(sb + lane * 128 + ((q ^ (lane & 7)) << 4)) =
