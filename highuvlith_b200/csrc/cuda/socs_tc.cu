@@ -404,35 +404,41 @@ __global__ void __launch_bounds__(192, 1)
 // out(y, g * 256 + j) = osc * sum_k P(y, k) Z(g * 256 + j, k) over hi/lo
 // planes (hi.hi + hi.lo + lo.hi): FP16 with osc = interp_scale(mean) for the
 // separable form (p.f16, p.mean), BF16 with osc = 1 for the Hermitian
-// half-band operands.  P's 128-row
-// tile stays resident in shared memory (64-wide boxes, 128B swizzle); Z's
-// 256-row tiles stream through a 3-stage ring of 32-wide boxes (64B
-// swizzle, 32 KB per stage with both planes), so each MMA is 128 x 256 x 16
-// and reads 12 KB of operands per 128 tensor cycles.  Accumulators
-// double-buffered in all 512 TMEM columns.  Roles as tc_dft_gemm MODE 1
-// (warp 0 TMA, warp 1 MMA issue, warps 2-5 epilogue with TMA stores).
-// grid: (1, a_rows / 128, problems); p.G = out columns / 256.
-constexpr int kW256Stages = 3;
-constexpr int kW256OutBufs = 2;           // 32 x 32 f32 staging tiles per epilogue warp
+// half-band operands.  P's 128-row tile stays resident in shared memory in
+// ABOX 32-wide boxes per plane (64B swizzle, 8 KB each: 80 KB at K = 160);
+// Z's 256-row tiles stream through a ring of STAGES stages, one plane of one
+// 32-wide box each (16 KB; the hi plane feeds hi.hi and lo.hi, the lo plane
+// hi.lo), so each MMA is 128 x 256 x 16.  The kernel is bound by how much
+// of Z is in flight: at M = 160 and 256 clips 4 / 5 / 6 / 7 stages of 16 KB
+// take 0.363 / 0.340 / 0.316 / 0.300 ms (3 stages of both planes, 32 KB
+// each: 0.317 ms); more staging tiles per epilogue warp than two do not help.
+// Accumulators double-buffered in all 512 TMEM columns.  Roles as
+// tc_dft_gemm MODE 1 (warp 0 TMA, warp 1 MMA issue, warps 2-5 epilogue with
+// TMA stores).  grid: (1, a_rows / 128, problems); p.G = out columns / 256,
+// p.kboxes = 32-wide A boxes.
+constexpr uint32_t kW256ABox = 128 * 64;  // one plane: 128 rows x 32 fp16
 constexpr uint32_t kW256BBox = 256 * 64;  // one plane: 256 rows x 32 fp16
-constexpr uint32_t kW256OutStage = 4 * kW256OutBufs * kOutTile;
-__host__ __device__ constexpr size_t w256_smem_bytes() {
-  return 1024 + 2 * 3 * static_cast<size_t>(kABox) + kW256Stages * 2 * static_cast<size_t>(kW256BBox) +
-         kW256OutStage + 256;
+__host__ __device__ constexpr size_t w256_smem_bytes(int abox, int stages, int outbufs) {
+  return 1024 + 2 * static_cast<size_t>(abox) * kW256ABox + static_cast<size_t>(stages) * kW256BBox +
+         4 * static_cast<size_t>(outbufs) * kOutTile + 256;
 }
-static_assert(w256_smem_bytes() <= 232448, "tc_interp_w256: more shared memory than one CTA may have");
+// K <= 160 (ten 16-wide K steps) and K <= 192
+static_assert(w256_smem_bytes(5, 7, 2) <= 232448, "tc_interp_w256: more shared memory than one CTA may have");
+static_assert(w256_smem_bytes(6, 6, 2) <= 232448, "tc_interp_w256: more shared memory than one CTA may have");
 
+template <int ABOX, int STAGES, int OUTBUFS>
 __global__ void __launch_bounds__(192, 1)
     tc_interp_w256(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const __grid_constant__ CUtensorMap tmO, TcGemmParams p) {
+  constexpr int kW256Stages = STAGES, kW256OutBufs = OUTBUFS;
   constexpr uint32_t kTmemCols = 512;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-  uint8_t* sA = base;                                    // [plane][3 boxes] x 16 KB
-  uint8_t* sB = sA + 2 * 3 * kABox;                      // [stage][plane] x 16 KB
-  uint8_t* sO = sB + kW256Stages * 2 * kW256BBox;        // epilogue staging
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sO + kW256OutStage);
+  uint8_t* sA = base;                                    // [plane][ABOX boxes] x 8 KB
+  uint8_t* sB = sA + 2 * ABOX * kW256ABox;               // [stage] x 16 KB (one plane)
+  uint8_t* sO = sB + kW256Stages * kW256BBox;            // epilogue staging
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sO + 4 * kW256OutBufs * kOutTile);
   uint64_t* full = bars;
   uint64_t* empty = bars + kW256Stages;
   uint64_t* a_full = bars + 2 * kW256Stages;
@@ -478,24 +484,27 @@ __global__ void __launch_bounds__(192, 1)
     if (lane == 0) {
       prefetch_tmap(&tmA);
       prefetch_tmap(&tmB);
-      mbar_arrive_expect_tx(a_full, 2u * p.kboxes * kABox);
+      mbar_arrive_expect_tx(a_full, 2u * p.kboxes * kW256ABox);
       for (int part = 0; part < 2; ++part)
         for (int kb = 0; kb < p.kboxes; ++kb)
-          tma_load_2d(sA + (part * 3 + kb) * kABox, &tmA, kb * 64, part * p.a_rows + m_tile * 128, a_full);
+          tma_load_2d(sA + (part * ABOX + kb) * kW256ABox, &tmA, kb * 32, part * p.a_rows + m_tile * 128, a_full);
       int it = 0;
       for (int g = 0; g < p.G && !*abort_flag; ++g) {
-        for (int kb = 0; kb < kbb; ++kb, ++it) {
-          const int s = it % kW256Stages;
-          const uint32_t ph = (it / kW256Stages) & 1;
-          if (!mbar_wait_or_abort(&empty[s], ph ^ 1, kWaitLimitNs, abort_flag)) {
-            fail(21);
-            break;
+        bool ok = true;
+        for (int kb = 0; kb < kbb && ok; ++kb)
+          for (int pl = 0; pl < 2; ++pl, ++it) {
+            const int s = it % kW256Stages;
+            const uint32_t ph = (it / kW256Stages) & 1;
+            if (!mbar_wait_or_abort(&empty[s], ph ^ 1, kWaitLimitNs, abort_flag)) {
+              fail(21);
+              ok = false;
+              break;
+            }
+            mbar_arrive_expect_tx(&full[s], kW256BBox);
+            const int row = prob * p.b_prob + g * 256 + pl * p.b_plane;
+            tma_load_2d(sB + s * kW256BBox, &tmB, kb * 32, row, &full[s]);
           }
-          mbar_arrive_expect_tx(&full[s], 2u * kW256BBox);
-          const int row = prob * p.b_prob + g * 256;
-          tma_load_2d(sB + (s * 2 + 0) * kW256BBox, &tmB, kb * 32, row, &full[s]);
-          tma_load_2d(sB + (s * 2 + 1) * kW256BBox, &tmB, kb * 32, row + p.b_plane, &full[s]);
-        }
+        if (!ok) break;
       }
       // Drain: every load issued must have landed before the CTA may exit.
       mbar_wait(a_full, 0, kWaitLimitNs);
@@ -521,33 +530,36 @@ __global__ void __launch_bounds__(192, 1)
         }
         tc_fence_after();
         const uint32_t d = tmem_base + buf * 256;
-        for (int kb = 0; kb < kbb; ++kb, ++it) {
-          const int s = it % kW256Stages;
-          if (!mbar_wait(&full[s], (it / kW256Stages) & 1, kWaitLimitNs)) {
-            fail(24);
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const uint64_t b_hi = smem_desc_sw64(smem_u32(sB + (s * 2 + 0) * kW256BBox));
-          const uint64_t b_lo = smem_desc_sw64(smem_u32(sB + (s * 2 + 1) * kW256BBox));
-#pragma unroll
-          for (int ks = 0; ks < 2; ++ks) {
-            const int kstep = kb * 2 + ks;
-            if (kstep < p.ksteps) {
-              // A: 64-wide box kstep / 4, 32 bytes per 16-wide K step inside it
-              const uint64_t a_hi =
-                  smem_desc_sw128(smem_u32(sA + (0 * 3 + kstep / 4) * kABox)) + static_cast<uint64_t>(2 * (kstep % 4));
-              const uint64_t a_lo =
-                  smem_desc_sw128(smem_u32(sA + (1 * 3 + kstep / 4) * kABox)) + static_cast<uint64_t>(2 * (kstep % 4));
-              const uint64_t adv = static_cast<uint64_t>(2 * ks);
-              tc_mma_bf16(d, a_hi, b_hi + adv, idesc, kstep > 0 ? 1u : 0u);
-              tc_mma_bf16(d, a_hi, b_lo + adv, idesc, 1u);
-              tc_mma_bf16(d, a_lo, b_hi + adv, idesc, 1u);
+        for (int kb = 0; kb < kbb && ok; ++kb)
+          for (int pl = 0; pl < 2; ++pl, ++it) {
+            const int s = it % kW256Stages;
+            if (!mbar_wait(&full[s], (it / kW256Stages) & 1, kWaitLimitNs)) {
+              fail(24);
+              ok = false;
+              break;
             }
+            tc_fence_after();
+            const uint64_t b = smem_desc_sw64(smem_u32(sB + s * kW256BBox));
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+              const int kstep = kb * 2 + ks;
+              if (kstep < p.ksteps) {
+                // A: 32-wide box kstep / 2 (= kb), 32 bytes per 16-wide K step inside it
+                const uint64_t a_hi = smem_desc_sw64(smem_u32(sA + (0 * ABOX + kb) * kW256ABox)) +
+                                      static_cast<uint64_t>(2 * ks);
+                const uint64_t a_lo = smem_desc_sw64(smem_u32(sA + (1 * ABOX + kb) * kW256ABox)) +
+                                      static_cast<uint64_t>(2 * ks);
+                const uint64_t adv = static_cast<uint64_t>(2 * ks);
+                if (pl == 0) {  // hi plane of B: hi.hi and lo.hi
+                  tc_mma_bf16(d, a_hi, b + adv, idesc, kstep > 0 ? 1u : 0u);
+                  tc_mma_bf16(d, a_lo, b + adv, idesc, 1u);
+                } else {  // lo plane of B: hi.lo
+                  tc_mma_bf16(d, a_hi, b + adv, idesc, 1u);
+                }
+              }
+            }
+            tc_commit(&empty[s]);
           }
-          tc_commit(&empty[s]);
-        }
         if (!ok) break;
         tc_commit(&tfull[buf]);
       }
@@ -836,7 +848,8 @@ bool make_map(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_
 }
 
 // 2-D fp16 / bf16 tensor map (box 32 x box_rows, 64B swizzle) over
-// [rows][cols], row stride kp elements: 256-row B tiles of tc_interp_w256.
+// [rows][cols], row stride kp elements: the 128-row A and 256-row B tiles of
+// tc_interp_w256.
 bool make_map_sw64(CUtensorMap* map, const void* ptr, uint64_t rows, int kp, int box_rows, int cols, bool f16) {
   auto fn = encode_fn();
   if (!fn) return false;
@@ -956,8 +969,11 @@ cudaError_t tc_set_smem() {
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<2, kRowBNWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, kRowBNWide, true)))))
     return e;
-  if ((e = cudaFuncSetAttribute(tc_interp_w256, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(w256_smem_bytes()))))
+  if ((e = cudaFuncSetAttribute(tc_interp_w256<5, 7, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(w256_smem_bytes(5, 7, 2)))))
+    return e;
+  if ((e = cudaFuncSetAttribute(tc_interp_w256<6, 6, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(w256_smem_bytes(6, 6, 2)))))
     return e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(tc_smem_bytes(3, 128)))))
@@ -1063,7 +1079,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     const auto pp = split_planes_f16(pm, n, M, kpP);
     check_cuda(cudaMalloc(&tc.gp, pp.size() * 2), "cudaMalloc(P)");
     check_cuda(cudaMemcpy(tc.gp, pp.data(), pp.size() * 2, cudaMemcpyHostToDevice), "upload P");
-    if (!make_map(&tc.map_pi, tc.gp, 2ull * n, kpP, 128, 0, true))
+    if (!make_map(&tc.map_pi, tc.gp, 2ull * n, kpP, 128, 0, true) ||
+        !make_map_sw64(&tc.map_pi32, tc.gp, 2ull * n, kpP, 128, kpP, true))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the interpolation operand");
   }
   if (!fft_field && !tc.gy) {
@@ -1099,7 +1116,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
     const auto pi = split_planes(ai, n, kcI, kpI);
     check_cuda(cudaMalloc(&tc.gx, pi.size() * 2), "cudaMalloc(A_I)");
     check_cuda(cudaMemcpy(tc.gx, pi.data(), pi.size() * 2, cudaMemcpyHostToDevice), "upload A_I");
-    if (!make_map(&tc.map_ai, tc.gx, 2ull * n, kpI, 128))
+    if (!make_map(&tc.map_ai, tc.gx, 2ull * n, kpI, 128) ||
+        !make_map_sw64(&tc.map_ai32, tc.gx, 2ull * n, kpI, 128, kpI, false))
       throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the DFT operands");
     tc.lgm = lgm;
   }
@@ -1334,13 +1352,19 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       if (!p.out_tma) mo = tc.map_ai;  // unused
       dim3 g(1, n / 128, nc);
       CUtensorMap mbZ64;
-      const bool w256 = p.out_tma && n % 256 == 0 &&
+      const int abox = (p.ksteps + 1) / 2;  // 32-wide A boxes
+      const bool w256 = p.out_tma && n % 256 == 0 && abox <= 6 &&
                         make_map_sw64(&mbZ64, BI, static_cast<uint64_t>(nc) * 2 * n, sep ? M : kbI, 256,
                                       sep ? M : kcI, sep);
       prof.begin("tc_dft_gemm<interp>", st);
-      if (w256) {  // 128 x 256 tiles, the B operand through 32-wide boxes
+      if (w256) {  // 128 x 256 tiles, A and B through 32-wide boxes
         p.G = n / 256;
-        tc_interp_w256<<<g, 192, w256_smem_bytes(), st>>>(sep ? tc.map_pi : tc.map_ai, mbZ64, mo, p);
+        p.kboxes = abox;
+        const CUtensorMap& ma = sep ? tc.map_pi32 : tc.map_ai32;
+        if (abox <= 5)
+          tc_interp_w256<5, 7, 2><<<g, 192, w256_smem_bytes(5, 7, 2), st>>>(ma, mbZ64, mo, p);
+        else
+          tc_interp_w256<6, 6, 2><<<g, 192, w256_smem_bytes(6, 6, 2), st>>>(ma, mbZ64, mo, p);
       } else if (sep)
         tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_pi, mbZ, mo, p);
       else

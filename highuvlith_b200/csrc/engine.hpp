@@ -76,6 +76,7 @@ struct TcState {
   void* gx = nullptr;   // A_I planes [2][N][kpI] bf16
   void* gp = nullptr;   // separable interpolation matrix planes [2][N][192] fp16 (M <= 192)
   CUtensorMap map_ae, map_ai, map_pi;
+  CUtensorMap map_ai32, map_pi32;  // the same planes in 32-wide boxes (64B swizzle)
 };
 
 // One kernel set on the device: band kernels K x B x B (complex FP32,
