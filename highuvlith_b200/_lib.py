@@ -136,6 +136,7 @@ SIGNATURES = {
                                    C.c_void_p, C.POINTER(C.c_float), C.c_void_p]),
     "huv_fno_train_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
                                      C.POINTER(C.c_float), C.c_void_p]),
+    "huv_fno_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
     "huv_plan_create": (C.c_int, [C.POINTER(Clip), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
     "huv_plan_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
     "huv_plan_describe": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),

@@ -27,6 +27,8 @@
 namespace huv_launch {
 // tensor-core forward of the FNO (csrc/cuda/fno_tc.cu)
 cudaError_t fno_tc_set_smem();
+bool fno_tc_layer_bwd(size_t pix, const float* dvnext, const __nv_bfloat16* z, const __nv_bfloat16* v, const float* W,
+                      int act, float* dz, float* dv, float* dW, float* db, int* err, cudaStream_t st);
 bool fno_tc_layer(int B, int S, int m, const __nv_bfloat16* v, const __nv_bfloat16* Wb, const __nv_bfloat16* Tw,
                   const __nv_bfloat16* Zs, const float* bias, int act, __nv_bfloat16* zsave, __nv_bfloat16* vnext,
                   int* err, cudaStream_t st);
@@ -969,8 +971,14 @@ struct Fno {
     float* dnext = dvA;
     float* dcur = dvB;
     for (int l = L - 1; l >= 0; --l) {
-      fno_layer_bwd<<<std::min(rows, 296), 256, kLayerBwdSmem, st>>>(
-          dnext, z[l], v[l], par + oW[l], S, l < L - 1 ? 1 : 0, dz, dcur, grad + oW[l], grad + ob[l], rows);
+      if (tc) {
+        if (!huv_launch::fno_tc_layer_bwd(pix, dnext, z[l], v[l], par + oW[l], l < L - 1 ? 1 : 0, dz, dcur,
+                                          grad + oW[l], grad + ob[l], tc_err, st))
+          throw Error(HUV_ERR_CUDA, "fno: tensor-core layer backward launch failed");
+      } else {
+        fno_layer_bwd<<<std::min(rows, 296), 256, kLayerBwdSmem, st>>>(
+            dnext, z[l], v[l], par + oW[l], S, l < L - 1 ? 1 : 0, dz, dcur, grad + oW[l], grad + ob[l], rows);
+      }
       fno_dft_x<float><<<rgrid, 256, kDftXSmem, st>>>(dz, S, m, twx, Xa, rows);
       fno_dft_y<false><<<ygrid, 256, 0, st>>>(Xa, S, C, m, twy, Y);
       fno_scale_modes<<<256, 256, 0, st>>>(Y, B, J, m, C, 1.f / (static_cast<float>(S) * S));
@@ -983,6 +991,19 @@ struct Fno {
     }
     fno_lift_bwd<<<1184, 256, 0, st>>>(masks, dnext, S, par + oWl, pix, grad + oWl, grad + obl, dmask);
     check_cuda(cudaGetLastError(), "fno backward");
+  }
+
+  // Synchronise and read (then clear) the flag a bounded wait of a
+  // tensor-core kernel sets when it gives up; throws if it was set.
+  void check_device_flag(cudaStream_t st) {
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    if (!tc_err) return;
+    int h = 0;
+    check_cuda(cudaMemcpy(&h, tc_err, sizeof(int), cudaMemcpyDeviceToHost), "read fno error flag");
+    if (h) {
+      check_cuda(cudaMemset(tc_err, 0, sizeof(int)), "reset fno error flag");
+      throw Error(HUV_ERR_DEVICE_TIMEOUT, "fno: a bounded device-side wait gave up; the results are not valid");
+    }
   }
 
   float mse(int B, const float* targets, cudaStream_t st) {
@@ -1112,6 +1133,7 @@ huv_status huv_fno_backward(void* fno, int32_t batch, const float* masks, const 
     f->backward(batch, masks, d, dmask, st);
     if (param_grad)
       huv::check_cuda(cudaMemcpyAsync(param_grad, f->grad, f->npar * 4, cudaMemcpyDeviceToDevice, st), "copy grad");
+    f->check_device_flag(st);
   });
 }
 
@@ -1127,6 +1149,15 @@ huv_status huv_fno_train_step(void* fno, int32_t batch, const float* masks, cons
     if (loss_host) *loss_host = l;
     f->backward(batch, masks, f->dout, nullptr, st);
     f->adam(lr, weight_decay, st);
+    f->check_device_flag(st);
+  });
+}
+
+huv_status huv_fno_device_status(void* fno, void* stream) {
+  return fno_guard([&] {
+    Fno* f = as_fno(fno);
+    huv::check_cuda(cudaSetDevice(f->device), "cudaSetDevice");
+    f->check_device_flag(static_cast<cudaStream_t>(stream));
   });
 }
 
@@ -1159,6 +1190,7 @@ huv_status huv_ilt_optimize_surrogate(void* engine, void* fno, const huv_ilt_par
     sur->n_judges = static_cast<int32_t>(rep.judge_errors.size());
     for (int i = 0; i < 64; ++i)
       sur->judge_errors[i] = i < static_cast<int>(rep.judge_errors.size()) ? rep.judge_errors[i] : 0.0;
+    f->check_device_flag(static_cast<cudaStream_t>(stream));
   });
 }
 

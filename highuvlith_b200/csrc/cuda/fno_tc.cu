@@ -220,6 +220,255 @@ __global__ void __launch_bounds__(192, 2)
   if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
 }
 
+// ------------------------------------------------------------------ backward
+// Backward of the pointwise layer on tcgen05, per 128-pixel tile:
+//   dz = dvnext * GELU'(z)  (or dvnext for the last layer), stored (f32);
+//   dv = dz W               (M 128 pixels, N 64 inputs, K 64 outputs), stored (f32);
+//   dW += dz^T v, db += sum dz over the CTA's tiles.
+// The elementwise part runs on CUDA cores (warps 5..20, two 8-channel chunks
+// of 32 pixels per thread, coalesced 32-byte rows) and writes the operands of
+// both GEMMs straight into shared memory in the 128B-swizzled K-major layout:
+// sA[px][o] = dz (A of dv), sX[ch][px] = (dz^T; v^T) (A of dW, 128 rows x 128
+// pixels in two 64-wide boxes; its rows 64..127, v^T, are also the B operand),
+// sWT[i][o] = W[o][i] (B of dv, converted from the f32 weights once per CTA).
+// dW is the top half of the 128 x 64 product (dz^T; v^T) v, accumulated in
+// tensor memory over every tile of the CTA and added to global memory once;
+// the bottom half (v^T v) is not used.  Warp 0 issues the MMAs (one thread),
+// warps 1..4 drain dv from tensor memory (one lane quadrant each).  Operand
+// stages and dv accumulators are double-buffered; one CTA per SM, persistent.
+// Every mbarrier wait is bounded; a timeout sets *err and unwinds.
+constexpr int kBwdXWarps = 16;                      // elementwise warps
+constexpr int kBwdThreads = 32 * (5 + kBwdXWarps);  // MMA + 4 epilogue + elementwise
+constexpr uint32_t kBwdStage = 16384 + 2 * 16384;   // sA + sX
+constexpr size_t kBwdSmem = 1024 + 8192 + 2 * static_cast<size_t>(kBwdStage) + 256;
+
+__device__ __forceinline__ float tc_gelu_grad(float x) {
+  const float cdf = 0.5f * (1.f + erff(x * 0.70710678118654752f));
+  const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
+  return cdf + x * pdf;
+}
+
+// byte offset of element (row, k) in a K-major 128B-swizzled tile of 128-byte rows
+__device__ __forceinline__ uint32_t sw128_off(int row, int k) {
+  return static_cast<uint32_t>(row) * 128u + ((static_cast<uint32_t>(k >> 3) ^ static_cast<uint32_t>(row & 7)) << 4) +
+         static_cast<uint32_t>(k & 7) * 2u;
+}
+
+struct FnoBwdParams {
+  int tiles;
+  int act;
+  const float* dvnext;      // [pix][64]
+  const __nv_bfloat16* z;   // [pix][64]
+  const __nv_bfloat16* v;   // [pix][64]
+  const float* W;           // [64 o][64 i]
+  float* dz;                // [pix][64]
+  float* dv;                // [pix][64]
+  float* dW;                // [64][64], accumulated
+  float* db;                // [64], accumulated
+  int* err;
+};
+
+__global__ void __launch_bounds__(kBwdThreads, 1) fno_tc_layer_bwd(FnoBwdParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  uint8_t* sWT = base;               // [64 i][64 o]
+  uint8_t* sS = base + 8192;         // [stage] { sA [128 px][64 o], sX [2 boxes][128 ch][64 px] }
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sS + 2 * kBwdStage);
+  uint64_t* full = bars;             // [2], one arrival per elementwise warp
+  uint64_t* empty = bars + 2;        // [2], MMA commit
+  uint64_t* tfull = bars + 4;        // [2]
+  uint64_t* tempty = bars + 6;       // [2], one arrival per epilogue warp
+  uint64_t* done = bars + 8;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 9);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr uint32_t kTmemCols = 256;  // dv accumulators at 0 / 64, dW at 128
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&full[s], kBwdXWarps);
+      mbar_init(&empty[s], 1);
+      mbar_init(&tfull[s], 1);
+      mbar_init(&tempty[s], 4);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, kTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  auto fail = [&](int code) {
+    *abort_flag = 1;
+    if (p.err) atomicExch(p.err, code);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16(128, 64);
+      const uint64_t bw = smem_desc_sw128(smem_u32(sWT));
+      int it = 0;
+      for (int t = blockIdx.x; t < p.tiles && !*abort_flag; t += gridDim.x, ++it) {
+        const int s = it & 1;
+        if (!mbar_wait_or_abort(&tempty[s], ((it >> 1) & 1) ^ 1, kFnoWaitNs, abort_flag)) {
+          fail(31);
+          break;
+        }
+        if (!mbar_wait_or_abort(&full[s], (it >> 1) & 1, kFnoWaitNs, abort_flag)) {
+          fail(32);
+          break;
+        }
+        tc_fence_after();
+        uint8_t* sA = sS + s * kBwdStage;
+        uint8_t* sX = sA + 16384;
+        const uint64_t aa = smem_desc_sw128(smem_u32(sA));
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) tc_mma_bf16(tmem_base + s * 64, aa + 2 * ks, bw + 2 * ks, idesc, ks > 0 ? 1u : 0u);
+        tc_commit(&tfull[s]);
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {
+          uint8_t* box = sX + (ks >> 2) * 16384;
+          const uint64_t ax = smem_desc_sw128(smem_u32(box)) + 2 * (ks & 3);
+          const uint64_t bx = smem_desc_sw128(smem_u32(box + 8192)) + 2 * (ks & 3);
+          tc_mma_bf16(tmem_base + 128, ax, bx, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+        }
+        tc_commit(&empty[s]);
+      }
+      tc_commit(done);
+      mbar_wait(done, 0, kFnoWaitNs);
+    }
+  } else if (warp <= 4) {
+    // dv epilogue: lane quadrant warp % 4, one pixel row per lane
+    const int quad = warp & 3;
+    int it = 0;
+    for (int t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
+      const int s = it & 1;
+      const bool got =
+          __all_sync(0xffffffffu, mbar_wait_or_abort(&tfull[s], (it >> 1) & 1, kFnoWaitNs, abort_flag));
+      if (!got) {
+        if (lane == 0) fail(33);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + s * 64;
+      float a[32], b[32];
+      tmem_ld32(taddr, a);
+      tmem_ld32(taddr + 32, b);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[s]);
+      float4* o = reinterpret_cast<float4*>(p.dv + (static_cast<size_t>(t) * 128 + quad * 32 + lane) * 64);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) o[q] = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) o[8 + q] = make_float4(b[4 * q], b[4 * q + 1], b[4 * q + 2], b[4 * q + 3]);
+    }
+    // dW rows o = lanes 0..63 of the second accumulator, once every MMA is complete
+    if (quad < 2) {
+      const bool fin = __all_sync(0xffffffffu, mbar_wait(done, 0, kFnoWaitNs));
+      if (fin && !*abort_flag) {
+        tc_fence_after();
+        const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + 128;
+        float a[32], b[32];
+        tmem_ld32(taddr, a);
+        tmem_ld32(taddr + 32, b);
+        float* w = p.dW + (quad * 32 + lane) * 64;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) atomicAdd(w + i, a[i]);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) atomicAdd(w + 32 + i, b[i]);
+      } else if (!fin && lane == 0) {
+        fail(34);
+      }
+    }
+  } else {
+    // elementwise warps: channel group og (8 channels), pixels 32 (2 jb + c) + lane
+    const int xw = warp - 5, og = xw & 7, jb = xw >> 3, o0 = 8 * og;
+    const int xt = threadIdx.x - 5 * 32;
+    // W^T into sWT once: element (o, i) of W is row i, column o of the B operand
+    for (int e = xt; e < 64 * 64; e += 32 * kBwdXWarps) {
+      const int o = e >> 6, i = e & 63;
+      *reinterpret_cast<__nv_bfloat16*>(sWT + sw128_off(i, o)) = __float2bfloat16_rn(p.W[e]);
+    }
+    float dbp[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) dbp[e] = 0.f;
+    int it = 0;
+    for (int t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
+      const int s = it & 1;
+      float4 g[2][2];
+      uint4 zz[2], vv[2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int px = 32 * (2 * jb + c) + lane;
+        const size_t off = (static_cast<size_t>(t) * 128 + px) * 64 + o0;
+        g[c][0] = *reinterpret_cast<const float4*>(p.dvnext + off);
+        g[c][1] = *reinterpret_cast<const float4*>(p.dvnext + off + 4);
+        zz[c] = p.act ? *reinterpret_cast<const uint4*>(p.z + off) : make_uint4(0, 0, 0, 0);
+        vv[c] = *reinterpret_cast<const uint4*>(p.v + off);
+      }
+      // stage s was last read by the MMAs of tile it - 2
+      const bool ok = __all_sync(0xffffffffu, mbar_wait_or_abort(&empty[s], ((it >> 1) & 1) ^ 1, kFnoWaitNs, abort_flag));
+      if (!ok) {
+        if (lane == 0) fail(35);
+        break;
+      }
+      uint8_t* sA = sS + s * kBwdStage;
+      uint8_t* sX = sA + 16384;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int px = 32 * (2 * jb + c) + lane;
+        const size_t off = (static_cast<size_t>(t) * 128 + px) * 64 + o0;
+        const float gv[8] = {g[c][0].x, g[c][0].y, g[c][0].z, g[c][0].w, g[c][1].x, g[c][1].y, g[c][1].z, g[c][1].w};
+        const __nv_bfloat16* zb = reinterpret_cast<const __nv_bfloat16*>(&zz[c]);
+        const __nv_bfloat16* vb = reinterpret_cast<const __nv_bfloat16*>(&vv[c]);
+        float d[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          d[e] = p.act ? gv[e] * tc_gelu_grad(__bfloat162float(zb[e])) : gv[e];
+          dbp[e] += d[e];
+        }
+        reinterpret_cast<float4*>(p.dz + off)[0] = make_float4(d[0], d[1], d[2], d[3]);
+        reinterpret_cast<float4*>(p.dz + off)[1] = make_float4(d[4], d[5], d[6], d[7]);
+        __align__(16) __nv_bfloat16 db16[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) db16[e] = __float2bfloat16_rn(d[e]);
+        // A of dv: row px, 16-byte chunk og
+        *reinterpret_cast<uint4*>(sA + sw128_off(px, o0)) = *reinterpret_cast<const uint4*>(db16);
+        // A of dW: rows o (dz^T) and 64 + i (v^T), column px
+        uint8_t* box = sX + (px >> 6) * 16384;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          *reinterpret_cast<__nv_bfloat16*>(box + sw128_off(o0 + e, px & 63)) = db16[e];
+          *reinterpret_cast<__nv_bfloat16*>(box + sw128_off(64 + o0 + e, px & 63)) = vb[e];
+        }
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&full[s]);
+    }
+    if (!*abort_flag) {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        float x = dbp[e];
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) x += __shfl_xor_sync(0xffffffffu, x, sh);
+        if (lane == 0) atomicAdd(p.db + o0 + e, x);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
+}
+
 // bf16 copy of an fp32 matrix (weights for the tensor-core operands).
 __global__ void fno_to_bf16(const float* __restrict__ a, int n, __nv_bfloat16* __restrict__ b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -276,6 +525,9 @@ cudaError_t fno_tc_set_smem() {
   if ((e = cudaFuncSetAttribute(huv_dev::fno_tc_pw<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(fno_tc_smem(0)))))
     return e;
+  if ((e = cudaFuncSetAttribute(huv_dev::fno_tc_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(huv_dev::kBwdSmem))))
+    return e;
   return cudaFuncSetAttribute(huv_dev::fno_tc_pw<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               static_cast<int>(fno_tc_smem(1)));
 }
@@ -321,6 +573,29 @@ bool fno_tc_proj(int B, int S, const __nv_bfloat16* v, const __nv_bfloat16* Q1b,
   p.err = err;
   const int grid = std::min(p.tiles, 2 * 148);
   huv_dev::fno_tc_pw<1><<<grid, 192, fno_tc_smem(1), st>>>(mv, mq, mq, mq, p);
+  return cudaGetLastError() == cudaSuccess;
+}
+// Layer backward on tensor cores (see fno_tc_layer_bwd); pix a multiple of 128.
+bool fno_tc_layer_bwd(size_t pix, const float* dvnext, const __nv_bfloat16* z, const __nv_bfloat16* v, const float* W,
+                      int act, float* dz, float* dv, float* dW, float* db, int* err, cudaStream_t st) {
+  if (pix % 128 != 0) return false;
+  huv_dev::FnoBwdParams p{};
+  p.tiles = static_cast<int>(pix / 128);
+  p.act = act;
+  p.dvnext = dvnext;
+  p.z = z;
+  p.v = v;
+  p.W = W;
+  p.dz = dz;
+  p.dv = dv;
+  p.dW = dW;
+  p.db = db;
+  p.err = err;
+  int sms = 0, dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return false;
+  const int grid = std::min(p.tiles, sms);
+  huv_dev::fno_tc_layer_bwd<<<grid, huv_dev::kBwdThreads, huv_dev::kBwdSmem, st>>>(p);
   return cudaGetLastError() == cudaSuccess;
 }
 void fno_tc_to_bf16(const float* a, int n, __nv_bfloat16* b, cudaStream_t st) {

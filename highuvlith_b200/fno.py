@@ -74,6 +74,14 @@ class FnoSurrogate:
         L.check(L.lib().huv_fno_forward(self._h, masks.shape[0], masks.data_ptr(), out.data_ptr(), st))
         return out
 
+    def device_status(self, stream=None) -> None:
+        """Synchronise the stream; raises HuvError (DEVICE_TIMEOUT) if a bounded
+        device-side wait of an earlier forward gave up (its images are then not
+        valid).  backward and train_step check this themselves."""
+        import torch
+        st = (stream or torch.cuda.current_stream()).cuda_stream
+        L.check(L.lib().huv_fno_device_status(self._h, st))
+
     def backward(self, masks, targets=None, dout=None, want_param_grad=True, want_input_grad=False, stream=None):
         import torch
         masks = self._maps(masks, "masks")

@@ -356,6 +356,12 @@ huv_status huv_fno_backward(void* fno, int32_t batch, const float* masks, const 
 /* One Adam step on the MSE to `targets`. */
 huv_status huv_fno_train_step(void* fno, int32_t batch, const float* masks, const float* targets, float lr,
                               float weight_decay, float* loss_host, void* stream);
+/* Synchronise `stream` and report HUV_ERR_DEVICE_TIMEOUT if a bounded wait of
+ * an FNO tensor-core kernel gave up since the last check (the results of those
+ * calls are then not valid); the flag is cleared.  huv_fno_backward and
+ * huv_fno_train_step check it themselves before returning; huv_fno_forward
+ * leaves the stream asynchronous, so its callers check here. */
+huv_status huv_fno_device_status(void* fno, void* stream);
 
 /* Allocation-free variant of huv_image_batch (no counterpart in the
  * reference, which has no device path).  For callers that cannot call

@@ -14,8 +14,9 @@ def _rel(a, b):
 
 @pytest.mark.parametrize("S,M,LAYERS", [(S, M, LAYERS), (128, 16, 2)])
 def test_fno_forward_and_gradients_match_fp64_reference(S, M, LAYERS):
-    """Small grid (one partial pixel tile per row) and a grid with several
-    64-pixel tiles per row and the full 16 retained modes."""
+    """Small grid (CUDA-core channel kernels, one partial pixel tile per row)
+    and a 128 grid (tcgen05 channel GEMMs in the forward and the backward,
+    BF16 operands; the full 16 retained modes)."""
     import torch
     from highuvlith_b200.fno import FnoSurrogate
     from oracle import fno_ref
@@ -26,6 +27,7 @@ def test_fno_forward_and_gradients_match_fp64_reference(S, M, LAYERS):
     params = net.get_params()
     dm = torch.from_numpy(masks).cuda()
     out = net.forward(dm).cpu().numpy()
+    net.device_status()  # no bounded device-side wait gave up
     ref, p, a = fno_ref.forward(params.astype(np.float64), masks, S, m=M, L=LAYERS, requires_grad=True)
     assert _rel(out, ref.detach().numpy()) < 2e-2
     # gradients of the MSE loss
