@@ -27,6 +27,9 @@
 namespace huv_launch {
 // tensor-core forward of the FNO (csrc/cuda/fno_tc.cu)
 cudaError_t fno_tc_set_smem();
+bool fno_tc_proj_bwd(size_t pix, const __nv_bfloat16* v, const float* Q1, const float* b1, const float* q2,
+                     const float* dout, float* dv, float* dQ1, float* db1, float* dQ2, float* db2, int* err,
+                     cudaStream_t st);
 bool fno_tc_layer_bwd(size_t pix, const float* dvnext, const __nv_bfloat16* z, const __nv_bfloat16* v, const float* W,
                       int act, float* dz, float* dv, float* dW, float* db, int* err, cudaStream_t st);
 bool fno_tc_layer(int B, int S, int m, const __nv_bfloat16* v, const __nv_bfloat16* Wb, const __nv_bfloat16* Tw,
@@ -966,8 +969,14 @@ struct Fno {
     const dim3 rgrid(std::min(rows, 4096));
     const dim3 ygrid((m * C + 63) / 64, B);
     check_cuda(cudaMemsetAsync(grad, 0, npar * 4, st), "memset grad");
-    fno_proj_bwd<<<std::min<size_t>((pix + 63) / 64, 148), 256, kProjBwdSmem, st>>>(
-        v[L], par + oQ1, par + ob1, par + oQ2, pix, dOut, dvA, grad + oQ1, grad + ob1, grad + oQ2, grad + ob2);
+    if (tc) {
+      if (!huv_launch::fno_tc_proj_bwd(pix, v[L], par + oQ1, par + ob1, par + oQ2, dOut, dvA, grad + oQ1, grad + ob1,
+                                       grad + oQ2, grad + ob2, tc_err, st))
+        throw Error(HUV_ERR_CUDA, "fno: tensor-core projection backward launch failed");
+    } else {
+      fno_proj_bwd<<<std::min<size_t>((pix + 63) / 64, 148), 256, kProjBwdSmem, st>>>(
+          v[L], par + oQ1, par + ob1, par + oQ2, pix, dOut, dvA, grad + oQ1, grad + ob1, grad + oQ2, grad + ob2);
+    }
     float* dnext = dvA;
     float* dcur = dvB;
     for (int l = L - 1; l >= 0; --l) {

@@ -469,6 +469,279 @@ __global__ void __launch_bounds__(kBwdThreads, 1) fno_tc_layer_bwd(FnoBwdParams 
   if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
 }
 
+// Backward of the projection head on tcgen05, per 128-pixel tile (h = Q1 v + b1):
+//   h - b1 = v Q1^T                 (M 128 px, N 128 j, K 64 c)   GEMM-h
+//   dh = dout Q2 GELU'(h), g = dout GELU(h)                        CUDA cores
+//   dv = dh Q1                      (M 128 px, N 64 c,  K 128 j)  GEMM-dv
+//   [dQ1 | db1] += dh^T [v | 1]     (M 128 j,  N 80,    K 128 px) GEMM-Q
+//   dQ2 += g^T 1                    (M 128 j,  N 16,    K 128 px) GEMM-G
+//   db2 += sum dout.
+// Warp 0 loads the v tile (TMA, 128B swizzle), warp 1 issues the MMAs (one
+// thread), warps 2..9 (two per tensor-memory lane quadrant, each half of
+// the columns) do the elementwise part, write the BF16 operands dh, dh^T,
+// g^T and v^T into shared memory (128B-swizzled K-major), and drain dv.
+// The weight-gradient sums stay in tensor memory over all tiles of the CTA
+// and are added to global memory once.  One CTA per SM, persistent.
+constexpr int kPbThreads = 320;
+constexpr uint32_t kPbQ1 = 0, kPbQ1T = 16384, kPbOnes = 32768, kPbV = 36864, kPbDH = 53248, kPbDHT = 86016,
+                   kPbGT = 118784, kPbBQ = 151552, kPbBars = 172032;
+constexpr size_t kPbSmem = 1024 + kPbBars + 256;
+
+struct FnoProjBwdParams {
+  int tiles;
+  const float* Q1;    // [128 j][64 c]
+  const float* b1;    // [128]
+  const float* q2;    // [128]
+  const float* dout;  // [pix]
+  float* dv;          // [pix][64]
+  float* dQ1;         // [128][64], accumulated
+  float* db1;         // [128]
+  float* dQ2;         // [128]
+  float* db2;         // [1]
+  int* err;
+};
+
+__global__ void __launch_bounds__(kPbThreads, 1)
+    fno_tc_proj_bwd(const __grid_constant__ CUtensorMap tmV, FnoProjBwdParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kPbBars);
+  uint64_t* v_full = bars + 0;
+  uint64_t* v_free = bars + 1;   // GEMM-h commit + 8 elementwise warps
+  uint64_t* h_full = bars + 2;
+  uint64_t* h_free = bars + 3;   // 8 elementwise warps
+  uint64_t* ops_full = bars + 4; // 8 elementwise warps
+  uint64_t* ops_free = bars + 5;
+  uint64_t* dv_full = bars + 6;
+  uint64_t* dv_free = bars + 7;  // 8 elementwise warps
+  uint64_t* w_ready = bars + 8;  // 8 elementwise warps
+  uint64_t* done = bars + 9;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr uint32_t kTmemCols = 512;
+  constexpr uint32_t cH = 0, cDV = 128, cQ = 192, cG = 272;  // accumulator columns
+
+  if (threadIdx.x == 0) {
+    mbar_init(v_full, 1);
+    mbar_init(v_free, 9);
+    mbar_init(h_full, 1);
+    mbar_init(h_free, 8);
+    mbar_init(ops_full, 8);
+    mbar_init(ops_free, 1);
+    mbar_init(dv_full, 1);
+    mbar_init(dv_free, 8);
+    mbar_init(w_ready, 8);
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, kTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  auto fail = [&](int code) {
+    *abort_flag = 1;
+    if (p.err) atomicExch(p.err, code);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      prefetch_tmap(&tmV);
+      int it = 0;
+      for (int t = blockIdx.x; t < p.tiles && !*abort_flag; t += gridDim.x, ++it) {
+        if (!mbar_wait_or_abort(v_free, (it & 1) ^ 1, kFnoWaitNs, abort_flag)) {
+          fail(41);
+          break;
+        }
+        mbar_arrive_expect_tx(v_full, kTile);
+        tma_load_2d(base + kPbV, &tmV, 0, t * 128, v_full);
+      }
+      // the last load issued lands before the CTA may exit
+      if (it > 0) mbar_wait(v_full, (it - 1) & 1, kFnoWaitNs);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      bool ok = mbar_wait_or_abort(w_ready, 0, kFnoWaitNs, abort_flag);
+      if (!ok) fail(42);
+      int it = 0;
+      for (int t = blockIdx.x; t < p.tiles && ok && !*abort_flag; t += gridDim.x, ++it) {
+        const uint32_t ph = it & 1;
+        if (!mbar_wait_or_abort(v_full, ph, kFnoWaitNs, abort_flag) ||
+            !mbar_wait_or_abort(h_free, ph ^ 1, kFnoWaitNs, abort_flag)) {
+          fail(43);
+          break;
+        }
+        tc_fence_after();
+        {
+          const uint64_t a = smem_desc_sw128(smem_u32(base + kPbV));
+          const uint64_t b = smem_desc_sw128(smem_u32(base + kPbQ1));
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks)
+            tc_mma_bf16(tmem_base + cH, a + 2 * ks, b + 2 * ks, idesc_bf16(128, 128), ks > 0 ? 1u : 0u);
+        }
+        tc_commit(h_full);
+        tc_commit(v_free);
+        if (!mbar_wait_or_abort(ops_full, ph, kFnoWaitNs, abort_flag) ||
+            !mbar_wait_or_abort(dv_free, ph ^ 1, kFnoWaitNs, abort_flag)) {
+          fail(44);
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {
+          const uint32_t bx = ks >> 2, kk = 2 * (ks & 3);
+          tc_mma_bf16(tmem_base + cDV, smem_desc_sw128(smem_u32(base + kPbDH + bx * 16384)) + kk,
+                      smem_desc_sw128(smem_u32(base + kPbQ1T + bx * 8192)) + kk, idesc_bf16(128, 64),
+                      ks > 0 ? 1u : 0u);
+        }
+        tc_commit(dv_full);
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {
+          const uint32_t bx = ks >> 2, kk = 2 * (ks & 3);
+          const uint32_t acc = (it > 0 || ks > 0) ? 1u : 0u;
+          tc_mma_bf16(tmem_base + cQ, smem_desc_sw128(smem_u32(base + kPbDHT + bx * 16384)) + kk,
+                      smem_desc_sw128(smem_u32(base + kPbBQ + bx * 10240)) + kk, idesc_bf16(128, 80), acc);
+          tc_mma_bf16(tmem_base + cG, smem_desc_sw128(smem_u32(base + kPbGT + bx * 16384)) + kk,
+                      smem_desc_sw128(smem_u32(base + kPbOnes + bx * 2048)) + kk, idesc_bf16(128, 16), acc);
+        }
+        tc_commit(ops_free);
+      }
+      tc_commit(done);
+      mbar_wait(done, 0, kFnoWaitNs);
+    }
+  } else {
+    // elementwise warps 2..9: lane quadrant warp % 4 (pixel rows of a tile,
+    // j rows of the weight-gradient sums), column half `half`
+    const int quad = warp & 3, half = (warp - 2) >> 2;
+    const int et = threadIdx.x - 64;  // 0..255
+    // resident operands: Q1 [j][c] (B of GEMM-h), Q1^T [c][j] (B of GEMM-dv),
+    // ones (B of GEMM-G: row 0), rows 64..79 of [v^T; 1] (row 64 ones)
+    for (int e = et; e < 128 * 64; e += 256) {
+      const int j = e >> 6, c = e & 63;
+      const __nv_bfloat16 q = __float2bfloat16_rn(p.Q1[e]);
+      *reinterpret_cast<__nv_bfloat16*>(base + kPbQ1 + sw128_off(j, c)) = q;
+      *reinterpret_cast<__nv_bfloat16*>(base + kPbQ1T + (j >> 6) * 8192 + sw128_off(c, j & 63)) = q;
+    }
+    const __nv_bfloat16 one = __float2bfloat16_rn(1.f), zero = __float2bfloat16_rn(0.f);
+    for (int e = et; e < 2 * 16 * 64; e += 256) {
+      const int bx = e >> 10, r = (e >> 6) & 15, k = e & 63;
+      *reinterpret_cast<__nv_bfloat16*>(base + kPbOnes + bx * 2048 + sw128_off(r, k)) = r == 0 ? one : zero;
+      *reinterpret_cast<__nv_bfloat16*>(base + kPbBQ + bx * 10240 + sw128_off(64 + r, k)) = r == 0 ? one : zero;
+    }
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(w_ready);
+
+    const int px = quad * 32 + lane;  // pixel row within the tile
+    const int bxp = px >> 6, kp = px & 63;
+    float gd2 = 0.f;
+    int it = 0;
+    for (int t = blockIdx.x; t < p.tiles; t += gridDim.x, ++it) {
+      const uint32_t ph = it & 1;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait_or_abort(h_full, ph, kFnoWaitNs, abort_flag) &&
+                                                  mbar_wait_or_abort(ops_free, ph ^ 1, kFnoWaitNs, abort_flag));
+      if (!ok) {
+        if (lane == 0) fail(45);
+        break;
+      }
+      tc_fence_after();
+      const float d = p.dout[static_cast<size_t>(t) * 128 + px];
+      if (half == 0) gd2 += d;
+#pragma unroll 1
+      for (int jc = 0; jc < 2; ++jc) {
+        const int j0 = half * 64 + jc * 32;
+        float h[32];
+        tmem_ld32(tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + cH + j0, h);
+        __align__(16) __nv_bfloat16 dhb[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const int j = j0 + i;
+          const float x = h[i] + __ldg(p.b1 + j);
+          const float cdf = 0.5f * (1.f + erff(x * 0.70710678118654752f));
+          const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
+          const float dh = d * __ldg(p.q2 + j) * (cdf + x * pdf);
+          dhb[i] = __float2bfloat16_rn(dh);
+          const __nv_bfloat16 gb = __float2bfloat16_rn(d * x * cdf);
+          // dh^T and g^T: row j, column px (2-byte stores, one row per warp store)
+          *reinterpret_cast<__nv_bfloat16*>(base + kPbDHT + bxp * 16384 + sw128_off(j, kp)) = dhb[i];
+          *reinterpret_cast<__nv_bfloat16*>(base + kPbGT + bxp * 16384 + sw128_off(j, kp)) = gb;
+        }
+        // dh: row px, four 16-byte chunks of 8 j
+        uint8_t* dbox = base + kPbDH + (j0 >> 6) * 16384;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          *reinterpret_cast<uint4*>(dbox + sw128_off(px, (j0 & 63) + 8 * q)) = reinterpret_cast<const uint4*>(dhb)[q];
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(h_free);
+      // v^T rows c (this half's 32 channels), column px, from the v tile
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c0 = half * 32 + 8 * q;
+        const uint4 w = *reinterpret_cast<const uint4*>(base + kPbV + sw128_off(px, c0));
+        const __nv_bfloat16* vb = reinterpret_cast<const __nv_bfloat16*>(&w);
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+          *reinterpret_cast<__nv_bfloat16*>(base + kPbBQ + bxp * 10240 + sw128_off(c0 + e, kp)) = vb[e];
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(v_free);
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(ops_full);
+      // dv: this half's 32 channels of pixel row px
+      const bool got = __all_sync(0xffffffffu, mbar_wait_or_abort(dv_full, ph, kFnoWaitNs, abort_flag));
+      if (!got) {
+        if (lane == 0) fail(46);
+        break;
+      }
+      tc_fence_after();
+      float o[32];
+      tmem_ld32(tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + cDV + half * 32, o);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(dv_free);
+      float4* dst = reinterpret_cast<float4*>(p.dv + (static_cast<size_t>(t) * 128 + px) * 64 + half * 32);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) dst[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+    }
+    // weight-gradient sums: rows j = lanes of the quadrant
+    const bool fin = __all_sync(0xffffffffu, mbar_wait(done, 0, kFnoWaitNs));
+    if (fin && !*abort_flag) {
+      tc_fence_after();
+      const int j = quad * 32 + lane;
+      const uint32_t lrow = static_cast<uint32_t>(quad * 32) << 16;
+      float a[32];
+      tmem_ld32(tmem_base + lrow + cQ + half * 32, a);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) atomicAdd(p.dQ1 + j * 64 + half * 32 + i, a[i]);
+      if (half == 0) {
+        float b[16], g[16];
+        tmem_ld16(tmem_base + lrow + cQ + 64, b);
+        tmem_ld16(tmem_base + lrow + cG, g);
+        atomicAdd(p.db1 + j, b[0]);
+        atomicAdd(p.dQ2 + j, g[0]);
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) gd2 += __shfl_xor_sync(0xffffffffu, gd2, sh);
+        if (lane == 0) atomicAdd(p.db2, gd2);
+      }
+    } else if (!fin && lane == 0) {
+      fail(47);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
+}
+
 // bf16 copy of an fp32 matrix (weights for the tensor-core operands).
 __global__ void fno_to_bf16(const float* __restrict__ a, int n, __nv_bfloat16* __restrict__ b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -527,6 +800,9 @@ cudaError_t fno_tc_set_smem() {
     return e;
   if ((e = cudaFuncSetAttribute(huv_dev::fno_tc_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(huv_dev::kBwdSmem))))
+    return e;
+  if ((e = cudaFuncSetAttribute(huv_dev::fno_tc_proj_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(huv_dev::kPbSmem))))
     return e;
   return cudaFuncSetAttribute(huv_dev::fno_tc_pw<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               static_cast<int>(fno_tc_smem(1)));
@@ -596,6 +872,33 @@ bool fno_tc_layer_bwd(size_t pix, const float* dvnext, const __nv_bfloat16* z, c
     return false;
   const int grid = std::min(p.tiles, sms);
   huv_dev::fno_tc_layer_bwd<<<grid, huv_dev::kBwdThreads, huv_dev::kBwdSmem, st>>>(p);
+  return cudaGetLastError() == cudaSuccess;
+}
+// Projection backward on tensor cores (see fno_tc_proj_bwd); v: [pix][64]
+// bf16, pix a multiple of 128.
+bool fno_tc_proj_bwd(size_t pix, const __nv_bfloat16* v, const float* Q1, const float* b1, const float* q2,
+                     const float* dout, float* dv, float* dQ1, float* db1, float* dQ2, float* db2, int* err,
+                     cudaStream_t st) {
+  if (pix % 128 != 0) return false;
+  CUtensorMap mv;
+  if (!tc_map_bf16(&mv, v, pix, 64, 128)) return false;
+  huv_dev::FnoProjBwdParams p{};
+  p.tiles = static_cast<int>(pix / 128);
+  p.Q1 = Q1;
+  p.b1 = b1;
+  p.q2 = q2;
+  p.dout = dout;
+  p.dv = dv;
+  p.dQ1 = dQ1;
+  p.db1 = db1;
+  p.dQ2 = dQ2;
+  p.db2 = db2;
+  p.err = err;
+  int sms = 0, dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return false;
+  const int grid = std::min(p.tiles, sms);
+  huv_dev::fno_tc_proj_bwd<<<grid, huv_dev::kPbThreads, huv_dev::kPbSmem, st>>>(mv, p);
   return cudaGetLastError() == cudaSuccess;
 }
 void fno_tc_to_bf16(const float* a, int n, __nv_bfloat16* b, cudaStream_t st) {
