@@ -501,7 +501,11 @@ __global__ void __launch_bounds__(fr_threads(L, S))
   }
   __syncthreads();
   const float2* cur = b0;
-  if constexpr (NP == 3) {
+  if constexpr (NP == 3 && fr_mid_inplace_ok(L, S)) {
+    // one buffer: more blocks per SM to keep the column loads in flight
+    fr_mid_pass_inplace<L, S, -1, 1>(t, b0, tw);
+    __syncthreads();
+  } else if constexpr (NP == 3) {
     fr_mid_pass<L, S, -1, 1>(t, b0, b1, tw);
     __syncthreads();
     cur = b1;
@@ -647,7 +651,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     const int S = xt_S(n);
     nblk = (B + S - 1) / S;
     const dim3 g(nblk, clips);
-    const size_t sm = xt_buf_bytes(n);
+    const size_t sm = band_cols_buf_bytes(n);
     switch (n) {
       case 128: band_cols_reg<128, 32><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 160: band_cols_reg<160, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
