@@ -1272,16 +1272,18 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       // per 80 tensor cycles at M = 160), else two halves (M = 192).
       const int bn1 = M <= 160 ? M : M / 2;
       const int ntile1 = M / bn1, mtiles = n / 128;
-      // Clips per CTA: the fewest (up to 8) whose grid fits one wave of one
-      // CTA per SM, else 8.  Each CTA's run is latency-bound (per step: one
+      // Clips per CTA: the fewest (up to 32) whose grid fits one wave of one
+      // CTA per SM, else 32.  Each CTA's run is latency-bound (per step: one
       // clip's B ring through 3 stages), so longer runs over a resident A
       // tile beat more CTAs: at 128 clips 1 / 2 / 4 / 8 clips per CTA time
-      // 1.24 / 1.12 / 1.03 / 0.99 ms per 20 launches.
+      // 1.24 / 1.12 / 1.03 / 0.99 ms per 20 launches; at 256 clips 15 per
+      // CTA (one wave of 144 CTAs) 0.084 ms per launch against 0.092 with 8
+      // (256 CTAs, 1.7 waves).
       int sms = 0, dev = 0;
       check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
       check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-      int G1 = 8;
-      for (int gc = 1; gc < 8; ++gc)
+      int G1 = 32;
+      for (int gc = 1; gc < 32; ++gc)
         if (static_cast<long long>(ntile1) * mtiles * ((nc + gc - 1) / gc) <= sms) {
           G1 = gc;
           break;
