@@ -11,9 +11,8 @@
 //
 // Set-up: the first call on a device takes the array's device address with
 // cudaGetSymbolAddress (the host-side symbol is only a stand-in, not a device
-// address) and sets the kernels' shared-memory limits; make that first call
-// before any stream capture.  Every GPU that loads the library holds the
-// array until the process exits.
+// address) and sets the kernels' shared-memory limits.  Every GPU that loads
+// the library holds the array until the process exits.
 //
 // All calls share the array, which keeps the last call's contents: calls
 // that overlap on the GPU (different streams, or different host threads)

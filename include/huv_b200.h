@@ -372,8 +372,8 @@ huv_status huv_fno_device_status(void* fno, void* stream);
  * loads the library holds it until exit); batches are processed in chunks
  * that fit it, and a grid whose single clip does not fit is rejected with
  * HUV_ERR_INVALID_PARAMETER.  The first call on a device performs the
- * set-up (takes the array's device address); make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race.
+ * set-up (takes the array's device address).  All calls share the array:
+ * calls that overlap on the GPU race.
  * form must be HUV_FORM_AUTO or HUV_FORM_FFT.  The engine's focus-plane
  * cache is only read: a plane it does not hold is built on the host for
  * this call and not cached, and on an engine whose kernels are built on the
