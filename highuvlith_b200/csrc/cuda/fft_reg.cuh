@@ -305,19 +305,10 @@ __host__ __device__ constexpr int xt_S(int L) {
   return L == 128 ? 32 : (L == 160 || L == 192 || L == 256) ? 16 : L == 512 ? 8 : L == 1024 ? 4 : L == 2048 ? 2 : 0;
 }
 __host__ __device__ constexpr size_t xt_buf_bytes(int L) {
-  return xt_S(L) ? (fr_passes(L) - 1) * static_cast<size_t>(fr_buf(L, xt_S(L))) * sizeof(float2) : 0;
+  // one buffer: the middle passes run in place (fr_mid_pass_inplace)
+  return xt_S(L) ? static_cast<size_t>(fr_buf(L, xt_S(L))) * sizeof(float2) : 0;
 }
 constexpr int kXtSmemMax = 110 * 1024;
-// Whether the middle pass of length L at S sequences per block can run in
-// place (three passes, exactly one middle-pass butterfly per thread), and
-// the one-buffer shared-memory bytes of the mask-band column kernel then.
-__host__ __device__ constexpr bool fr_mid_inplace_ok(int L, int S) {
-  return fr_passes(L) == 3 && fr_nb(L, S, 1) == fr_threads(L, S);
-}
-__host__ __device__ constexpr size_t band_cols_buf_bytes(int L) {
-  return xt_S(L) && fr_mid_inplace_ok(L, xt_S(L)) ? static_cast<size_t>(fr_buf(L, xt_S(L))) * sizeof(float2)
-                                                  : xt_buf_bytes(L);
-}
 
 // First pass (radix 16, no twiddles) for thread t, reading a zero-padded
 // band: position i of sequence s holds P[s][mx] for the order mx - hb = i
@@ -388,30 +379,41 @@ __host__ __device__ __forceinline__ void fr_mid_pass(int t, const float2* src, f
   }
 }
 
-// Middle pass in place (fr_mid_inplace_ok): every thread loads the inputs
-// of its one butterfly, the block synchronises, then every thread
-// transforms and stores into the same buffer.  Called by all threads.
+// Middle pass `pass` in place: every thread loads the inputs of all its
+// butterflies, the block synchronises, then every thread transforms and
+// stores into the same buffer (one FFT buffer per block instead of two, so
+// more blocks fit an SM).  Called by all threads of the block.
 template <int L, int S, int DIR, int PASS>
 __device__ __forceinline__ void fr_mid_pass_inplace(int t, float2* buf, const float2* tw) {
-  static_assert(PASS == 1 && fr_mid_inplace_ok(L, S), "one middle-pass butterfly per thread");
-  constexpr int R = fr_radix(L, PASS), Ns = fr_ns(L, PASS);
+  constexpr int R = fr_radix(L, PASS), Ns = fr_ns(L, PASS), T = fr_threads(L, S), PER = fr_per(L, S, PASS);
   constexpr int stride = L / (Ns * R);
-  const int s = t % S, j = t / S;
-  const int k = j & (Ns - 1);
-  float2 v[R];
+  float2 v[PER][R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) v[r] = buf[fr_idx<S>(j + r * (L / R), s)];
+  for (int b = 0; b < PER; ++b) {
+    const int u = t + b * T;
+    if (u >= fr_nb(L, S, PASS)) break;
+    const int s = u % S, j = u / S;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[b][r] = buf[fr_idx<S>(j + r * (L / R), s)];
+  }
   __syncthreads();
 #pragma unroll
-  for (int r = 1; r < R; ++r) {
-    float2 w = tw[r * k * stride];
-    if (DIR > 0) w.y = -w.y;
-    v[r] = fr_mul(v[r], w);
-  }
-  fr_dft<R, DIR>(v);
-  const int base = (j - k) * R + k;
+  for (int b = 0; b < PER; ++b) {
+    const int u = t + b * T;
+    if (u >= fr_nb(L, S, PASS)) break;
+    const int s = u % S, j = u / S;
+    const int k = j & (Ns - 1);
 #pragma unroll
-  for (int r = 0; r < R; ++r) buf[fr_idx<S>(base + r * Ns, s)] = v[r];
+    for (int r = 1; r < R; ++r) {
+      float2 w = tw[r * k * stride];
+      if (DIR > 0) w.y = -w.y;
+      v[b][r] = fr_mul(v[b][r], w);
+    }
+    fr_dft<R, DIR>(v[b]);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) buf[fr_idx<S>(base + r * Ns, s)] = v[b][r];
+  }
 }
 
 // Last pass for butterfly u: loads, twiddles and transforms; returns the

@@ -474,13 +474,19 @@ __global__ void ilt_finish(const float* __restrict__ theta, const float* __restr
 // The same as ilt_finish for grids that are multiples of TS: a block takes a
 // TS x TS tile, computes m = sigmoid(beta theta) once for the tile and its
 // 1-pixel periodic halo in shared memory (instead of up to nine sigmoids per
-// pixel), and writes its share of the regulariser cost to parts[mask][tile].
-// grid: ((n / TS)^2, masks), block 256.
+// pixel; the halo's loads are all issued before the first sigmoid), then
+// each thread takes runs of 4 pixels of a row (16-byte loads of dC/dm and
+// stores of the gradient), and writes its share of the regulariser cost to
+// parts[mask][tile].  grid: ((n / TS)^2, masks), block 256.
 template <int TS>
 __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict__ theta,
                                                          const float* __restrict__ dcdm, int n, float beta,
                                                          float tv_w, float tv_eps, float bin_w,
                                                          float* __restrict__ grad, double* __restrict__ parts) {
+  static_assert(TS % 4 == 0 && (TS * TS) % 1024 == 0, "tiles of whole 4-pixel runs, 256 threads");
+  constexpr int NE = (TS + 2) * (TS + 2), NQ = (NE + 255) / 256;
+  constexpr int RUNS = TS / 4;               // 4-pixel runs per row
+  constexpr int ROWS_PER_PASS = 256 / RUNS;  // rows a pass of the block covers
   __shared__ float sm[TS + 2][TS + 3];
   __shared__ double red[32];
   const int mask = blockIdx.y;
@@ -489,44 +495,65 @@ __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict_
   const int ti = blockIdx.x / tiles_x, tj = blockIdx.x - ti * tiles_x;
   const float* th = theta + mask * npix;
   const float inv_n = 1.f / static_cast<float>(npix);
-  for (int e = threadIdx.x; e < (TS + 2) * (TS + 2); e += blockDim.x) {
-    const int r = e / (TS + 2), c = e - r * (TS + 2);
-    int i = ti * TS - 1 + r, j = tj * TS - 1 + c;
-    i = i < 0 ? i + n : (i >= n ? i - n : i);
-    j = j < 0 ? j + n : (j >= n ? j - n : j);
-    sm[r][c] = 1.f / (1.f + __expf(-beta * th[static_cast<size_t>(i) * n + j]));
+  float tv[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const int e = threadIdx.x + 256 * q;
+    tv[q] = 0.f;
+    if (e < NE) {
+      const int r = e / (TS + 2), c = e - r * (TS + 2);
+      int i = ti * TS - 1 + r, j = tj * TS - 1 + c;
+      i = i < 0 ? i + n : (i >= n ? i - n : i);
+      j = j < 0 ? j + n : (j >= n ? j - n : j);
+      tv[q] = th[static_cast<size_t>(i) * n + j];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const int e = threadIdx.x + 256 * q;
+    if (e < NE) {
+      const int r = e / (TS + 2), c = e - r * (TS + 2);
+      sm[r][c] = 1.f / (1.f + __expf(-beta * tv[q]));
+    }
   }
   __syncthreads();
-  // per-thread partials of the 4 pixels in FP32, the block sum in FP64
+  // per-thread partials in FP32, the block sum in FP64
   float tv_part = 0.f, bin_part = 0.f;
   const float eps2 = tv_eps * tv_eps;
-  for (int q = 0; q < TS * TS / 256; ++q) {
-    const int pidx = threadIdx.x + 256 * q;
-    const int r = pidx / TS + 1, c = pidx % TS + 1;
-    const float m = sm[r][c];
-    float g = 0.f;
-    if (tv_w > 0.f) {
-      const float gx = sm[r][c + 1] - m, gy = sm[r + 1][c] - m;
-      const float qv = gx * gx + gy * gy + eps2;
-      const float iv = rsqrtf(qv);
-      tv_part += qv * iv - tv_eps;
-      if (grad) {
-        const float ml = sm[r][c - 1], mu = sm[r - 1][c];
-        const float gxl = m - ml, gyl = sm[r + 1][c - 1] - ml;
-        const float il = rsqrtf(gxl * gxl + gyl * gyl + eps2);
-        const float gxu = sm[r - 1][c + 1] - mu, gyu = m - mu;
-        const float iu = rsqrtf(gxu * gxu + gyu * gyu + eps2);
-        g += tv_w * inv_n * (-(gx + gy) * iv + gxl * il + gyu * iu);
+  const int c4 = (threadIdx.x % RUNS) * 4, r0 = threadIdx.x / RUNS;
+#pragma unroll 2
+  for (int q = 0; q < TS / ROWS_PER_PASS; ++q) {
+    const int r = r0 + q * ROWS_PER_PASS + 1;
+    const size_t gp = mask * npix + static_cast<size_t>(ti * TS + r - 1) * n + tj * TS + c4;
+    const float4 d4 = dcdm ? *reinterpret_cast<const float4*>(dcdm + gp) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float dv[4] = {d4.x, d4.y, d4.z, d4.w};
+    float out[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = c4 + 1 + i;
+      const float m = sm[r][c];
+      float g = 0.f;
+      if (tv_w > 0.f) {
+        const float gx = sm[r][c + 1] - m, gy = sm[r + 1][c] - m;
+        const float qv = gx * gx + gy * gy + eps2;
+        const float iv = rsqrtf(qv);
+        tv_part += qv * iv - tv_eps;
+        if (grad) {
+          const float ml = sm[r][c - 1], mu = sm[r - 1][c];
+          const float gxl = m - ml, gyl = sm[r + 1][c - 1] - ml;
+          const float il = rsqrtf(gxl * gxl + gyl * gyl + eps2);
+          const float gxu = sm[r - 1][c + 1] - mu, gyu = m - mu;
+          const float iu = rsqrtf(gxu * gxu + gyu * gyu + eps2);
+          g += tv_w * inv_n * (-(gx + gy) * iv + gxl * il + gyu * iu);
+        }
       }
+      if (bin_w > 0.f) {
+        bin_part += m * (1.f - m);
+        g += bin_w * 4.f * (1.f - 2.f * m) * inv_n;
+      }
+      out[i] = (dv[i] + g) * beta * m * (1.f - m);
     }
-    if (bin_w > 0.f) {
-      bin_part += m * (1.f - m);
-      g += bin_w * 4.f * (1.f - 2.f * m) * inv_n;
-    }
-    if (grad) {
-      const size_t gp = mask * npix + static_cast<size_t>(ti * TS + r - 1) * n + tj * TS + c - 1;
-      grad[gp] = ((dcdm ? dcdm[gp] : 0.f) + g) * beta * m * (1.f - m);
-    }
+    if (grad) *reinterpret_cast<float4*>(grad + gp) = make_float4(out[0], out[1], out[2], out[3]);
   }
   const double cost = (static_cast<double>(tv_w) * tv_part + 4.0 * static_cast<double>(bin_w) * bin_part) * inv_n;
   const double cs = block_sum_double(cost, red);

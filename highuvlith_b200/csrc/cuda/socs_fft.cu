@@ -247,7 +247,7 @@ __global__ void socs_cols_inv(const float2* __restrict__ T, int K, int hb, int l
 // shared memory allows it (3.6 % faster at M = 160); the long transforms
 // are held to three (their buffers allow three blocks at most).
 template <int L, int S>
-__global__ void __launch_bounds__(fr_threads(L, S), (L <= 256 ? 6 : 3))
+__global__ void __launch_bounds__(fr_threads(L, S), (L <= 256 ? 6 : 4))
     socs_rows_xt(const float2* __restrict__ kband, float scale, const float2* __restrict__ Mband, int K, int hb,
                  float2* __restrict__ Tt, const float2* __restrict__ tw) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
@@ -260,7 +260,6 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L <= 256 ? 6 : 3))
   const int t = threadIdx.x;
   float2* P = smem;  // [S][B] band products
   float2* b0 = smem + S * B;
-  float2* b1 = b0 + fr_buf(L, S);
   const float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
   // one warp per sequence: (k, my) once per row, lanes along mx (no divisions)
   for (int s = t >> 5; s < S; s += T / 32) {
@@ -281,9 +280,8 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L <= 256 ? 6 : 3))
   __syncthreads();
   const float2* src = b0;
   if constexpr (NP == 3) {
-    fr_mid_pass<L, S, +1, 1>(t, b0, b1, tw);
+    fr_mid_pass_inplace<L, S, +1, 1>(t, b0, tw);
     __syncthreads();
-    src = b1;
   }
 #pragma unroll
   for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
@@ -313,7 +311,7 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L <= 256 ? 6 : 3))
 // L = 160 (7.7 % faster than two; its 10 outputs per thread fit without
 // spills); two elsewhere, where 12 or more outputs per thread would spill.
 template <int L, int S, int MODE>
-__global__ void __launch_bounds__(fr_threads(L, S), (L == 160 && MODE == 0 ? 3 : 2))
+__global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || (L >= 512 && MODE == 1) ? 3 : 2))
     socs_cols_xt(const float2* __restrict__ Tt, int K, int hb, float keep, float flare,
                  const float* __restrict__ mean, float* __restrict__ out, const float2* __restrict__ tw,
                  __half* __restrict__ split) {
@@ -327,7 +325,6 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L == 160 && MODE == 0 ? 3 :
   const int t = threadIdx.x;
   float2* P = smem;  // [S][B]
   float2* b0 = smem + S * B;
-  float2* b1 = b0 + fr_buf(L, S);
   constexpr int NO = fr_per(L, S, NP - 1) * R;  // outputs per thread
   float acc[NO];
   float2 res[NO];
@@ -338,7 +335,7 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L == 160 && MODE == 0 ? 3 :
   }
   // MODE 0: kernel k's band columns (one contiguous block of S B values)
   // arrive by cp.async in P[k & 1] while kernel k - 1 is transformed.
-  float2* P2 = b0 + (NP - 1) * fr_buf(L, S);  // second band buffer (MODE 0), after the FFT buffers used
+  float2* P2 = b0 + fr_buf(L, S);  // second band buffer (MODE 0), after the FFT buffer
   auto prefetch = [&](int k) {
     const float2* src = Tt + ((static_cast<size_t>(clip) * K + k) * L + x0) * B;
     float2* dst = (k & 1) ? P2 : P;
@@ -372,9 +369,8 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L == 160 && MODE == 0 ? 3 :
     __syncthreads();
     const float2* cur = b0;
     if constexpr (NP == 3) {
-      fr_mid_pass<L, S, +1, 1>(t, b0, b1, tw);
+      fr_mid_pass_inplace<L, S, +1, 1>(t, b0, tw);
       __syncthreads();
-      cur = b1;
     }
 #pragma unroll
     for (int b = 0; b < fr_per(L, S, NP - 1); ++b) {
@@ -427,7 +423,7 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L == 160 && MODE == 0 ? 3 :
 // two real rows' bands are split from Z(m) and conj Z(-m).
 // grid: (clips * L / (2 S)); X: [clip][y][B].
 template <int L, int S, typename In = float>
-__global__ void __launch_bounds__(fr_threads(L, S))
+__global__ void __launch_bounds__(fr_threads(L, S), (L >= 512 ? 4 : 1))
     band_rows_reg(const In* __restrict__ in, int hb, float2* __restrict__ X, const float2* __restrict__ tw) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
   extern __shared__ float2 smem[];
@@ -435,7 +431,6 @@ __global__ void __launch_bounds__(fr_threads(L, S))
   const size_t row0 = static_cast<size_t>(blockIdx.x) * 2 * S;
   const int t = threadIdx.x;
   float2* b0 = smem;
-  float2* b1 = b0 + fr_buf(L, S);
   if (t < fr_nb(L, S, 0)) {
     const int s = t % S, j = t / S;
     const In* ra = in + (row0 + 2 * s) * L + j;
@@ -447,13 +442,10 @@ __global__ void __launch_bounds__(fr_threads(L, S))
   }
   __syncthreads();
   float2* cur = b0;
+  fr_mid_pass_inplace<L, S, -1, 1>(t, b0, tw);
   if constexpr (NP == 3) {
-    fr_mid_pass<L, S, -1, 1>(t, b0, b1, tw);
     __syncthreads();
-    fr_mid_pass<L, S, -1, 2>(t, b1, b0, tw);
-  } else {
-    fr_mid_pass<L, S, -1, 1>(t, b0, b1, tw);
-    cur = b1;
+    fr_mid_pass_inplace<L, S, -1, 2>(t, b0, tw);
   }
   __syncthreads();
   for (int e = t; e < S * B; e += T) {
@@ -486,7 +478,6 @@ __global__ void __launch_bounds__(fr_threads(L, S))
   const int c0 = blockIdx.x * S;
   const int t = threadIdx.x;
   float2* b0 = smem;
-  float2* b1 = b0 + fr_buf(L, S);
   const float2* Xc = X + static_cast<size_t>(clip) * L * B;
   if (t < fr_nb(L, S, 0)) {
     const int s = t % S, j = t / S;
@@ -501,14 +492,10 @@ __global__ void __launch_bounds__(fr_threads(L, S))
   }
   __syncthreads();
   const float2* cur = b0;
-  if constexpr (NP == 3 && fr_mid_inplace_ok(L, S)) {
+  if constexpr (NP == 3) {
     // one buffer: more blocks per SM to keep the column loads in flight
     fr_mid_pass_inplace<L, S, -1, 1>(t, b0, tw);
     __syncthreads();
-  } else if constexpr (NP == 3) {
-    fr_mid_pass<L, S, -1, 1>(t, b0, b1, tw);
-    __syncthreads();
-    cur = b1;
   }
   float2* Mc = Mband + static_cast<size_t>(clip) * B * B;
   float part = 0.f;
@@ -609,7 +596,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   if (kind == 1 && (n == 1024 || n == 160 || n == 192 || n == 2048) && xt_ok(n, hb)) {
     const int Sr = xt_S(n);
     const dim3 gr(static_cast<unsigned>(static_cast<size_t>(clips) * n / (2 * Sr)));
-    const size_t smr = 2 * static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
+    const size_t smr = static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
     const float* fin = static_cast<const float*>(in);
     if (n == 1024)
       band_rows_reg<1024, 4><<<gr, 256, smr, st>>>(fin, hb, X, tw);
@@ -626,7 +613,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   if (kind == 0 && rows_tc != cudaSuccess && n == 2048 && xt_ok(n, hb)) {
     const int Sr = xt_S(n);
     const dim3 gr(static_cast<unsigned>(static_cast<size_t>(clips) * n / (2 * Sr)));
-    const size_t smr = 2 * static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
+    const size_t smr = static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
     band_rows_reg<2048, 2, uint8_t><<<gr, 256, smr, st>>>(static_cast<const uint8_t*>(in), hb, X, tw);
     rows_tc = cudaSuccess;
   }
@@ -651,7 +638,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     const int S = xt_S(n);
     nblk = (B + S - 1) / S;
     const dim3 g(nblk, clips);
-    const size_t sm = band_cols_buf_bytes(n);
+    const size_t sm = xt_buf_bytes(n);
     switch (n) {
       case 128: band_cols_reg<128, 32><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 160: band_cols_reg<160, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
@@ -721,9 +708,8 @@ namespace {
 cudaError_t cols_xt(const float2* T, int K, int hb, int L, int clips, float keep, float flare, const float* mean,
                     float* out, int mode, const float2* tw, cudaStream_t st, __half* split) {
   const int B = 2 * hb + 1, S = xt_S(L);
-  // band columns (mode 0: double-buffered) and the FFT buffers the passes use
-  const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) * (mode == 0 ? 2 : 1) +
-                    (fr_passes(L) - 1) * static_cast<size_t>(fr_buf(L, S)) * sizeof(float2);
+  // band columns (mode 0: double-buffered) and the one FFT buffer
+  const size_t sm = static_cast<size_t>(S) * B * sizeof(float2) * (mode == 0 ? 2 : 1) + xt_buf_bytes(L);
   const dim3 g(L / (mode == 0 ? S : 2 * S), clips);
 #define HUV_COLS_XT(LL, SS)                                                                                   \
   if (mode == 0)                                                                                            \
