@@ -134,7 +134,11 @@ __host__ __device__ __forceinline__ void fr_dft5(float2 (&v)[5]) {
 // R-point DFT of v in place, natural order in and out.
 template <int R, int DIR>
 __host__ __device__ __forceinline__ void fr_dft(float2 (&v)[R]) {
-  if constexpr (R == 4) {
+  if constexpr (R == 2) {
+    const float2 a = v[0];
+    v[0] = fr_add(a, v[1]);
+    v[1] = fr_sub(a, v[1]);
+  } else if constexpr (R == 4) {
     fr_dft4<DIR>(v[0], v[1], v[2], v[3]);
   } else if constexpr (R == 8) {
     // n = q + 2 m, k = p + 4 q': X = sum_q W2^{q q'} W8^{q p} [sum_m v W4^{m p}]
@@ -250,17 +254,19 @@ __host__ __device__ __forceinline__ void fr_dft16_band(float2 (&v)[16]) {
 }
 
 // Radix plan by length: 128 = 16 x 8, 160 = 16 x 10, 192 = 16 x 12,
-// 256 = 16 x 16, 512 = 16 x 8 x 4, 1024 = 16 x 16 x 4, 2048 = 16 x 16 x 8.
+// 256 = 16 x 16, 384 = 16 x 12 x 2, 512 = 16 x 8 x 4, 1024 = 16 x 16 x 4,
+// 2048 = 16 x 16 x 8.
 __host__ __device__ constexpr int fr_passes(int L) { return L <= 256 ? 2 : 3; }
 __host__ __device__ constexpr int fr_radix(int L, int pass) {
   return pass == 0 ? 16
-                   : (L == 128 ? 8
-                               : (L == 160 ? 10
-                                           : (L == 192 ? 12
-                                                       : (L == 256 ? 16
-                                                                   : (L == 512 ? (pass == 1 ? 8 : 4)
-                                                                               : (L == 2048 ? (pass == 1 ? 16 : 8)
-                                                                                            : (pass == 1 ? 16 : 4)))))));
+         : L == 128 ? 8
+         : L == 160 ? 10
+         : L == 192 ? 12
+         : L == 256 ? 16
+         : L == 384 ? (pass == 1 ? 12 : 2)
+         : L == 512 ? (pass == 1 ? 8 : 4)
+         : L == 2048 ? (pass == 1 ? 16 : 8)
+                     : (pass == 1 ? 16 : 4);
 }
 // Stockham sub-transform size before pass `pass`.
 __host__ __device__ constexpr int fr_ns(int L, int pass) {
@@ -302,7 +308,12 @@ __device__ __forceinline__ void fr_cp_wait() {
 // threads each), 0 where no instance exists; shared-memory bytes of the
 // ping-pong buffers of one block and the kernels' shared-memory ceiling.
 __host__ __device__ constexpr int xt_S(int L) {
-  return L == 128 ? 32 : (L == 160 || L == 192 || L == 256) ? 16 : L == 512 ? 8 : L == 1024 ? 4 : L == 2048 ? 2 : 0;
+  return L == 128 ? 32
+         : (L == 160 || L == 192 || L == 256) ? 16
+         : (L == 384 || L == 512) ? 8
+         : L == 1024 ? 4
+         : L == 2048 ? 2
+                     : 0;
 }
 __host__ __device__ constexpr size_t xt_buf_bytes(int L) {
   // one buffer: the middle passes run in place (fr_mid_pass_inplace)
@@ -362,7 +373,7 @@ __host__ __device__ __forceinline__ void fr_mid_pass(int t, const float2* src, f
     const int u = t + b * T;
     if (u >= fr_nb(L, S, PASS)) break;
     const int s = u % S, j = u / S;
-    const int k = j & (Ns - 1);
+    const int k = j % Ns;  // Ns need not be a power of two (384 = 16 x 12 x 2)
     float2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[fr_idx<S>(j + r * (L / R), s)];
@@ -402,7 +413,7 @@ __device__ __forceinline__ void fr_mid_pass_inplace(int t, float2* buf, const fl
     const int u = t + b * T;
     if (u >= fr_nb(L, S, PASS)) break;
     const int s = u % S, j = u / S;
-    const int k = j & (Ns - 1);
+    const int k = j % Ns;  // Ns need not be a power of two (384 = 16 x 12 x 2)
 #pragma unroll
     for (int r = 1; r < R; ++r) {
       float2 w = tw[r * k * stride];

@@ -772,7 +772,9 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   // the smallest supported grid above 4h: 160 or 192 where the register-radix
   // forward and adjoint kernels serve it, else a power of two
   int M = choose_eval_grid(ds, 0, true);
-  if ((M & (M - 1)) != 0 && ilt_adj_xt_smem(M, hb) > static_cast<size_t>(kXtSmemMax)) M = choose_eval_grid(ds, 0);
+  // the adjoint kernels have 160 and 192 instances but not 384
+  if ((M & (M - 1)) != 0 && (M == 384 || ilt_adj_xt_smem(M, hb) > static_cast<size_t>(kXtSmemMax)))
+    M = choose_eval_grid(ds, 0);
   const int lgm = ilog2i(M);  // rounded up where M is 160 or 192 (radix-4 paths are not used then)
   const bool coarse = M < n;
   const size_t npix = static_cast<size_t>(n) * n, mpix = static_cast<size_t>(M) * M;

@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L <= 256 ? 6 : 4))
 // L = 160 (7.7 % faster than two; its 10 outputs per thread fit without
 // spills); two elsewhere, where 12 or more outputs per thread would spill.
 template <int L, int S, int MODE>
-__global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || (L >= 512 && MODE == 1) ? 3 : 2))
+__global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || (L >= 384 && MODE == 1) ? 3 : 2))
     socs_cols_xt(const float2* __restrict__ Tt, int K, int hb, float keep, float flare,
                  const float* __restrict__ mean, float* __restrict__ out, const float2* __restrict__ tw,
                  __half* __restrict__ split) {
@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || 
 // two real rows' bands are split from Z(m) and conj Z(-m).
 // grid: (clips * L / (2 S)); X: [clip][y][B].
 template <int L, int S, typename In = float>
-__global__ void __launch_bounds__(fr_threads(L, S), (L >= 512 ? 4 : 1))
+__global__ void __launch_bounds__(fr_threads(L, S), (L >= 384 ? 4 : 1))
     band_rows_reg(const In* __restrict__ in, int hb, float2* __restrict__ X, const float2* __restrict__ tw) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
   extern __shared__ float2 smem[];
@@ -593,7 +593,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     x_transposed = rows_tc == cudaSuccess && cols_reg;
     if (rows_tc != cudaSuccess && rows_tc != cudaErrorNotSupported) return rows_tc;
   }
-  if (kind == 1 && (n == 1024 || n == 160 || n == 192 || n == 2048) && xt_ok(n, hb)) {
+  if (kind == 1 && (n == 1024 || n == 160 || n == 192 || n == 384 || n == 2048) && xt_ok(n, hb)) {
     const int Sr = xt_S(n);
     const dim3 gr(static_cast<unsigned>(static_cast<size_t>(clips) * n / (2 * Sr)));
     const size_t smr = static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
@@ -602,6 +602,8 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
       band_rows_reg<1024, 4><<<gr, 256, smr, st>>>(fin, hb, X, tw);
     else if (n == 2048)
       band_rows_reg<2048, 2><<<gr, 256, smr, st>>>(fin, hb, X, tw);
+    else if (n == 384)
+      band_rows_reg<384, 8><<<gr, 256, smr, st>>>(fin, hb, X, tw);
     else if (n == 160)
       band_rows_reg<160, 16><<<gr, 256, smr, st>>>(fin, hb, X, tw);
     else
@@ -644,6 +646,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
       case 160: band_cols_reg<160, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 192: band_cols_reg<192, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 256: band_cols_reg<256, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 384: band_cols_reg<384, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 512: band_cols_reg<512, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 2048: band_cols_reg<2048, 2><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       case 1024: band_cols_reg<1024, 4><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
@@ -696,6 +699,7 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
     case 160: socs_rows_xt<160, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 192: socs_rows_xt<192, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 256: socs_rows_xt<256, 16><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
+    case 384: socs_rows_xt<384, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 512: socs_rows_xt<512, 8><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 2048: socs_rows_xt<2048, 2><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
     case 1024: socs_rows_xt<1024, 4><<<g, 256, sm, st>>>(kband, scale, Mband, K, hb, T, tw); break;
@@ -721,6 +725,7 @@ cudaError_t cols_xt(const float2* T, int K, int hb, int L, int clips, float keep
     case 160: HUV_COLS_XT(160, 16) break;
     case 192: HUV_COLS_XT(192, 16) break;
     case 256: HUV_COLS_XT(256, 16) break;
+    case 384: HUV_COLS_XT(384, 8) break;
     case 512: HUV_COLS_XT(512, 8) break;
     case 2048: HUV_COLS_XT(2048, 2) break;
     case 1024: HUV_COLS_XT(1024, 4) break;
@@ -795,10 +800,10 @@ cudaError_t set_smem_limits() {
 #define HUV_XT_ALL(LL, SS)                                                                                \
   HUV_XT_ATTR((socs_rows_xt<LL, SS>)) HUV_XT_ATTR((socs_cols_xt<LL, SS, 0>))                           \
   HUV_XT_ATTR((socs_cols_xt<LL, SS, 1>)) HUV_XT_ATTR((band_cols_reg<LL, SS>))
-  HUV_XT_ALL(128, 32) HUV_XT_ALL(160, 16) HUV_XT_ALL(192, 16) HUV_XT_ALL(256, 16) HUV_XT_ALL(512, 8)
+  HUV_XT_ALL(128, 32) HUV_XT_ALL(160, 16) HUV_XT_ALL(192, 16) HUV_XT_ALL(256, 16) HUV_XT_ALL(384, 8) HUV_XT_ALL(512, 8)
   HUV_XT_ALL(1024, 4) HUV_XT_ALL(2048, 2)
   HUV_XT_ATTR((band_rows_reg<1024, 4>)) HUV_XT_ATTR((band_rows_reg<160, 16>))
-  HUV_XT_ATTR((band_rows_reg<192, 16>)) HUV_XT_ATTR((band_rows_reg<2048, 2>))
+  HUV_XT_ATTR((band_rows_reg<192, 16>)) HUV_XT_ATTR((band_rows_reg<2048, 2>)) HUV_XT_ATTR((band_rows_reg<384, 8>))
   HUV_XT_ATTR((band_rows_reg<2048, 2, uint8_t>))
 #undef HUV_XT_ALL
 #undef HUV_XT_ATTR

@@ -503,12 +503,13 @@ void* Engine::workspace(size_t bytes) {
 int Engine::choose_eval_grid(const DeviceSet& ds, int requested, bool mixed) const {
   const int min_m = 4 * ds.hb + 1;
   const bool mixed_ok = [&](int m) {
-    return (m == 160 || m == 192) && m <= n && huv_launch::xt_ok(m, ds.hb) && huv_launch::xt_ok(m, 2 * ds.hb);
+    return (m == 160 || m == 192 || m == 384) && m <= n && huv_launch::xt_ok(m, ds.hb) &&
+           huv_launch::xt_ok(m, 2 * ds.hb);
   }(requested);
   if (requested > 0) {
     if (((requested & (requested - 1)) != 0 && !(mixed && mixed_ok)) || requested > n || requested < min_m)
-      throw Error(HUV_ERR_INVALID_PARAMETER, "eval_grid: must be a power of two (or 160 / 192 for the FFT and "
-                                             "hybrid forms) with 4h < M <= N (h = " + std::to_string(ds.hb) + ")");
+      throw Error(HUV_ERR_INVALID_PARAMETER, "eval_grid: must be a power of two (or 160 / 192 / 384 for the FFT "
+                                             "and hybrid forms) with 4h < M <= N (h = " + std::to_string(ds.hb) + ")");
     return requested;
   }
   int m = 8;
@@ -516,7 +517,7 @@ int Engine::choose_eval_grid(const DeviceSet& ds, int requested, bool mixed) con
   m = std::min(m, n);
   if (mixed) {
     // a register-radix length between 4h and the next power of two
-    for (int c : {160, 192})
+    for (int c : {160, 192, 384})
       if (c >= min_m && c < m && c < n && huv_launch::xt_ok(c, ds.hb) && huv_launch::xt_ok(c, 2 * ds.hb)) return c;
   }
   return m;
@@ -531,7 +532,7 @@ bool Engine::field_fused(const DeviceSet& ds, int M) const {
 
 void Engine::run_fft_form(const huv_batch& b, const DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use,
                           const float* W_use) {
-  const int lgn = ilog2(n), lgm = ilog2(M);  // lgm: rounded up where M is 160 or 192
+  const int lgn = ilog2(n), lgm = ilog2(M);  // lgm: rounded up where M is 160, 192 or 384
   const int B = ds.B, K = K_use > 0 ? K_use : ds.K, hb = ds.hb;
   const float* Wf = W_use ? W_use : ds.W;
   const bool coarse = M < n;

@@ -132,7 +132,7 @@ std::vector<Choice> candidates(Engine* e, DeviceSet& ds) {
   while (m < 4 * ds.hb + 1) m <<= 1;
   m = std::min(m, n);
   const int mtc = std::max(m, 128);
-  // the FFT and hybrid forms may evaluate on a register-radix grid (160, 192)
+  // the FFT and hybrid forms may evaluate on a register-radix grid (160, 192, 384)
   // between 4h and the next power of two
   const int mx = e->choose_eval_grid(ds, 0, true);
   if (mtc <= n && e->tc_supported(ds, mtc)) out.push_back(Choice{HUV_FORM_TC, mtc, 0});

@@ -159,11 +159,11 @@ typedef struct {
                              0: plain FFT of the samples (compute_from_transmittance, aerial.rs:1789) */
   double defocus_nm;      /* focus plane; kernel sets are built and cached per plane */
   int32_t form;           /* huv_form */
-  int32_t eval_grid;      /* 0 = automatic (the smallest supported M > 4h: 160 or 192 for the FFT and
-                             hybrid forms where they beat the next power of two, a power of two of at
-                             least 128 for the tensor-core y-contraction); N = evaluate on the full
-                             grid; M < N (power of two, or 160 / 192 for the FFT and hybrid forms,
-                             M > 4h) = exact evaluation on an M grid + exact band interpolation */
+  int32_t eval_grid;      /* 0 = automatic (the smallest supported M > 4h: 160, 192 or 384 for the FFT
+                             and hybrid forms where they beat the next power of two, a power of two of
+                             at least 128 for the tensor-core y-contraction); N = evaluate on the full
+                             grid; M < N (power of two, or 160 / 192 / 384 for the FFT and hybrid
+                             forms, M > 4h) = exact evaluation on an M grid + exact band interpolation */
 } huv_batch;
 
 /* Last error message on this thread (never NULL). */

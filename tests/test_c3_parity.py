@@ -88,7 +88,9 @@ def test_euv_quasar_every_form_at_k64(n):
         assert h == 47
         cases += [("tc", 0), ("hybrid", 0), ("auto", 0)]
     else:
+        # automatic grid: 384 (16 x 12 x 2 register-radix plan); 512 the power of two
         assert h == 95
+        cases += [("fft", 384), ("fft", m), ("auto", 0)]
     for form, eg in cases:
         img = eng.compute_batch(d, form=form, eval_grid=eg).cpu().numpy()[0]
         _check(img, ref, FFT_TOL if form == "fft" else REL_TOL, (form, eg))
