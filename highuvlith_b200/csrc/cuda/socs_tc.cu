@@ -1063,26 +1063,7 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   // carried as I_M / interp_scale(mean); the final GEMM multiplies it back.
   const bool sep = fft_field && M <= 192 && M % 16 == 0 && xt_ok(M, hb);
   TcState& tc = ds.tc[M];
-  if (sep && !tc.gp) {
-    constexpr int kpP = 192;
-    std::vector<double> pm(static_cast<size_t>(n) * M);
-    const double nm = static_cast<double>(n) * M;
-    for (int y = 0; y < n; ++y)
-      for (int m = 0; m < M; ++m) {
-        // t = Y/N - m/M = q / (N M); sum_{|f|<=H} e^{2 pi i f t} = sin((2H+1) pi t) / sin(pi t)
-        const long long q = static_cast<long long>(y) * M - static_cast<long long>(m) * n;
-        const double v = q == 0 ? static_cast<double>(2 * h2 + 1)
-                                : std::sin((2 * h2 + 1) * kPi * static_cast<double>(q) / nm) /
-                                      std::sin(kPi * static_cast<double>(q) / nm);
-        pm[static_cast<size_t>(y) * M + m] = v / M;
-      }
-    const auto pp = split_planes_f16(pm, n, M, kpP);
-    check_cuda(cudaMalloc(&tc.gp, pp.size() * 2), "cudaMalloc(P)");
-    check_cuda(cudaMemcpy(tc.gp, pp.data(), pp.size() * 2, cudaMemcpyHostToDevice), "upload P");
-    if (!make_map(&tc.map_pi, tc.gp, 2ull * n, kpP, 128, 0, true) ||
-        !make_map_sw64(&tc.map_pi32, tc.gp, 2ull * n, kpP, 128, kpP, true))
-      throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the interpolation operand");
-  }
+  if (sep) interp_matrix(ds, M);
   if (!fft_field && !tc.gy) {
     // A_E: rows (y, re/im) over the M grid, K = (my, re/im).
     std::vector<double> ae(static_cast<size_t>(2 * M) * kcE);
@@ -1263,62 +1244,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       prof.end(st);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<0>");
     }
-    CUtensorMap mbZ;
     if (sep) {
-      // Z^T[clip][plane][Y][y] = sum_x P(Y, x) I_M(y, x) / s, FP16 split planes:
-      // A = P (rows Y), B = I_M / s (rows y, K = x), s = interp_scale(mean);
-      // G1 clips per CTA share the A tile.  The MMA covers all M columns at
-      // once where the B ring fits (M = 128, 160: N = M, 4 + 5 KB of operands
-      // per 80 tensor cycles at M = 160), else two halves (M = 192).
-      const int bn1 = M <= 160 ? M : M / 2;
-      const int ntile1 = M / bn1, mtiles = n / 128;
-      // Clips per CTA: the fewest (up to 32) whose grid fits one wave of one
-      // CTA per SM, else 32.  Each CTA's run is latency-bound (per step: one
-      // clip's B ring through 3 stages), so longer runs over a resident A
-      // tile beat more CTAs: at 128 clips 1 / 2 / 4 / 8 clips per CTA time
-      // 1.24 / 1.12 / 1.03 / 0.99 ms per 20 launches; at 256 clips 15 per
-      // CTA (one wave of 144 CTAs) 0.084 ms per launch against 0.092 with 8
-      // (256 CTAs, 1.7 waves).
-      int sms = 0, dev = 0;
-      check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-      check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-      int G1 = 32;
-      for (int gc = 1; gc < 32; ++gc)
-        if (static_cast<long long>(ntile1) * mtiles * ((nc + gc - 1) / gc) <= sms) {
-          G1 = gc;
-          break;
-        }
-      CUtensorMap mbS;
-      if (!make_map(&mbS, IM, static_cast<uint64_t>(nc) * 2 * M, M, bn1, M, true) ||
-          !make_map(&mbZ, BI, static_cast<uint64_t>(nc) * 2 * n, M, kTcBN, M, true))
-        throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the interpolation operands");
-      TcGemmParams p{};
-      p.kboxes = (M + 63) / 64;
-      p.ksteps = M / 16;
-      p.G = G1;
-      p.nprob = nc;
-      p.a_rows = n;
-      p.b_prob = G1 * 2 * M;
-      p.b_step = 2 * M;
-      p.b_plane = M;
-      p.err = dev_err;
-      p.probe_wait_ns = huv_launch::probe_wait_ns();
-      p.bop = BI;
-      p.bop_prob = 2ll * n * M;
-      p.bop_plane = static_cast<long long>(n) * M;
-      p.bop_ld = M;
-      const dim3 g(ntile1, mtiles, (nc + G1 - 1) / G1);
-      prof.begin("tc_dft_gemm<interp_x>", st);
-      if (bn1 == 128)
-        tc_dft_gemm<3, 128><<<g, 192, tc_smem_bytes(3, 128), st>>>(tc.map_pi, mbS, tc.map_pi, p);
-      else if (bn1 == 160)
-        tc_dft_gemm<3, 160><<<g, 192, tc_smem_bytes(3, 160), st>>>(tc.map_pi, mbS, tc.map_pi, p);
-      else if (bn1 == 96)
-        tc_dft_gemm<3, 96><<<g, 192, tc_smem_bytes(3, 96), st>>>(tc.map_pi, mbS, tc.map_pi, p);
-      else
-        throw Error(HUV_ERR_UNSUPPORTED, "separable interpolation: evaluation grid must be 128, 160 or 192");
-      prof.end(st);
-      check_cuda(cudaGetLastError(), "tc_dft_gemm<3>");
+      interp_separable(ds, M, nc, IM, mean, BI, o, st, true);
     } else {
       prof.begin("interp_band", st);
       check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st,
@@ -1331,10 +1258,10 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       check_cuda(cudaGetLastError(), "socs_rows_tc(interp)");
       prof.end(st);
     }
-    {
+    if (!sep) {
       TcGemmParams p{};
-      p.kboxes = sep ? (M + 63) / 64 : kpI / 64;
-      p.ksteps = sep ? M / 16 : kstI;
+      p.kboxes = kpI / 64;
+      p.ksteps = kstI;
       p.G = n / kTcBN;
       p.a_rows = n;
       p.b_prob = 2 * n;
@@ -1344,8 +1271,8 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       p.out_plane = static_cast<long long>(n) * n;
       p.keep = 1.f;
       p.flare = 0.f;
-      p.mean = sep ? mean : nullptr;  // separable: undo the planes' scale
-      p.f16 = sep ? 1 : 0;
+      p.mean = nullptr;
+      p.f16 = 0;
       p.out = o;
       p.err = dev_err;
       p.probe_wait_ns = huv_launch::probe_wait_ns();
@@ -1356,21 +1283,18 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
       CUtensorMap mbZ64;
       const int abox = (p.ksteps + 1) / 2;  // 32-wide A boxes
       const bool w256 = p.out_tma && n % 256 == 0 && abox <= 6 &&
-                        make_map_sw64(&mbZ64, BI, static_cast<uint64_t>(nc) * 2 * n, sep ? M : kbI, 256,
-                                      sep ? M : kcI, sep);
+                        make_map_sw64(&mbZ64, BI, static_cast<uint64_t>(nc) * 2 * n, kbI, 256, kcI, false);
       prof.begin("tc_dft_gemm<interp>", st);
       if (w256) {  // 128 x 256 tiles, A and B through 32-wide boxes
         p.G = n / 256;
         p.kboxes = abox;
-        const CUtensorMap& ma = sep ? tc.map_pi32 : tc.map_ai32;
         if (abox <= 5)
-          tc_interp_w256<5, 7, 2><<<g, 192, w256_smem_bytes(5, 7, 2), st>>>(ma, mbZ64, mo, p);
+          tc_interp_w256<5, 7, 2><<<g, 192, w256_smem_bytes(5, 7, 2), st>>>(tc.map_ai32, mbZ64, mo, p);
         else
-          tc_interp_w256<6, 6, 2><<<g, 192, w256_smem_bytes(6, 6, 2), st>>>(ma, mbZ64, mo, p);
-      } else if (sep)
-        tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_pi, mbZ, mo, p);
-      else
+          tc_interp_w256<6, 6, 2><<<g, 192, w256_smem_bytes(6, 6, 2), st>>>(tc.map_ai32, mbZ64, mo, p);
+      } else {
         tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_ai, mbI, mo, p);
+      }
       prof.end(st);
       check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
     }
@@ -1380,6 +1304,153 @@ void Engine::run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, c
   }
 }
 
+bool Engine::separable_ok(const DeviceSet& ds, int M) const {
+  return M <= 192 && M % 16 == 0 && M < n && huv_launch::xt_ok(M, ds.hb) && hybrid_supported(ds, M);
+}
+
+// P(Y, m) = (1/M) sum_{|f| <= h2} exp(2 pi i f (Y/N - m/M)) (a Dirichlet
+// kernel) as FP16 hi/lo planes [2][N][192], built once per (set, M).
+void Engine::interp_matrix(DeviceSet& ds, int M) {
+  using namespace huv_launch;
+  TcState& tc = ds.tc[M];
+  const int h2 = 2 * ds.hb;
+  if (!tc.gp) {
+    constexpr int kpP = 192;
+    std::vector<double> pm(static_cast<size_t>(n) * M);
+    const double nm = static_cast<double>(n) * M;
+    for (int y = 0; y < n; ++y)
+      for (int m = 0; m < M; ++m) {
+        // t = Y/N - m/M = q / (N M); sum_{|f|<=H} e^{2 pi i f t} = sin((2H+1) pi t) / sin(pi t)
+        const long long q = static_cast<long long>(y) * M - static_cast<long long>(m) * n;
+        const double v = q == 0 ? static_cast<double>(2 * h2 + 1)
+                                : std::sin((2 * h2 + 1) * kPi * static_cast<double>(q) / nm) /
+                                      std::sin(kPi * static_cast<double>(q) / nm);
+        pm[static_cast<size_t>(y) * M + m] = v / M;
+      }
+    const auto pp = split_planes_f16(pm, n, M, kpP);
+    check_cuda(cudaMalloc(&tc.gp, pp.size() * 2), "cudaMalloc(P)");
+    check_cuda(cudaMemcpy(tc.gp, pp.data(), pp.size() * 2, cudaMemcpyHostToDevice), "upload P");
+    if (!make_map(&tc.map_pi, tc.gp, 2ull * n, kpP, 128, 0, true) ||
+        !make_map_sw64(&tc.map_pi32, tc.gp, 2ull * n, kpP, 128, kpP, true))
+      throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the interpolation operand");
+  }
+}
+
+void Engine::interp_separable(DeviceSet& ds, int M, int nc, const void* im_split, const float* mean, void* BIv,
+                              float* o, cudaStream_t st, bool profile) {
+  using namespace huv_launch;
+  static std::atomic<uint64_t> smem_set{0};
+  once_per_device(smem_set, [] { check_cuda(tc_set_smem(), "cudaFuncSetAttribute(tc)"); });
+  interp_matrix(ds, M);
+  TcState& tc = ds.tc[M];
+  const void* IM = im_split;
+  __nv_bfloat16* BI = static_cast<__nv_bfloat16*>(BIv);
+  struct Region {  // the profiler's regions only when the caller is not inside one of its own
+    Prof& pr;
+    bool on;
+    void begin(const char* nm, cudaStream_t s) {
+      if (on) pr.begin(nm, s);
+    }
+    void end(cudaStream_t s) {
+      if (on) pr.end(s);
+    }
+  } prof{this->prof, profile};
+  CUtensorMap mbZ;
+  {
+    // Z^T[clip][plane][Y][y] = sum_x P(Y, x) I_M(y, x) / s, FP16 split planes:
+    // A = P (rows Y), B = I_M / s (rows y, K = x), s = interp_scale(mean);
+    // G1 clips per CTA share the A tile.  The MMA covers all M columns at
+    // once where the B ring fits (M = 128, 160: N = M, 4 + 5 KB of operands
+    // per 80 tensor cycles at M = 160), else two halves (M = 192).
+    const int bn1 = M <= 160 ? M : M / 2;
+    const int ntile1 = M / bn1, mtiles = n / 128;
+    // Clips per CTA: the fewest (up to 32) whose grid fits one wave of one
+    // CTA per SM, else 32.  Each CTA's run is latency-bound (per step: one
+    // clip's B ring through 3 stages), so longer runs over a resident A
+    // tile beat more CTAs: at 128 clips 1 / 2 / 4 / 8 clips per CTA time
+    // 1.24 / 1.12 / 1.03 / 0.99 ms per 20 launches; at 256 clips 15 per
+    // CTA (one wave of 144 CTAs) 0.084 ms per launch against 0.092 with 8
+    // (256 CTAs, 1.7 waves).
+    int sms = 0, dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    int G1 = 32;
+    for (int gc = 1; gc < 32; ++gc)
+      if (static_cast<long long>(ntile1) * mtiles * ((nc + gc - 1) / gc) <= sms) {
+        G1 = gc;
+        break;
+      }
+    CUtensorMap mbS;
+    if (!make_map(&mbS, IM, static_cast<uint64_t>(nc) * 2 * M, M, bn1, M, true) ||
+        !make_map(&mbZ, BI, static_cast<uint64_t>(nc) * 2 * n, M, kTcBN, M, true))
+      throw Error(HUV_ERR_CUDA, "cuTensorMapEncodeTiled failed for the interpolation operands");
+    TcGemmParams p{};
+    p.kboxes = (M + 63) / 64;
+    p.ksteps = M / 16;
+    p.G = G1;
+    p.nprob = nc;
+    p.a_rows = n;
+    p.b_prob = G1 * 2 * M;
+    p.b_step = 2 * M;
+    p.b_plane = M;
+    p.err = dev_err;
+    p.probe_wait_ns = huv_launch::probe_wait_ns();
+    p.bop = BI;
+    p.bop_prob = 2ll * n * M;
+    p.bop_plane = static_cast<long long>(n) * M;
+    p.bop_ld = M;
+    const dim3 g(ntile1, mtiles, (nc + G1 - 1) / G1);
+    prof.begin("tc_dft_gemm<interp_x>", st);
+    if (bn1 == 128)
+      tc_dft_gemm<3, 128><<<g, 192, tc_smem_bytes(3, 128), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+    else if (bn1 == 160)
+      tc_dft_gemm<3, 160><<<g, 192, tc_smem_bytes(3, 160), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+    else if (bn1 == 96)
+      tc_dft_gemm<3, 96><<<g, 192, tc_smem_bytes(3, 96), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+    else
+      throw Error(HUV_ERR_UNSUPPORTED, "separable interpolation: evaluation grid must be 128, 160 or 192");
+    prof.end(st);
+    check_cuda(cudaGetLastError(), "tc_dft_gemm<3>");
+  }
+  TcGemmParams p{};
+  p.kboxes = (M + 63) / 64;
+  p.ksteps = M / 16;
+  p.G = n / kTcBN;
+  p.a_rows = n;
+  p.b_prob = 2 * n;
+  p.b_step = kTcBN;
+  p.b_plane = n;
+  p.out_ld = n;
+  p.out_plane = static_cast<long long>(n) * n;
+  p.keep = 1.f;
+  p.flare = 0.f;
+  p.mean = mean;  // undo the planes' scale
+  p.f16 = 1;
+  p.out = o;
+  p.err = dev_err;
+  p.probe_wait_ns = huv_launch::probe_wait_ns();
+  CUtensorMap mo;
+  p.out_tma = make_out_map(&mo, o, static_cast<uint64_t>(nc) * n, n) ? 1 : 0;
+  if (!p.out_tma) mo = tc.map_pi;  // unused
+  dim3 g(1, n / 128, nc);
+  CUtensorMap mbZ64;
+  const int abox = (p.ksteps + 1) / 2;  // 32-wide A boxes
+  const bool w256 = p.out_tma && n % 256 == 0 && abox <= 6 &&
+                    make_map_sw64(&mbZ64, BI, static_cast<uint64_t>(nc) * 2 * n, M, 256, M, true);
+  prof.begin("tc_dft_gemm<interp>", st);
+  if (w256) {  // 128 x 256 tiles, A and B through 32-wide boxes
+    p.G = n / 256;
+    p.kboxes = abox;
+    if (abox <= 5)
+      tc_interp_w256<5, 7, 2><<<g, 192, w256_smem_bytes(5, 7, 2), st>>>(tc.map_pi32, mbZ64, mo, p);
+    else
+      tc_interp_w256<6, 6, 2><<<g, 192, w256_smem_bytes(6, 6, 2), st>>>(tc.map_pi32, mbZ64, mo, p);
+  } else {
+    tc_dft_gemm<1><<<g, 192, tc_smem_bytes(3, kTcBN, false, true), st>>>(tc.map_pi, mbZ, mo, p);
+  }
+  prof.end(st);
+  check_cuda(cudaGetLastError(), "tc_dft_gemm<1>");
+}
 }  // namespace huv
 
 extern "C" huv_status huv_debug_probe_wait(int64_t ns) {

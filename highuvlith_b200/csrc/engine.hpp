@@ -246,6 +246,14 @@ struct Engine {
                     const float* W_use = nullptr);
   void run_tc_form(const huv_batch& b, DeviceSet& ds, int M, float* out, cudaStream_t st, int K_use = 0,
                    const float* W_use = nullptr, int core = kTcCoreFftRows);
+  // Separable band interpolation of nc coarse images to the N grid on
+  // tcgen05: im_split holds I_M / interp_scale(mean) as FP16 hi/lo planes
+  // [clip][2][M][M] (socs_cols_split), BI is 2 N M halves of workspace per
+  // clip, out receives I_N = P I_M P^T.  Applies where separable_ok.
+  bool separable_ok(const DeviceSet& ds, int M) const;
+  void interp_matrix(DeviceSet& ds, int M);
+  void interp_separable(DeviceSet& ds, int M, int nc, const void* im_split, const float* mean, void* BI, float* out,
+                        cudaStream_t st, bool profile);
   // Flare weights W = sum_{k < K} lambda_k |u_k|^2 / N^4 of the first K kernels (device, cached).
   const float* flare_weights(DeviceSet& ds, int K);
   // Kernel count for a budget of `max_kernels` under the reference's truncation rule.
