@@ -178,7 +178,7 @@ __global__ void ilt_cols_adj(const float2* __restrict__ T, const float* __restri
 // ilt_rows_adj).  grid: (L / S, masks); shared: P (S B), two FFT buffers,
 // a second band buffer P2 (S B).
 template <int L, int S>
-__global__ void __launch_bounds__(fr_threads(L, S))
+__global__ void __launch_bounds__(fr_threads(L, S), (L == 160 || L == 192) ? 3 : 1)
     ilt_cols_adj_xt(const float2* __restrict__ Tt, const float* __restrict__ G, int K, int hb, float keep,
                     const double* __restrict__ sums, float flare_over_n, float2* __restrict__ V,
                     const float2* __restrict__ tw) {
@@ -298,7 +298,7 @@ __global__ void hermitian_part(float2* __restrict__ Q, int B, int masks) {
 // the same order (warp shuffles), then over the batches in registers.
 // grid: (B, masks); shared: two FFT buffers.
 template <int L, int S>
-__global__ void __launch_bounds__(fr_threads(L, S))
+__global__ void __launch_bounds__(fr_threads(L, S), (L == 160 || L == 192) ? 3 : 1)
     ilt_rows_adj_xt(const float2* __restrict__ V, const float2* __restrict__ kband, int K, int hb,
                     float2* __restrict__ Q, const float2* __restrict__ tw) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
@@ -695,6 +695,8 @@ cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, i
                         float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols_x(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
                         const float* mean, float* out, int mode, const float2* tw, cudaStream_t st);
+cudaError_t socs_cols_split(const float2* T, int K, int hb, int L, int clips, float keep, float flare,
+                            const float* mean, void* split, const float2* tw, cudaStream_t st);
 
 bool xt_ok(int L, int hb);
 
@@ -790,6 +792,12 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   const size_t s_im = coarse ? a256(sizeof(float) * mpix) : 0;  // I on M, then G' on M
   const size_t s_c = coarse ? a256(sizeof(float2) * B2 * B2) : 0;
   const size_t s_x2 = coarse ? a256(sizeof(float2) * static_cast<size_t>(std::max(M, n)) * B2) : 0;
+  // the image's interpolation from M to N: the separable tcgen05 GEMMs (as
+  // the hybrid form) where they serve M, else the band transform of I_M and
+  // N-point row and column syntheses
+  const bool xt_fwd = M <= 1024 && xt_ok(M, hb) && ilt_adj_xt_smem(M, hb) <= static_cast<size_t>(kXtSmemMax);
+  const bool sep = coarse && xt_fwd && separable_ok(ds, M);
+  const size_t s_bi = sep ? a256(sizeof(uint16_t) * 2 * static_cast<size_t>(n) * M) : 0;
   const size_t s_img = a256(sizeof(float) * npix);         // image on N, then G
   const size_t s_V = grad ? a256(sizeof(float2) * static_cast<size_t>(K) * B * M) : 0;
   const size_t s_q = grad ? a256(sizeof(float2) * B * B) : 0;
@@ -802,7 +810,7 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   const int reg_parts = tiled ? (n / tile) * (n / tile) : kRedBlocks;
   const size_t s_preg = a256(sizeof(double) * std::max(reg_parts, 2 * kRedBlocks));
   const size_t per = s_t + s_x + s_m + s_mean + s_T + s_im + s_c + s_x2 + s_img + s_V + s_q + s_t2 + 2 * s_parts +
-                     s_preg + a256(sizeof(double) * 4);
+                     s_preg + s_bi + a256(sizeof(double) * 4);
   const size_t budget = chunk_budget();
   const int chunk = balanced_chunk(static_cast<int>(std::max<size_t>(1, budget / per)), masks);
   char* base = static_cast<char*>(workspace(per * chunk + 4096));
@@ -828,6 +836,7 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
   double* preg = reinterpret_cast<double*>(take(s_preg));
   double* sums = reinterpret_cast<double*>(take(s_parts));
   double* regsum = reinterpret_cast<double*>(take(a256(sizeof(double) * 4)));
+  void* BI = sep ? static_cast<void*>(take(s_bi)) : nullptr;
   prof.begin(grad ? "ilt_cost_grad" : "ilt_cost", st);
   for (int c0 = 0; c0 < masks; c0 += chunk) {
     const int nc = std::min(chunk, masks - c0);
@@ -842,15 +851,20 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     // register-radix column pass fits too, else the [k][my][x] layout
     // (the ILT's grids are powers of two; ilt_cols_adj_xt has no 160 / 192 instance)
     // (the adjoint pair is instantiated up to 1024 points)
-    const bool xt = M <= 1024 && xt_ok(M, hb) && ilt_adj_xt_smem(M, hb) <= static_cast<size_t>(kXtSmemMax);
-    if (xt) {
+    const bool xt = xt_fwd;
+    if (sep) {
+      // I_M / interp_scale(mean) as FP16 split planes (in IM's bytes), then I_N = P I_M P^T
+      check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "ilt socs_rows");
+      check_cuda(socs_cols_split(T, K, hb, M, nc, keep, flare, mean, IM, twm, st), "ilt socs_cols");
+      interp_separable(ds, M, nc, IM, mean, BI, img, st, false);
+    } else if (xt) {
       check_cuda(socs_rows_x(ds.kband, 0.f, Mb, K, hb, M, nc, T, twm, st), "ilt socs_rows");
       check_cuda(socs_cols_x(T, K, hb, M, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
     } else {
       check_cuda(socs_rows(ds.kband, 0.f, Mb, K, hb, lgm, nc, T, twm, st), "ilt socs_rows");
       check_cuda(socs_cols(T, K, hb, lgm, nc, keep, flare, mean, coarse ? IM : img, 0, twm, st), "ilt socs_cols");
     }
-    if (coarse) {
+    if (coarse && !sep) {
       check_cuda(band_forward(IM, HUV_INPUT_RASTER_F32, M, lgm, h2, nc, X2, C, nullptr, nullptr, nullptr, twm, st, nullptr,
                               nullptr),
                  "ilt band(I)");
@@ -934,7 +948,7 @@ void Engine::ilt_eval(const huv_ilt_params& p, int masks, const float* theta, co
     ilt_combine<<<(nc + 127) / 128, 128, 0, st>>>(sums, regsum, nc, p.weight, 1.0 / static_cast<double>(npix),
                                                   cost_dev + c0);
     check_cuda(cudaGetLastError(), "ilt kernels");
-    prof.launches += (grad ? 17 : 10) + (coarse ? (grad ? 9 : 4) : 0);
+    prof.launches += (grad ? 17 : 10) + (coarse ? (grad ? 9 : 4) : 0) - (sep ? 2 : 0);
   }
   prof.end(st);
 }
