@@ -352,6 +352,35 @@ __host__ __device__ __forceinline__ void fr_first_pass_band(int t, const float2*
   for (int r = 0; r < 16; ++r) dst[fr_idx<S>(j * 16 + r, s)] = v[r];
 }
 
+// The pruned band first pass (4 hb < L) with its input offsets computed
+// once: off[q] is the index into P (sequence s's band row, s B + mx) of
+// input r = q (q < 4) or r = q + 8 (q >= 4), -1 where it lies outside the
+// band.  The offsets depend only on the thread, so a kernel that runs the
+// pass for many band blocks (one per SOCS kernel) computes them once.
+template <int L, int S>
+__host__ __device__ __forceinline__ void fr_band_offsets(int t, int B, int hb, int (&off)[8]) {
+  const int s = t % S, j = t / S;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int r = q < 4 ? q : q + 8;
+    const int i = j + r * (L / 16);
+    const int mx = r < 4 ? (i <= hb ? i + hb : -1) : (i >= L - hb ? i - L + hb : -1);
+    off[q] = mx >= 0 ? s * B + mx : -1;
+  }
+}
+template <int L, int S, int DIR>
+__host__ __device__ __forceinline__ void fr_first_pass_band_off(int t, const float2* P, const int (&off)[8],
+                                                                float2* dst) {
+  if (t >= fr_nb(L, S, 0)) return;
+  const int s = t % S, j = t / S;
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) v[q < 4 ? q : q + 8] = off[q] >= 0 ? P[off[q]] : make_float2(0.f, 0.f);
+  fr_dft16_band<DIR>(v);
+#pragma unroll
+  for (int r = 0; r < 16; ++r) dst[fr_idx<S>(j * 16 + r, s)] = v[r];
+}
+
 // First pass (radix 16, no twiddles) for thread t given its 16 inputs
 // v[r] = element j + r L / 16 of sequence s (s = t % S, j = t / S).
 template <int L, int S, int DIR>

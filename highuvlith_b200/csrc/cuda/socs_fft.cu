@@ -345,6 +345,11 @@ __global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || 
   if (MODE == 0) prefetch(0);
   float2 lw[fr_per(L, S, NP - 1)][R - 1];  // last-pass twiddles, the same for every kernel
   fr_last_twiddles<L, S, +1>(t, tw, lw);
+  // first-pass input offsets into a kernel's band block, the same for every
+  // kernel (MODE 0 loops over K kernels; MODE 1 has one)
+  const bool pruned = MODE == 0 && 4 * hb < L;
+  int boff[8];
+  if (pruned) fr_band_offsets<L, S>(t, B, hb, boff);
   for (int k = 0; k < K; ++k) {
     const float2* Pk = P;
     if (MODE == 0) {
@@ -365,7 +370,10 @@ __global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || 
       }
     }
     __syncthreads();
-    fr_first_pass_band<L, S, +1>(t, Pk, B, hb, b0);
+    if (pruned)
+      fr_first_pass_band_off<L, S, +1>(t, Pk, boff, b0);
+    else
+      fr_first_pass_band<L, S, +1>(t, Pk, B, hb, b0);
     __syncthreads();
     const float2* cur = b0;
     if constexpr (NP == 3) {
