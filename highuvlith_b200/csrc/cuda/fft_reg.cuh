@@ -298,6 +298,12 @@ __device__ __forceinline__ void fr_cp_async8(void* smem_dst, const void* gmem_sr
                "l"(gmem_src)
                : "memory");
 }
+// 16-byte variant (L2 only): both addresses 16-byte aligned.
+__device__ __forceinline__ void fr_cp_async16(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem_dst))),
+               "l"(gmem_src)
+               : "memory");
+}
 __device__ __forceinline__ void fr_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void fr_cp_wait() {

@@ -318,6 +318,7 @@ __global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || 
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
   constexpr int R = fr_radix(L, NP - 1);
   constexpr int XS = MODE == 1 ? 2 * S : S;
+  static_assert(L % 2 == 0 && S % 2 == 0, "band blocks copied two elements (16 bytes) at a time");
   extern __shared__ float2 smem[];
   const int B = 2 * hb + 1;
   const int clip = blockIdx.y;
@@ -336,10 +337,13 @@ __global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || 
   // MODE 0: kernel k's band columns (one contiguous block of S B values)
   // arrive by cp.async in P[k & 1] while kernel k - 1 is transformed.
   float2* P2 = b0 + fr_buf(L, S);  // second band buffer (MODE 0), after the FFT buffer
+  // The block is 16-byte aligned at both ends (L and S are even, so the
+  // element offset ((clip K + k) L + x0) B and the length S B are even):
+  // two elements per copy.
   auto prefetch = [&](int k) {
     const float2* src = Tt + ((static_cast<size_t>(clip) * K + k) * L + x0) * B;
     float2* dst = (k & 1) ? P2 : P;
-    for (int e = t; e < S * B; e += T) fr_cp_async8(dst + e, src + e);
+    for (int e = 2 * t; e < S * B; e += 2 * T) fr_cp_async16(dst + e, src + e);
     fr_cp_commit();
   };
   if (MODE == 0) prefetch(0);
