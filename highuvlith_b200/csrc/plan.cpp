@@ -23,6 +23,10 @@
 #include "../../include/huv_b200.h"
 #include "engine.hpp"
 
+namespace huv_launch {
+cudaError_t plan_copy(const void* const* src, void* const* dst, size_t bytes, int count, cudaStream_t st);
+}
+
 namespace huv {
 
 namespace {
@@ -49,6 +53,13 @@ struct Group {
   float* out_base = nullptr;
   void* stage_in = nullptr;
   float* stage_out = nullptr;
+  // device pointer arrays of the gather / scatter kernel (non-contiguous
+  // groups whose buffers and clip sizes are 16-byte aligned)
+  bool copy_kernel = false;
+  const void** gather_src = nullptr;
+  void** gather_dst = nullptr;
+  const void** scatter_src = nullptr;
+  void** scatter_dst = nullptr;
 };
 
 }  // namespace
@@ -80,6 +91,7 @@ struct Plan {
     for (auto& g : groups) {
       cudaFree(g.stage_in);
       cudaFree(g.stage_out);
+      cudaFree(const_cast<void**>(g.gather_src));  // one allocation holds all four arrays
     }
     for (void* w : ws) cudaFree(w);
     for (cudaStream_t b : bstream) cudaStreamDestroy(b);
@@ -95,11 +107,15 @@ struct Plan {
                                 : static_cast<int>(g.clips.size());
     const void* in = g.contiguous ? g.in_base : g.stage_in;
     float* out = g.contiguous ? g.out_base : g.stage_out;
-    if (!g.contiguous)
-      for (int i = 0; i < count; ++i)
-        check_cuda(cudaMemcpyAsync(static_cast<char*>(g.stage_in) + in_bytes * i, clips[g.clips[i]].input, in_bytes,
-                                   cudaMemcpyDeviceToDevice, st),
-                   "plan gather");
+    if (!g.contiguous) {
+      if (g.copy_kernel)
+        check_cuda(huv_launch::plan_copy(g.gather_src, g.gather_dst, in_bytes, count, st), "plan gather");
+      else
+        for (int i = 0; i < count; ++i)
+          check_cuda(cudaMemcpyAsync(static_cast<char*>(g.stage_in) + in_bytes * i, clips[g.clips[i]].input,
+                                     in_bytes, cudaMemcpyDeviceToDevice, st),
+                     "plan gather");
+    }
     huv_batch b{};
     b.n_clips = count;
     b.input_kind = g.kind;
@@ -115,11 +131,15 @@ struct Plan {
       g.e->run_tc_form(b, ds, c.M, out, st, g.K, g.W, kTcCoreFftField);
     else
       g.e->run_fft_form(b, ds, c.M, out, st, g.K, g.W);
-    if (!g.contiguous)
-      for (int i = 0; i < count; ++i)
-        check_cuda(cudaMemcpyAsync(clips[g.clips[i]].out, reinterpret_cast<char*>(g.stage_out) + out_bytes * i,
-                                   out_bytes, cudaMemcpyDeviceToDevice, st),
-                   "plan scatter");
+    if (!g.contiguous) {
+      if (g.copy_kernel)
+        check_cuda(huv_launch::plan_copy(g.scatter_src, g.scatter_dst, out_bytes, count, st), "plan scatter");
+      else
+        for (int i = 0; i < count; ++i)
+          check_cuda(cudaMemcpyAsync(clips[g.clips[i]].out, reinterpret_cast<char*>(g.stage_out) + out_bytes * i,
+                                     out_bytes, cudaMemcpyDeviceToDevice, st),
+                     "plan scatter");
+    }
   }
 };
 
@@ -221,6 +241,30 @@ huv_status huv_plan_create(const huv_clip* clips, int32_t n_clips, int32_t pixel
         huv::check_cuda(cudaMalloc(&g.stage_in, in_bytes * g.clips.size()), "cudaMalloc(plan stage in)");
         huv::check_cuda(cudaMalloc(reinterpret_cast<void**>(&g.stage_out), out_bytes * g.clips.size()),
                         "cudaMalloc(plan stage out)");
+        const size_t nc = g.clips.size();
+        bool aligned = in_bytes % 16 == 0 && out_bytes % 16 == 0 && nc <= 65535;
+        for (size_t j = 0; j < nc && aligned; ++j)
+          aligned = (reinterpret_cast<uintptr_t>(clips[g.clips[j]].input) & 15u) == 0 &&
+                    (reinterpret_cast<uintptr_t>(clips[g.clips[j]].out) & 15u) == 0;
+        if (aligned) {
+          std::vector<const void*> ptrs(4 * nc);
+          for (size_t j = 0; j < nc; ++j) {
+            ptrs[j] = clips[g.clips[j]].input;                                              // gather src
+            ptrs[nc + j] = static_cast<const char*>(g.stage_in) + in_bytes * j;             // gather dst
+            ptrs[2 * nc + j] = reinterpret_cast<const char*>(g.stage_out) + out_bytes * j;  // scatter src
+            ptrs[3 * nc + j] = clips[g.clips[j]].out;                                       // scatter dst
+          }
+          void** d = nullptr;
+          huv::check_cuda(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(void*) * 4 * nc),
+                          "cudaMalloc(plan copy pointers)");
+          huv::check_cuda(cudaMemcpy(d, ptrs.data(), sizeof(void*) * 4 * nc, cudaMemcpyHostToDevice),
+                          "upload plan copy pointers");
+          g.gather_src = const_cast<const void**>(d);
+          g.gather_dst = d + nc;
+          g.scatter_src = const_cast<const void**>(d + 2 * nc);
+          g.scatter_dst = d + 3 * nc;
+          g.copy_kernel = true;
+        }
       }
       const auto key = std::make_tuple(g.n, g.h, g.K, g.kind);
       bool cached = false;
@@ -237,7 +281,14 @@ huv_status huv_plan_create(const huv_clip* clips, int32_t n_clips, int32_t pixel
         if (!autotune) {
           g.choice = cands.front();
         } else {
-          const int probe = std::min<int>(8, static_cast<int>(g.clips.size()));
+          // a sample large enough to fill the GPU (at least 32 clips or
+          // 256 MB of images): with a handful of clips the launches' fixed
+          // cost dominates and favours the forms with the fewest launches
+          // (e.g. the full grid over a coarse grid plus interpolation), which
+          // lose at the group's real size
+          const size_t img_bytes = sizeof(float) * static_cast<size_t>(g.n) * g.n;
+          const int want = static_cast<int>(std::max<size_t>(32, (size_t(256) << 20) / img_bytes));
+          const int probe = std::min<int>(want, static_cast<int>(g.clips.size()));
           cudaEvent_t e0, e1;
           huv::check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
           huv::check_cuda(cudaEventCreate(&e1), "cudaEventCreate");

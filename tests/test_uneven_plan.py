@@ -52,3 +52,28 @@ def test_plan_matches_per_clip_engines():
         ref = ref_eng.compute_batch(torch.from_numpy(raster).cuda(), form="fft").cpu().numpy()[0]
         got = out.cpu().numpy()
         assert np.max(np.abs(got - ref)) / np.max(ref) < 1e-4, (src, n, kmax)
+
+
+def test_plan_group_merged_from_two_stores():
+    """ArF immersion dipole at 256^2 keeps 8 kernels for budgets 16 and 48, so
+    the two budgets' clips form one group; each budget's clips sit in a
+    store of their own (two contiguous runs), which the plan gathers and
+    scatters run by run.  Every clip against a single-clip call."""
+    import torch
+    arfi = HB.SimulationEngine(HB.SourceConfig(193.368, "dipole", (0.8, 0.1, 0.0)),
+                               HB.OpticsConfig.immersion(1.35), grid=HB.GridConfig(256, 1.0), max_kernels=48)
+    stores = []
+    for seed in (300, 400):
+        _, r = gen_batch(3, 256, base_seed=seed, wmin=5, wmax=40)
+        stores.append((r, torch.from_numpy(r).cuda(), torch.zeros((3, 256, 256), dtype=torch.float32, device="cuda")))
+    clips = [(arfi, kmax, inp[i], out[i]) for kmax, (_, inp, out) in zip((16, 48), stores) for i in range(3)]
+    plan = HB.UnevenPlan(clips, autotune=True)
+    groups = plan.describe()
+    assert len(groups) == 1 and groups[0]["clips"] == 6 and groups[0]["contiguous"] == 0
+    plan.launch()
+    torch.cuda.synchronize()
+    for kmax, (r, _, out) in zip((16, 48), stores):
+        ref_eng = HB.SimulationEngine(arfi.source, arfi.optics, grid=HB.GridConfig(256, 1.0), max_kernels=kmax)
+        ref = ref_eng.compute_batch(torch.from_numpy(r).cuda(), form="fft").cpu().numpy()
+        got = out.cpu().numpy()
+        assert np.max(np.abs(got - ref)) / np.max(ref) < 1e-4, kmax
