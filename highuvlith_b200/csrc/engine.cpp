@@ -671,7 +671,12 @@ void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t 
   const size_t out_per = sizeof(float) * static_cast<size_t>(n) * n;
   const int by_bytes = static_cast<int>(std::max<size_t>(1, (size_t(128) << 20) / out_per));
   const int chunk = std::max(1, std::min((b.n_clips + 3) / 4, by_bytes));
-  const int nchunks = (b.n_clips + chunk - 1) / chunk;
+  // The first chunk is a quarter of the others, so that the copy-out stream
+  // (the bound: images are 4x the bytes of u8 rasters) starts sooner.
+  const int first = std::max(1, chunk / 4);
+  std::vector<int> starts{0};
+  while (starts.back() < b.n_clips) starts.push_back(std::min(b.n_clips, starts.back() + (starts.size() == 1 ? first : chunk)));
+  const int nchunks = static_cast<int>(starts.size()) - 1;
   const int ring = std::min(nchunks, 3);
   {
     std::lock_guard<std::mutex> lock(mu);
@@ -706,7 +711,7 @@ void Engine::image_batch_host(const huv_batch& b, float* out_host, cudaStream_t 
   cudaEvent_t* out_done = io_ev[2];
   for (int i = 0; i < nchunks; ++i) {
     const int slot = i % ring;
-    const int c0 = i * chunk, nc = std::min(chunk, b.n_clips - c0);
+    const int c0 = starts[i], nc = starts[i + 1] - starts[i];
     char* din = static_cast<char*>(io_in) + in_per * chunk * slot;
     float* dout = reinterpret_cast<float*>(static_cast<char*>(io_out) + out_per * chunk * slot);
     // the input slot is free once the imaging of chunk i - ring has run
