@@ -684,9 +684,6 @@ __global__ void scatter_blocks(const int* __restrict__ idx, const float* __restr
 
 // ================================================================== host
 namespace huv_launch {
-cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
-                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
-                         const uint8_t* row_digits, int* err);
 cudaError_t socs_rows(const float2* kband, float scale, const float2* Mband, int K, int hb, int lgm, int clips,
                       float2* T, const float2* tw, cudaStream_t st);
 cudaError_t socs_cols(const float2* T, int K, int hb, int lgm, int clips, float keep, float flare,

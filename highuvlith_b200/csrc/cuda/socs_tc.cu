@@ -805,9 +805,6 @@ cudaError_t socs_field_fused(const float2* kband, const float2* Mband, int K, in
                              float flare, const float* mean, float* out, void* split, float* part, const float2* tw,
                              cudaStream_t st);
 unsigned long long probe_wait_ns() { return g_probe_wait_ns.load(std::memory_order_relaxed); }
-cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
-                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
-                         const uint8_t* row_digits, int* err);
 bool xt_ok(int L, int hb);
 cudaError_t socs_rows_x(const float2* kband, float scale, const float2* Mband, int K, int hb, int L, int clips,
                         float2* T, const float2* tw, cudaStream_t st);

@@ -14,6 +14,14 @@
 
 #include "host/host.hpp"
 
+namespace huv_launch {
+// Band of the 2-D spectrum of `clips` rasters (csrc/cuda/socs_fft.cu): the
+// one declaration every caller sees.
+cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int clips, float2* X, float2* Mband,
+                         const float* ptx, const float* W, float* mean, const float2* tw, cudaStream_t st,
+                         const uint8_t* row_digits, int* err);
+}  // namespace huv_launch
+
 namespace huv {
 
 // Clips per chunk when a batch of n must be cut into chunks of at most
