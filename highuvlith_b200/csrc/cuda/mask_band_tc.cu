@@ -49,7 +49,8 @@ __host__ __device__ constexpr size_t mb_smem_bytes(int N) {
 }
 
 // grid: (rows / 128); rows = clips * L.  X: [rows][2 hb + 1], or with
-// `transposed` [clip][2 hb + 1][L] (each order's column contiguous in y).
+// `transposed` the orders m = 0..hb alone as [clip][hb + 1][L] (each
+// order's column contiguous in y; the orders m < 0 are their conjugates).
 __global__ void __launch_bounds__(192, 1)
     band_rows_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmD, int kboxes,
                  int N, int hb, uint32_t tmem_cols, int L, int transposed, float2* __restrict__ X, int* err) {
@@ -172,15 +173,15 @@ __global__ void __launch_bounds__(192, 1)
       __syncwarp();
       const int B = 2 * hb + 1;
       if (transposed) {
+        // orders m = 0..hb only (the raster is real, X(y, -m) = conj X(y, m)),
         // one order per store: 32 consecutive y of one column (256 bytes)
         const int grow = row0 + quad * 32;
         const int clip = grow / L, y0 = grow - clip * L;
-        float2* out = X + static_cast<size_t>(clip) * B * L + y0 + lane;
-        for (int mi = 0; mi < B; ++mi) {
-          const int m = mi - hb, am = m < 0 ? -m : m;
-          const float c = stage[lane * ld + 1 + am];
-          const float s = am ? stage[lane * ld + hb + 1 + am] : 0.f;
-          out[static_cast<size_t>(mi) * L] = make_float2(c, m >= 0 ? -s : s);
+        float2* out = X + static_cast<size_t>(clip) * (hb + 1) * L + y0 + lane;
+        for (int m = 0; m <= hb; ++m) {
+          const float c = stage[lane * ld + 1 + m];
+          const float s = m ? stage[lane * ld + hb + 1 + m] : 0.f;
+          out[static_cast<size_t>(m) * L] = make_float2(c, -s);
         }
       } else {
         float2* out = X + static_cast<size_t>(row0 + quad * 32) * B;
@@ -272,7 +273,7 @@ std::vector<uint8_t> mask_rows_tc_digits(int n, int hb) {
   return tab;
 }
 
-// X[clip][y][m + hb] (or, with `transposed`, X[clip][m + hb][y]) for u8
+// X[clip][y][m + hb] (or, with `transposed`, X[clip][m][y] for m = 0..hb) for u8
 // rasters [clips][n][n] on the tensor cores.  `digits` is
 // mask_rows_tc_digits(n, hb) on the device.  Returns cudaErrorNotSupported
 // when the shape or the input's alignment rules the path out (the caller

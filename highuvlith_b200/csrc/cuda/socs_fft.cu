@@ -432,14 +432,14 @@ __global__ void __launch_bounds__(fr_threads(L, S), ((L == 160 && MODE == 0) || 
 // band_rows_fwd<1> (f32 rasters) with register-radix passes: S complex
 // sequences per block, sequence s packing rows (2s, 2s+1) as re / im; the
 // last pass leaves the spectra in natural order in shared memory, and the
-// two real rows' bands are split from Z(m) and conj Z(-m).
-// grid: (clips * L / (2 S)); X: [clip][y][B].
+// two real rows' bands are split from Z(m) and conj Z(-m).  The rows are
+// real, X(y, -m) = conj X(y, m), so X holds the orders m = 0..hb alone.
+// grid: (clips * L / (2 S)); X: [clip][y][hb + 1].
 template <int L, int S, typename In = float>
 __global__ void __launch_bounds__(fr_threads(L, S), (L >= 384 ? 4 : 1))
     band_rows_reg(const In* __restrict__ in, int hb, float2* __restrict__ X, const float2* __restrict__ tw) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
   extern __shared__ float2 smem[];
-  const int B = 2 * hb + 1;
   const size_t row0 = static_cast<size_t>(blockIdx.x) * 2 * S;
   const int t = threadIdx.x;
   float2* b0 = smem;
@@ -460,25 +460,29 @@ __global__ void __launch_bounds__(fr_threads(L, S), (L >= 384 ? 4 : 1))
     fr_mid_pass_inplace<L, S, -1, 2>(t, b0, tw);
   }
   __syncthreads();
-  for (int e = t; e < S * B; e += T) {
-    const int s = e / B, mi = e - s * B;
-    const int idx = mi - hb < 0 ? mi - hb + L : mi - hb;
-    const float2 z = cur[fr_idx<S>(idx, s)];
-    const float2 zc = cconj(cur[fr_idx<S>(idx == 0 ? 0 : L - idx, s)]);
+  const int H = hb + 1;
+  for (int e = t; e < S * H; e += T) {
+    const int s = e / H, m = e - s * H;
+    const float2 z = cur[fr_idx<S>(m, s)];
+    const float2 zc = cconj(cur[fr_idx<S>(m == 0 ? 0 : L - m, s)]);
     const float2 xa = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y + zc.y));
     const float2 d = csub(z, zc);
     const float2 xb = make_float2(0.5f * d.y, -0.5f * d.x);
-    X[(row0 + 2 * s) * B + mi] = xa;
-    X[(row0 + 2 * s + 1) * B + mi] = xb;
+    X[(row0 + 2 * s) * H + m] = xa;
+    X[(row0 + 2 * s + 1) * H + m] = xb;
   }
 }
 
 // band_cols_fwd with register-radix passes: forward FFT along y of S band
-// columns of X[clip][y][B] (or of X[clip][B][y] with `transposed`) per block,
-// the first pass reading X directly.  grid: (ceil(B / S), clips).
+// columns per block, the first pass reading X directly.  X is [clip][y][B]
+// (every order mx = -hb..hb), or, with `half`, the orders mx = 0..hb of a
+// real raster alone, [clip][y][hb + 1] or (`transposed`) [clip][hb + 1][y]:
+// the band of a real raster is Hermitian, M(-my, -mx) = conj M(my, mx), so
+// the columns mx > 0 also give the columns -mx.  grid: (ceil(columns / S),
+// clips).
 template <int L, int S>
 __global__ void __launch_bounds__(fr_threads(L, S))
-    band_cols_reg(const float2* __restrict__ X, bool transposed, int hb, const float* __restrict__ ptx,
+    band_cols_reg(const float2* __restrict__ X, bool half, bool transposed, int hb, const float* __restrict__ ptx,
                   const float* __restrict__ W, float2* __restrict__ Mband, float* __restrict__ parts,
                   const float2* __restrict__ tw) {
   constexpr int T = fr_threads(L, S), NP = fr_passes(L);
@@ -486,17 +490,18 @@ __global__ void __launch_bounds__(fr_threads(L, S))
   extern __shared__ float2 smem[];
   __shared__ float red[T / 32];
   const int B = 2 * hb + 1;
+  const int NC = half ? hb + 1 : B;  // columns held in X
   const int clip = blockIdx.y;
   const int c0 = blockIdx.x * S;
   const int t = threadIdx.x;
   float2* b0 = smem;
-  const float2* Xc = X + static_cast<size_t>(clip) * L * B;
+  const float2* Xc = X + static_cast<size_t>(clip) * L * NC;
   if (t < fr_nb(L, S, 0)) {
     const int s = t % S, j = t / S;
-    const bool live = c0 + s < B;
+    const bool live = c0 + s < NC;
     float2 v[16];
     const size_t col_base = transposed ? static_cast<size_t>(c0 + s) * L : static_cast<size_t>(c0 + s);
-    const size_t row_step = transposed ? 1 : static_cast<size_t>(B);
+    const size_t row_step = transposed ? 1 : static_cast<size_t>(NC);
 #pragma unroll
     for (int r = 0; r < 16; ++r)
       v[r] = live ? Xc[col_base + static_cast<size_t>(j + r * (L / 16)) * row_step] : make_float2(0.f, 0.f);
@@ -524,12 +529,12 @@ __global__ void __launch_bounds__(fr_threads(L, S))
         const int idx = ju + p * (L / R);
         need = need || idx <= hb || idx >= L - hb;
       }
-      if (!need || c0 + su >= B) continue;
+      if (!need || c0 + su >= NC) continue;
     }
     int s, j;
     float2 v[R];
     fr_last_pass<L, S, -1>(t + b * T, cur, tw, s, j, v);
-    const int mx = c0 + s;
+    const int mx = half ? hb + c0 + s : c0 + s;
 #pragma unroll
     for (int p = 0; p < R; ++p) {
       const int idx = j + p * (L / R);
@@ -543,6 +548,18 @@ __global__ void __launch_bounds__(fr_threads(L, S))
       }
       Mc[static_cast<size_t>(mi) * B + mx] = val;
       if (W) part += W[mi * B + mx] * (val.x * val.x + val.y * val.y);
+      if (half && mx > hb) {
+        // the mirrored order (-my, -mx)
+        const int mi2 = 2 * hb - mi, mx2 = 2 * hb - mx;
+        float2 w2 = cconj(v[p]);
+        if (ptx) {
+          const float f = ptx[mi2] * ptx[mx2];
+          w2.x *= f;
+          w2.y *= f;
+        }
+        Mc[static_cast<size_t>(mi2) * B + mx2] = w2;
+        if (W) part += W[mi2 * B + mx2] * (w2.x * w2.x + w2.y * w2.y);
+      }
     }
   }
   if (parts) {
@@ -599,10 +616,12 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
   // the register-radix columns read a transposed row band ([clip][m][y]) when
   // the tensor-core rows produce it
   const bool cols_reg = xt_ok(n, hb);
-  bool x_transposed = false;
+  // (and then, as the register-radix rows do, only the orders m = 0..hb of
+  // the real rasters: `half`)
+  bool x_transposed = false, half = false;
   if (kind == 0 && row_digits) {
     rows_tc = mask_rows_tc(in, n, hb, clips, X, row_digits, err, st, cols_reg);
-    x_transposed = rows_tc == cudaSuccess && cols_reg;
+    x_transposed = half = rows_tc == cudaSuccess && cols_reg;
     if (rows_tc != cudaSuccess && rows_tc != cudaErrorNotSupported) return rows_tc;
   }
   if (kind == 1 && (n == 1024 || n == 160 || n == 192 || n == 384 || n == 2048) && xt_ok(n, hb)) {
@@ -621,6 +640,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     else
       band_rows_reg<192, 16><<<gr, 256, smr, st>>>(fin, hb, X, tw);
     rows_tc = cudaSuccess;
+    half = true;
   }
   // u8 rows of 2048 points whose band is too wide for the tensor-core rows
   // (3 digit-plane accumulators past 512 TMEM columns): register-radix rows
@@ -630,6 +650,7 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     const size_t smr = static_cast<size_t>(fr_buf(n, Sr)) * sizeof(float2);
     band_rows_reg<2048, 2, uint8_t><<<gr, 256, smr, st>>>(static_cast<const uint8_t*>(in), hb, X, tw);
     rows_tc = cudaSuccess;
+    half = true;
   }
   if (!pow2 && rows_tc != cudaSuccess) return cudaErrorInvalidValue;  // no radix-4 kernel for this length
   // Only device rasters come here (rectangle clips take the analytic path).
@@ -650,18 +671,18 @@ cudaError_t band_forward(const void* in, int kind, int n, int lg, int hb, int cl
     // register-radix columns: S <= 4 ... 32 columns per block, at most
     // ceil(B / 4) parts per clip as the callers size them
     const int S = xt_S(n);
-    nblk = (B + S - 1) / S;
+    nblk = ((half ? hb + 1 : B) + S - 1) / S;
     const dim3 g(nblk, clips);
     const size_t sm = xt_buf_bytes(n);
     switch (n) {
-      case 128: band_cols_reg<128, 32><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 160: band_cols_reg<160, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 192: band_cols_reg<192, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 256: band_cols_reg<256, 16><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 384: band_cols_reg<384, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 512: band_cols_reg<512, 8><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 2048: band_cols_reg<2048, 2><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
-      case 1024: band_cols_reg<1024, 4><<<g, 256, sm, st>>>(X, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 128: band_cols_reg<128, 32><<<g, 256, sm, st>>>(X, half, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 160: band_cols_reg<160, 16><<<g, 256, sm, st>>>(X, half, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 192: band_cols_reg<192, 16><<<g, 256, sm, st>>>(X, half, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 256: band_cols_reg<256, 16><<<g, 256, sm, st>>>(X, half, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 384: band_cols_reg<384, 8><<<g, 256, sm, st>>>(X, half, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 512: band_cols_reg<512, 8><<<g, 256, sm, st>>>(X, half, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 2048: band_cols_reg<2048, 2><<<g, 256, sm, st>>>(X, half, x_transposed, hb, ptx, W, Mband, parts, tw); break;
+      case 1024: band_cols_reg<1024, 4><<<g, 256, sm, st>>>(X, half, x_transposed, hb, ptx, W, Mband, parts, tw); break;
       default: return cudaErrorInvalidValue;
     }
   } else {
