@@ -655,7 +655,8 @@ def run_ours(args):
                  "socs_rows_tc": 4 * K * m_f * kb + 8 * Bb * Bb,
                  "tc_dft_gemm<interp>": 4 * N_GRID * N_GRID + 4 * N_GRID * (k_int if sep else kb),
                  "tc_dft_gemm<interp_x>": 4 * m_f * m_f + 4 * N_GRID * m_f,
-                 "mask_band": N_GRID * N_GRID + 16 * N_GRID * Bb + 8 * Bb * Bb,
+                 # u8 raster in, the row band's orders m >= 0 out and back in, the band out
+                 "mask_band": N_GRID * N_GRID + 16 * N_GRID * (hb_ + 1) + 8 * Bb * Bb,
                  # mask band in, the band kernels (8 K S, as the whole-path count has them), I_M out
                  "socs_field_fused": 8 * Bb * Bb + 8 * K * S + 4 * m_f * m_f}
     bytes_per_image = 4 * N_GRID ** 2 + 4 * N_GRID ** 2 + 8 * K * S
