@@ -95,9 +95,20 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bflo
 constexpr uint32_t kOutTile = 32 * 32 * 4;
 constexpr uint32_t kOutStage = 4 * 2 * kOutTile;
 
+// B stages of the ring: MODE 3 fills 120 KB with as many as fit (3 to 8:
+// its CTAs are bound by how much of B is in flight), the others take 3.
+__host__ __device__ constexpr int tc_stages(int mode, int bn) {
+  return mode != 3 ? kTcStages
+                   : (122880 / (2 * static_cast<int>(b_box_bytes(bn))) > 8
+                          ? 8
+                          : (122880 / (2 * static_cast<int>(b_box_bytes(bn))) < kTcStages
+                                 ? kTcStages
+                                 : 122880 / (2 * static_cast<int>(b_box_bytes(bn)))));
+}
+
 __host__ __device__ constexpr size_t tc_smem_bytes(int kboxes, int bn = kTcBN, bool stage = false,
-                                                   bool out_stage = false) {
-  return 1024 + 2 * static_cast<size_t>(kboxes) * kABox + kTcStages * 2 * static_cast<size_t>(b_box_bytes(bn)) +
+                                                   bool out_stage = false, int stages = kTcStages) {
+  return 1024 + 2 * static_cast<size_t>(kboxes) * kABox + stages * 2 * static_cast<size_t>(b_box_bytes(bn)) +
          (out_stage ? kOutStage : 0) + 256 + (stage ? 4 * static_cast<size_t>(stage_words(bn)) * sizeof(uint32_t) : 0);
 }
 
@@ -123,20 +134,21 @@ __global__ void __launch_bounds__(192, 1)
                 const __grid_constant__ CUtensorMap tmO, TcGemmParams p) {
   constexpr uint32_t kBBox = b_box_bytes(BN);
   constexpr uint32_t kTmemCols = 2 * BN <= 128 ? 128 : (2 * BN <= 256 ? 256 : 512);
+  constexpr int kSt = tc_stages(MODE, BN);
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   uint8_t* sA = base;
   uint8_t* sB = base + 2 * p.kboxes * kABox;
-  uint8_t* sO = sB + kTcStages * 2 * kBBox;  // MODE 1 output staging (1024-aligned)
+  uint8_t* sO = sB + kSt * 2 * kBBox;  // MODE 1 output staging (1024-aligned)
   uint64_t* bars = reinterpret_cast<uint64_t*>(sO + (MODE == 1 ? kOutStage : 0));
   uint64_t* full = bars;
-  uint64_t* empty = bars + kTcStages;
-  uint64_t* a_full = bars + 2 * kTcStages;
-  uint64_t* tfull = bars + 2 * kTcStages + 1;
-  uint64_t* tempty = bars + 2 * kTcStages + 3;
-  uint64_t* done = bars + 2 * kTcStages + 5;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kTcStages + 6);
+  uint64_t* empty = bars + kSt;
+  uint64_t* a_full = bars + 2 * kSt;
+  uint64_t* tfull = bars + 2 * kSt + 1;
+  uint64_t* tempty = bars + 2 * kSt + 3;
+  uint64_t* done = bars + 2 * kSt + 5;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kSt + 6);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -145,7 +157,7 @@ __global__ void __launch_bounds__(192, 1)
   const int G = MODE == 3 ? min(p.G, p.nprob - prob * p.G) : p.G;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kTcStages; ++s) {
+    for (int s = 0; s < kSt; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -183,8 +195,8 @@ __global__ void __launch_bounds__(192, 1)
       int it = 0;
       for (int g = 0; g < G && !*abort_flag; ++g) {
         for (int kb = 0; kb < p.kboxes; ++kb, ++it) {
-          const int s = it % kTcStages;
-          const uint32_t ph = (it / kTcStages) & 1;
+          const int s = it % kSt;
+          const uint32_t ph = (it / kSt) & 1;
           if (!mbar_wait_or_abort(&empty[s], ph ^ 1, kWaitLimitNs, abort_flag)) {
             fail(1);
             break;
@@ -197,8 +209,8 @@ __global__ void __launch_bounds__(192, 1)
       }
       // Drain: every load issued must have landed before the CTA may exit.
       mbar_wait(a_full, 0, kWaitLimitNs);
-      for (int q = (it > kTcStages ? it - kTcStages : 0); q < it; ++q)
-        mbar_wait(&full[q % kTcStages], (q / kTcStages) & 1, kWaitLimitNs);
+      for (int q = (it > kSt ? it - kSt : 0); q < it; ++q)
+        mbar_wait(&full[q % kSt], (q / kSt) & 1, kWaitLimitNs);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -220,8 +232,8 @@ __global__ void __launch_bounds__(192, 1)
         tc_fence_after();
         const uint32_t d = tmem_base + buf * BN;
         for (int kb = 0; kb < p.kboxes; ++kb, ++it) {
-          const int s = it % kTcStages;
-          if (!mbar_wait(&full[s], (it / kTcStages) & 1, kWaitLimitNs)) {
+          const int s = it % kSt;
+          if (!mbar_wait(&full[s], (it / kSt) & 1, kWaitLimitNs)) {
             fail(4);
             ok = false;
             break;
@@ -972,14 +984,14 @@ cudaError_t tc_set_smem() {
   if ((e = cudaFuncSetAttribute(tc_interp_w256<6, 6, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(w256_smem_bytes(6, 6, 2)))))
     return e;
-  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(tc_smem_bytes(3, 128)))))
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(2, 64, false, false, tc_stages(3, 64))))))
     return e;
-  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 160>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(tc_smem_bytes(3, 160)))))
+  if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 80>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc_smem_bytes(3, 80, false, false, tc_stages(3, 80))))))
     return e;
   if ((e = cudaFuncSetAttribute(tc_dft_gemm<3, 96>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(tc_smem_bytes(3, 96)))))
+                                static_cast<int>(tc_smem_bytes(3, 96, false, false, tc_stages(3, 96))))))
     return e;
   if ((e = cudaFuncSetAttribute(socs_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
   const int reg_bytes = 110 * 1024;
@@ -1356,18 +1368,18 @@ void Engine::interp_separable(DeviceSet& ds, int M, int nc, const void* im_split
   {
     // Z^T[clip][plane][Y][y] = sum_x P(Y, x) I_M(y, x) / s, FP16 split planes:
     // A = P (rows Y), B = I_M / s (rows y, K = x), s = interp_scale(mean);
-    // G1 clips per CTA share the A tile.  The MMA covers all M columns at
-    // once where the B ring fits (M = 128, 160: N = M, 4 + 5 KB of operands
-    // per 80 tensor cycles at M = 160), else two halves (M = 192).
-    const int bn1 = M <= 160 ? M : M / 2;
+    // G1 clips per CTA share the A tile.  Each CTA takes half of the M
+    // columns (N = M / 2), so that two clips' B tiles fit the ring
+    // (tc_stages: 7 / 6 / 5 stages at M = 128 / 160 / 192).
+    const int bn1 = M / 2;
     const int ntile1 = M / bn1, mtiles = n / 128;
     // Clips per CTA: the fewest (up to 32) whose grid fits one wave of one
-    // CTA per SM, else 32.  Each CTA's run is latency-bound (per step: one
-    // clip's B ring through 3 stages), so longer runs over a resident A
-    // tile beat more CTAs: at 128 clips 1 / 2 / 4 / 8 clips per CTA time
-    // 1.24 / 1.12 / 1.03 / 0.99 ms per 20 launches; at 256 clips 15 per
-    // CTA (one wave of 144 CTAs) 0.084 ms per launch against 0.092 with 8
-    // (256 CTAs, 1.7 waves).
+    // CTA per SM, else 32.  Each CTA's run is latency-bound (how much of the
+    // clips' B tiles is in flight), so longer runs over a resident A tile
+    // beat more CTAs: at 128 clips 1 / 2 / 4 / 8 clips per CTA time
+    // 1.24 / 1.12 / 1.03 / 0.99 ms per 20 launches (N = M); at 256 clips
+    // and N = M, 15 per CTA (one wave of 144 CTAs) 0.084 ms per launch
+    // against 0.092 with 8 (256 CTAs, 1.7 waves).
     int sms = 0, dev = 0;
     check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
@@ -1398,12 +1410,15 @@ void Engine::interp_separable(DeviceSet& ds, int M, int nc, const void* im_split
     p.bop_ld = M;
     const dim3 g(ntile1, mtiles, (nc + G1 - 1) / G1);
     prof.begin("tc_dft_gemm<interp_x>", st);
-    if (bn1 == 128)
-      tc_dft_gemm<3, 128><<<g, 192, tc_smem_bytes(3, 128), st>>>(tc.map_pi, mbS, tc.map_pi, p);
-    else if (bn1 == 160)
-      tc_dft_gemm<3, 160><<<g, 192, tc_smem_bytes(3, 160), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+    if (bn1 == 64)
+      tc_dft_gemm<3, 64><<<g, 192, tc_smem_bytes(p.kboxes, 64, false, false, tc_stages(3, 64)), st>>>(
+          tc.map_pi, mbS, tc.map_pi, p);
+    else if (bn1 == 80)
+      tc_dft_gemm<3, 80><<<g, 192, tc_smem_bytes(p.kboxes, 80, false, false, tc_stages(3, 80)), st>>>(
+          tc.map_pi, mbS, tc.map_pi, p);
     else if (bn1 == 96)
-      tc_dft_gemm<3, 96><<<g, 192, tc_smem_bytes(3, 96), st>>>(tc.map_pi, mbS, tc.map_pi, p);
+      tc_dft_gemm<3, 96><<<g, 192, tc_smem_bytes(p.kboxes, 96, false, false, tc_stages(3, 96)), st>>>(
+          tc.map_pi, mbS, tc.map_pi, p);
     else
       throw Error(HUV_ERR_UNSUPPORTED, "separable interpolation: evaluation grid must be 128, 160 or 192");
     prof.end(st);
