@@ -626,7 +626,7 @@ def run_ours(args):
     traffic_per_clip = {"tc_dft_gemm<sumsq>": (166.38e6 + 6.65e6) / 32,
                         "socs_rows_tc": (19.29e6 + 110.03e6) / 32,
                         "tc_dft_gemm<interp>": (22.75e6 + 70.90e6) / 32,
-                        "mask_band": (33.82e6 + 19.75e6 + 0.01e6) / 32,
+                        "mask_band": (33.82e6 + 10.03e6) / 32,
                         "socs_cols_inv": (95.29e6 + 0.13e6) / 32,
                         "socs_rows_inv": (2.87e6 + 33.84e6) / 32,
                         "interp_band": (3.29e6 + 6.12e6) / 32,
