@@ -474,12 +474,15 @@ __global__ void ilt_finish(const float* __restrict__ theta, const float* __restr
 // The same as ilt_finish for grids that are multiples of TS: a block takes a
 // TS x TS tile, computes m = sigmoid(beta theta) once for the tile and its
 // 1-pixel periodic halo in shared memory (instead of up to nine sigmoids per
-// pixel; the halo's loads are all issued before the first sigmoid), then
-// each thread takes runs of 4 pixels of a row (16-byte loads of dC/dm and
-// stores of the gradient), and writes its share of the regulariser cost to
-// parts[mask][tile].  grid: ((n / TS)^2, masks), block 256.
+// pixel), then each thread takes runs of 4 pixels of a row (16-byte loads of
+// dC/dm and stores of the gradient), and writes its share of the regulariser
+// cost to parts[mask][tile].  The thread's dC/dm runs and the halo's theta
+// are all loaded before the first sigmoid, so both streams are in flight
+// together (held to 64 registers, four blocks per SM: 1.597 -> 1.589 ms per
+// C4 gradient; at three blocks per SM it was slower).  grid: ((n / TS)^2,
+// masks), block 256.
 template <int TS>
-__global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict__ theta,
+__global__ void __launch_bounds__(256, 4) ilt_finish_tiled(const float* __restrict__ theta,
                                                          const float* __restrict__ dcdm, int n, float beta,
                                                          float tv_w, float tv_eps, float bin_w,
                                                          float* __restrict__ grad, double* __restrict__ parts) {
@@ -495,6 +498,14 @@ __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict_
   const int ti = blockIdx.x / tiles_x, tj = blockIdx.x - ti * tiles_x;
   const float* th = theta + mask * npix;
   const float inv_n = 1.f / static_cast<float>(npix);
+  constexpr int NPASS = TS / ROWS_PER_PASS;
+  const int c4 = (threadIdx.x % RUNS) * 4, r0 = threadIdx.x / RUNS;
+  float4 d4[NPASS];
+#pragma unroll
+  for (int q = 0; q < NPASS; ++q) {
+    const size_t gp = mask * npix + static_cast<size_t>(ti * TS + r0 + q * ROWS_PER_PASS) * n + tj * TS + c4;
+    d4[q] = dcdm ? *reinterpret_cast<const float4*>(dcdm + gp) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   float tv[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
@@ -520,13 +531,11 @@ __global__ void __launch_bounds__(256) ilt_finish_tiled(const float* __restrict_
   // per-thread partials in FP32, the block sum in FP64
   float tv_part = 0.f, bin_part = 0.f;
   const float eps2 = tv_eps * tv_eps;
-  const int c4 = (threadIdx.x % RUNS) * 4, r0 = threadIdx.x / RUNS;
-#pragma unroll 2
-  for (int q = 0; q < TS / ROWS_PER_PASS; ++q) {
+#pragma unroll
+  for (int q = 0; q < NPASS; ++q) {
     const int r = r0 + q * ROWS_PER_PASS + 1;
     const size_t gp = mask * npix + static_cast<size_t>(ti * TS + r - 1) * n + tj * TS + c4;
-    const float4 d4 = dcdm ? *reinterpret_cast<const float4*>(dcdm + gp) : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float dv[4] = {d4.x, d4.y, d4.z, d4.w};
+    const float dv[4] = {d4[q].x, d4[q].y, d4[q].z, d4[q].w};
     float out[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
